@@ -1,0 +1,213 @@
+/*
+ * nectb.h - C ABI of the B200-native NeCT hot path (libnectb.so).
+ *
+ * Every entry point takes plain device pointers, sizes and a cudaStream_t
+ * (passed as void*), returns an int status (0 = NECTB_OK) and never allocates
+ * device memory: callers own every buffer, including workspaces whose sizes the
+ * *_workspace_bytes() queries report.  Nothing here synchronises the device;
+ * work is ordered on the given stream.  A failed call leaves a message that
+ * nectb_last_error() returns (thread-local).
+ *
+ * Reference interfaces each entry point replaces are cited as
+ * path:line within the haakonnese/nect source tree.
+ */
+#ifndef NECTB_H_
+#define NECTB_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+enum {
+  NECTB_OK = 0,
+  NECTB_ERR_INVALID = 1,   /* bad argument (null pointer, size, mode)     */
+  NECTB_ERR_CUDA = 2,      /* a CUDA launch or runtime call failed         */
+  NECTB_ERR_WORKSPACE = 3, /* workspace smaller than *_workspace_bytes()   */
+  NECTB_ERR_TOO_LARGE = 4  /* size beyond a documented maximum             */
+};
+
+/* ---- geometry ---------------------------------------------------------- */
+/* Geometry kinds: the four C++ structs the reference binds
+ * (nect/sampling/ct_sampling.cu:7-115, bindings :650-749). */
+enum {
+  NECTB_CONE_VOXEL = 0,
+  NECTB_CONE_CYLINDRICAL = 1,
+  NECTB_PARALLEL_VOXEL = 2,
+  NECTB_PARALLEL_CYLINDRICAL = 3
+};
+
+/* Flat mirror of the reference geometry structs.  Field meaning and units
+ * are those of nect/sampling/ct_sampling.cu:7-115; tuples keep their order
+ * (nDetector = (rows, cols); sVoxel/dVoxel = (z, y, x); rotDetector =
+ * (roll, pitch, yaw)).  Fields a kind does not use are ignored. */
+typedef struct NectbGeometry {
+  int32_t kind;
+  int32_t nDetector[2];
+  float dDetector[2];
+  float offOrigin[3];
+  float offDetector[2];
+  float rotDetector[3];
+  float COR;
+  float distance_source_to_origin;   /* cone kinds */
+  float distance_origin_to_detector; /* cone kinds */
+  float sVoxel[3];                   /* voxel kinds */
+  float dVoxel[3];                   /* voxel kinds */
+  float object_radius;               /* cylindrical kinds */
+  float object_height;
+  float remove_factor_top;
+  float remove_factor_bottom;
+} NectbGeometry;
+
+/* Ray sampling; replaces sample<T> (nect/sampling/ct_sampling.cu:606-648)
+ * and its kernel sample_points<T> (:578-602).  The two random draws the
+ * reference makes inside the call (:619-622) are inputs here:
+ *   jitter[num_rays]             = U[0,1) - 0.5       (per-ray start offset)
+ *   detector_offset[num_rays*2]  = (U[0,1) - 0.5) * random_detector_offset
+ * Outputs: points[num_rays*S*3] fp32 in (z,y,x) order with unwritten samples
+ * exactly 0 (the kernel writes the zeros; no memset is needed), distances
+ * [num_rays] fp32, and optionally counts[num_rays] int32 = samples written per
+ * ray (may be NULL).  points may be NULL to compute only distances/counts. */
+int nectb_sample(const NectbGeometry* geometry, const int64_t* random_ray_index,
+                 int64_t random_ray_index_len, int64_t starting_ray_index,
+                 int32_t num_rays, int32_t num_points_per_ray, float angle_rad,
+                 float max_ray_distance_per_point, int32_t uniform_ray_spacing,
+                 const float* jitter, const float* detector_offset,
+                 float* points, float* distances, int32_t* counts, void* stream);
+
+/* ---- hash grid + MLP model -------------------------------------------- */
+enum { NECTB_F32 = 0, NECTB_F16 = 1, NECTB_BF16 = 2 };
+enum {
+  NECTB_ACT_NONE = 0,
+  NECTB_ACT_RELU = 1,
+  NECTB_ACT_LEAKY_RELU = 2,
+  NECTB_ACT_SOFTPLUS = 3,
+  NECTB_ACT_SIGMOID = 4
+};
+#define NECTB_MAX_LEVELS 24
+
+/* Multiresolution hash encoding (Mueller et al., ACM TOG 41(4) 2022), the
+ * encoding the reference builds through tiny-cuda-nn from
+ * HashEncoderConfig.get_encoder_config (nect/config.py:86-112).  n_dims is 3
+ * (z,y,x) or 4 (z,y,x,t).  Level l has spatial resolution
+ * floor(base_resolution * per_level_scale^l) and temporal resolution
+ * floor(base_resolution_t * per_level_scale^l) (4D only).  A level is stored
+ * densely when its (res+1)^d vertices fit in 2^log2_hashmap_size entries,
+ * otherwise it is hashed.  params_f32 layout: level after level, entry after
+ * entry, n_features contiguous values per entry; offsets from
+ * nectb_hashgrid_layout(). */
+typedef struct NectbHashGrid {
+  int32_t n_dims;
+  int32_t n_levels;
+  int32_t n_features;
+  int32_t log2_hashmap_size;
+  int32_t feature_dtype; /* NECTB_F32 or NECTB_F16 (table storage) */
+  double base_resolution;
+  double per_level_scale;
+  double base_resolution_t;
+} NectbHashGrid;
+
+/* Fully connected network without biases (the tiny-cuda-nn FullyFusedMLP the
+ * reference configures via MLPNetConfig.get_network_config, nect/config.py:
+ * 115-135).  Weights are one fp32 buffer in PyTorch Linear layout
+ * ([out][in]): W0 [width x n_input], W1..W_{H-1} [width x width],
+ * W_out [1 x width].  compute_dtype NECTB_F32 runs the plain SIMT path;
+ * NECTB_BF16 runs the tensor-core path (bf16 operands, fp32 accumulation). */
+typedef struct NectbMLP {
+  int32_t n_input;
+  int32_t n_hidden_layers;
+  int32_t width;
+  int32_t activation;
+  int32_t output_activation;
+  int32_t compute_dtype;
+} NectbMLP;
+
+/* Per-level layout: resolution, table offset (entries), entries and whether
+ * the level is hashed.  Returns the total number of entries. */
+int64_t nectb_hashgrid_layout(const NectbHashGrid* grid, int32_t* resolution,
+                              int32_t* resolution_t, int64_t* offset,
+                              int64_t* entries, int32_t* hashed);
+int64_t nectb_mlp_param_count(const NectbMLP* mlp);
+
+/* Encoding of n points x[n*n_dims] (fp32, coordinates in [0,1]) into
+ * out[n * n_levels * n_features] fp32.  Replaces the tcnn Encoding forward
+ * behind nect/network/networks.py:95-102. */
+int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* params,
+                          const float* x, int64_t n, float* out, void* stream);
+
+/* Model forward sigma = MLP(encode(x)) for n points (queries, export,
+ * create_volume).  Replaces NetworkWithInputEncoding forward as called by
+ * HashGrid.forward (nect/network/networks.py:59-65) and the export loops
+ * (nect/static_export.py:113-138, nect/dynamic_export.py:413-428).  For 4D
+ * grids x holds (z,y,x) and t is broadcast (networks.py:85). */
+int nectb_model_forward(const NectbHashGrid* grid, const NectbMLP* mlp,
+                        const void* grid_params, const float* mlp_params,
+                        const float* x, int64_t n, float t, float* sigma,
+                        void* stream);
+
+/* ---- fused training step ------------------------------------------------ */
+/* One batch of rays from one projection.  Fuses Projector.__call__
+ * (nect/sampling/projector.py:102-131), the zero-point mask and chunked
+ * model calls (nect/trainers/base_trainer.py:523-551), the line integral
+ * (:552-554), the loss (nect/config.py:481-497) and its backward
+ * (base_trainer.py:650): positions and encodings never reach HBM.
+ * measured[num_rays] are the projection values proj[perm[start:start+R]]
+ * (already gathered by the caller or gathered here when measured_full is
+ * given, see nectb_train_step).  Outputs y_pred[num_rays], loss (mean over
+ * rays), and gradients ADDED into grid_grad (fp32, same layout as the fp32
+ * table) and mlp_grad (fp32).  loss_type: 1 = L1, 2 = L2.  scale =
+ * distances/max_distance_traveled factor is computed in-kernel. */
+typedef struct NectbTrainBatch {
+  const int64_t* random_ray_index;
+  int64_t random_ray_index_len;
+  int64_t starting_ray_index;
+  int32_t num_rays;
+  int32_t num_points_per_ray;
+  float angle_rad;
+  float t;                          /* timestep in [0,1] (4D grids) */
+  float max_ray_distance_per_point;
+  int32_t uniform_ray_spacing;
+  float max_distance_traveled;
+  const float* jitter;              /* [num_rays]   */
+  const float* detector_offset;     /* [num_rays*2] */
+  const float* projection;          /* full flattened projection [P] */
+  int32_t loss_type;
+  float loss_scale;                 /* multiplies dL/dy (1 = plain mean) */
+} NectbTrainBatch;
+
+size_t nectb_train_workspace_bytes(const NectbHashGrid* grid, const NectbMLP* mlp,
+                                   int32_t num_rays);
+
+/* Fused forward+backward.  grid_params is the table in grid->feature_dtype
+ * (fp32 or fp16); mlp_params fp32.  Gradients are accumulated (+=) into
+ * grid_grad (fp32, nectb_hashgrid_layout total * n_features) and mlp_grad
+ * (fp32, nectb_mlp_param_count).  y_pred[num_rays] and loss[1] are written.
+ * workspace: nectb_train_workspace_bytes() bytes of device memory. */
+int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                     const NectbMLP* mlp, const void* grid_params,
+                     const float* mlp_params, const NectbTrainBatch* batch,
+                     float* grid_grad, float* mlp_grad, float* y_pred,
+                     float* loss, void* workspace, size_t workspace_bytes,
+                     void* stream);
+
+/* Adam (torch.optim.Adam semantics, as configured in nect/config.py:400-414)
+ * over n fp32 parameters with fp32 moments; step is the 1-based step count.
+ * When param_half is non-NULL the updated parameter is also written there as
+ * fp16 (the mixed path's table copy).  grad is zeroed after use when
+ * zero_grad != 0 (optim.zero_grad, base_trainer.py:518). */
+int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq,
+                    int64_t n, float lr, float beta1, float beta2, float eps,
+                    float weight_decay, int32_t step, void* param_half,
+                    int32_t zero_grad, void* stream);
+
+/* Version string and last error message of the calling thread. */
+const char* nectb_version(void);
+const char* nectb_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* NECTB_H_ */

@@ -1,0 +1,32 @@
+// Shared host/device helpers for libnectb: error reporting and small utilities.
+#pragma once
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <cuda_runtime.h>
+
+#include "../../include/nectb.h"
+
+namespace nectb {
+
+// Records a message for nectb_last_error() and returns code.
+int set_error(int code, const char* fmt, ...);
+void clear_error();
+
+inline int cuda_status(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) return set_error(NECTB_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+  return NECTB_OK;
+}
+
+// Checks the launch that was just enqueued (configuration errors only; the
+// call never synchronises).
+inline int launch_status(const char* what) { return cuda_status(cudaGetLastError(), what); }
+
+inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+}  // namespace nectb
+
+#define NECTB_REQUIRE(cond, ...)                                        \
+  do {                                                                  \
+    if (!(cond)) return ::nectb::set_error(NECTB_ERR_INVALID, __VA_ARGS__); \
+  } while (0)

@@ -1,0 +1,181 @@
+// Multiresolution hash encoding on the device: per-level layout, corner
+// indices and weights, gather (forward) and atomic scatter (backward).
+//
+// Method: Mueller et al., "Instant Neural Graphics Primitives with a
+// Multiresolution Hash Encoding", ACM TOG 41(4), 2022, section 3 (the
+// encoding the reference takes from tiny-cuda-nn, nect/network/networks.py:
+// 52-57 and 478-481).  Build-defined details, identical in oracle/hashgrid.py:
+//   - level resolution floor(base * scale^l) (t axis: floor(base_t * scale^l));
+//   - p = x * res in fp32, cell = clamp(floor(p), 0, res-1), frac = p - cell;
+//   - dense storage when (res+1)^d vertices fit in T (entries rounded up to a
+//     multiple of 8), else hash XOR_k v_k * pi_k mod T with
+//     pi = (1, 2654435761, 805459861, 2246822519);
+//   - axis k of the input (z, y, x[, t]) has pi_k / stride_k.
+// Corner c has bit k set when it takes the upper vertex along axis k; its
+// weight is the product over k of (bit ? frac_k : 1 - frac_k) in axis order.
+#pragma once
+#include <cuda_fp16.h>
+#include <cstdint>
+
+#include "../../include/nectb.h"
+
+namespace nectb {
+
+constexpr uint32_t kPrime1 = 2654435761u;
+constexpr uint32_t kPrime2 = 805459861u;
+constexpr uint32_t kPrime3 = 2246822519u;
+
+struct GridDev {
+  int n_dims;
+  int n_levels;
+  int n_features;
+  uint32_t hash_mask;
+  uint32_t hashed_bits;  // bit l: level l is hashed
+  int res[NECTB_MAX_LEVELS][4];
+  uint32_t stride[NECTB_MAX_LEVELS][4];
+  int64_t offset[NECTB_MAX_LEVELS];  // first entry of level l
+  int64_t total_entries;
+};
+
+// Host: fill GridDev from the C-ABI description (returns false when invalid).
+bool make_grid_dev(const NectbHashGrid* g, GridDev* out);
+
+template <int D>
+struct LevelCorners {
+  uint32_t idx[1 << D];  // entry index within the level
+  float w[1 << D];
+};
+
+template <int D>
+__device__ __forceinline__ void level_corners(const GridDev& g, int l, const float* x, LevelCorners<D>& lc) {
+  int c[D];
+  float f[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    const int r = g.res[l][k];
+    const float p = x[k] * (float)r;
+    int ci = (int)floorf(p);
+    ci = ci < 0 ? 0 : (ci > r - 1 ? r - 1 : ci);
+    c[k] = ci;
+    f[k] = p - (float)ci;
+  }
+  const bool hashed = (g.hashed_bits >> l) & 1u;
+#pragma unroll
+  for (int corner = 0; corner < (1 << D); ++corner) {
+    uint32_t v[D];
+#pragma unroll
+    for (int k = 0; k < D; ++k) v[k] = (uint32_t)c[k] + ((corner >> k) & 1);
+    uint32_t id;
+    if (hashed) {
+      id = v[0];
+      if (D > 1) id ^= v[1] * kPrime1;
+      if (D > 2) id ^= v[2] * kPrime2;
+      if (D > 3) id ^= v[3 % D] * kPrime3;
+      id &= g.hash_mask;
+    } else {
+      id = v[0];
+#pragma unroll
+      for (int k = 1; k < D; ++k) id += v[k] * g.stride[l][k];
+    }
+    float w = 1.f;
+#pragma unroll
+    for (int k = 0; k < D; ++k) w = w * (((corner >> k) & 1) ? f[k] : (1.f - f[k]));
+    lc.idx[corner] = id;
+    lc.w[corner] = w;
+  }
+}
+
+// ---- feature loads -----------------------------------------------------
+template <int F, typename T>
+struct Feat;
+
+template <>
+struct Feat<2, float> {
+  static __device__ __forceinline__ void load(const float* base, int64_t entry, float* out) {
+    const float2 v = __ldg(reinterpret_cast<const float2*>(base + entry * 2));
+    out[0] = v.x;
+    out[1] = v.y;
+  }
+};
+template <>
+struct Feat<4, float> {
+  static __device__ __forceinline__ void load(const float* base, int64_t entry, float* out) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(base + entry * 4));
+    out[0] = v.x;
+    out[1] = v.y;
+    out[2] = v.z;
+    out[3] = v.w;
+  }
+};
+template <>
+struct Feat<2, __half> {
+  static __device__ __forceinline__ void load(const __half* base, int64_t entry, float* out) {
+    const unsigned int raw = __ldg(reinterpret_cast<const unsigned int*>(base + entry * 2));
+    const __half2 h = *reinterpret_cast<const __half2*>(&raw);
+    const float2 v = __half22float2(h);
+    out[0] = v.x;
+    out[1] = v.y;
+  }
+};
+template <>
+struct Feat<4, __half> {
+  static __device__ __forceinline__ void load(const __half* base, int64_t entry, float* out) {
+    const uint2 raw = __ldg(reinterpret_cast<const uint2*>(base + entry * 4));
+    const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+    const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+    out[0] = a.x;
+    out[1] = a.y;
+    out[2] = b.x;
+    out[3] = b.y;
+  }
+};
+
+// Encodes one point: out[l*F + f] for all levels.  x has D coordinates in [0,1].
+template <int D, int F, typename T>
+__device__ __forceinline__ void encode_point(const GridDev& g, const T* __restrict__ table, const float* x,
+                                             float* out) {
+#pragma unroll 1
+  for (int l = 0; l < g.n_levels; ++l) {
+    LevelCorners<D> lc;
+    level_corners<D>(g, l, x, lc);
+    float vals[1 << D][F];
+#pragma unroll
+    for (int c = 0; c < (1 << D); ++c) Feat<F, T>::load(table, g.offset[l] + lc.idx[c], vals[c]);
+    float acc[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) acc[f] = 0.f;
+#pragma unroll
+    for (int c = 0; c < (1 << D); ++c)
+#pragma unroll
+      for (int f = 0; f < F; ++f) acc[f] = fmaf(lc.w[c], vals[c][f], acc[f]);
+#pragma unroll
+    for (int f = 0; f < F; ++f) out[l * F + f] = acc[f];
+  }
+}
+
+// Gradient scatter of one point: grad[offset + idx][f] += w * dout[l*F + f].
+template <int D, int F>
+__device__ __forceinline__ void scatter_point(const GridDev& g, float* __restrict__ grad, const float* x,
+                                              const float* dout) {
+#pragma unroll 1
+  for (int l = 0; l < g.n_levels; ++l) {
+    LevelCorners<D> lc;
+    level_corners<D>(g, l, x, lc);
+#pragma unroll
+    for (int c = 0; c < (1 << D); ++c) {
+      float* dst = grad + (g.offset[l] + lc.idx[c]) * F;
+      if constexpr (F == 2) {
+        atomicAdd(reinterpret_cast<float2*>(dst), make_float2(lc.w[c] * dout[l * F], lc.w[c] * dout[l * F + 1]));
+      } else if constexpr (F == 4) {
+        atomicAdd(reinterpret_cast<float4*>(dst),
+                  make_float4(lc.w[c] * dout[l * F], lc.w[c] * dout[l * F + 1], lc.w[c] * dout[l * F + 2],
+                              lc.w[c] * dout[l * F + 3]));
+      } else {
+#pragma unroll
+        for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * dout[l * F + f]);
+      }
+    }
+  }
+}
+
+}  // namespace nectb
