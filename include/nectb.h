@@ -137,6 +137,13 @@ int64_t nectb_mlp_param_count(const NectbMLP* mlp);
 int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* params,
                           const float* x, int64_t n, float* out, void* stream);
 
+/* Diagnostic: per-level corner indices (entry index within the level, int32)
+ * and d-linear weights of n points, idx/w[n][n_levels][2^n_dims].  No
+ * counterpart in the reference (tiny-cuda-nn keeps them internal); it lets
+ * tests check the integer hash arithmetic bit for bit. */
+int nectb_hashgrid_corners(const NectbHashGrid* grid, const float* x, int64_t n,
+                           int32_t* idx, float* w, void* stream);
+
 /* Model forward sigma = MLP(encode(x)) for n points (queries, export,
  * create_volume).  Replaces NetworkWithInputEncoding forward as called by
  * HashGrid.forward (nect/network/networks.py:59-65) and the export loops

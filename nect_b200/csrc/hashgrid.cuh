@@ -130,10 +130,11 @@ struct Feat<4, __half> {
   }
 };
 
-// Encodes one point: out[l*F + f] for all levels.  x has D coordinates in [0,1].
+// Encodes one point: out[(l*F + f) * stride] for all levels.  x has D
+// coordinates in [0,1].
 template <int D, int F, typename T>
 __device__ __forceinline__ void encode_point(const GridDev& g, const T* __restrict__ table, const float* x,
-                                             float* out) {
+                                             float* out, int stride = 1) {
 #pragma unroll 1
   for (int l = 0; l < g.n_levels; ++l) {
     LevelCorners<D> lc;
@@ -149,30 +150,32 @@ __device__ __forceinline__ void encode_point(const GridDev& g, const T* __restri
 #pragma unroll
       for (int f = 0; f < F; ++f) acc[f] = fmaf(lc.w[c], vals[c][f], acc[f]);
 #pragma unroll
-    for (int f = 0; f < F; ++f) out[l * F + f] = acc[f];
+    for (int f = 0; f < F; ++f) out[(l * F + f) * stride] = acc[f];
   }
 }
 
-// Gradient scatter of one point: grad[offset + idx][f] += w * dout[l*F + f].
+// Gradient scatter of one point: grad[offset + idx][f] += w * dout[(l*F + f) * stride].
 template <int D, int F>
 __device__ __forceinline__ void scatter_point(const GridDev& g, float* __restrict__ grad, const float* x,
-                                              const float* dout) {
+                                              const float* dsrc, int stride = 1) {
 #pragma unroll 1
   for (int l = 0; l < g.n_levels; ++l) {
     LevelCorners<D> lc;
     level_corners<D>(g, l, x, lc);
+    float d[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) d[f] = dsrc[(l * F + f) * stride];
 #pragma unroll
     for (int c = 0; c < (1 << D); ++c) {
       float* dst = grad + (g.offset[l] + lc.idx[c]) * F;
       if constexpr (F == 2) {
-        atomicAdd(reinterpret_cast<float2*>(dst), make_float2(lc.w[c] * dout[l * F], lc.w[c] * dout[l * F + 1]));
+        atomicAdd(reinterpret_cast<float2*>(dst), make_float2(lc.w[c] * d[0], lc.w[c] * d[1]));
       } else if constexpr (F == 4) {
         atomicAdd(reinterpret_cast<float4*>(dst),
-                  make_float4(lc.w[c] * dout[l * F], lc.w[c] * dout[l * F + 1], lc.w[c] * dout[l * F + 2],
-                              lc.w[c] * dout[l * F + 3]));
+                  make_float4(lc.w[c] * d[0], lc.w[c] * d[1], lc.w[c] * d[2], lc.w[c] * d[3]));
       } else {
 #pragma unroll
-        for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * dout[l * F + f]);
+        for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * d[f]);
       }
     }
   }

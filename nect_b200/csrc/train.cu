@@ -1,0 +1,119 @@
+// C-ABI entry points of the fused training step and the Adam update.
+#include <algorithm>
+
+#include "mlp_simt.cuh"
+#include "train_common.cuh"
+
+namespace nectb {
+
+int validate_geometry(const NectbGeometry* g);
+int validate_mlp(const NectbMLP* m, const GridDev& g);
+int64_t mlp_param_count(const NectbMLP* m);
+int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const float* table,
+                const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
+                float* y_pred, float* loss, cudaStream_t s);
+int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const void* table,
+                const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
+                float* y_pred, float* loss, cudaStream_t s);
+
+namespace {
+
+// torch.optim.Adam (no amsgrad, not maximize), one element per thread.
+__global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float wd,
+                            float bc1, float bc2_sqrt, __half* __restrict__ p_half, int zero_grad) {
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
+    float grad = g[i];
+    float param = p[i];
+    if (wd != 0.f) grad = fmaf(wd, param, grad);
+    const float mi = fmaf(b1, m[i] - grad, grad);           // m = b1*m + (1-b1)*g  (lerp form)
+    const float vi = fmaf(b2, v[i], (1.f - b2) * grad * grad);
+    m[i] = mi;
+    v[i] = vi;
+    const float denom = sqrtf(vi) / bc2_sqrt + eps;
+    param = param - (lr / bc1) * (mi / denom);
+    p[i] = param;
+    if (p_half) p_half[i] = __float2half_rn(param);
+    if (zero_grad) g[i] = 0.f;
+  }
+}
+
+}  // namespace
+}  // namespace nectb
+
+using namespace nectb;
+
+extern "C" size_t nectb_train_workspace_bytes(const NectbHashGrid* grid, const NectbMLP* mlp, int32_t num_rays) {
+  (void)grid;
+  (void)mlp;
+  return workspace_bytes(std::max(num_rays, 1));
+}
+
+extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                                float* grid_grad, float* mlp_grad, float* y_pred, float* loss, void* workspace,
+                                size_t workspace_size, void* stream) {
+  clear_error();
+  if (int rc = validate_geometry(geometry)) return rc;
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  if (int rc = validate_mlp(mlp, g)) return rc;
+  NECTB_REQUIRE(batch != nullptr, "batch is null");
+  NECTB_REQUIRE(g.n_levels == 16, "fused training needs n_levels == 16 (got %d)", g.n_levels);
+  NECTB_REQUIRE(batch->num_rays >= 0 && batch->num_points_per_ray >= 1, "bad batch sizes");
+  NECTB_REQUIRE(batch->loss_type == 1 || batch->loss_type == 2, "loss_type must be 1 (L1) or 2 (L2)");
+  NECTB_REQUIRE(batch->max_distance_traveled > 0.f, "max_distance_traveled must be positive");
+  NECTB_REQUIRE(grid_params && mlp_params && grid_grad && mlp_grad && y_pred && loss, "null parameter/output");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
+  if (batch->num_rays == 0) return NECTB_OK;
+  NECTB_REQUIRE(batch->random_ray_index && batch->jitter && batch->detector_offset && batch->projection,
+                "null batch input");
+  if (!workspace || workspace_size < workspace_bytes(batch->num_rays))
+    return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
+                     workspace_bytes(batch->num_rays));
+  TrainArgs a;
+  a.perm = batch->random_ray_index;
+  a.perm_len = batch->random_ray_index_len;
+  a.start = batch->starting_ray_index;
+  a.num_rays = batch->num_rays;
+  a.S = batch->num_points_per_ray;
+  a.angle = batch->angle_rad;
+  a.t = batch->t;
+  a.maxd = batch->max_ray_distance_per_point;
+  a.uniform = batch->uniform_ray_spacing;
+  a.max_dist = batch->max_distance_traveled;
+  a.jitter = batch->jitter;
+  a.det_off = batch->detector_offset;
+  a.projection = batch->projection;
+  a.loss_type = batch->loss_type;
+  a.loss_scale = batch->loss_scale;
+  Workspace ws = carve_workspace(workspace, a.num_rays);
+  if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
+  const int nW = (int)mlp_param_count(mlp);
+  if (mlp->compute_dtype == NECTB_F32) {
+    NECTB_REQUIRE(grid->feature_dtype == NECTB_F32, "plain path needs an fp32 table");
+    return train_plain(*geometry, g, *mlp, (const float*)grid_params, mlp_params, nW, a, ws, grid_grad, mlp_grad,
+                       y_pred, loss, s);
+  }
+  return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, a, ws, grid_grad, mlp_grad, y_pred, loss, s);
+}
+
+extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr,
+                               float beta1, float beta2, float eps, float weight_decay, int32_t step,
+                               void* param_half, int32_t zero_grad, void* stream) {
+  clear_error();
+  if (n == 0) return NECTB_OK;
+  NECTB_REQUIRE(param && grad && exp_avg && exp_avg_sq && n > 0 && step >= 1, "bad Adam arguments");
+  const double bc1 = 1.0 - std::pow((double)beta1, step);
+  const double bc2 = 1.0 - std::pow((double)beta2, step);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 8);
+  adam_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, lr, beta1, beta2, eps,
+                                                        weight_decay, (float)bc1, (float)std::sqrt(bc2),
+                                                        (__half*)param_half, zero_grad);
+  return launch_status("adam_kernel");
+}

@@ -1,0 +1,328 @@
+// Plain fp32 fused training step (SIMT MLP), the path the mixed-precision
+// tensor-core kernels are measured against.
+//
+// Three launches per batch:
+//   1. ray_prep_kernel   warp per ray: entry/exit, count, measured value.
+//   2. fwd_plain_kernel  warp per ray: regenerate each sample, encode, MLP,
+//                        warp-shuffle sum along the ray -> y_pred, loss,
+//                        dL/dsigma for the ray.
+//   3. bwd_plain_kernel  blocks of NT threads step through tiles of NT
+//                        samples: re-encode, forward, backward through the
+//                        MLP, fp32 weight-gradient tile products accumulated
+//                        in registers, table gradients by float2/float4
+//                        atomics.
+// Sample positions and encodings live only in registers and shared memory.
+#include <algorithm>
+
+#include "mlp_simt.cuh"
+#include "train_common.cuh"
+
+namespace nectb {
+
+__global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict__ recs) {
+  const int lane = threadIdx.x & 31;
+  const int tid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (tid >= a.num_rays) return;
+  int ray_index = 0;
+  RaySetup r;
+  r.valid = 0;
+  r.distance = 0.f;
+  const bool ok = ray_lookup(a.perm, a.perm_len, a.start, tid, a.num_rays, g, ray_index);
+  if (ok)
+    ray_setup(g, ray_index, a.det_off[2 * (int64_t)tid], a.det_off[2 * (int64_t)tid + 1], a.jitter[tid], a.angle,
+              a.S, a.maxd, a.uniform != 0, r);
+  int count = 0;
+  if (r.valid) count = warp_sample_count(g, r, a.S, lane);
+  if (lane == 0) {
+    RayRec rec;
+    rec.sx = r.start.x;
+    rec.sy = r.start.y;
+    rec.sz = r.start.z;
+    rec.dx = r.step.x;
+    rec.dy = r.step.y;
+    rec.dz = r.step.z;
+    rec.count = count;
+    rec.scale = r.distance / a.max_dist;
+    // proj[perm[start:start+R]] (projector.py:130); rays past the end of the
+    // permutation are not part of the reference batch and get y = 0 here.
+    const bool in_range = ok && ray_index >= 0;
+    rec.y = in_range ? a.projection[ray_index] : 0.f;
+    rec.gsig = 0.f;
+    recs[tid] = rec;
+  }
+}
+
+namespace {
+
+constexpr int kPlainFwdThreads = 128;
+
+template <int D, int F, int IN, int H>
+__global__ void __launch_bounds__(kPlainFwdThreads)
+fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __restrict__ W, TrainArgs a,
+                 RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int act, int out_act,
+                 float* __restrict__ y_pred, float* __restrict__ loss) {
+  constexpr int NT = kPlainFwdThreads;
+  constexpr int LD = NT + 4;
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const SimtWeights sw = stage_weights<IN, H, false>(W, smem);
+  float* cols = smem + simt_weight_floats<IN, H, false>();
+  const int t = threadIdx.x;
+  float* x = cols + t;                 // [IN][LD]
+  float* hid = cols + IN * LD + t;     // [(H-1)*64][LD]
+  __syncthreads();
+  const int lane = t & 31;
+  float loss_acc = 0.f;
+  while (true) {
+    int r = 0;
+    if (lane == 0) r = (int)atomicAdd(counter, 1u);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= a.num_rays) break;
+    const RayRec rec = load_ray(recs, r);
+    float sum = 0.f;
+    for (int base = 0; base < rec.count; base += 32) {
+      const int i = base + lane;
+      float p[4];
+      bool valid = false;
+      if (i < rec.count) valid = sample_point(rec, i, p);
+      if (D == 4) p[3] = a.t;
+      if (valid) {
+        encode_point<D, F, float>(grid, table, p, x, LD);
+        const float* in = x;
+        if (H == 1) {
+          sum += act_fwd(gemv_dot<IN, LD>(sw.WT[0], in, sw.wout, act), out_act);
+        } else {
+          gemv_cols<IN, kWidth, LD>(sw.WT[0], in, hid, act);
+#pragma unroll
+          for (int k = 1; k < H - 1; ++k)
+            gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + (k - 1) * kWidth * LD, hid + k * kWidth * LD, act);
+          sum += act_fwd(gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + (H - 2) * kWidth * LD, sw.wout, act), out_act);
+        }
+      }
+    }
+    sum = warp_sum(sum);
+    if (lane == 0) {
+      const float yp = sum * rec.scale;
+      y_pred[r] = yp;
+      recs[r].gsig = loss_grad(yp, rec.y, a.loss_type, a.num_rays, rec.scale) * a.loss_scale;
+      loss_acc += loss_term(yp, rec.y, a.loss_type);
+    }
+  }
+  __shared__ float red[NT / 32];
+  if (lane == 0) red[t >> 5] = loss_acc;
+  __syncthreads();
+  if (t == 0) {
+    float s = 0.f;
+    for (int w = 0; w < NT / 32; ++w) s += red[w];
+    atomicAdd(loss, s / (float)a.num_rays);
+  }
+}
+
+// acc[a][b] += sum_t G[(4*jb + a)*LD + t] * A[(ib*IB + b)*LD + t] over the
+// tile's NT samples (weight gradient dW[j][i] = sum_t G[t][j] A[t][i]).
+// Thread p owns rows 4*jb..4*jb+3 and columns ib*IB..ib*IB+IB-1.
+template <int K, int NT, int LD>
+struct WGrad {
+  static constexpr int IBLK = NT / 16;
+  static constexpr int IB = K / IBLK;
+  static_assert(16 * IBLK == NT && IB * IBLK == K, "tile shape");
+  float acc[4][IB];
+  __device__ __forceinline__ void zero() {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < IB; ++b) acc[a][b] = 0.f;
+  }
+  __device__ __forceinline__ void add(const float* __restrict__ G, const float* __restrict__ A) {
+    const int jb = threadIdx.x / IBLK, ib = threadIdx.x % IBLK;
+#pragma unroll 2
+    for (int t = 0; t < NT; t += 4) {
+      float4 g[4], v[IB];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) g[a] = *reinterpret_cast<const float4*>(G + (4 * jb + a) * LD + t);
+#pragma unroll
+      for (int b = 0; b < IB; ++b) v[b] = *reinterpret_cast<const float4*>(A + (ib * IB + b) * LD + t);
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < IB; ++b) {
+          acc[a][b] = fmaf(g[a].x, v[b].x, acc[a][b]);
+          acc[a][b] = fmaf(g[a].y, v[b].y, acc[a][b]);
+          acc[a][b] = fmaf(g[a].z, v[b].z, acc[a][b]);
+          acc[a][b] = fmaf(g[a].w, v[b].w, acc[a][b]);
+        }
+    }
+  }
+  __device__ __forceinline__ void flush(float* __restrict__ dst) const {  // dst [64][K]
+    const int jb = threadIdx.x / IBLK, ib = threadIdx.x % IBLK;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < IB; ++b) atomicAdd(dst + (4 * jb + a) * K + ib * IB + b, acc[a][b]);
+  }
+};
+
+template <int D, int F, int IN, int H, int NT>
+__global__ void __launch_bounds__(NT, 1)
+bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __restrict__ W, TrainArgs a,
+                 const RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int act, int out_act,
+                 float* __restrict__ table_grad, float* __restrict__ W_grad) {
+  constexpr int NW = NT / 32;
+  constexpr int LD = NT + 4;
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const SimtWeights sw = stage_weights<IN, H, true>(W, smem);
+  float* cols = smem + simt_weight_floats<IN, H, true>();
+  float* sX = cols;                      // [IN][LD]
+  float* sA = sX + IN * LD;              // [H][64][LD]  a_1..a_H
+  float* sG = sA + H * kWidth * LD;      // [64][LD]
+  float* sG2 = sG + kWidth * LD;         // [64][LD]
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  (void)NW;
+  WGrad<IN, NT, LD> g0;
+  g0.zero();
+  WGrad<kWidth, NT, LD> gh[H > 1 ? H - 1 : 1];
+#pragma unroll
+  for (int k = 0; k < H - 1; ++k) gh[k].zero();
+  float dwout[2] = {0.f, 0.f};  // lane owns w_out[lane] and w_out[lane + 32]
+
+  int ray = -1, base = 0;
+  RayRec rec;
+  rec.count = 0;
+  rec.gsig = 0.f;
+  __syncthreads();
+  while (true) {
+    if (ray < a.num_rays && (ray < 0 || base >= rec.count)) {
+      while (true) {
+        int r = 0;
+        if (lane == 0) r = (int)atomicAdd(counter, 1u);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r >= a.num_rays) {
+          ray = a.num_rays;
+          rec.count = 0;
+          break;
+        }
+        rec = load_ray(recs, r);
+        ray = r;
+        base = 0;
+        if (rec.count > 0) break;
+      }
+    }
+    const bool warp_active = ray < a.num_rays;
+    if (!__syncthreads_or(warp_active)) break;
+
+    const int i = base + lane;
+    float p[4];
+    bool valid = false;
+    if (warp_active && i < rec.count) valid = sample_point(rec, i, p);
+    if (D == 4) p[3] = a.t;
+    if (valid) {
+      encode_point<D, F, float>(grid, table, p, sX + t, LD);
+    } else {
+      for (int k = 0; k < IN; ++k) sX[k * LD + t] = 0.f;
+    }
+    // forward: a_1..a_H into sA
+    gemv_cols<IN, kWidth, LD>(sw.WT[0], sX + t, sA + t, act);
+#pragma unroll
+    for (int k = 1; k < H; ++k)
+      gemv_cols<kWidth, kWidth, LD>(sw.WT[k], sA + (k - 1) * kWidth * LD + t, sA + k * kWidth * LD + t, act);
+    const float* aH = sA + (H - 1) * kWidth * LD + t;
+    const float z = dot_col<kWidth, LD>(sw.wout, aH);
+    const float dz = valid ? rec.gsig * act_grad_z(z, out_act) : 0.f;
+    // w_out gradient (sum over the warp's samples), and G_H = dz * w_out * act'(a_H)
+#pragma unroll 4
+    for (int j = 0; j < kWidth; ++j) {
+      const float aj = aH[j * LD];
+      const float v = warp_sum(dz * aj);
+      if ((j & 31) == lane) dwout[j >> 5] += v;
+      sG[j * LD + t] = dz * sw.wout[j] * act_grad_a(aj, act);
+    }
+    float* G = sG;
+    float* G2 = sG2;
+#pragma unroll
+    for (int k = H - 1; k >= 1; --k) {
+      __syncthreads();
+      gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      // G_k = (W_k^T G_{k+1}) * act'(a_k); W_k is [64 out][64 in] = M[j][i]
+      gemv_cols<kWidth, kWidth, LD>(sw.W[k], G + t, G2 + t, NECTB_ACT_NONE);
+      const float* ak = sA + (k - 1) * kWidth * LD + t;
+      for (int j = 0; j < kWidth; ++j) G2[j * LD + t] *= act_grad_a(ak[j * LD], act);
+      float* tmp = G;
+      G = G2;
+      G2 = tmp;
+    }
+    __syncthreads();
+    g0.add(G, sX);
+    // dX = W_0^T G_1 (W_0 is [64][IN] = M[j][i]) into G2, then scatter
+    gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
+    if (valid) scatter_point<D, F>(grid, table_grad, p, G2 + t, LD);
+    __syncthreads();
+    base += 32;
+  }
+  g0.flush(W_grad);
+#pragma unroll
+  for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+  const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
+  // combine the warps' w_out partials through shared memory (reuse sG)
+  __syncthreads();
+  float* red = sG;  // [NW][64]
+  red[(t >> 5) * kWidth + lane] = dwout[0];
+  red[(t >> 5) * kWidth + lane + 32] = dwout[1];
+  __syncthreads();
+  if (t < kWidth) {
+    float s = 0.f;
+    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + t];
+    atomicAdd(W_grad + nHidden + t, s);
+  }
+}
+
+template <int D, int F, int H>
+int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table, const float* W, const TrainArgs& a,
+              Workspace ws, int act, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
+              cudaStream_t s) {
+  constexpr int IN = 16 * F;
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+
+  ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
+  if (int rc = launch_status("ray_prep_kernel")) return rc;
+
+  constexpr int FNT = kPlainFwdThreads;
+  auto fk = fwd_plain_kernel<D, F, IN, H>;
+  const size_t fsmem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (FNT + 4)) * 4;
+  cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, FNT, fsmem);
+  const int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
+  fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.counters, act, out_act, y_pred, loss);
+  if (int rc = launch_status("fwd_plain_kernel")) return rc;
+
+  constexpr int NT = 128;
+  auto bk = bwd_plain_kernel<D, F, IN, H, NT>;
+  const size_t bsmem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
+  if (bsmem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "plain backward needs %zu B of shared memory", bsmem);
+  cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+  const int bblocks = std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, NT / 32)));
+  bk<<<bblocks, NT, bsmem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, act, out_act, table_grad, W_grad);
+  return launch_status("bwd_plain_kernel");
+}
+
+}  // namespace
+
+int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const float* table,
+                const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
+                float* y_pred, float* loss, cudaStream_t s) {
+  (void)nW;
+  const int D = grid.n_dims, F = grid.n_features, H = mlp.n_hidden_layers;
+  const int act = mlp.activation, oact = mlp.output_activation;
+  if (D == 3 && F == 2 && H == 2)
+    return run_plain<3, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+  if (D == 4 && F == 2 && H == 2)
+    return run_plain<4, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+  return set_error(NECTB_ERR_INVALID, "plain path supports 16x2 grids with 2 hidden layers (got n_dims %d, "
+                   "n_features %d, hidden %d)", D, F, H);
+}
+
+}  // namespace nectb

@@ -1,0 +1,206 @@
+"""Fused training: one CUDA pipeline per batch of rays instead of the
+reference's sample -> mask -> model -> sum -> loss -> backward sequence
+(nect/trainers/base_trainer.py:517-653).
+
+* ``train_step`` calls ``nectb_train_step`` once: it regenerates the samples of
+  every ray (bit-identical to the sampler), encodes, runs the MLP, integrates
+  along the ray, evaluates the L1/L2 loss and ADDS the gradients of the table
+  and the MLP into fp32 buffers.
+* ``FusedRayLoss`` wraps it as a torch.autograd.Function (the hand-written
+  backward: gradients are computed in the same fused pass and returned scaled
+  by the incoming gradient), so a standard torch optimizer works.
+* ``Trainer`` reproduces the per-projection loop (randperm of the detector,
+  ``batch_per_proj`` batches, Adam) with a fused Adam kernel that also
+  refreshes the fp16 table on the mixed path.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import torch
+
+from . import _lib
+from .network import _HashGridModel
+from .sampling.ct_sampling import draw_ray_randoms
+from .sampling.geometry import Geometry
+
+LOSS = {"l1": 1, "l2": 2}
+
+
+@dataclass
+class RayBatch:
+    """One batch of rays of one projection (Projector.__call__ arguments)."""
+    perm: torch.Tensor            # int64 [P] randperm of detector pixels
+    start: int                    # starting_ray_index
+    num_rays: int
+    points_per_ray: int
+    angle: float
+    max_ray_distance_per_point: float
+    jitter: torch.Tensor          # [R]
+    detector_offset: torch.Tensor # [R, 2]
+    projection: torch.Tensor      # fp32 [P] flattened projection (min-max scaled)
+    t: float = 0.0
+    uniform_ray_spacing: bool = True
+
+
+class Workspace:
+    """Caller-owned device workspace for nectb_train_step, grown on demand."""
+
+    def __init__(self):
+        self.buf = None
+
+    def get(self, model: _HashGridModel, num_rays: int, device) -> tuple[int, int]:
+        need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
+                                                    num_rays)
+        if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
+            self.buf = torch.empty(need, dtype=torch.uint8, device=device)
+        return self.buf.data_ptr(), self.buf.numel()
+
+
+def c_batch(batch: RayBatch, max_distance_traveled: float, loss: str, loss_scale: float = 1.0):
+    b = _lib.NectbTrainBatch()
+    b.random_ray_index = batch.perm.data_ptr()
+    b.random_ray_index_len = batch.perm.numel()
+    b.starting_ray_index = int(batch.start)
+    b.num_rays = int(batch.num_rays)
+    b.num_points_per_ray = int(batch.points_per_ray)
+    b.angle_rad = float(batch.angle)
+    b.t = float(batch.t)
+    b.max_ray_distance_per_point = float(batch.max_ray_distance_per_point)
+    b.uniform_ray_spacing = 1 if batch.uniform_ray_spacing else 0
+    b.max_distance_traveled = float(max_distance_traveled)
+    b.jitter = batch.jitter.data_ptr()
+    b.detector_offset = batch.detector_offset.data_ptr()
+    b.projection = batch.projection.data_ptr()
+    b.loss_type = LOSS[loss.lower()]
+    b.loss_scale = float(loss_scale)
+    return b
+
+
+def train_step(model: _HashGridModel, c_geometry, batch: RayBatch, max_distance_traveled: float,
+               table_grad: torch.Tensor, mlp_grad: torch.Tensor, workspace: Workspace, loss: str = "l2",
+               loss_scale: float = 1.0):
+    """Fused forward+backward; gradients are ADDED to table_grad / mlp_grad.
+
+    Returns (loss [1] device tensor, y_pred [R])."""
+    dev = batch.perm.device
+    for name, t in (("perm", batch.perm), ("jitter", batch.jitter), ("detector_offset", batch.detector_offset),
+                    ("projection", batch.projection)):
+        _lib.require_cuda(t, name)
+    y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
+    loss_out = torch.empty(1, device=dev, dtype=torch.float32)
+    ws_ptr, ws_size = workspace.get(model, batch.num_rays, dev)
+    cb = c_batch(batch, max_distance_traveled, loss, loss_scale)
+    rc = _lib.lib.nectb_train_step(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                   ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(), model.mlp.data_ptr(),
+                                   ctypes.byref(cb), table_grad.data_ptr(), mlp_grad.data_ptr(), y_pred.data_ptr(),
+                                   loss_out.data_ptr(), ws_ptr, ws_size, _lib.stream_ptr(dev))
+    _lib.check(rc, "nectb_train_step")
+    return loss_out, y_pred
+
+
+class FusedRayLoss(torch.autograd.Function):
+    """loss = L(y_pred(table, mlp), y) with the hand-written fused backward."""
+
+    @staticmethod
+    def forward(ctx, table, mlp, model, c_geometry, batch, max_distance_traveled, loss, workspace):
+        tg = torch.zeros_like(table)
+        mg = torch.zeros_like(mlp)
+        out, _ = train_step(model, c_geometry, batch, max_distance_traveled, tg, mg, workspace, loss)
+        ctx.save_for_backward(tg, mg)
+        return out[0]
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        tg, mg = ctx.saved_tensors
+        return tg * grad_out, mg * grad_out, None, None, None, None, None, None
+
+
+def adam_step(param: torch.Tensor, grad: torch.Tensor, m: torch.Tensor, v: torch.Tensor, step: int, lr: float,
+              betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0, half: torch.Tensor | None = None,
+              zero_grad: bool = True):
+    rc = _lib.lib.nectb_adam_step(param.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), param.numel(),
+                                  float(lr), float(betas[0]), float(betas[1]), float(eps), float(weight_decay),
+                                  int(step), half.data_ptr() if half is not None else None, 1 if zero_grad else 0,
+                                  _lib.stream_ptr(param.device))
+    _lib.check(rc, "nectb_adam_step")
+
+
+class Trainer:
+    """Per-projection training loop on the fused kernels.
+
+    Mirrors BaseTrainer.fit's inner structure (base_trainer.py:492-655): for each
+    projection a device randperm of the detector pixels, up to ``batch_per_proj``
+    batches of ``points_per_batch // points_per_ray`` rays, each followed by an
+    Adam step (lr fixed unless a schedule is passed)."""
+
+    def __init__(self, model: _HashGridModel, geometry: Geometry, points_per_batch: int, points_per_ray: int,
+                 loss: str = "l2", lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8,
+                 weight_decay: float = 0.0, batch_per_proj: int = 1, random_offset_detector: float = 0.0,
+                 uniform_ray_spacing: bool = True, device="cuda"):
+        self.model = model
+        self.geometry = geometry
+        self.c_geometry = geometry.get_c_geometry()
+        self.device = torch.device(device)
+        self.points_per_batch = points_per_batch
+        self.points_per_ray = points_per_ray
+        self.loss = loss
+        self.lr = lr
+        self.betas = betas
+        self.eps = eps
+        self.weight_decay = weight_decay
+        self.batch_per_proj = batch_per_proj
+        self.random_offset_detector = random_offset_detector
+        self.uniform_ray_spacing = uniform_ray_spacing
+        self.table_grad = torch.zeros_like(model.table)
+        self.mlp_grad = torch.zeros_like(model.mlp)
+        self.m_table = torch.zeros_like(model.table)
+        self.v_table = torch.zeros_like(model.table)
+        self.m_mlp = torch.zeros_like(model.mlp)
+        self.v_mlp = torch.zeros_like(model.mlp)
+        self.step_count = 0
+        self.workspace = Workspace()
+
+    @property
+    def batch_size(self) -> int:
+        return self.points_per_batch // self.points_per_ray
+
+    def make_batch(self, perm: torch.Tensor, batch_num: int, angle: float, projection: torch.Tensor,
+                   t: float = 0.0) -> RayBatch | None:
+        P = perm.numel()
+        bs = self.batch_size
+        start, size = batch_num * bs, bs
+        if (batch_num + 1) * bs > P:  # projector.py:108-112
+            if batch_num == 0:
+                size = P % bs
+            else:
+                return None
+        jitter, det_off = draw_ray_randoms(size, self.random_offset_detector, self.device)
+        return RayBatch(perm=perm, start=start, num_rays=size, points_per_ray=self.points_per_ray, angle=angle,
+                        max_ray_distance_per_point=self.geometry.max_distance_traveled / self.points_per_ray,
+                        jitter=jitter, detector_offset=det_off, projection=projection, t=t,
+                        uniform_ray_spacing=self.uniform_ray_spacing)
+
+    def step(self, batch: RayBatch) -> torch.Tensor:
+        loss, _ = train_step(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
+                             self.table_grad, self.mlp_grad, self.workspace, self.loss)
+        self.step_count += 1
+        adam_step(self.model.table, self.table_grad, self.m_table, self.v_table, self.step_count, self.lr,
+                  self.betas, self.eps, self.weight_decay, half=self.model.table_half)
+        adam_step(self.model.mlp, self.mlp_grad, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas,
+                  self.eps, self.weight_decay)
+        return loss
+
+    def train_projection(self, projection: torch.Tensor, angle: float, t: float = 0.0) -> torch.Tensor | None:
+        """All batches of one projection (flattened, min-max scaled, on device)."""
+        P = projection.numel()
+        perm = torch.randperm(P, dtype=torch.int64, device=self.device)
+        n_batches = P // self.batch_size + (1 if P % self.batch_size else 0)
+        loss = None
+        for b in range(min(self.batch_per_proj, n_batches)):
+            batch = self.make_batch(perm, b, angle, projection, t)
+            if batch is None:
+                continue
+            loss = self.step(batch)
+        return loss

@@ -1,0 +1,137 @@
+"""GPU parity of the hash-grid encoding, the model forward and the fused
+training step (called through the C ABI) against the fp64 oracle.
+
+Tolerances (plain fp32 path vs fp64 oracle): hash indices bit-exact;
+interpolation weights to 1 ulp-level (2e-6 abs); encodings and sigma rel
+1e-5; y_pred and loss rel 1e-4; gradients within 1e-3 of the largest
+gradient entry.
+"""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import hashgrid as ohg
+from oracle import sampling as osamp
+
+pytestmark = pytest.mark.gpu
+
+
+def make_model(n_dims, log2_T=12, base=4, finest=128, precision="plain_fp32", table_scale=0.5, seed=0,
+               out_act="Softplus"):
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig
+    from nect_b200.network import HashGrid, HashGrid4D
+
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_T, base_resolution=base,
+                            finest_resolution=finest, base_resolution_t=2 if n_dims == 4 else None)
+    net = MLPNetConfig(n_hidden_layers=2, n_neurons=64, activation="ReLU", output_activation=out_act)
+    cls = HashGrid if n_dims == 3 else HashGrid4D
+    m = cls(enc, net, precision=precision, device="cuda", seed=seed)
+    with torch.no_grad():
+        g = torch.Generator(device="cpu").manual_seed(seed + 1)
+        m.table.copy_((torch.rand(m.table.shape, generator=g) * 2 - 1) * table_scale)
+        m.refresh_half()
+    return m, enc
+
+
+def oracle_levels(m, enc, n_dims):
+    levels, total = ohg.layout(n_dims, 16, enc.log2_hashmap_size, float(enc.base_resolution),
+                               float(enc.per_level_scale), float(enc.base_resolution_t or enc.base_resolution))
+    return levels, total
+
+
+@pytest.mark.parametrize("n_dims", [3, 4])
+def test_layout_matches_oracle(cuda_device, n_dims):
+    m, enc = make_model(n_dims)
+    levels, total = oracle_levels(m, enc, n_dims)
+    assert m.table.shape[0] == total
+    assert [lv.offset for lv in levels] == m.level_offset
+    assert [lv.hashed for lv in levels] == m.level_hashed
+    assert any(m.level_hashed) and not all(m.level_hashed)
+
+
+@pytest.mark.parametrize("n_dims", [3, 4])
+def test_corner_indices_bit_exact(cuda_device, n_dims):
+    m, enc = make_model(n_dims)
+    levels, _ = oracle_levels(m, enc, n_dims)
+    g = torch.Generator(device="cpu").manual_seed(3)
+    x = torch.rand(4096, n_dims, generator=g)
+    x[:64] = torch.round(x[:64] * 8) / 8          # exact vertices
+    x[64:80] = 1.0                                # upper boundary
+    x[80:96] = 0.0
+    idx, w = m.corners(x.cuda())
+    idx, w = idx.cpu(), w.cpu()
+    for l, lv in enumerate(levels):
+        oi, ow = ohg.corner_indices(x, lv, enc.log2_hashmap_size)
+        assert torch.equal(idx[:, l].to(torch.int64), oi), f"level {l} indices differ"
+        assert torch.allclose(w[:, l], ow, atol=2e-6, rtol=0), f"level {l} weights differ"
+
+
+@pytest.mark.parametrize("n_dims,precision", [(3, "plain_fp32"), (4, "plain_fp32"), (3, "mixed"), (4, "mixed")])
+def test_model_forward_matches_oracle(cuda_device, n_dims, precision):
+    m, enc = make_model(n_dims, precision=precision)
+    levels, _ = oracle_levels(m, enc, n_dims)
+    g = torch.Generator(device="cpu").manual_seed(4)
+    x = torch.rand(3000, 3, generator=g)
+    t = 0.37
+    out = (m(x.cuda()) if n_dims == 3 else m(x.cuda(), t)).cpu().double()
+    xin = x if n_dims == 3 else torch.cat([x, torch.full((x.shape[0], 1), t)], 1)
+    table = m.grid_table.detach().cpu().double()
+    Ws = ohg.split_mlp_params(m.mlp.detach().cpu().double(), 32, 64, 2)
+    ref = ohg.mlp(ohg.encode(xin, table, levels, enc.log2_hashmap_size), Ws, "relu", "softplus")
+    assert torch.allclose(out, ref, rtol=1e-5, atol=1e-6), (out - ref).abs().max()
+
+
+def run_train_case(n_dims, precision, loss, geom_kind="parallel"):
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import RayBatch, Workspace, train_step
+
+    torch.manual_seed(11)
+    if geom_kind == "parallel":
+        geo = Geometry(nDetector=[32, 32], dDetector=[1 / 32, 1 / 32], mode="parallel", nVoxel=[32, 32, 32],
+                       dVoxel=[1 / 32] * 3)
+    else:
+        geo = Geometry(nDetector=[40, 48], dDetector=[1.5, 1.5], mode="cone", DSD=300.0, DSO=200.0,
+                       nVoxel=[32, 32, 32], dVoxel=[1.0] * 3)
+    m, enc = make_model(n_dims, precision=precision)
+    cg = geo.get_c_geometry()
+    P = geo.nDetector[0] * geo.nDetector[1]
+    S, R, start = 64, 700, 100
+    perm = torch.randperm(P, device="cuda")
+    jitter = torch.rand(R, device="cuda") - 0.5
+    det_off = torch.zeros(R, 2, device="cuda")
+    proj = torch.rand(P, device="cuda")
+    angle, t = 0.7, 0.45
+    maxd = geo.max_distance_traveled / S
+    batch = RayBatch(perm=perm, start=start, num_rays=R, points_per_ray=S, angle=angle,
+                     max_ray_distance_per_point=maxd, jitter=jitter, detector_offset=det_off, projection=proj, t=t)
+    tg = torch.zeros_like(m.table)
+    mg = torch.zeros_like(m.mlp)
+    L, y_pred = train_step(m, cg, batch, geo.max_distance_traveled, tg, mg, Workspace(), loss)
+    torch.cuda.synchronize()
+    # oracle: same samples (C oracle with the device's trig values), fp64 network
+    a = torch.tensor([angle, 0.0], dtype=torch.float32, device="cuda")
+    c, s = torch.cos(a).cpu().numpy(), torch.sin(a).cpu().numpy()
+    trig = np.array([c[0], s[0], c[1], c[1], c[1], s[1], s[1], s[1]], np.float32)
+    pts, dist, counts = osamp.oracle_sample(osamp.to_struct(cg), perm.cpu().numpy(), start, R, S, angle, maxd, True,
+                                            jitter.cpu().numpy(), det_off.cpu().numpy(), trig=trig)
+    levels, _ = oracle_levels(m, enc, n_dims)
+    measured = proj.cpu().numpy()[perm.cpu().numpy()[start:start + R]]
+    yo, Lo, gto, gmo = ohg.train_step(pts, counts, dist, measured, m.grid_table.detach().cpu(),
+                                      m.mlp.detach().cpu(), levels, enc.log2_hashmap_size, 32, 64, 2,
+                                      geo.max_distance_traveled, loss=loss, t=t if n_dims == 4 else None)
+    return (y_pred.cpu().double(), float(L.item()), tg.cpu().double(), mg.cpu().double()), (yo, float(Lo), gto, gmo)
+
+
+def rel_max(a, b):
+    return float((a - b).abs().max() / b.abs().max().clamp(min=1e-30))
+
+
+@pytest.mark.parametrize("n_dims,loss,geom", [(3, "l2", "parallel"), (3, "l1", "cone"), (4, "l2", "cone")])
+def test_fused_plain_step_matches_oracle(cuda_device, n_dims, loss, geom):
+    (y, L, gt, gm), (yo, Lo, gto, gmo) = run_train_case(n_dims, "plain_fp32", loss, geom)
+    assert rel_max(y, yo) < 1e-4
+    assert abs(L - Lo) / abs(Lo) < 1e-4
+    assert rel_max(gm, gmo) < 1e-3, rel_max(gm, gmo)
+    assert rel_max(gt, gto) < 1e-3, rel_max(gt, gto)
