@@ -1,0 +1,442 @@
+"""Benchmark of the fused NeCT training step on B200.
+
+One step = one batch of rays of one projection through the whole hot path:
+device randperm of the detector pixels, per-ray jitter draw, fused
+sample -> encode -> MLP -> line integral -> loss -> backward (nectb_train_step),
+and the Adam update of the table and the MLP (fused Adam kernel).
+
+Default workload (N=1): static cone beam, 512x512 detector (one batch = all
+262,144 pixels of a projection), 256^3 porous-medium phantom, 512 jittered
+samples per ray, 16 levels x 2 features, 2^20 entries per level, 2x64 MLP.
+Inputs are seeded synthetic projections (exact line integrals) made before
+the timed region.  Timing: W warm-up steps, then K steps bracketed by a
+barrier and cuda synchronize, CUDA events on the launching stream, max over
+ranks.  Per-step state (tables, gradients, Adam moments) exceeds the 126 MB L2,
+so consecutive steps do not hit a warm L2.
+
+--impl reference times the reference path's CPU restatement (the oracle:
+C sampler + PyTorch-CPU hash grid, MLP, loss, autograd backward and
+torch.optim.Adam) on the host cores, on a bounded sample of rays per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "train rays/s fwd+bwd"
+
+
+# ----------------------------------------------------------------- workloads
+def workload_spec(name: str, precision: str):
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig
+
+    if name == "c2_static_cone":
+        geo = dict(nDetector=[512, 512], dDetector=[1.0, 1.0], mode="cone", DSD=1000.0, DSO=500.0,
+                   nVoxel=[256, 256, 256], dVoxel=[1.0, 1.0, 1.0])
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=20, base_resolution=16,
+                                max_resolution_factor=2.0, nDetector=[512, 512], nVoxel=[256] * 3)
+        return dict(geo=geo, model=ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), precision),
+                    S=512, rays=1 << 18, n_angles=720, turns=1, phantom="porous", n_dims=3)
+    if name == "c1_static_parallel":
+        geo = dict(nDetector=[128, 128], dDetector=[1 / 128, 1 / 128], mode="parallel", nVoxel=[128] * 3,
+                   dVoxel=[1 / 128] * 3)
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=19, base_resolution=16,
+                                finest_resolution=1024)
+        return dict(geo=geo, model=ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), precision),
+                    S=256, rays=65536, n_angles=180, turns=0.5, phantom="ellipsoids", n_dims=3)
+    if name == "c3_dynamic_cone":
+        geo = dict(nDetector=[512, 512], dDetector=[1.0, 1.0], mode="cone", DSD=1000.0, DSO=500.0,
+                   nVoxel=[256, 256, 256], dVoxel=[1.0, 1.0, 1.0])
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=21, base_resolution=16,
+                                max_resolution_factor=2.0, nDetector=[512, 512], base_resolution_t=4)
+        return dict(geo=geo, model=ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision),
+                    S=512, rays=1 << 18, n_angles=3600, turns=10, phantom="porous", n_dims=4)
+    raise ValueError(name)
+
+
+def make_projections(spec, geometry, n_proj: int, device, seed: int = 0):
+    from nect_b200 import phantoms
+
+    angles_all = np.linspace(0, 2 * math.pi * spec["turns"], spec["n_angles"], endpoint=False)
+    idx = np.linspace(0, spec["n_angles"] - 1, n_proj).astype(int)
+    angles = angles_all[idx]
+    ts = idx / max(spec["n_angles"] - 1, 1)
+    if spec["phantom"] == "ellipsoids":
+        ph = phantoms.ellipsoid_phantom(20, seed)
+        projs = torch.stack([phantoms.ellipsoid_projection(ph, geometry, float(a), device) for a in angles])
+    else:
+        ph = phantoms.porous_phantom(geometry.nVoxel[0], seed=seed, attempts=60000)
+        projs = torch.stack([phantoms.porous_projection(ph, geometry, float(a), device) for a in angles])
+    projs, _, _ = phantoms.minmax_scale(projs)
+    return projs.reshape(n_proj, -1).contiguous(), [float(a) for a in angles], [float(t) for t in ts]
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        under_load = [s for s in sm if smax and s > 0.3 * smax] or sm
+        return {"sm_mhz": float(np.median(under_load)) if under_load else None, "sm_max_mhz": smax,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------ CPU baseline
+def cpu_port_step(spec, geometry, model_cfg, table, mlp_flat, proj_flat_cpu, angle, t, rays: int, opt, rng):
+    """One step of the reference path's CPU restatement on a bounded sample."""
+    from oracle import hashgrid as ohg
+    from oracle import sampling as osamp
+
+    S = spec["S"]
+    P = proj_flat_cpu.numel()
+    perm = torch.randperm(P).numpy()
+    jitter = (rng.random(rays, dtype=np.float32) - 0.5).astype(np.float32)
+    det_off = np.zeros((rays, 2), np.float32)
+    cg = osamp.to_struct(geometry.get_c_geometry())
+    maxd = geometry.max_distance_traveled / S
+    pts, dist, counts = osamp.oracle_sample(cg, perm, 0, rays, S, angle, maxd, True, jitter, det_off)
+    enc = model_cfg.encoder
+    levels, _ = ohg.layout(spec["n_dims"], enc.n_levels, enc.log2_hashmap_size, float(enc.base_resolution),
+                           float(enc.per_level_scale), float(enc.base_resolution_t or enc.base_resolution))
+    keep = ~torch.all(torch.from_numpy(pts).clamp(0, 1).view(-1, 3) == 0, dim=-1)
+    x = torch.from_numpy(pts).clamp(0, 1).view(-1, 3)[keep]
+    if spec["n_dims"] == 4:
+        x = torch.cat([x, torch.full((x.shape[0], 1), t)], 1)
+    opt.zero_grad()
+    Ws = ohg.split_mlp_params(mlp_flat, enc.n_levels * enc.n_features_per_level, 64, 2)
+    sig = ohg.mlp(ohg.encode(x, table, levels, enc.log2_hashmap_size), Ws, "relu", "softplus").squeeze(-1)
+    full = torch.zeros(rays * S).masked_scatter(keep, sig)
+    y_pred = full.view(rays, S).sum(1) * (torch.from_numpy(dist) / geometry.max_distance_traveled)
+    y = proj_flat_cpu[torch.from_numpy(perm[:rays])]
+    loss = torch.nn.functional.mse_loss(y_pred, y)
+    loss.backward()
+    opt.step()
+    return float(loss)
+
+
+def run_cpu(spec, geometry, model, projs, angles, ts, steps: int, warmup: int, rays: int):
+    threads = os.cpu_count() or 1
+    torch.set_num_threads(threads)
+    table = model.table.detach().cpu().clone().requires_grad_(True)
+    mlp = model.mlp.detach().cpu().clone().requires_grad_(True)
+    opt = torch.optim.Adam([table, mlp], lr=1e-3)
+    rng = np.random.default_rng(0)
+    pc = projs.cpu()
+    for k in range(warmup):
+        cpu_port_step(spec, geometry, model_cfg_of(model), table, mlp, pc[k % len(pc)], angles[k % len(pc)],
+                      ts[k % len(pc)], rays, opt, rng)
+    t0 = time.perf_counter()
+    for k in range(steps):
+        cpu_port_step(spec, geometry, model_cfg_of(model), table, mlp, pc[k % len(pc)], angles[k % len(pc)],
+                      ts[k % len(pc)], rays, opt, rng)
+    dt = time.perf_counter() - t0
+    return rays * steps / dt, threads, dt / steps
+
+
+def model_cfg_of(model):
+    return model._bench_cfg
+
+
+# ----------------------------------------------------------------- GPU arm
+def collect_profile():
+    from nect_b200 import _lib
+    import ctypes
+
+    n = (ctypes.c_int32 * 8)()
+    ms = (ctypes.c_double * 8)()
+    _lib.lib.nectb_profile_collect(ctypes.addressof(n), ctypes.addressof(ms))
+    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "slot6", "slot7"]
+    return {names[i]: (int(n[i]), float(ms[i])) for i in range(8) if n[i]}
+
+
+def valid_samples(trainer, batches) -> int:
+    """Sum of per-ray sample counts of the timed batches (the sampler's counts,
+    identical by construction to what the fused kernels regenerate)."""
+    from nect_b200.sampling import ct_sampling
+
+    total = 0
+    for b in batches:
+        _, _, counts = ct_sampling.sample_with_draws(b.perm, trainer.c_geometry, b.angle, b.points_per_ray,
+                                                     b.num_rays, b.start, b.max_ray_distance_per_point, True,
+                                                     b.jitter, b.detector_offset, want_points=False,
+                                                     want_counts=True)
+        total += int(counts.sum().item())
+    return total
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c2_static_cone",
+                    choices=["c2_static_cone", "c1_static_parallel", "c3_dynamic_cone"])
+    ap.add_argument("--precision", default=os.environ.get("NECTB_PRECISION", "mixed"),
+                    choices=["mixed", "plain_fp32"])
+    ap.add_argument("--cpu-rays", type=int, default=2048)
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference" and rank != 0:
+        return
+    if world > 1 and args.impl == "b200":
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
+    if dev.type == "cuda":
+        torch.cuda.set_device(dev)
+
+    from nect_b200.config import get_model
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import Trainer
+
+    spec = workload_spec(args.workload, args.precision)
+    geometry = Geometry(**spec["geo"])
+    S, R = spec["S"], spec["rays"]
+    model_cfg = spec["model"]
+    wl_name = (f"{args.workload}: {geometry.mode} {geometry.nDetector[0]}x{geometry.nDetector[1]} detector, "
+               f"{geometry.nVoxel[0]}^3 volume, S={S}, hash {model_cfg.encoder.n_levels}x"
+               f"{model_cfg.encoder.n_features_per_level} 2^{model_cfg.encoder.log2_hashmap_size}"
+               f"{' 4D' if spec['n_dims'] == 4 else ''}, MLP {model_cfg.net.n_hidden_layers}x64")
+
+    if args.impl == "reference":
+        torch.manual_seed(0)
+        projs, angles, ts = make_projections(spec, geometry, 2, "cpu")
+        model = get_model(model_cfg, device="cpu") if False else None
+        from nect_b200.network import HashGrid, HashGrid4D  # noqa: F401 (layout only)
+
+        class _M:  # CPU parameters with the same shapes and init as the model
+            pass
+
+        m = _M()
+        enc = model_cfg.encoder
+        from oracle import hashgrid as ohg
+
+        _, total = ohg.layout(spec["n_dims"], enc.n_levels, enc.log2_hashmap_size, float(enc.base_resolution),
+                              float(enc.per_level_scale), float(enc.base_resolution_t or enc.base_resolution))
+        g = torch.Generator().manual_seed(1337)
+        m.table = (torch.rand(total, enc.n_features_per_level, generator=g) * 2 - 1) * 1e-4
+        n_in = enc.n_levels * enc.n_features_per_level
+        m.mlp = torch.cat([(torch.rand(o * i, generator=g) * 2 - 1) * math.sqrt(6 / (o + i))
+                           for o, i in [(64, n_in), (64, 64), (1, 64)]])
+        m._bench_cfg = model_cfg
+        rays = args.cpu_rays
+        val, threads, per = run_cpu(spec, geometry, m, projs, angles, ts, args.steps, args.warmup, rays)
+        sample = f"{rays} rays x {S} samples per step of the {args.workload} workload"
+        print(json.dumps({
+            "metric": METRIC, "value": val, "unit": "rays/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wl_name, "precision": "plain_fp32 (CPU)", "rays_per_step": rays},
+            "cpu_baseline": {"value": val, "unit": "rays/s", "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": val, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }))
+        return
+
+    torch.manual_seed(1234 + rank)
+    n_proj = 8
+    projs, angles, ts = make_projections(spec, geometry, n_proj, dev, seed=rank)
+    model = get_model(model_cfg, device=dev)
+    model._bench_cfg = model_cfg
+    trainer = Trainer(model, geometry, points_per_batch=R * S, points_per_ray=S, loss="l2", lr=1e-3, device=dev)
+    P = projs.shape[1]
+
+    def make_step_batch(k):
+        perm = torch.randperm(P, dtype=torch.int64, device=dev)
+        return trainer.make_batch(perm, 0, angles[k % n_proj], projs[k % n_proj], ts[k % n_proj])
+
+    for k in range(args.warmup):
+        trainer.step(make_step_batch(k))
+    torch.cuda.synchronize()
+
+    from nect_b200 import _lib
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    clocks = ClockSampler(dev.index or 0)
+    clocks.start()
+    time.sleep(0.3)
+    _lib.lib.nectb_profile_enable(1)
+    batches = []
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for k in range(args.steps):
+        b = make_step_batch(args.warmup + k)
+        batches.append(b)
+        trainer.step(b)
+    ev1.record()
+    torch.cuda.synchronize()
+    barrier()
+    _lib.lib.nectb_profile_enable(0)
+    clock_info = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    prof = collect_profile()
+    if world > 1:
+        import torch.distributed as dist
+
+        t_ = torch.tensor([ms], device=dev)
+        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+        ms = float(t_.item())
+    rays_per_step = batches[0].num_rays
+    value = world * rays_per_step * args.steps / (ms / 1e3)
+
+    # ---- roofline of the dominant kernel (algorithmic bytes / event time)
+    n_valid = valid_samples(trainer, batches)
+    enc = model_cfg.encoder
+    corners = 1 << spec["n_dims"]
+    feat_bytes = 2 if args.precision == "mixed" else 4
+    gather = enc.n_levels * corners * enc.n_features_per_level * feat_bytes
+    scatter = enc.n_levels * corners * enc.n_features_per_level * 4
+    n_params = model.table.numel() + model.mlp.numel()
+    per_launch_bytes = {
+        "backward": n_valid / args.steps * (gather + scatter),
+        "forward": n_valid / args.steps * gather,
+        "adam": n_params * (32 + (2 if args.precision == "mixed" else 0)) / 2,  # two launches per step
+        "ray_prep": rays_per_step * 64.0,
+    }
+    kernel_ms = {k: v[1] / max(v[0], 1) for k, v in prof.items()}
+    dominant = max(prof, key=lambda k: prof[k][1]) if prof else "backward"
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
+    achieved = per_launch_bytes.get(dominant, 0.0) / (kernel_ms[dominant] / 1e3) / 1e9 if dominant in kernel_ms else None
+    traffic = None
+    tfile = ROOT / "profiles" / f"traffic_{args.workload}_{args.precision}.json"
+    if tfile.exists():
+        traffic = json.loads(tfile.read_text()).get(dominant)
+
+    # ---- end to end through the public API, host buffers
+    e2e = None
+    if world == 1 or True:
+        host = projs.cpu().pin_memory()
+        dproj = torch.empty_like(projs[0])
+        loss_host = torch.empty(1, pin_memory=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            dproj.copy_(host[k % n_proj], non_blocking=True)
+            loss = trainer.train_projection(dproj, angles[k % n_proj], ts[k % n_proj])
+            loss_host.copy_(loss, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
+
+            t_ = torch.tensor([ems], device=dev)
+            dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+            ems = float(t_.item())
+        e2e = {"value": world * rays_per_step * args.steps / (ems / 1e3), "unit": "rays/s",
+               "h2d_bytes_per_step": int(P * 4), "d2h_bytes_per_step": 4}
+
+    cpu_baseline = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        val, threads, per = run_cpu(spec, geometry, model, projs, angles, ts, args.cpu_steps, 1, args.cpu_rays)
+        cpu_baseline = {"value": val, "unit": "rays/s", "cores": threads, "kind": "port",
+                        "sample": f"{args.cpu_rays} rays x {S} samples per step, {args.cpu_steps} steps, of the "
+                                  f"same workload (C sampler + PyTorch-CPU fp32 hash grid/MLP/autograd/Adam)"}
+
+    gpu_launches = sum(v[0] for v in prof.values())
+    out = {
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f16/bf16" if args.precision == "mixed" else "f32", "data": "synthetic",
+        "config": {"workload": wl_name, "precision": args.precision, "rays_per_step": rays_per_step,
+                   "samples_per_ray": S, "valid_samples_per_step": n_valid / args.steps,
+                   "samples_per_s": world * n_valid / (ms / 1e3),
+                   "l2": "per-step state (tables, gradients, Adam moments) exceeds the 126 MB L2",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes.get(dominant),
+                     "kernel_ms": kernel_ms},
+        "cpu_baseline": cpu_baseline,
+        "e2e": e2e,
+        "gpu_launches": gpu_launches,
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -209,6 +209,16 @@ int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq
                     float weight_decay, int32_t step, void* param_half,
                     int32_t zero_grad, void* stream);
 
+/* Per-kernel timing of the library's own launches with CUDA events recorded
+ * on the launch stream around each kernel (off by default).  Slots:
+ * 0 ray preparation, 1 forward, 2 backward, 3 Adam, 4 sampling, 5 model
+ * forward.  nectb_profile_collect waits for the recorded events, adds their
+ * durations and returns per slot the launch count and total milliseconds.
+ * No counterpart in the reference, which has no profiler. */
+#define NECTB_PROFILE_SLOTS 8
+int nectb_profile_enable(int32_t enable);
+int nectb_profile_collect(int32_t* launches, double* total_ms);
+
 /* Version string and last error message of the calling thread. */
 const char* nectb_version(void);
 const char* nectb_last_error(void);

@@ -118,6 +118,8 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
          ctypes.POINTER(NectbTrainBatch), c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_size, c_ptr],
     ),
+    "nectb_profile_enable": (c_int, [c_int]),
+    "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
     "nectb_adam_step": (
         c_int,
         [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_f32, c_f32, c_f32, c_f32, c_int, c_ptr, c_int, c_ptr],

@@ -21,3 +21,79 @@ void clear_error() { g_last_error[0] = 0; }
 
 extern "C" const char* nectb_version(void) { return "nectb 0.1 sm_100a"; }
 extern "C" const char* nectb_last_error(void) { return nectb::g_last_error; }
+
+// ---- per-kernel event profiler --------------------------------------------
+#include <mutex>
+#include <vector>
+
+namespace nectb {
+namespace {
+struct ProfRec {
+  int slot;
+  cudaEvent_t a, b;
+};
+std::mutex g_prof_mu;
+bool g_prof_on = false;
+std::vector<ProfRec> g_prof_pending;
+std::vector<cudaEvent_t> g_prof_free;
+int g_prof_launches[NECTB_PROFILE_SLOTS];
+double g_prof_ms[NECTB_PROFILE_SLOTS];
+
+cudaEvent_t prof_event() {
+  if (!g_prof_free.empty()) {
+    cudaEvent_t e = g_prof_free.back();
+    g_prof_free.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+}  // namespace
+
+ProfScope::ProfScope(int slot, cudaStream_t s) : slot_(slot), s_(s), a_(nullptr) {
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  if (!g_prof_on) return;
+  a_ = prof_event();
+  cudaEventRecord((cudaEvent_t)a_, s_);
+}
+
+ProfScope::~ProfScope() {
+  if (!a_) return;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  cudaEvent_t b = prof_event();
+  cudaEventRecord(b, s_);
+  g_prof_pending.push_back({slot_, (cudaEvent_t)a_, b});
+}
+
+}  // namespace nectb
+
+extern "C" int nectb_profile_enable(int32_t enable) {
+  std::lock_guard<std::mutex> lk(nectb::g_prof_mu);
+  nectb::g_prof_on = enable != 0;
+  return NECTB_OK;
+}
+
+extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
+  using namespace nectb;
+  std::lock_guard<std::mutex> lk(g_prof_mu);
+  for (auto& r : g_prof_pending) {
+    cudaEventSynchronize(r.b);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, r.a, r.b);
+    if (r.slot >= 0 && r.slot < NECTB_PROFILE_SLOTS) {
+      g_prof_launches[r.slot] += 1;
+      g_prof_ms[r.slot] += ms;
+    }
+    g_prof_free.push_back(r.a);
+    g_prof_free.push_back(r.b);
+  }
+  g_prof_pending.clear();
+  for (int i = 0; i < NECTB_PROFILE_SLOTS; ++i) {
+    if (launches) launches[i] = g_prof_launches[i];
+    if (total_ms) total_ms[i] = g_prof_ms[i];
+    g_prof_launches[i] = 0;
+    g_prof_ms[i] = 0.0;
+  }
+  return NECTB_OK;
+}

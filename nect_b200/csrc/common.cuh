@@ -24,6 +24,22 @@ inline int launch_status(const char* what) { return cuda_status(cudaGetLastError
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Records CUDA events around a kernel launch while profiling is enabled
+// (nectb_profile_enable); slots are listed in include/nectb.h.
+enum { kProfRayPrep = 0, kProfForward = 1, kProfBackward = 2, kProfAdam = 3, kProfSample = 4, kProfModel = 5 };
+class ProfScope {
+ public:
+  ProfScope(int slot, cudaStream_t s);
+  ~ProfScope();
+  ProfScope(const ProfScope&) = delete;
+  ProfScope& operator=(const ProfScope&) = delete;
+
+ private:
+  int slot_;
+  cudaStream_t s_;
+  void* a_;
+};
+
 }  // namespace nectb
 
 #define NECTB_REQUIRE(cond, ...)                                        \

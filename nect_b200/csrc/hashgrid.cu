@@ -122,6 +122,7 @@ int launch_model(const GridDev& g, const void* params, const float* W, const flo
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kModelThreads, smem);
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kModelThreads), (int64_t)sms * std::max(per_sm, 1)));
+  ProfScope ps(kProfModel, s);
   k<<<blocks, kModelThreads, smem, s>>>(g, (const T*)params, W, x, n, t, act, out_act, sigma);
   return launch_status("model_forward_kernel");
 }

@@ -73,6 +73,7 @@ extern "C" int nectb_sample(const NectbGeometry* geometry, const int64_t* random
   NECTB_REQUIRE(random_ray_index && jitter && detector_offset && distances, "null input/output pointer");
   NECTB_REQUIRE((int64_t)num_rays * num_points_per_ray * 3 < (int64_t(1) << 40), "points tensor too large");
   const int blocks = (int)ceil_div(num_rays, 8);
+  ProfScope ps(kProfSample, (cudaStream_t)stream);
   sample_kernel<<<blocks, 8 * 32, 0, (cudaStream_t)stream>>>(
       *geometry, random_ray_index, random_ray_index_len, starting_ray_index, num_rays, num_points_per_ray, angle_rad,
       max_ray_distance_per_point, uniform_ray_spacing, jitter, detector_offset, points, distances, counts);

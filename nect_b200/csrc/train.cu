@@ -112,6 +112,7 @@ extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float*
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 8);
+  ProfScope ps(kProfAdam, (cudaStream_t)stream);
   adam_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, lr, beta1, beta2, eps,
                                                         weight_decay, (float)bc1, (float)std::sqrt(bc2),
                                                         (__half*)param_half, zero_grad);

@@ -286,7 +286,10 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
 
-  ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
+  {
+    ProfScope ps(kProfRayPrep, s);
+    ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
+  }
   if (int rc = launch_status("ray_prep_kernel")) return rc;
 
   constexpr int FNT = kPlainFwdThreads;
@@ -296,7 +299,10 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, FNT, fsmem);
   const int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
-  fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.counters, act, out_act, y_pred, loss);
+  {
+    ProfScope ps(kProfForward, s);
+    fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.counters, act, out_act, y_pred, loss);
+  }
   if (int rc = launch_status("fwd_plain_kernel")) return rc;
 
   constexpr int NT = 128;
@@ -305,7 +311,10 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   if (bsmem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "plain backward needs %zu B of shared memory", bsmem);
   cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   const int bblocks = std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, NT / 32)));
-  bk<<<bblocks, NT, bsmem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, act, out_act, table_grad, W_grad);
+  {
+    ProfScope ps(kProfBackward, s);
+    bk<<<bblocks, NT, bsmem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, act, out_act, table_grad, W_grad);
+  }
   return launch_status("bwd_plain_kernel");
 }
 

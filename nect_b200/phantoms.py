@@ -1,0 +1,255 @@
+"""Seeded synthetic phantoms and exact line-integral projections.
+
+Stand-ins for the reference's data (its demo data sets are downloaded from
+Zenodo and its porous phantoms need porespy, neither available here), built to
+the shapes, sizes and value ranges of the BASELINE workloads:
+
+* ``ellipsoid_phantom``: additive sum of seeded random ellipsoids in the unit
+  cube (static parallel-beam workload, 128^3, 20 ellipsoids).
+* ``porous_phantom``: a cylinder (attenuation 0.2) filled with non-overlapping
+  spheres (attenuation 0.8) by seeded random sequential insertion, largest
+  radii first (static cone-beam workload, 256^3).  Random sequential
+  insertion jams well below 60 % packing; the achieved fraction is reported.
+* ``dynamic_porous``: the porous medium plus a brine front (attenuation 0.5)
+  rising in z as a sigmoid in t with a value-noise-perturbed interface, and 30
+  grains that shrink linearly in time (4D workload).
+
+Projections are exact line integrals (sums of analytic chord lengths), the
+limit the ray-marched integrals of the workload description converge to;
+rays follow the sampler's conventions (nect/sampling/ct_sampling.cu:226-389:
+source at -DSO on x, detector column -> -y, row -> z, rotation about z after
+the centre-of-rotation shift).  The time-dependent brine front has no closed
+form and is ray-marched at 4 samples per voxel.  Everything runs in torch on
+the given device and is used only to make inputs (it is not part of the
+training path).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+
+# ---------------------------------------------------------------- rays ----
+def detector_rays(geometry, angle: float, device, dtype=torch.float64):
+    """World-space ray origins/directions [P,3] (x,y,z) for every detector pixel.
+
+    Uses the nect_b200.sampling.Geometry conventions (detector binning 1)."""
+    nr, nc = geometry.nDetector
+    rows = torch.arange(nr, device=device, dtype=dtype)
+    cols = torch.arange(nc, device=device, dtype=dtype)
+    u = (cols - (nc - 1) / 2) * geometry.dDetector[1] + geometry.offDetector[1]
+    v = (rows - (nr - 1) / 2) * geometry.dDetector[0] + geometry.offDetector[0]
+    V, U = torch.meshgrid(v, u, indexing="ij")
+    y = -U.reshape(-1)
+    z = V.reshape(-1)
+    P = y.numel()
+    if geometry.mode == "cone":
+        src = torch.tensor([-geometry.DSO, 0.0, 0.0], device=device, dtype=dtype).expand(P, 3)
+        det = torch.stack([torch.full_like(y, geometry.DSD - geometry.DSO), y, z], 1)
+    else:
+        L = 2.0 * max(geometry.sVoxel)
+        src = torch.stack([torch.full_like(y, -L), y, z], 1)
+        det = torch.stack([torch.full_like(y, L), y, z], 1)
+    c, s = math.cos(angle), math.sin(angle)
+
+    def rot(p):
+        x, yy, zz = p[:, 0], p[:, 1] - geometry.COR, p[:, 2]
+        return torch.stack([c * x - s * yy, s * x + c * yy, zz], 1)
+
+    a, b = rot(src), rot(det)
+    d = b - a
+    return a, d / d.norm(dim=1, keepdim=True)
+
+
+def _sphere_chords(o, d, centers, radii, chunk=2048):
+    """Sum over spheres handled by the caller: returns [P, S] chord lengths."""
+    out = []
+    for i in range(0, centers.shape[0], chunk):
+        c = centers[i:i + chunk]
+        r = radii[i:i + chunk]
+        oc = o[:, None, :] - c[None]
+        b = (oc * d[:, None, :]).sum(-1)
+        q = (oc * oc).sum(-1) - b * b
+        h = r[None] ** 2 - q
+        out.append(2 * torch.sqrt(torch.clamp(h, min=0)))
+    return torch.cat(out, 1)
+
+
+def _cylinder_chord(o, d, radius, half_height):
+    """Chord of each line with {x^2 + y^2 <= r^2, |z| <= h}."""
+    a = d[:, 0] ** 2 + d[:, 1] ** 2
+    b = 2 * (o[:, 0] * d[:, 0] + o[:, 1] * d[:, 1])
+    c = o[:, 0] ** 2 + o[:, 1] ** 2 - radius ** 2
+    disc = b * b - 4 * a * c
+    ok = (disc > 0) & (a > 1e-12)
+    sq = torch.sqrt(torch.clamp(disc, min=0))
+    t0 = torch.where(ok, (-b - sq) / (2 * a).clamp(min=1e-12), torch.zeros_like(a))
+    t1 = torch.where(ok, (-b + sq) / (2 * a).clamp(min=1e-12), torch.zeros_like(a))
+    # clip by the slab |z| <= h
+    dz = d[:, 2]
+    safe = torch.where(dz.abs() > 1e-12, dz, torch.full_like(dz, 1e-12))
+    z0 = (-half_height - o[:, 2]) / safe
+    z1 = (half_height - o[:, 2]) / safe
+    zl, zh = torch.minimum(z0, z1), torch.maximum(z0, z1)
+    flat = dz.abs() <= 1e-12
+    inside_slab = o[:, 2].abs() <= half_height
+    zl = torch.where(flat, torch.where(inside_slab, torch.full_like(zl, -1e30), torch.full_like(zl, 1e30)), zl)
+    zh = torch.where(flat, torch.where(inside_slab, torch.full_like(zh, 1e30), torch.full_like(zh, -1e30)), zh)
+    lo, hi = torch.maximum(t0, zl), torch.minimum(t1, zh)
+    return torch.where(ok, torch.clamp(hi - lo, min=0), torch.zeros_like(a))
+
+
+# ------------------------------------------------------- ellipsoids (C1) ----
+@dataclass
+class EllipsoidPhantom:
+    centers: np.ndarray   # [E,3] world (x,y,z), unit cube centred at 0
+    axes: np.ndarray      # [E,3] semi-axes
+    rot: np.ndarray       # [E,3,3] rotation (columns = ellipsoid axes)
+    mu: np.ndarray        # [E]
+
+
+def ellipsoid_phantom(n: int = 20, seed: int = 0) -> EllipsoidPhantom:
+    """Centres U[-0.6,0.6]^3 in the cube [-1,1]^3 scaled to the unit cube
+    (i.e. U[-0.3,0.3] in world units), semi-axes U[0.05,0.35] of the [-1,1]
+    cube (world U[0.025,0.175]), uniform random rotations, attenuation
+    U[0.1,1.0]."""
+    rng = np.random.default_rng(seed)
+    centers = rng.uniform(-0.6, 0.6, (n, 3)) * 0.5
+    axes = rng.uniform(0.05, 0.35, (n, 3)) * 0.5
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    rot = np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], -1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], -1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], -1),
+    ], 1)
+    mu = rng.uniform(0.1, 1.0, n)
+    return EllipsoidPhantom(centers, axes, rot, mu)
+
+
+def ellipsoid_projection(ph: EllipsoidPhantom, geometry, angle: float, device) -> torch.Tensor:
+    o, d = detector_rays(geometry, angle, device)
+    C = torch.as_tensor(ph.centers, device=device)
+    A = torch.as_tensor(ph.axes, device=device)
+    Rm = torch.as_tensor(ph.rot, device=device)
+    mu = torch.as_tensor(ph.mu, device=device)
+    oc = o[:, None, :] - C[None]                       # [P,E,3]
+    ol = torch.einsum("pei,eij->pej", oc, Rm) / A[None]
+    dl = torch.einsum("pi,eij->pej", d, Rm) / A[None]
+    a = (dl * dl).sum(-1)
+    b = 2 * (ol * dl).sum(-1)
+    c = (ol * ol).sum(-1) - 1
+    disc = torch.clamp(b * b - 4 * a * c, min=0)
+    chord = torch.sqrt(disc) / a                       # t2 - t1 with |d| = 1
+    return (chord * mu[None]).sum(1).to(torch.float32).reshape(geometry.nDetector[0], geometry.nDetector[1])
+
+
+def ellipsoid_volume(ph: EllipsoidPhantom, n: int, device) -> torch.Tensor:
+    """Voxel-centre samples [z,y,x] of the attenuation on an n^3 grid."""
+    c = (torch.arange(n, device=device, dtype=torch.float64) + 0.5) / n - 0.5
+    Z, Y, X = torch.meshgrid(c, c, c, indexing="ij")
+    p = torch.stack([X, Y, Z], -1).reshape(-1, 3)
+    vol = torch.zeros(p.shape[0], device=device, dtype=torch.float64)
+    for e in range(len(ph.mu)):
+        lp = (p - torch.as_tensor(ph.centers[e], device=device)) @ torch.as_tensor(ph.rot[e], device=device)
+        inside = ((lp / torch.as_tensor(ph.axes[e], device=device)) ** 2).sum(1) <= 1
+        vol += inside.double() * ph.mu[e]
+    return vol.reshape(n, n, n).float()
+
+
+# ------------------------------------------------------ porous medium (C2) ----
+@dataclass
+class PorousPhantom:
+    radius: float          # cylinder radius (world units = voxels)
+    half_height: float
+    mu_cyl: float
+    mu_grain: float
+    centers: np.ndarray    # [G,3] (x,y,z)
+    radii: np.ndarray      # [G]
+    packing: float         # achieved grain volume fraction of the cylinder
+
+
+def porous_phantom(n: int = 256, seed: int = 0, r_min: float = 3.0, r_max: float = 12.0, target: float = 0.6,
+                   attempts: int = 400_000) -> PorousPhantom:
+    rng = np.random.default_rng(seed)
+    R, H = n / 2 - 0.5, n / 2 - 0.5
+    vol_cyl = math.pi * R * R * 2 * H
+    cell = 2 * r_max
+    grid: dict = {}
+    centers, radii = [], []
+    filled = 0.0
+    radii_pool = np.sort(rng.uniform(r_min, r_max, attempts))[::-1]
+    for k in range(attempts):
+        r = radii_pool[k]
+        rho = (R - r) * math.sqrt(rng.uniform())
+        th = rng.uniform(0, 2 * math.pi)
+        c = np.array([rho * math.cos(th), rho * math.sin(th), rng.uniform(-H + r, H - r)])
+        key = tuple((c // cell).astype(int))
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
+                        if np.sum((centers[j] - c) ** 2) < (radii[j] + r) ** 2:
+                            ok = False
+                            break
+                    if not ok:
+                        break
+                if not ok:
+                    break
+            if not ok:
+                break
+        if ok:
+            grid.setdefault(key, []).append(len(centers))
+            centers.append(c)
+            radii.append(r)
+            filled += 4 / 3 * math.pi * r ** 3
+            if filled / vol_cyl >= target:
+                break
+    return PorousPhantom(R, H, 0.2, 0.8, np.array(centers), np.array(radii), filled / vol_cyl)
+
+
+def porous_projection(ph: PorousPhantom, geometry, angle: float, device, chunk: int | None = None,
+                      grain_scale: np.ndarray | None = None) -> torch.Tensor:
+    o, d = detector_rays(geometry, angle, device)
+    if chunk is None:  # bound the [rays, grains, 3] temporaries to ~400 MB
+        chunk = max(256, int(4e8 / (max(len(ph.radii), 1) * 3 * 8)))
+    C = torch.as_tensor(ph.centers, device=device)
+    r = torch.as_tensor(ph.radii if grain_scale is None else ph.radii * grain_scale, device=device)
+    out = torch.empty(o.shape[0], device=device, dtype=torch.float64)
+    for i in range(0, o.shape[0], chunk):
+        oo, dd = o[i:i + chunk], d[i:i + chunk]
+        cyl = _cylinder_chord(oo, dd, ph.radius, ph.half_height)
+        sph = _sphere_chords(oo, dd, C, r).sum(1)
+        out[i:i + chunk] = ph.mu_cyl * cyl + (ph.mu_grain - ph.mu_cyl) * sph
+    return out.to(torch.float32).reshape(geometry.nDetector[0], geometry.nDetector[1])
+
+
+def porous_volume(ph: PorousPhantom, n: int, device) -> torch.Tensor:
+    c = torch.arange(n, device=device, dtype=torch.float32) - (n - 1) / 2
+    Z, Y, X = torch.meshgrid(c, c, c, indexing="ij")
+    vol = ((X ** 2 + Y ** 2 <= ph.radius ** 2) & (Z.abs() <= ph.half_height)).float() * ph.mu_cyl
+    C = torch.as_tensor(ph.centers, device=device, dtype=torch.float32)
+    Rr = torch.as_tensor(ph.radii, device=device, dtype=torch.float32)
+    for j in range(C.shape[0]):
+        cx, cy, cz = C[j]
+        r = float(Rr[j])
+        lo = [max(0, int(math.floor(float(v) + (n - 1) / 2 - r))) for v in (cz, cy, cx)]
+        hi = [min(n, int(math.ceil(float(v) + (n - 1) / 2 + r)) + 1) for v in (cz, cy, cx)]
+        sub = (Z[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] - cz) ** 2 + (Y[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] - cy) ** 2 \
+            + (X[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] - cx) ** 2
+        v = vol[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
+        v[sub <= r * r] = ph.mu_grain
+    return vol
+
+
+def minmax_scale(projs: torch.Tensor):
+    """Dataset-wide min-max scaling to [0,1] (nect/data.py:177-183)."""
+    mn = projs.min()
+    projs = projs - mn
+    mx = projs.max()
+    return projs / mx, float(mn), float(mx)
