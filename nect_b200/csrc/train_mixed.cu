@@ -1,11 +1,541 @@
-// Mixed-precision fused training step (fp16 tables, bf16 tcgen05 MLP).
+// Mixed-precision fused training step: fp16 hash tables, bf16 MLP on the
+// 5th-generation tensor cores (tcgen05.mma, fp32 accumulators in TMEM), fp32
+// Kahan-compensated line integral, fp32 gradient tables.
+//
+// Block = 4 warps = one warpgroup; a tile is 128 samples (each warp 32
+// consecutive samples of its current ray), i.e. the M = 128 rows of every
+// MMA and the 128 TMEM lanes (warp w reads lanes 32w..32w+31 with
+// tcgen05.ld.32x32b, so each thread owns its sample's row).  Per tile:
+//   forward:  X[128xIN] -> A1 = relu(X W0^T) -> A2 = relu(A1 W1^T) -> sigma
+//   backward: G2 = dsigma * w_out * 1[A2>0]
+//             dA1 = G2 W1            dW1 += G2^T A1   (TMEM accumulator)
+//             G1 = dA1 * 1[A1>0]
+//             dX = G1 W0             dW0 += G1^T X    (TMEM accumulator)
+//             table_grad[corner] += w_corner * dX   (fp32 vector atomics)
+// Operands are 128-byte-swizzled bf16 tiles in shared memory; the same tile
+// is the K-major A operand of the next layer and the MN-major operand of the
+// weight-gradient product, so no transposed copies are made.  The weight
+// gradients use M = 128 with the 64 real rows first (rows 64..127 read a
+// second, unused tile and are never stored).  One thread issues the MMAs and
+// commits them to an mbarrier; every wait is bounded and reports through an
+// error word instead of hanging.
+#include <algorithm>
+
+#include "mlp_simt.cuh"
+#include "tcgen05.cuh"
 #include "train_common.cuh"
 
 namespace nectb {
 
-int train_mixed(const NectbGeometry&, const GridDev&, const NectbMLP&, const void*, const float*, int,
-                const TrainArgs&, Workspace, float*, float*, float*, float*, cudaStream_t) {
-  return set_error(NECTB_ERR_INVALID, "mixed-precision path not built yet");
+namespace {
+
+constexpr int kMixThreads = 128;
+constexpr uint32_t kTile = 128 * 128;  // bytes of a [128][64 bf16] tile
+constexpr uint32_t kWTile = 64 * 128;  // bytes of a [64][64 bf16] tile
+
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+// fp32 weights (PyTorch layout) -> bf16 swizzled tiles: W0 rows o (IN used
+// columns), W1 rows o (64 columns); w_out stays fp32.
+template <int IN>
+__device__ __forceinline__ void stage_mixed_weights(const float* __restrict__ W, uint8_t* sW0, uint8_t* sW1,
+                                                    float* sWout) {
+  for (int e = threadIdx.x; e < 64 * (IN / 8); e += blockDim.x) {
+    const int o = e / (IN / 8), j = e % (IN / 8);
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
+    tc::st_chunk_bf16(sW0, o, j, v);
+  }
+  const float* W1 = W + 64 * IN;
+  for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
+    const int o = e / 8, j = e % 8;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = W1[o * 64 + 8 * j + q];
+    tc::st_chunk_bf16(sW1, o, j, v);
+  }
+  for (int e = threadIdx.x; e < 64; e += blockDim.x) sWout[e] = W[64 * IN + 64 * 64 + e];
+}
+
+// Encodes one sample into row r of the swizzled X tile (bf16), 8 features
+// (one 16-byte chunk) at a time; invalid samples write zeros.
+template <int D, int F>
+__device__ __forceinline__ void encode_row(const GridDev& g, const __half* __restrict__ table, const float* p,
+                                           bool valid, uint8_t* sX, int r) {
+  constexpr int LPC = 8 / F;  // levels per 16-byte chunk
+#pragma unroll 1
+  for (int j = 0; j < 16 / LPC; ++j) {
+    float v[8];
+    if (valid) {
+#pragma unroll
+      for (int q = 0; q < LPC; ++q) {
+        const int l = j * LPC + q;
+        LevelCorners<D> lc;
+        level_corners<D>(g, l, p, lc);
+        float vals[1 << D][F];
+#pragma unroll
+        for (int c = 0; c < (1 << D); ++c) Feat<F, __half>::load(table, g.offset[l] + lc.idx[c], vals[c]);
+#pragma unroll
+        for (int f = 0; f < F; ++f) {
+          float acc = 0.f;
+#pragma unroll
+          for (int c = 0; c < (1 << D); ++c) acc = fmaf(lc.w[c], vals[c][f], acc);
+          v[q * F + f] = acc;
+        }
+      }
+    } else {
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = 0.f;
+    }
+    tc::st_chunk_bf16(sX, r, j, v);
+  }
+}
+
+// Loads 64 fp32 TMEM columns [col, col+64) of this thread's lane.
+__device__ __forceinline__ void ld64(uint32_t taddr, float* v) {
+#pragma unroll
+  for (int c = 0; c < 4; ++c) tc::tmem_ld16(taddr + 16 * c, v + 16 * c);
+  tc::tmem_wait_ld();
+}
+
+// Per-warp ray cursor shared by the mixed kernels.
+struct RayCursor {
+  int ray = -1;
+  int base = 0;
+  RayRec rec;
+};
+
+// Advances the warp to a ray with work; rays without samples are passed to
+// on_empty (the forward writes their y_pred = 0).  Returns false when no rays
+// are left.
+template <typename OnEmpty>
+__device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* counter, int num_rays,
+                                           int lane, OnEmpty on_empty) {
+  if (cur.ray >= num_rays) return false;
+  if (cur.ray >= 0 && cur.base < cur.rec.count) return true;
+  while (true) {
+    int r = 0;
+    if (lane == 0) r = (int)atomicAdd(counter, 1u);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r >= num_rays) {
+      cur.ray = num_rays;
+      cur.rec.count = 0;
+      return false;
+    }
+    cur.rec = load_ray(recs, r);
+    cur.ray = r;
+    cur.base = 0;
+    if (cur.rec.count > 0) return true;
+    on_empty(r, cur.rec);
+  }
+}
+
+template <int D, int F>
+__global__ void __launch_bounds__(kMixThreads, 2)
+fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
+                 RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int out_act,
+                 float* __restrict__ y_pred, float* __restrict__ loss, unsigned int* __restrict__ err) {
+  constexpr int IN = 16 * F;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = align1024(smem_raw);
+  uint8_t* sW0 = base;
+  uint8_t* sW1 = sW0 + kWTile;
+  uint8_t* sX = sW1 + kWTile;
+  uint8_t* sA = sX + kTile;
+  float* sWout = reinterpret_cast<float*>(sA + kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  float* red = reinterpret_cast<float*>(tslot + 4);
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  stage_mixed_weights<IN>(W, sW0, sW1, sWout);
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 128);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) tc::mbar_init(bar, 1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tm = *tslot;
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
+  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA);
+  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
+
+  uint32_t phase = 0;
+  float loss_acc = 0.f;
+  float ksum = 0.f, kcomp = 0.f;  // Kahan sum of sigma along the warp's current ray (per lane)
+  RayCursor cur;
+  auto finish_empty = [&](int r, const RayRec& rec) {
+    if (lane == 0) {
+      y_pred[r] = 0.f;
+      recs[r].gsig = loss_grad(0.f, rec.y, a.loss_type, a.num_rays, rec.scale) * a.loss_scale;
+      loss_acc += loss_term(0.f, rec.y, a.loss_type);
+    }
+  };
+  bool timed_out = false;
+  while (true) {
+    const bool active = next_chunk(cur, recs, counter, a.num_rays, lane, finish_empty);
+    if (!__syncthreads_or(active)) break;
+    const int i = cur.base + lane;
+    float p[4];
+    bool valid = false;
+    if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
+    if (D == 4) p[3] = a.t;
+    encode_row<D, F>(grid, table, p, valid, sX, t);
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), idesc, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    float h[64];
+    ld64(my_lanes, h);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = fmaxf(h[8 * j + q], 0.f);
+      tc::st_chunk_bf16(sA, t, j, v);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), idesc, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    ld64(my_lanes + 64, h);
+    float z = 0.f;
+#pragma unroll
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    if (valid) {  // Kahan-compensated accumulation along the ray
+      const float y = act_fwd(z, out_act) - kcomp;
+      const float s = ksum + y;
+      kcomp = (s - ksum) - y;
+      ksum = s;
+    }
+    tc::fence_before();
+    if (active) {
+      cur.base += 32;
+      if (cur.base >= cur.rec.count) {
+        const float sum = warp_sum(ksum);
+        if (lane == 0) {
+          const float yp = sum * cur.rec.scale;
+          y_pred[cur.ray] = yp;
+          recs[cur.ray].gsig = loss_grad(yp, cur.rec.y, a.loss_type, a.num_rays, cur.rec.scale) * a.loss_scale;
+          loss_acc += loss_term(yp, cur.rec.y, a.loss_type);
+        }
+        ksum = 0.f;
+        kcomp = 0.f;
+      }
+    }
+  }
+  if (timed_out && t == 0) atomicOr(err, 1u);
+  if (lane == 0) red[warp] = loss_acc;
+  tc::fence_before();
+  __syncthreads();
+  if (t == 0) atomicAdd(loss, (red[0] + red[1] + red[2] + red[3]) / (float)a.num_rays);
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tm, 128);
+  }
+}
+
+template <int D, int F>
+__global__ void __launch_bounds__(kMixThreads, 2)
+bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
+                 const RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int out_act,
+                 float* __restrict__ table_grad, float* __restrict__ W_grad, unsigned int* __restrict__ err) {
+  constexpr int IN = 16 * F;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = align1024(smem_raw);
+  // Tile order matters: the padded (M = 128) weight-gradient operands read a
+  // second 16 KB block right after their tile, so sG is followed by sA and sA
+  // by sX, all inside this block's allocation.
+  uint8_t* sW0 = base;
+  uint8_t* sW1 = sW0 + kWTile;
+  uint8_t* sG = sW1 + kWTile;  // G2
+  uint8_t* sA = sG + kTile;    // A1, later G1
+  uint8_t* sX = sA + kTile;
+  float* sWout = reinterpret_cast<float*>(sX + kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  stage_mixed_weights<IN>(W, sW0, sW1, sWout);
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 256);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) tc::mbar_init(bar, 1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tm = *tslot;
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
+  // TMEM columns: [0,64) acc0, [64,128) acc1, [128,192) dW1, [192,192+IN) dW0
+  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sG_a = tc::smem_u32(sG);
+  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  // M = 128 weight-gradient products: rows 64..127 of A come from the tile kTile further on.
+  const uint32_t pad_lbo = kTile;
+  constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
+  constexpr uint32_t id_dA = tc::idesc_bf16(128, 64, false, true);
+  constexpr uint32_t id_dW1 = tc::idesc_bf16(128, 64, true, true);
+  constexpr uint32_t id_dX = tc::idesc_bf16(128, IN, false, true);
+  constexpr uint32_t id_dW0 = tc::idesc_bf16(128, IN, true, true);
+
+  uint32_t phase = 0;
+  uint32_t wacc = 0;  // weight-gradient accumulators start at the first tile
+  float dwout0 = 0.f, dwout1 = 0.f;
+  RayCursor cur;
+  auto skip_empty = [](int, const RayRec&) {};
+  bool timed_out = false;
+  while (true) {
+    const bool active = next_chunk(cur, recs, counter, a.num_rays, lane, skip_empty);
+    if (!__syncthreads_or(active)) break;
+    const int i = cur.base + lane;
+    float p[4];
+    bool valid = false;
+    if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
+    if (D == 4) p[3] = a.t;
+    encode_row<D, F>(grid, table, p, valid, sX, t);
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), id_fwd, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    float h[64];
+    ld64(my_lanes, h);
+    uint32_t m1lo = 0, m1hi = 0;  // relu masks of A1
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const float x = h[8 * j + q];
+        v[q] = fmaxf(x, 0.f);
+        const uint32_t bit = x > 0.f ? 1u : 0u;
+        if (8 * j + q < 32) m1lo |= bit << (8 * j + q); else m1hi |= bit << (8 * j + q - 32);
+      }
+      tc::st_chunk_bf16(sA, t, j, v);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), id_fwd, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    ld64(my_lanes + 64, h);
+    float z = 0.f;
+#pragma unroll
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
+    // w_out gradient over the warp's samples; G2 = dz * w_out * 1[a2 > 0]
+#pragma unroll
+    for (int j = 0; j < 64; ++j) {
+      const float s = warp_sum(dz * fmaxf(h[j], 0.f));
+      if (j == lane) dwout0 += s;
+      if (j == lane + 32) dwout1 += s;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = h[8 * j + q] > 0.f ? dz * sWout[8 * j + q] : 0.f;
+      tc::st_chunk_bf16(sG, t, j, v);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+      // dA1 = G2 W1 (A = G2 K-major, B = W1 MN-major)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tc::mma(tm, tc::desc_k(sG_a, k), tc::desc_mn(sW1_a, k, kWTile), id_dA, k > 0);
+      // dW1 += G2^T A1 (A = G2 MN-major, M = 128 padded; B = A1 MN-major; K = 128 samples)
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        tc::mma(tm + 128, tc::desc_mn(sG_a, k, pad_lbo), tc::desc_mn(sA_a, k, kTile), id_dW1, (k > 0) | wacc);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    ld64(my_lanes, h);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const int c = 8 * j + q;
+        const uint32_t bit = c < 32 ? (m1lo >> c) & 1u : (m1hi >> (c - 32)) & 1u;
+        v[q] = bit ? h[c] : 0.f;
+      }
+      tc::st_chunk_bf16(sA, t, j, v);  // G1 replaces A1 (the dW1 product has completed)
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+      // dX = G1 W0 (A = G1 K-major, B = W0 MN-major, N = IN)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_mn(sW0_a, k, kWTile), id_dX, k > 0);
+      // dW0 += G1^T X (A = G1 MN-major, M = 128 padded; B = X MN-major; K = 128 samples)
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        tc::mma(tm + 192, tc::desc_mn(sA_a, k, pad_lbo), tc::desc_mn(sX_a, k, kTile), id_dW0, (k > 0) | wacc);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    wacc = 1;
+    tc::fence_after();
+    float dx[IN];
+#pragma unroll
+    for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, dx + 16 * c);
+    tc::tmem_wait_ld();
+    if (valid) scatter_point<D, F>(grid, table_grad, p, dx, 1);
+    tc::fence_before();
+    __syncthreads();
+    if (active) cur.base += 32;
+  }
+  if (timed_out) {
+    if (t == 0) atomicOr(err, 2u);
+    tc::mbar_wait(bar, phase);  // let the MMAs in flight retire (bounded) before freeing TMEM
+  } else if (wacc) {
+    // flush the weight gradients: TMEM lanes 0..63 (warps 0 and 1) hold rows o = 0..63
+    tc::fence_after();
+    if (warp < 2) {
+      const int o = t;
+      float v[64];
+      ld64(my_lanes + 128, v);
+#pragma unroll
+      for (int i2 = 0; i2 < 64; ++i2) atomicAdd(W_grad + 64 * IN + o * 64 + i2, v[i2]);
+      float w0[IN];
+#pragma unroll
+      for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 192 + 16 * c, w0 + 16 * c);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int i2 = 0; i2 < IN; ++i2) atomicAdd(W_grad + o * IN + i2, w0[i2]);
+    }
+  }
+  red[warp * 64 + lane] = dwout0;
+  red[warp * 64 + lane + 32] = dwout1;
+  tc::fence_before();
+  __syncthreads();
+  if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tm, 256);
+  }
+}
+
+template <int D, int F>
+int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W, const TrainArgs& a,
+              Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
+              cudaStream_t s) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  {
+    ProfScope ps(kProfRayPrep, s);
+    ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
+  }
+  if (int rc = launch_status("ray_prep_kernel")) return rc;
+  unsigned int* err = ws.counters + 2;
+  const int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
+  {
+    auto k = fwd_mixed_kernel<D, F>;
+    const size_t smem = 1024 + 2 * kWTile + 2 * kTile + 64 * 4 + 64;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ProfScope ps(kProfForward, s);
+    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.counters, out_act, y_pred, loss, err);
+  }
+  if (int rc = launch_status("fwd_mixed_kernel")) return rc;
+  {
+    auto k = bwd_mixed_kernel<D, F>;
+    // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
+    const size_t smem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    ProfScope ps(kProfBackward, s);
+    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, out_act, table_grad, W_grad,
+                                        err);
+  }
+  return launch_status("bwd_mixed_kernel");
+}
+
+}  // namespace
+
+int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const void* table,
+                const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
+                float* y_pred, float* loss, cudaStream_t s) {
+  (void)nW;
+  const int D = grid.n_dims, F = grid.n_features;
+  if (mlp.n_hidden_layers != 2 || mlp.activation != NECTB_ACT_RELU)
+    return set_error(NECTB_ERR_INVALID, "mixed path: needs 2 hidden ReLU layers (got %d, act %d)",
+                     mlp.n_hidden_layers, mlp.activation);
+  const __half* tab = (const __half*)table;
+  const int oact = mlp.output_activation;
+  if (D == 3 && F == 2) return run_mixed<3, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  if (D == 4 && F == 2) return run_mixed<4, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  return set_error(NECTB_ERR_INVALID, "mixed path: unsupported grid (n_dims %d, n_features %d)", D, F);
 }
 
 }  // namespace nectb
