@@ -233,6 +233,7 @@ def main():
     ap.add_argument("--cpu-rays", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling of smaller cases)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -257,7 +258,7 @@ def main():
 
     spec = workload_spec(args.workload, args.precision)
     geometry = Geometry(**spec["geo"])
-    S, R = spec["S"], spec["rays"]
+    S, R = spec["S"], (args.rays or spec["rays"])
     model_cfg = spec["model"]
     wl_name = (f"{args.workload}: {geometry.mode} {geometry.nDetector[0]}x{geometry.nDetector[1]} detector, "
                f"{geometry.nVoxel[0]}^3 volume, S={S}, hash {model_cfg.encoder.n_levels}x"
