@@ -184,8 +184,8 @@ typedef struct NectbTrainBatch {
   float loss_scale;                 /* multiplies dL/dy (1 = plain mean) */
 } NectbTrainBatch;
 
-size_t nectb_train_workspace_bytes(const NectbHashGrid* grid, const NectbMLP* mlp,
-                                   int32_t num_rays);
+size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                   const NectbMLP* mlp, int32_t num_rays);
 
 /* Fused forward+backward.  grid_params is the table in grid->feature_dtype
  * (fp32 or fp16); mlp_params fp32.  Gradients are accumulated (+=) into

@@ -112,7 +112,7 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_ptr, c_ptr],
     ),
     "nectb_train_workspace_bytes": (
-        c_size, [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int]),
+        c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int]),
     "nectb_train_step": (
         c_int,
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,

@@ -60,26 +60,37 @@ __device__ __forceinline__ void level_corners(const GridDev& g, int l, const flo
     f[k] = p - (float)ci;
   }
   const bool hashed = (g.hashed_bits >> l) & 1u;
+  // Per-axis terms of the lower/upper vertex: the hash XORs v_k * pi_k and the
+  // dense index adds v_k * stride_k, and (c+1)*m = c*m + m in 32-bit
+  // arithmetic, so each corner costs one XOR/add per axis.  Identical integers
+  // to evaluating every corner from scratch.
+  uint32_t term[D][2];
+  float wt[D][2];
+#pragma unroll
+  for (int k = 0; k < D; ++k) {
+    uint32_t m;
+    if (hashed)
+      m = (k == 0) ? 1u : (k == 1 ? kPrime1 : (k == 2 ? kPrime2 : kPrime3));
+    else
+      m = (k == 0) ? 1u : g.stride[l][k];
+    term[k][0] = (uint32_t)c[k] * m;
+    term[k][1] = term[k][0] + m;
+    wt[k][0] = 1.f - f[k];
+    wt[k][1] = f[k];
+  }
+  // Weight products in axis order, shared prefixes computed once.
+  float w01[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) w01[q] = wt[0][q & 1] * wt[1][(q >> 1) & 1];
 #pragma unroll
   for (int corner = 0; corner < (1 << D); ++corner) {
-    uint32_t v[D];
+    uint32_t id = term[0][corner & 1];
 #pragma unroll
-    for (int k = 0; k < D; ++k) v[k] = (uint32_t)c[k] + ((corner >> k) & 1);
-    uint32_t id;
-    if (hashed) {
-      id = v[0];
-      if (D > 1) id ^= v[1] * kPrime1;
-      if (D > 2) id ^= v[2] * kPrime2;
-      if (D > 3) id ^= v[3 % D] * kPrime3;
-      id &= g.hash_mask;
-    } else {
-      id = v[0];
+    for (int k = 1; k < D; ++k) id = hashed ? (id ^ term[k][(corner >> k) & 1]) : (id + term[k][(corner >> k) & 1]);
+    if (hashed) id &= g.hash_mask;
+    float w = w01[corner & 3];
 #pragma unroll
-      for (int k = 1; k < D; ++k) id += v[k] * g.stride[l][k];
-    }
-    float w = 1.f;
-#pragma unroll
-    for (int k = 0; k < D; ++k) w = w * (((corner >> k) & 1) ? f[k] : (1.f - f[k]));
+    for (int k = 2; k < D; ++k) w = w * wt[k][(corner >> k) & 1];
     lc.idx[corner] = id;
     lc.w[corner] = w;
   }

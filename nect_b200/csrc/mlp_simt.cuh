@@ -136,6 +136,34 @@ __device__ __forceinline__ float warp_sum(float v) {
   return v;
 }
 
+namespace detail {
+template <int N>
+__device__ __forceinline__ void rs_step(const float* in, float* out, int lane, int offset) {
+  const bool up = (lane & offset) != 0;
+#pragma unroll
+  for (int k = 0; k < N; ++k) {
+    const float send = up ? in[k] : in[k + N];
+    const float keep = up ? in[k + N] : in[k];
+    out[k] = keep + __shfl_xor_sync(0xffffffffu, send, offset);
+  }
+}
+}  // namespace detail
+
+// Butterfly reduce-scatter of 64 per-lane values over the warp: lane L ends
+// with the warp sums of entries j0 and j0 + 1 (62 shuffles instead of 320 for
+// 64 separate warp sums).
+__device__ __forceinline__ void warp_reduce_scatter64(const float* v, int lane, float& s0, float& s1, int& j0) {
+  float a[32], b[16], c[8], d[4], e[2];
+  detail::rs_step<32>(v, a, lane, 16);
+  detail::rs_step<16>(a, b, lane, 8);
+  detail::rs_step<8>(b, c, lane, 4);
+  detail::rs_step<4>(c, d, lane, 2);
+  detail::rs_step<2>(d, e, lane, 1);
+  s0 = e[0];
+  s1 = e[1];
+  j0 = ((lane >> 4) & 1) * 32 + ((lane >> 3) & 1) * 16 + ((lane >> 2) & 1) * 8 + ((lane >> 1) & 1) * 4 + (lane & 1) * 2;
+}
+
 // Weights in shared memory for the SIMT paths: for every layer k both the
 // transposed copy WT_k [in][64] (forward products) and the PyTorch layout
 // W_k [64][in] (backward products), then w_out [64].

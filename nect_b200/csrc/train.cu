@@ -44,10 +44,12 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 
 using namespace nectb;
 
-extern "C" size_t nectb_train_workspace_bytes(const NectbHashGrid* grid, const NectbMLP* mlp, int32_t num_rays) {
+extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                              const NectbMLP* mlp, int32_t num_rays) {
   (void)grid;
   (void)mlp;
-  return workspace_bytes(std::max(num_rays, 1));
+  const int P = geometry ? geometry->nDetector[0] * geometry->nDetector[1] : 0;
+  return workspace_bytes(std::max(num_rays, 1), std::max(P, 0));
 }
 
 extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
@@ -70,10 +72,12 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   if (batch->num_rays == 0) return NECTB_OK;
   NECTB_REQUIRE(batch->random_ray_index && batch->jitter && batch->detector_offset && batch->projection,
                 "null batch input");
-  if (!workspace || workspace_size < workspace_bytes(batch->num_rays))
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  if (!workspace || workspace_size < workspace_bytes(batch->num_rays, P))
     return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
-                     workspace_bytes(batch->num_rays));
+                     workspace_bytes(batch->num_rays, P));
   TrainArgs a;
+  a.n_pixels = P;
   a.perm = batch->random_ray_index;
   a.perm_len = batch->random_ray_index_len;
   a.start = batch->starting_ray_index;
@@ -89,8 +93,15 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   a.projection = batch->projection;
   a.loss_type = batch->loss_type;
   a.loss_scale = batch->loss_scale;
-  Workspace ws = carve_workspace(workspace, a.num_rays);
+  Workspace ws = carve_workspace(workspace, a.num_rays, P);
   if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
+  if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
+  {
+    ProfScope ps(kProfRayPrep, s);
+    ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters,
+                                                                       y_pred, loss);
+  }
+  if (int rc = launch_status("ray_prep_kernel")) return rc;
   const int nW = (int)mlp_param_count(mlp);
   if (mlp->compute_dtype == NECTB_F32) {
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F32, "plain path needs an fp32 table");

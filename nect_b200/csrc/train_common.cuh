@@ -1,6 +1,6 @@
 // Pieces shared by the plain (fp32 SIMT) and mixed (bf16 tcgen05) fused
-// training kernels: per-ray records, the ray-preparation kernel, sample
-// regeneration and the workspace layout.
+// training kernels: per-ray records, the ray-preparation kernel, the ray
+// scheduler, sample regeneration and the workspace layout.
 #pragma once
 #include <cstdint>
 
@@ -27,6 +27,7 @@ struct TrainArgs {
   int64_t perm_len;
   int64_t start;
   int num_rays;
+  int n_pixels;  // nDetector[0] * nDetector[1]
   int S;
   float angle;
   float t;
@@ -40,23 +41,32 @@ struct TrainArgs {
   float loss_scale;
 };
 
-// Workspace: RayRec[R] then two scheduling counters (fwd, bwd) and padding.
+enum : unsigned int { kFlagDuplicatePixels = 1u };
+
+// Workspace: RayRec[R] | slot[P] (int32: batch index of the ray through each
+// detector pixel, -1 if none) | 64-byte control block (scheduling cursors of
+// the forward and backward, error word, flags).
 struct Workspace {
   RayRec* rays;
-  unsigned int* counters;  // [0] forward ray cursor, [1] backward ray cursor
+  int32_t* slot;
+  unsigned int* counters;  // [0] forward cursor, [1] backward cursor, [2] error word, [3] flags
 };
 
-inline size_t workspace_bytes(int R) { return (size_t)R * sizeof(RayRec) + 256; }
+inline size_t workspace_bytes(int R, int P) { return (size_t)R * sizeof(RayRec) + (size_t)P * 4 + 256; }
 
-inline Workspace carve_workspace(void* ws, int R) {
+inline Workspace carve_workspace(void* ws, int R, int P) {
   Workspace w;
   w.rays = (RayRec*)ws;
-  w.counters = (unsigned int*)((char*)ws + (size_t)R * sizeof(RayRec));
+  w.slot = (int32_t*)((char*)ws + (size_t)R * sizeof(RayRec));
+  w.counters = (unsigned int*)((char*)w.slot + (((size_t)P * 4 + 63) & ~size_t(63)));
   return w;
 }
 
-// Warp per ray: set-up, sample count (warp ballot), measured value, scale.
-__global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict__ recs);
+// Warp per ray: set-up, sample count (warp ballot), measured value, scale;
+// claims the ray's detector pixel in slot[]; finalises rays without samples
+// (y_pred = 0, their loss term and gradient).
+__global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict__ recs, int32_t* __restrict__ slot,
+                                unsigned int* __restrict__ ctrl, float* __restrict__ y_pred, float* __restrict__ loss);
 
 // Position of sample i of a prepared ray, after the Projector clamp
 // (projector.py:127); returns false for the zero points the trainer drops
@@ -73,7 +83,29 @@ __device__ __forceinline__ bool sample_point(const RayRec& r, int i, float* p) {
 
 __device__ __forceinline__ RayRec load_ray(const RayRec* recs, int r) { return recs[r]; }
 
-// Loss gradient dL/dy_pred for one ray (mean over rays, nect/config.py:481-497).
+// Warp-uniform scheduler: hands out the rays of the batch that have samples,
+// in detector-pixel order (neighbouring rays run together, so the blocks in
+// flight touch a compact part of the tables and the L2 keeps it), or in batch
+// order when the batch repeats a pixel.  Returns -1 when none are left.
+__device__ __forceinline__ int next_ray(unsigned int* cursor, const int32_t* __restrict__ slot,
+                                        const RayRec* __restrict__ recs, int R, int P, bool by_pixel, int lane) {
+  while (true) {
+    unsigned int idx = 0;
+    if (lane == 0) idx = atomicAdd(cursor, 1u);
+    idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (by_pixel) {
+      if (idx >= (unsigned)P) return -1;
+      const int r = slot[idx];
+      if (r >= 0) return r;
+    } else {
+      if (idx >= (unsigned)R) return -1;
+      if (recs[idx].count > 0) return (int)idx;
+    }
+  }
+}
+
+// Loss gradient dL/dy_pred for one ray (mean over rays, nect/config.py:481-497),
+// times the ray's scale (dy_pred/dsigma).
 __device__ __forceinline__ float loss_grad(float y_pred, float y, int loss_type, int R, float scale) {
   const float d = y_pred - y;
   float g;

@@ -108,37 +108,33 @@ struct RayCursor {
   RayRec rec;
 };
 
-// Advances the warp to a ray with work; rays without samples are passed to
-// on_empty (the forward writes their y_pred = 0).  Returns false when no rays
-// are left.
-template <typename OnEmpty>
-__device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* counter, int num_rays,
-                                           int lane, OnEmpty on_empty) {
-  if (cur.ray >= num_rays) return false;
+// Advances the warp to its next chunk of 32 samples (a new ray from the
+// scheduler when the current one is done).  Returns false when no rays are
+// left.  Rays without samples were finalised by the preparation kernel.
+__device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* cursor,
+                                           const int32_t* slot, const TrainArgs& a, bool by_pixel, int lane) {
+  if (cur.ray >= a.num_rays) return false;
   if (cur.ray >= 0 && cur.base < cur.rec.count) return true;
-  while (true) {
-    int r = 0;
-    if (lane == 0) r = (int)atomicAdd(counter, 1u);
-    r = __shfl_sync(0xffffffffu, r, 0);
-    if (r >= num_rays) {
-      cur.ray = num_rays;
-      cur.rec.count = 0;
-      return false;
-    }
-    cur.rec = load_ray(recs, r);
-    cur.ray = r;
-    cur.base = 0;
-    if (cur.rec.count > 0) return true;
-    on_empty(r, cur.rec);
+  const int r = next_ray(cursor, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane);
+  if (r < 0) {
+    cur.ray = a.num_rays;
+    cur.rec.count = 0;
+    return false;
   }
+  cur.rec = load_ray(recs, r);
+  cur.ray = r;
+  cur.base = 0;
+  return true;
 }
 
 template <int D, int F>
 __global__ void __launch_bounds__(kMixThreads, 2)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
-                 RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int out_act,
-                 float* __restrict__ y_pred, float* __restrict__ loss, unsigned int* __restrict__ err) {
+                 RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
+                 int out_act, float* __restrict__ y_pred, float* __restrict__ loss) {
   constexpr int IN = 16 * F;
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   uint8_t* sW0 = base;
@@ -171,16 +167,9 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   float loss_acc = 0.f;
   float ksum = 0.f, kcomp = 0.f;  // Kahan sum of sigma along the warp's current ray (per lane)
   RayCursor cur;
-  auto finish_empty = [&](int r, const RayRec& rec) {
-    if (lane == 0) {
-      y_pred[r] = 0.f;
-      recs[r].gsig = loss_grad(0.f, rec.y, a.loss_type, a.num_rays, rec.scale) * a.loss_scale;
-      loss_acc += loss_term(0.f, rec.y, a.loss_type);
-    }
-  };
   bool timed_out = false;
   while (true) {
-    const bool active = next_chunk(cur, recs, counter, a.num_rays, lane, finish_empty);
+    const bool active = next_chunk(cur, recs, ctrl, slot, a, by_pixel, lane);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4];
@@ -269,9 +258,11 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 template <int D, int F>
 __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
-                 const RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int out_act,
-                 float* __restrict__ table_grad, float* __restrict__ W_grad, unsigned int* __restrict__ err) {
+                 const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
+                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad) {
   constexpr int IN = 16 * F;
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   // Tile order matters: the padded (M = 128) weight-gradient operands read a
@@ -313,12 +304,12 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 
   uint32_t phase = 0;
   uint32_t wacc = 0;  // weight-gradient accumulators start at the first tile
-  float dwout0 = 0.f, dwout1 = 0.f;
+  float dwout0 = 0.f, dwout1 = 0.f;  // w_out gradient entries j0_out and j0_out + 1 of this lane
+  int j0_out = 0;
   RayCursor cur;
-  auto skip_empty = [](int, const RayRec&) {};
   bool timed_out = false;
   while (true) {
-    const bool active = next_chunk(cur, recs, counter, a.num_rays, lane, skip_empty);
+    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4];
@@ -379,11 +370,14 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
     const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
     // w_out gradient over the warp's samples; G2 = dz * w_out * 1[a2 > 0]
+    {
+      float v[64];
 #pragma unroll
-    for (int j = 0; j < 64; ++j) {
-      const float s = warp_sum(dz * fmaxf(h[j], 0.f));
-      if (j == lane) dwout0 += s;
-      if (j == lane + 32) dwout1 += s;
+      for (int j = 0; j < 64; ++j) v[j] = dz * fmaxf(h[j], 0.f);
+      float s0, s1;
+      warp_reduce_scatter64(v, lane, s0, s1, j0_out);
+      dwout0 += s0;
+      dwout1 += s1;
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -476,8 +470,15 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
       for (int i2 = 0; i2 < IN; ++i2) atomicAdd(W_grad + o * IN + i2, w0[i2]);
     }
   }
-  red[warp * 64 + lane] = dwout0;
-  red[warp * 64 + lane + 32] = dwout1;
+  {
+    float s0, s1;
+    float zero[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) zero[j] = 0.f;
+    warp_reduce_scatter64(zero, lane, s0, s1, j0_out);  // j0_out of this lane (also when no tile ran)
+  }
+  red[warp * 64 + j0_out] = dwout0;
+  red[warp * 64 + j0_out + 1] = dwout1;
   tc::fence_before();
   __syncthreads();
   if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
@@ -494,19 +495,14 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  {
-    ProfScope ps(kProfRayPrep, s);
-    ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
-  }
-  if (int rc = launch_status("ray_prep_kernel")) return rc;
-  unsigned int* err = ws.counters + 2;
+  (void)geo;
   const int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
   {
     auto k = fwd_mixed_kernel<D, F>;
     const size_t smem = 1024 + 2 * kWTile + 2 * kTile + 64 * 4 + 64;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     ProfScope ps(kProfForward, s);
-    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.counters, out_act, y_pred, loss, err);
+    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
   }
   if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   {
@@ -515,8 +511,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     const size_t smem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     ProfScope ps(kProfBackward, s);
-    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, out_act, table_grad, W_grad,
-                                        err);
+    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+                                        W_grad);
   }
   return launch_status("bwd_mixed_kernel");
 }

@@ -19,7 +19,8 @@
 
 namespace nectb {
 
-__global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict__ recs) {
+__global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict__ recs, int32_t* __restrict__ slot,
+                                unsigned int* __restrict__ ctrl, float* __restrict__ y_pred, float* __restrict__ loss) {
   const int lane = threadIdx.x & 31;
   const int tid = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (tid >= a.num_rays) return;
@@ -48,6 +49,14 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
     const bool in_range = ok && ray_index >= 0;
     rec.y = in_range ? a.projection[ray_index] : 0.f;
     rec.gsig = 0.f;
+    if (count > 0) {
+      if (atomicCAS(slot + ray_index, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
+    } else {
+      // no samples: y_pred = 0 (the reference's zero attenuation sum)
+      y_pred[tid] = 0.f;
+      rec.gsig = loss_grad(0.f, rec.y, a.loss_type, a.num_rays, rec.scale) * a.loss_scale;
+      atomicAdd(loss, loss_term(0.f, rec.y, a.loss_type) / (float)a.num_rays);
+    }
     recs[tid] = rec;
   }
 }
@@ -59,9 +68,10 @@ constexpr int kPlainFwdThreads = 128;
 template <int D, int F, int IN, int H>
 __global__ void __launch_bounds__(kPlainFwdThreads)
 fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __restrict__ W, TrainArgs a,
-                 RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int act, int out_act,
-                 float* __restrict__ y_pred, float* __restrict__ loss) {
+                 RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
+                 int act, int out_act, float* __restrict__ y_pred, float* __restrict__ loss) {
   constexpr int NT = kPlainFwdThreads;
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   constexpr int LD = NT + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
@@ -74,10 +84,8 @@ fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   const int lane = t & 31;
   float loss_acc = 0.f;
   while (true) {
-    int r = 0;
-    if (lane == 0) r = (int)atomicAdd(counter, 1u);
-    r = __shfl_sync(0xffffffffu, r, 0);
-    if (r >= a.num_rays) break;
+    const int r = next_ray(ctrl, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane);
+    if (r < 0) break;
     const RayRec rec = load_ray(recs, r);
     float sum = 0.f;
     for (int base = 0; base < rec.count; base += 32) {
@@ -165,9 +173,10 @@ struct WGrad {
 template <int D, int F, int IN, int H, int NT>
 __global__ void __launch_bounds__(NT, 1)
 bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __restrict__ W, TrainArgs a,
-                 const RayRec* __restrict__ recs, unsigned int* __restrict__ counter, int act, int out_act,
-                 float* __restrict__ table_grad, float* __restrict__ W_grad) {
+                 const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
+                 int act, int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad) {
   constexpr int NW = NT / 32;
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   constexpr int LD = NT + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
@@ -194,19 +203,14 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   __syncthreads();
   while (true) {
     if (ray < a.num_rays && (ray < 0 || base >= rec.count)) {
-      while (true) {
-        int r = 0;
-        if (lane == 0) r = (int)atomicAdd(counter, 1u);
-        r = __shfl_sync(0xffffffffu, r, 0);
-        if (r >= a.num_rays) {
-          ray = a.num_rays;
-          rec.count = 0;
-          break;
-        }
+      const int r = next_ray(ctrl + 1, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane);
+      if (r < 0) {
+        ray = a.num_rays;
+        rec.count = 0;
+      } else {
         rec = load_ray(recs, r);
         ray = r;
         base = 0;
-        if (rec.count > 0) break;
       }
     }
     const bool warp_active = ray < a.num_rays;
@@ -285,12 +289,7 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-
-  {
-    ProfScope ps(kProfRayPrep, s);
-    ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(geo, a, ws.rays);
-  }
-  if (int rc = launch_status("ray_prep_kernel")) return rc;
+  (void)geo;
 
   constexpr int FNT = kPlainFwdThreads;
   auto fk = fwd_plain_kernel<D, F, IN, H>;
@@ -301,7 +300,7 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   const int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
   {
     ProfScope ps(kProfForward, s);
-    fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.counters, act, out_act, y_pred, loss);
+    fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred, loss);
   }
   if (int rc = launch_status("fwd_plain_kernel")) return rc;
 
@@ -313,7 +312,8 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   const int bblocks = std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, NT / 32)));
   {
     ProfScope ps(kProfBackward, s);
-    bk<<<bblocks, NT, bsmem, s>>>(grid, table, W, a, ws.rays, ws.counters + 1, act, out_act, table_grad, W_grad);
+    bk<<<bblocks, NT, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, table_grad,
+                                  W_grad);
   }
   return launch_status("bwd_plain_kernel");
 }

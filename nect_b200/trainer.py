@@ -50,9 +50,9 @@ class Workspace:
     def __init__(self):
         self.buf = None
 
-    def get(self, model: _HashGridModel, num_rays: int, device) -> tuple[int, int]:
-        need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
-                                                    num_rays)
+    def get(self, model: _HashGridModel, c_geometry, num_rays: int, device) -> tuple[int, int]:
+        need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                                    ctypes.byref(model.mlp_desc), num_rays)
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         return self.buf.data_ptr(), self.buf.numel()
@@ -90,7 +90,7 @@ def train_step(model: _HashGridModel, c_geometry, batch: RayBatch, max_distance_
         _lib.require_cuda(t, name)
     y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
     loss_out = torch.empty(1, device=dev, dtype=torch.float32)
-    ws_ptr, ws_size = workspace.get(model, batch.num_rays, dev)
+    ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev)
     cb = c_batch(batch, max_distance_traveled, loss, loss_scale)
     rc = _lib.lib.nectb_train_step(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
                                    ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(), model.mlp.data_ptr(),

@@ -83,7 +83,7 @@ def test_model_forward_matches_oracle(cuda_device, n_dims, precision):
     assert torch.allclose(out, ref, rtol=1e-5, atol=1e-6), (out - ref).abs().max()
 
 
-def run_train_case(n_dims, precision, loss, geom_kind="parallel"):
+def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=False):
     from nect_b200.sampling import Geometry
     from nect_b200.trainer import RayBatch, Workspace, train_step
 
@@ -99,6 +99,8 @@ def run_train_case(n_dims, precision, loss, geom_kind="parallel"):
     P = geo.nDetector[0] * geo.nDetector[1]
     S, R, start = 64, 700, 100
     perm = torch.randperm(P, device="cuda")
+    if duplicates:  # a batch that repeats pixels (scheduler falls back to batch order)
+        perm[start + 1:start + 40] = perm[start]
     jitter = torch.rand(R, device="cuda") - 0.5
     det_off = torch.zeros(R, 2, device="cuda")
     proj = torch.rand(P, device="cuda")
@@ -164,3 +166,13 @@ def test_mixed_error_word_clear(cuda_device):
 
     ws = Workspace()
     run_train_case(3, "mixed", "l2", "cone")
+
+
+@pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
+def test_batch_with_repeated_pixels(cuda_device, precision):
+    """Every ray of the batch is processed when pixels repeat (the pixel-order
+    scheduler's fallback), with the same tolerances as above."""
+    (y, L, gt, gm), (yo, Lo, gto, gmo) = run_train_case(3, precision, "l2", "cone", duplicates=True)
+    tol = 1e-4 if precision == "plain_fp32" else 2e-2
+    assert rel_max(y, yo) < tol
+    assert cosine(gt, gto) > 0.99
