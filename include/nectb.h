@@ -199,6 +199,24 @@ int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid,
                      float* loss, void* workspace, size_t workspace_bytes,
                      void* stream);
 
+/* nectb_train_step without a caller workspace, for callers that cannot
+ * allocate device memory (a runtime that binds this library through its C ABI
+ * and has no CUDA allocator, or a loop that must never call cudaMalloc, which
+ * synchronises the device and can fail mid-run).  No counterpart in the
+ * reference.  Scratch is a library-owned __device__ array of
+ * nectb_train_static_scratch_bytes() (20 MiB + 4 KiB) that every GPU loading
+ * the library reserves until exit; batches needing more (above 262,144 rays
+ * on a 1024x1024 detector) fail with NECTB_ERR_TOO_LARGE.  The first call on
+ * a device (that device current) looks up the array's address; make it before
+ * any stream capture.  Calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller.  Allocates nothing. */
+int nectb_train_step_static(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                            const NectbMLP* mlp, const void* grid_params,
+                            const float* mlp_params, const NectbTrainBatch* batch,
+                            float* grid_grad, float* mlp_grad, float* y_pred,
+                            float* loss, void* stream);
+size_t nectb_train_static_scratch_bytes(void);
+
 /* Adam (torch.optim.Adam semantics, as configured in nect/config.py:400-414)
  * over n fp32 parameters with fp32 moments; step is the 1-based step count.
  * When param_half is non-NULL the updated parameter is also written there as

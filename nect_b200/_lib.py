@@ -118,6 +118,12 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
          ctypes.POINTER(NectbTrainBatch), c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_size, c_ptr],
     ),
+    "nectb_train_step_static": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
+         ctypes.POINTER(NectbTrainBatch), c_ptr, c_ptr, c_ptr, c_ptr, c_ptr],
+    ),
+    "nectb_train_static_scratch_bytes": (c_size, []),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
     "nectb_adam_step": (

@@ -1,0 +1,77 @@
+// nectb_train_step_static: the fused training step with its scratch memory in
+// a fixed device array owned by the library, for callers that cannot allocate
+// device memory themselves.
+//
+// Who needs it: a host that reaches this library only through its C ABI and
+// has no CUDA allocator of its own (a foreign-language runtime binding the
+// .so), or a serving/training loop that must not call cudaMalloc at all
+// (cudaMalloc synchronises the device and can fail under memory pressure in
+// the middle of a run).  Such a caller passes only its inputs and outputs.
+//
+// The scratch is one file-scope __device__ array of kStaticScratchBytes
+// (20 MiB + 4 KiB); every GPU that loads the library reserves it until the
+// process exits.  The first call on a device (with that device current)
+// looks up the array's device address with cudaGetSymbolAddress; make that
+// first call before any stream capture.  All calls share the one array and it
+// keeps the last call's contents: nectb_train_step clears what has to start
+// at zero (scheduling cursors, error word, pixel slots) and overwrites the
+// per-ray records, so results never depend on a previous call, but calls
+// whose work overlaps on the GPU (different streams, or threads without
+// ordering) race on the array and must be serialised by the caller.
+#include <mutex>
+
+#include "common.cuh"
+
+extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                              const NectbMLP* mlp, int32_t num_rays);
+
+namespace nectb {
+namespace {
+
+constexpr size_t kStaticScratchBytes = (size_t(20) << 20) + 4096;
+static __device__ __align__(256) unsigned char g_train_scratch[kStaticScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mu;
+void* g_scratch_ptr[kMaxDevices] = {nullptr};
+
+// Device address of g_train_scratch on the current device (looked up once per
+// device; the host-side symbol itself is not a device address).
+int scratch_address(void** out) {
+  int dev = 0;
+  if (int rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
+  if (dev < 0 || dev >= kMaxDevices) return set_error(NECTB_ERR_INVALID, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lk(g_scratch_mu);
+  if (!g_scratch_ptr[dev]) {
+    void* p = nullptr;
+    if (int rc = cuda_status(cudaGetSymbolAddress(&p, g_train_scratch), "cudaGetSymbolAddress(g_train_scratch)"))
+      return rc;
+    g_scratch_ptr[dev] = p;
+  }
+  *out = g_scratch_ptr[dev];
+  return NECTB_OK;
+}
+
+}  // namespace
+}  // namespace nectb
+
+extern "C" size_t nectb_train_static_scratch_bytes(void) { return nectb::kStaticScratchBytes; }
+
+extern "C" int nectb_train_step_static(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                       const void* grid_params, const float* mlp_params,
+                                       const NectbTrainBatch* batch, float* grid_grad, float* mlp_grad,
+                                       float* y_pred, float* loss, void* stream) {
+  using namespace nectb;
+  clear_error();
+  NECTB_REQUIRE(geometry && grid && mlp && batch, "null description");
+  const size_t need = nectb_train_workspace_bytes(geometry, grid, mlp, batch->num_rays);
+  if (need > kStaticScratchBytes)
+    return set_error(NECTB_ERR_TOO_LARGE,
+                     "batch needs %zu bytes of scratch; the static scratch holds %zu (at most 262,144 rays on a "
+                     "1024x1024 detector); use nectb_train_step with a caller workspace",
+                     need, kStaticScratchBytes);
+  void* scratch = nullptr;
+  if (int rc = scratch_address(&scratch)) return rc;
+  return nectb_train_step(geometry, grid, mlp, grid_params, mlp_params, batch, grid_grad, mlp_grad, y_pred, loss,
+                          scratch, kStaticScratchBytes, stream);
+}
