@@ -44,6 +44,7 @@ template <int D>
 struct LevelCorners {
   uint32_t idx[1 << D];  // entry index within the level
   float w[1 << D];
+  uint64_t cell;         // spatial cell (z, y, x) packed 21 bits per axis
 };
 
 template <int D>
@@ -59,6 +60,7 @@ __device__ __forceinline__ void level_corners(const GridDev& g, int l, const flo
     c[k] = ci;
     f[k] = p - (float)ci;
   }
+  lc.cell = (uint64_t)(uint32_t)c[0] | ((uint64_t)(uint32_t)c[1] << 21) | ((uint64_t)(uint32_t)c[2] << 42);
   const bool hashed = (g.hashed_bits >> l) & 1u;
   // Per-axis terms of the lower/upper vertex: the hash XORs v_k * pi_k and the
   // dense index adds v_k * stride_k, and (c+1)*m = c*m + m in 32-bit
@@ -187,6 +189,83 @@ __device__ __forceinline__ void scatter_point(const GridDev& g, float* __restric
       } else {
 #pragma unroll
         for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * d[f]);
+      }
+    }
+  }
+}
+
+// Levels on which the 32 consecutive samples a warp holds of one ray share
+// cells: expected samples per cell = 1 / (res * (|dx| + |dy| + |dz|)) in
+// normalised coordinates.  Bit l is set when that exceeds ~1.3.
+__device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, double dy, double dz) {
+  const float cross = (float)(fabs(dx) + fabs(dy) + fabs(dz));
+  uint32_t m = 0;
+  for (int l = 0; l < g.n_levels; ++l)
+    if ((float)g.res[l][0] * cross < 0.75f) m |= 1u << l;
+  return m;
+}
+
+// Warp-cooperative gradient scatter of 32 samples of one ray (all lanes call;
+// `valid` masks lanes without a sample).  On levels in agg_levels, lanes in the
+// same cell form contiguous runs along the ray; each run's contributions to
+// each corner are summed with a segmented shuffle reduction and written by the
+// run's first lane, so the table sees one atomic per (cell, corner) instead of
+// one per sample.  Other levels scatter per sample.  Sums equal the
+// per-sample atomics up to fp32 reassociation.
+template <int D, int F>
+__device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict__ grad, const float* x, bool valid,
+                                             const float* dsrc, int stride, uint32_t agg_levels) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll 1
+  for (int l = 0; l < g.n_levels; ++l) {
+    LevelCorners<D> lc;
+    level_corners<D>(g, l, x, lc);
+    float d[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[(l * F + f) * stride] : 0.f;
+    float* base = grad + g.offset[l] * F;
+    if ((agg_levels >> l) & 1u) {
+      // runs of lanes in the same spatial cell (t is the same for the whole
+      // batch, so the spatial cell fixes every corner index)
+      const uint64_t key = valid ? lc.cell : ~uint64_t(0);
+      const uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
+      const bool head = (lane == 0) || (prev != key);
+      const uint32_t heads = __ballot_sync(0xffffffffu, head);
+      const uint32_t later = heads & ~((2u << lane) - 1u);
+      const int end = later ? (__ffs(later) - 2) : 31;
+#pragma unroll
+      for (int c = 0; c < (1 << D); ++c) {
+        float v[F];
+#pragma unroll
+        for (int f = 0; f < F; ++f) v[f] = lc.w[c] * d[f];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+          for (int f = 0; f < F; ++f) {
+            const float tv = __shfl_down_sync(0xffffffffu, v[f], o);
+            if (lane + o <= end) v[f] += tv;
+          }
+        }
+        if (head && valid) {
+          float* dst = base + (int64_t)lc.idx[c] * F;
+          if constexpr (F == 2) atomicAdd(reinterpret_cast<float2*>(dst), make_float2(v[0], v[1]));
+          else if constexpr (F == 4) atomicAdd(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
+          else
+#pragma unroll
+            for (int f = 0; f < F; ++f) atomicAdd(dst + f, v[f]);
+        }
+      }
+    } else if (valid) {
+#pragma unroll
+      for (int c = 0; c < (1 << D); ++c) {
+        float* dst = base + (int64_t)lc.idx[c] * F;
+        if constexpr (F == 2) atomicAdd(reinterpret_cast<float2*>(dst), make_float2(lc.w[c] * d[0], lc.w[c] * d[1]));
+        else if constexpr (F == 4)
+          atomicAdd(reinterpret_cast<float4*>(dst),
+                    make_float4(lc.w[c] * d[0], lc.w[c] * d[1], lc.w[c] * d[2], lc.w[c] * d[3]));
+        else
+#pragma unroll
+          for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * d[f]);
       }
     }
   }

@@ -172,7 +172,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     const bool active = next_chunk(cur, recs, ctrl, slot, a, by_pixel, lane);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
-    float p[4];
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
@@ -312,7 +312,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
-    float p[4];
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
@@ -445,7 +445,8 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 #pragma unroll
     for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, dx + 16 * c);
     tc::tmem_wait_ld();
-    if (valid) scatter_point<D, F>(grid, table_grad, p, dx, 1);
+    scatter_warp<D, F>(grid, table_grad, p, valid, dx, 1,
+                       active ? run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u);
     tc::fence_before();
     __syncthreads();
     if (active) cur.base += 32;

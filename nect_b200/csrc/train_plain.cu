@@ -90,7 +90,7 @@ fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     float sum = 0.f;
     for (int base = 0; base < rec.count; base += 32) {
       const int i = base + lane;
-      float p[4];
+      float p[4] = {0.f, 0.f, 0.f, 0.f};
       bool valid = false;
       if (i < rec.count) valid = sample_point(rec, i, p);
       if (D == 4) p[3] = a.t;
@@ -217,7 +217,7 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     if (!__syncthreads_or(warp_active)) break;
 
     const int i = base + lane;
-    float p[4];
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (warp_active && i < rec.count) valid = sample_point(rec, i, p);
     if (D == 4) p[3] = a.t;
@@ -260,7 +260,9 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     g0.add(G, sX);
     // dX = W_0^T G_1 (W_0 is [64][IN] = M[j][i]) into G2, then scatter
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
-    if (valid) scatter_point<D, F>(grid, table_grad, p, G2 + t, LD);
+    // per-sample atomics: the SIMT path is issue-bound and the run reduction's
+    // shuffles cost it more than the atomics they save (measured)
+    scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, LD, 0u);
     __syncthreads();
     base += 32;
   }
