@@ -154,6 +154,51 @@ int nectb_model_forward(const NectbHashGrid* grid, const NectbMLP* mlp,
                         const float* x, int64_t n, float t, float* sigma,
                         void* stream);
 
+/* ---- queries -------------------------------------------------------------- */
+/* One work item of a query: an nu x nv grid of points
+ * x(i, j) = origin + i*du + j*dv (normalised (z,y,x) coordinates, i fast),
+ * evaluated at time t and written as sigma*out_scale + out_offset to
+ * out[j*out_stride + i].  Slices (axis-aligned or oblique) are one or more
+ * items; a volume export is one item per z-slice.  The scale/offset carry the
+ * reference's de-normalisation /max_distance_traveled*(max-min)+min
+ * (nect/static_export.py:139-140, nect/trainers/base_trainer.py:442-444). */
+typedef struct NectbQueryItem {
+  float origin[3];
+  float du[3];
+  float dv[3];
+  int32_t nu;
+  int32_t nv;
+  float t;
+  float out_scale;
+  float out_offset;
+  float* out;
+  int64_t out_stride;
+  int64_t chunk_begin; /* first 128-point chunk of this item (prefix sum, set by the caller) */
+} NectbQueryItem;
+
+/* Evaluates n_items work items (device array) in one persistent launch; the
+ * items' chunk_begin must be the exclusive prefix sum of ceil(nu*nv/128).
+ * Replaces the per-slice model calls of create_volume / export_volume(s) /
+ * export_video (nect/trainers/base_trainer.py:402-450,
+ * nect/static_export.py:106-144, nect/dynamic_export.py:297-544), which
+ * materialise coordinate grids and call the model one slice at a time.
+ * counter: one device uint32 the kernel uses as its work cursor (zeroed here). */
+int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                       const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
+                       int64_t total_chunks, unsigned int* counter, void* stream);
+
+/* Re-projection of the model: line integrals for every detector pixel of a
+ * view at (angle, t), y[p] = sum_s sigma * distances/max_distance_traveled
+ * with the training sampler (no jitter, no detector offset), i.e. the
+ * reference's training forward (base_trainer.py:520-554) without the loss.
+ * The reference has no standalone re-projection query.  workspace:
+ * nectb_train_workspace_bytes(geometry, grid, mlp, P) bytes. */
+int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                          const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
+                          float angle_rad, float t, int32_t num_points_per_ray,
+                          float max_ray_distance_per_point, float max_distance_traveled,
+                          float* out, void* workspace, size_t workspace_bytes, void* stream);
+
 /* ---- fused training step ------------------------------------------------ */
 /* One batch of rays from one projection.  Fuses Projector.__call__
  * (nect/sampling/projector.py:102-131), the zero-point mask and chunked

@@ -1,0 +1,398 @@
+// Query kernels: slice / volume points and detector re-projections of a
+// trained model.
+//
+// nectb_query_points runs one persistent launch over the 128-point chunks of
+// any number of work items (slices, volume slabs) of any number of requests:
+// each block takes chunks from an atomic cursor, finds the chunk's item by
+// binary search over the items' chunk offsets, generates the points from the
+// item's origin and step vectors (no coordinate arrays in memory), evaluates
+// the model and writes de-normalised values.  The mixed model runs its MLP on
+// tcgen05 (the forward tile of the training kernel); the plain model the fp32
+// SIMT MLP.  nectb_query_reproject reuses the fused training forward over all
+// detector pixels of a view.
+#include <algorithm>
+
+#include "mlp_simt.cuh"
+#include "tcgen05.cuh"
+#include "train_common.cuh"
+
+namespace nectb {
+
+int validate_geometry(const NectbGeometry* g);
+int validate_mlp(const NectbMLP* m, const GridDev& g);
+int64_t mlp_param_count(const NectbMLP* m);
+int train_forward_only(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const void* table,
+                       const float* W, const TrainArgs& a, Workspace ws, float* y_pred, float* loss, cudaStream_t s);
+
+namespace {
+
+constexpr int kQThreads = 128;
+constexpr uint32_t kQTile = 128 * 128;
+constexpr uint32_t kQWTile = 64 * 128;
+
+__device__ __forceinline__ int find_item(const NectbQueryItem* __restrict__ items, int n, int64_t chunk) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (items[mid].chunk_begin <= chunk)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  return lo;
+}
+
+struct QPoint {
+  float p[4];
+  bool valid;
+  float* dst;
+  float scale, offset;
+};
+
+__device__ __forceinline__ QPoint query_point(const NectbQueryItem& it, int64_t chunk, int t) {
+  QPoint q;
+  const int64_t k = (chunk - it.chunk_begin) * 128 + t;
+  const int64_t n = (int64_t)it.nu * it.nv;
+  q.valid = k < n;
+  q.p[0] = q.p[1] = q.p[2] = 0.f;
+  q.p[3] = it.t;
+  q.dst = nullptr;
+  q.scale = it.out_scale;
+  q.offset = it.out_offset;
+  if (q.valid) {
+    const int i = (int)(k % it.nu), j = (int)(k / it.nu);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) q.p[a] = clamp01f(it.origin[a] + (float)i * it.du[a] + (float)j * it.dv[a]);
+    q.dst = it.out + (int64_t)j * it.out_stride + i;
+  }
+  return q;
+}
+
+__device__ __forceinline__ uint8_t* qalign1024(uint8_t* p) {
+  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
+}
+
+template <int D, int F>
+__global__ void __launch_bounds__(kQThreads, 2)
+query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W,
+                   const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
+                   unsigned int* __restrict__ counter, int out_act) {
+  constexpr int IN = 16 * F;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = qalign1024(smem_raw);
+  uint8_t* sW0 = base;
+  uint8_t* sW1 = sW0 + kQWTile;
+  uint8_t* sX = sW1 + kQWTile;
+  uint8_t* sA = sX + kQTile;
+  float* sWout = reinterpret_cast<float*>(sA + kQTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  long long* s_chunk = reinterpret_cast<long long*>(tslot + 2);
+  int* s_item = reinterpret_cast<int*>(s_chunk + 1);
+
+  const int t = threadIdx.x, warp = t >> 5;
+  // fp32 weights -> bf16 swizzled tiles (same layout as the training kernels)
+  for (int e = t; e < 64 * (IN / 8); e += kQThreads) {
+    const int o = e / (IN / 8), j = e % (IN / 8);
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
+    tc::st_chunk_bf16(sW0, o, j, v);
+  }
+  for (int e = t; e < 64 * 8; e += kQThreads) {
+    const int o = e / 8, j = e % 8;
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = W[64 * IN + o * 64 + 8 * j + q];
+    tc::st_chunk_bf16(sW1, o, j, v);
+  }
+  for (int e = t; e < 64; e += kQThreads) sWout[e] = W[64 * IN + 64 * 64 + e];
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 128);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) tc::mbar_init(bar, 1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tm = *tslot;
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
+  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA);
+  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
+  uint32_t phase = 0;
+  bool timed_out = false;
+  while (true) {
+    if (t == 0) {
+      const long long c = (long long)atomicAdd(counter, 1u);
+      *s_chunk = c;
+      *s_item = c < total_chunks ? find_item(items, n_items, c) : 0;
+    }
+    __syncthreads();
+    const long long chunk = *s_chunk;
+    if (chunk >= total_chunks) break;
+    const QPoint q = query_point(items[*s_item], chunk, t);
+    // the encoder's row writer (fp16 gathers, bf16 row)
+    {
+      constexpr int LPC = 8 / F;
+#pragma unroll 1
+      for (int j = 0; j < 16 / LPC; ++j) {
+        float v[8];
+        if (q.valid) {
+#pragma unroll
+          for (int qq = 0; qq < LPC; ++qq) {
+            const int l = j * LPC + qq;
+            LevelCorners<D> lc;
+            level_corners<D>(grid, l, q.p, lc);
+            float vals[1 << D][F];
+#pragma unroll
+            for (int c = 0; c < (1 << D); ++c) Feat<F, __half>::load(table, grid.offset[l] + lc.idx[c], vals[c]);
+#pragma unroll
+            for (int f = 0; f < F; ++f) {
+              float acc = 0.f;
+#pragma unroll
+              for (int c = 0; c < (1 << D); ++c) acc = fmaf(lc.w[c], vals[c][f], acc);
+              v[qq * F + f] = acc;
+            }
+          }
+        } else {
+#pragma unroll
+          for (int qq = 0; qq < 8; ++qq) v[qq] = 0.f;
+        }
+        tc::st_chunk_bf16(sX, t, j, v);
+      }
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), idesc, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+    float h[64];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) tc::tmem_ld16(my_lanes + 16 * c, h + 16 * c);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      float v[8];
+#pragma unroll
+      for (int qq = 0; qq < 8; ++qq) v[qq] = fmaxf(h[8 * j + qq], 0.f);
+      tc::st_chunk_bf16(sA, t, j, v);
+    }
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+#pragma unroll
+      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), idesc, k > 0);
+      tc::commit(bar);
+    }
+    timed_out = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(timed_out)) {
+      timed_out = true;
+      break;
+    }
+    tc::fence_after();
+#pragma unroll
+    for (int c = 0; c < 4; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, h + 16 * c);
+    tc::tmem_wait_ld();
+    float z = 0.f;
+#pragma unroll
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    if (q.valid) *q.dst = fmaf(act_fwd(z, out_act), q.scale, q.offset);
+    tc::fence_before();
+    __syncthreads();
+  }
+  if (timed_out) tc::mbar_wait(bar, phase);
+  tc::fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tm, 128);
+  }
+}
+
+template <int D, int F, typename T, int H>
+__global__ void __launch_bounds__(kQThreads)
+query_plain_kernel(GridDev grid, const T* __restrict__ table, const float* __restrict__ W,
+                   const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
+                   unsigned int* __restrict__ counter, int act, int out_act) {
+  constexpr int IN = 16 * F;
+  constexpr int LD = kQThreads + 4;
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const SimtWeights sw = stage_weights<IN, H, false>(W, smem);
+  float* xe = smem + simt_weight_floats<IN, H, false>() + threadIdx.x;
+  float* hid = xe + IN * LD;
+  __shared__ long long s_chunk;
+  __shared__ int s_item;
+  const int t = threadIdx.x;
+  __syncthreads();
+  while (true) {
+    if (t == 0) {
+      const long long c = (long long)atomicAdd(counter, 1u);
+      s_chunk = c;
+      s_item = c < total_chunks ? find_item(items, n_items, c) : 0;
+    }
+    __syncthreads();
+    const long long chunk = s_chunk;
+    if (chunk >= total_chunks) break;
+    const QPoint q = query_point(items[s_item], chunk, t);
+    if (q.valid) {
+      encode_point<D, F, T>(grid, table, q.p, xe, LD);
+      float z;
+      if (H == 1) {
+        z = gemv_dot<IN, LD>(sw.WT[0], xe, sw.wout, act);
+      } else {
+        gemv_cols<IN, kWidth, LD>(sw.WT[0], xe, hid, act);
+#pragma unroll
+        for (int k = 1; k < H - 1; ++k)
+          gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + (k - 1) * kWidth * LD, hid + k * kWidth * LD, act);
+        z = gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + (H - 2) * kWidth * LD, sw.wout, act);
+      }
+      *q.dst = fmaf(act_fwd(z, out_act), q.scale, q.offset);
+    }
+    __syncthreads();
+  }
+}
+
+int sm_count() {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  return sms;
+}
+
+template <int D, int F>
+int launch_query_mixed(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
+                       int64_t chunks, unsigned int* counter, int oact, cudaStream_t s) {
+  auto k = query_mixed_kernel<D, F>;
+  const size_t smem = 1024 + 2 * kQWTile + 2 * kQTile + 64 * 4 + 64;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 2 * sm_count()));
+  ProfScope ps(kProfModel, s);
+  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);
+  return launch_status("query_mixed_kernel");
+}
+
+template <int D, int F, typename T, int H>
+int launch_query_plain(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
+                       int64_t chunks, unsigned int* counter, int act, int oact, cudaStream_t s) {
+  constexpr int IN = 16 * F;
+  auto k = query_plain_kernel<D, F, T, H>;
+  const size_t smem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (kQThreads + 4)) * 4;
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQThreads, smem);
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count() * std::max(per_sm, 1)));
+  ProfScope ps(kProfModel, s);
+  k<<<blocks, kQThreads, smem, s>>>(g, (const T*)table, W, items, n, chunks, counter, act, oact);
+  return launch_status("query_plain_kernel");
+}
+
+}  // namespace
+}  // namespace nectb
+
+using namespace nectb;
+
+extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                  const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
+                                  int64_t total_chunks, unsigned int* counter, void* stream) {
+  clear_error();
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  if (int rc = validate_mlp(mlp, g)) return rc;
+  NECTB_REQUIRE(g.n_levels == 16, "queries need n_levels == 16");
+  if (n_items == 0 || total_chunks == 0) return NECTB_OK;
+  NECTB_REQUIRE(grid_params && mlp_params && items && counter && n_items > 0 && total_chunks > 0,
+                "null pointer or empty query");
+  NECTB_REQUIRE(total_chunks < (int64_t(1) << 31), "too many chunks in one launch");
+  cudaStream_t s = (cudaStream_t)stream;
+  if (int rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s), "memset query counter")) return rc;
+  const int D = g.n_dims, F = g.n_features, H = mlp->n_hidden_layers;
+  const bool mixed = mlp->compute_dtype != NECTB_F32;
+  if (mixed) {
+    NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
+    NECTB_REQUIRE(H == 2 && mlp->activation == NECTB_ACT_RELU, "mixed queries need 2 hidden ReLU layers");
+    if (D == 3 && F == 2)
+      return launch_query_mixed<3, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                      mlp->output_activation, s);
+    if (D == 4 && F == 2)
+      return launch_query_mixed<4, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                      mlp->output_activation, s);
+  } else {
+    const int act = mlp->activation, oact = mlp->output_activation;
+    const bool h = grid->feature_dtype == NECTB_F16;
+    if (D == 3 && F == 2 && H == 2)
+      return h ? launch_query_plain<3, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
+                                                     counter, act, oact, s)
+               : launch_query_plain<3, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
+                                                    counter, act, oact, s);
+    if (D == 4 && F == 2 && H == 2)
+      return h ? launch_query_plain<4, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
+                                                     counter, act, oact, s)
+               : launch_query_plain<4, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
+                                                    counter, act, oact, s);
+  }
+  return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, hidden %d)", D,
+                   F, H);
+}
+
+extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                     const void* grid_params, const float* mlp_params, float angle_rad, float t,
+                                     int32_t num_points_per_ray, float max_ray_distance_per_point,
+                                     float max_distance_traveled, float* out, void* workspace,
+                                     size_t workspace_size, void* stream) {
+  clear_error();
+  if (int rc = validate_geometry(geometry)) return rc;
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  if (int rc = validate_mlp(mlp, g)) return rc;
+  NECTB_REQUIRE(grid_params && mlp_params && out, "null pointer");
+  NECTB_REQUIRE(num_points_per_ray >= 1 && max_distance_traveled > 0.f, "bad sampling parameters");
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  if (!workspace || workspace_size < workspace_bytes(P, P))
+    return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
+                     workspace_bytes(P, P));
+  TrainArgs a;
+  a.perm = nullptr;  // every pixel, in pixel order
+  a.perm_len = P;
+  a.start = 0;
+  a.num_rays = P;
+  a.n_pixels = P;
+  a.S = num_points_per_ray;
+  a.angle = angle_rad;
+  a.t = t;
+  a.maxd = max_ray_distance_per_point;
+  a.uniform = 1;
+  a.max_dist = max_distance_traveled;
+  a.jitter = nullptr;
+  a.det_off = nullptr;
+  a.projection = nullptr;
+  a.loss_type = 2;
+  a.loss_scale = 0.f;
+  Workspace ws = carve_workspace(workspace, P, P);
+  cudaStream_t s = (cudaStream_t)stream;
+  float* loss = reinterpret_cast<float*>(ws.counters + 8);
+  if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
+  if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
+  {
+    ProfScope ps(kProfRayPrep, s);
+    ray_prep_kernel<<<(unsigned)ceil_div(P, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters, out, loss);
+  }
+  if (int rc = launch_status("ray_prep_kernel")) return rc;
+  return train_forward_only(*geometry, g, *mlp, grid_params, mlp_params, a, ws, out, loss, s);
+}

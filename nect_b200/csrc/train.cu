@@ -40,6 +40,18 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 }
 
 }  // namespace
+
+// Forward kernels only (y_pred and loss; no gradients) after ray_prep_kernel
+// has filled the workspace: used by re-projection queries.
+int train_forward_only(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const void* table,
+                       const float* W, const TrainArgs& a, Workspace ws, float* y_pred, float* loss,
+                       cudaStream_t s) {
+  const int nW = (int)mlp_param_count(&mlp);
+  if (mlp.compute_dtype == NECTB_F32)
+    return train_plain(geo, grid, mlp, (const float*)table, W, nW, a, ws, nullptr, nullptr, y_pred, loss, s);
+  return train_mixed(geo, grid, mlp, table, W, nW, a, ws, nullptr, nullptr, y_pred, loss, s);
+}
+
 }  // namespace nectb
 
 using namespace nectb;

@@ -506,6 +506,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
   }
   if (int rc = launch_status("fwd_mixed_kernel")) return rc;
+  if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)
   {
     auto k = bwd_mixed_kernel<D, F>;
     // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM

@@ -28,10 +28,19 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
   RaySetup r;
   r.valid = 0;
   r.distance = 0.f;
-  const bool ok = ray_lookup(a.perm, a.perm_len, a.start, tid, a.num_rays, g, ray_index);
+  // perm == nullptr: every detector pixel in order (re-projection queries);
+  // jitter / detector offsets default to 0 when absent.
+  bool ok;
+  if (a.perm) {
+    ok = ray_lookup(a.perm, a.perm_len, a.start, tid, a.num_rays, g, ray_index);
+  } else {
+    ray_index = tid;
+    ok = tid < a.n_pixels;
+  }
   if (ok)
-    ray_setup(g, ray_index, a.det_off[2 * (int64_t)tid], a.det_off[2 * (int64_t)tid + 1], a.jitter[tid], a.angle,
-              a.S, a.maxd, a.uniform != 0, r);
+    ray_setup(g, ray_index, a.det_off ? a.det_off[2 * (int64_t)tid] : 0.f,
+              a.det_off ? a.det_off[2 * (int64_t)tid + 1] : 0.f, a.jitter ? a.jitter[tid] : 0.f, a.angle, a.S,
+              a.maxd, a.uniform != 0, r);
   int count = 0;
   if (r.valid) count = warp_sample_count(g, r, a.S, lane);
   if (lane == 0) {
@@ -47,7 +56,7 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
     // proj[perm[start:start+R]] (projector.py:130); rays past the end of the
     // permutation are not part of the reference batch and get y = 0 here.
     const bool in_range = ok && ray_index >= 0;
-    rec.y = in_range ? a.projection[ray_index] : 0.f;
+    rec.y = (in_range && a.projection) ? a.projection[ray_index] : 0.f;
     rec.gsig = 0.f;
     if (count > 0) {
       if (atomicCAS(slot + ray_index, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
@@ -305,6 +314,7 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
     fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred, loss);
   }
   if (int rc = launch_status("fwd_plain_kernel")) return rc;
+  if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)
 
   constexpr int NT = 128;
   auto bk = bwd_plain_kernel<D, F, IN, H, NT>;
