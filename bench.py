@@ -439,5 +439,117 @@ def main():
         dist.destroy_process_group()
 
 
+def run_serving(args):
+    """Query serving of the 4D dynamic cone-beam model (16 x 2 fp16 features,
+    2^21 entries per level, 2 x 64 MLP): a seeded Poisson request stream, and
+    the same request classes answered one at a time by the plain fp32 model.
+    Weights are seeded random values of the trained model's architecture
+    (serving cost does not depend on the values)."""
+    from nect_b200.config import get_model
+    from nect_b200.sampling import Geometry
+    from nect_b200.serving import QueryServer, Request, reproject, query_points, slice_items, volume_items
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    spec = workload_spec("c3_dynamic_cone", "mixed")
+    geometry = Geometry(**spec["geo"])
+    S = spec["S"]
+    model = get_model(spec["model"], device=dev)
+    rng = np.random.default_rng(0)
+    n_req = int(args.serve_rate * args.serve_seconds)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
+    reqs = []
+    for k in range(n_req):
+        u = rng.random()
+        t = float(rng.random())
+        if args.serve_mix == "no_reproject" and 0.6 <= u < 0.9:
+            u = 0.0
+        if u < 0.6:
+            size = int(rng.choice([256, 384, 512, 768, 1024]))
+            if rng.random() < 0.5:
+                axis = int(rng.integers(3))
+                uu, vv = [(0.0, 0.0, 1.0), (0.0, 1.0, 0.0)], None
+                basis = np.eye(3)
+                others = [b for b in range(3) if b != axis]
+                uu, vv = tuple(basis[others[1]]), tuple(basis[others[0]])
+            else:
+                q = rng.normal(size=(2, 3))
+                uu = q[0] / np.linalg.norm(q[0])
+                vv = q[1] - (q[1] @ uu) * uu
+                vv = tuple(vv / np.linalg.norm(vv))
+                uu = tuple(uu)
+            reqs.append(dict(kind="slice", size=size, t=t, centre=tuple(0.3 + 0.4 * rng.random(3)), u=uu, v=vv))
+        elif u < 0.9:
+            reqs.append(dict(kind="reproject", t=t, angle=float(rng.random() * 2 * math.pi)))
+        else:
+            reqs.append(dict(kind="volume", size=256, t=t))
+    srv = QueryServer(model, geometry, memory_budget=40 << 30, points_per_ray=S)
+    warm = [srv.submit(Request(**d)) for d in reqs[:6]]
+    for r in warm:
+        r.event.wait(120)
+    srv.completed.clear()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    submitted = []
+    for d, ta in zip(reqs, arrivals):
+        delay = t0 + ta - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        submitted.append(srv.submit(Request(**d)))
+    for r in submitted:
+        r.event.wait(600)
+    makespan = max(r.done for r in submitted) - t0
+    srv.close()
+    stats = srv.latency_stats()
+    s512 = np.array([r.latency_ms() for r in submitted if r.kind == "slice" and r.size == 512])
+    w512 = np.array([r.wait_ms() for r in submitted if r.kind == "slice" and r.size == 512])
+    voxels = sum(int(np.prod(r.out_shape(geometry))) for r in submitted)
+
+    # one request at a time, plain fp32 model of the same architecture
+    plain_cfg = workload_spec("c3_dynamic_cone", "plain_fp32")["model"]
+    pm = get_model(plain_cfg, device=dev)
+    base = {}
+    for kind, n in (("slice", 10), ("reproject", 4), ("volume", 2)):
+        lat = []
+        for k in range(n + 1):
+            torch.cuda.synchronize()
+            a = time.perf_counter()
+            if kind == "slice":
+                out = torch.empty(512, 512, device=dev)
+                query_points(pm, slice_items(out, out.shape, 0.5))
+            elif kind == "reproject":
+                out = reproject(pm, geometry, 0.3 * k, 0.5, S)
+            else:
+                out = torch.empty(256, 256, 256, device=dev)
+                query_points(pm, volume_items(out, out.shape, 0.5))
+            host = out.cpu()
+            torch.cuda.synchronize()
+            if k:
+                lat.append((time.perf_counter() - a) * 1e3)
+        base[kind] = {"n": n, "p50_ms": float(np.percentile(lat, 50))}
+    print(json.dumps({
+        "metric": "query latency p50/p99 (serving, 4D model)", "unit": "ms", "higher_is_better": False,
+        "value": float(np.percentile(s512, 99)) if s512.size else None, "value_is": "p99 of 512^2 slices",
+        "n_gpus": 1, "requests": n_req, "rate_per_s": args.serve_rate, "seconds": args.serve_seconds,
+        "makespan_s": makespan, "voxels_per_s": voxels / makespan, "classes": stats,
+        "slice512": {"n": int(s512.size), "p50_ms": float(np.percentile(s512, 50)) if s512.size else None,
+                     "p99_ms": float(np.percentile(s512, 99)) if s512.size else None,
+                     "wait_p99_ms": float(np.percentile(w512, 99)) if w512.size else None},
+        "one_at_a_time_plain_fp32": base,
+        "config": {"workload": "4D cone 512x512, 2^21 x 16 x 2 fp16, MLP 2x64 (bf16 tensor cores); requests: "
+                               "60% slices 256^2-1024^2 axis/oblique, 30% re-projections 512^2 (S=512), "
+                               "10% volumes 256^3, random t; 40 GB admission budget",
+                   "data": "synthetic (seeded random weights of the trained architecture)"},
+    }))
+
+
 if __name__ == "__main__":
-    main()
+    if "--serving" in sys.argv:
+        ap = argparse.ArgumentParser()
+        ap.add_argument("--serving", action="store_true")
+        ap.add_argument("--serve-rate", type=float, default=200.0)
+        ap.add_argument("--serve-seconds", type=float, default=5.0)
+        ap.add_argument("--serve-mix", default="full", choices=["full", "no_reproject"])
+        run_serving(ap.parse_args())
+    else:
+        main()

@@ -185,19 +185,22 @@ typedef struct NectbQueryItem {
  * counter: one device uint32 the kernel uses as its work cursor (zeroed here). */
 int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
                        const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
-                       int64_t total_chunks, unsigned int* counter, void* stream);
+                       int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream);
 
 /* Re-projection of the model: line integrals for every detector pixel of a
  * view at (angle, t), y[p] = sum_s sigma * distances/max_distance_traveled
  * with the training sampler (no jitter, no detector offset), i.e. the
  * reference's training forward (base_trainer.py:520-554) without the loss.
  * The reference has no standalone re-projection query.  workspace:
- * nectb_train_workspace_bytes(geometry, grid, mlp, P) bytes. */
+ * nectb_train_workspace_bytes(geometry, grid, mlp, P) bytes.
+ * max_blocks > 0 caps the persistent grid of either query (a server keeps
+ * SMs free for latency-critical launches on higher-priority streams). */
 int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid,
                           const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
                           float angle_rad, float t, int32_t num_points_per_ray,
                           float max_ray_distance_per_point, float max_distance_traveled,
-                          float* out, void* workspace, size_t workspace_bytes, void* stream);
+                          float* out, void* workspace, size_t workspace_bytes, int32_t max_blocks,
+                          void* stream);
 
 /* ---- fused training step ------------------------------------------------ */
 /* One batch of rays from one projection.  Fuses Projector.__call__

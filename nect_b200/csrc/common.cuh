@@ -24,6 +24,21 @@ inline int launch_status(const char* what) { return cuda_status(cudaGetLastError
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Sets a kernel's dynamic shared memory and its L1/shared split.  An SM keeps
+// one split while any block is resident, so a kernel that shares SMs with
+// other launches (a capped background grid, serving queries) asks for a split
+// with room for three ~51 KB blocks (164 of 228 KB, 92 KB left as L1):
+// otherwise the split sized for it alone leaves no room for another kernel's
+// blocks until the SM drains.  Kernels that own the GPU keep the driver's
+// default split.
+constexpr int kSharedCarveoutPercent = 72;
+template <typename K>
+inline void set_smem(K k, size_t bytes, bool shares_sms) {
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
+                       shares_sms ? kSharedCarveoutPercent : (int)cudaSharedmemCarveoutDefault);
+}
+
 // Records CUDA events around a kernel launch while profiling is enabled
 // (nectb_profile_enable); slots are listed in include/nectb.h.
 enum { kProfRayPrep = 0, kProfForward = 1, kProfBackward = 2, kProfAdam = 3, kProfSample = 4, kProfModel = 5 };

@@ -278,11 +278,12 @@ int sm_count() {
 
 template <int D, int F>
 int launch_query_mixed(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
-                       int64_t chunks, unsigned int* counter, int oact, cudaStream_t s) {
+                       int64_t chunks, unsigned int* counter, int oact, int max_blocks, cudaStream_t s) {
   auto k = query_mixed_kernel<D, F>;
   const size_t smem = 1024 + 2 * kQWTile + 2 * kQTile + 64 * 4 + 64;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 2 * sm_count()));
+  set_smem(k, smem, true);
+  int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 2 * sm_count()));
+  if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   ProfScope ps(kProfModel, s);
   k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);
   return launch_status("query_mixed_kernel");
@@ -290,14 +291,15 @@ int launch_query_mixed(const GridDev& g, const void* table, const float* W, cons
 
 template <int D, int F, typename T, int H>
 int launch_query_plain(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
-                       int64_t chunks, unsigned int* counter, int act, int oact, cudaStream_t s) {
+                       int64_t chunks, unsigned int* counter, int act, int oact, int max_blocks, cudaStream_t s) {
   constexpr int IN = 16 * F;
   auto k = query_plain_kernel<D, F, T, H>;
   const size_t smem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (kQThreads + 4)) * 4;
-  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  set_smem(k, smem, true);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQThreads, smem);
-  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count() * std::max(per_sm, 1)));
+  int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count() * std::max(per_sm, 1)));
+  if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   ProfScope ps(kProfModel, s);
   k<<<blocks, kQThreads, smem, s>>>(g, (const T*)table, W, items, n, chunks, counter, act, oact);
   return launch_status("query_plain_kernel");
@@ -310,7 +312,7 @@ using namespace nectb;
 
 extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
                                   const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
-                                  int64_t total_chunks, unsigned int* counter, void* stream) {
+                                  int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream) {
   clear_error();
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
@@ -329,23 +331,23 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
     NECTB_REQUIRE(H == 2 && mlp->activation == NECTB_ACT_RELU, "mixed queries need 2 hidden ReLU layers");
     if (D == 3 && F == 2)
       return launch_query_mixed<3, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                      mlp->output_activation, s);
+                                      mlp->output_activation, max_blocks, s);
     if (D == 4 && F == 2)
       return launch_query_mixed<4, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                      mlp->output_activation, s);
+                                      mlp->output_activation, max_blocks, s);
   } else {
     const int act = mlp->activation, oact = mlp->output_activation;
     const bool h = grid->feature_dtype == NECTB_F16;
     if (D == 3 && F == 2 && H == 2)
       return h ? launch_query_plain<3, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                     counter, act, oact, s)
+                                                     counter, act, oact, max_blocks, s)
                : launch_query_plain<3, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                    counter, act, oact, s);
+                                                    counter, act, oact, max_blocks, s);
     if (D == 4 && F == 2 && H == 2)
       return h ? launch_query_plain<4, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                     counter, act, oact, s)
+                                                     counter, act, oact, max_blocks, s)
                : launch_query_plain<4, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                    counter, act, oact, s);
+                                                    counter, act, oact, max_blocks, s);
   }
   return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, hidden %d)", D,
                    F, H);
@@ -355,7 +357,7 @@ extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbH
                                      const void* grid_params, const float* mlp_params, float angle_rad, float t,
                                      int32_t num_points_per_ray, float max_ray_distance_per_point,
                                      float max_distance_traveled, float* out, void* workspace,
-                                     size_t workspace_size, void* stream) {
+                                     size_t workspace_size, int32_t max_blocks, void* stream) {
   clear_error();
   if (int rc = validate_geometry(geometry)) return rc;
   GridDev g;
@@ -384,6 +386,7 @@ extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbH
   a.projection = nullptr;
   a.loss_type = 2;
   a.loss_scale = 0.f;
+  a.max_blocks = max_blocks;
   Workspace ws = carve_workspace(workspace, P, P);
   cudaStream_t s = (cudaStream_t)stream;
   float* loss = reinterpret_cast<float*>(ws.counters + 8);

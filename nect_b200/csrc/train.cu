@@ -105,6 +105,7 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   a.projection = batch->projection;
   a.loss_type = batch->loss_type;
   a.loss_scale = batch->loss_scale;
+  a.max_blocks = 0;
   Workspace ws = carve_workspace(workspace, a.num_rays, P);
   if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
   if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;

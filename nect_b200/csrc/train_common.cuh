@@ -39,6 +39,7 @@ struct TrainArgs {
   const float* projection;
   int loss_type;
   float loss_scale;
+  int max_blocks;  // > 0: cap on the persistent grids (queries); 0: default
 };
 
 enum : unsigned int { kFlagDuplicatePixels = 1u };

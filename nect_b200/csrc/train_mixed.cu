@@ -497,11 +497,12 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   (void)geo;
-  const int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
+  int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
+  if (a.max_blocks > 0) blocks = std::min(blocks, a.max_blocks);
   {
     auto k = fwd_mixed_kernel<D, F>;
     const size_t smem = 1024 + 2 * kWTile + 2 * kTile + 64 * 4 + 64;
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    set_smem(k, smem, a.max_blocks > 0);
     ProfScope ps(kProfForward, s);
     k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
   }

@@ -305,10 +305,11 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   constexpr int FNT = kPlainFwdThreads;
   auto fk = fwd_plain_kernel<D, F, IN, H>;
   const size_t fsmem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (FNT + 4)) * 4;
-  cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsmem);
+  set_smem(fk, fsmem, a.max_blocks > 0);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, FNT, fsmem);
-  const int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
+  int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
+  if (a.max_blocks > 0) fblocks = std::min(fblocks, a.max_blocks);
   {
     ProfScope ps(kProfForward, s);
     fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred, loss);

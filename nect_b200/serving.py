@@ -6,20 +6,23 @@ export_volume, nect/static_export.py:15-144; export_volumes/_at_timesteps and
 export_video, nect/dynamic_export.py:145-544).  Here:
 
 * ``slice_items`` / ``volume_items`` describe the points of a request as
-  compact work items (origin + step vectors); ``query_points`` evaluates any
-  set of items of any requests in ONE persistent launch (nectb_query_points),
-  generating coordinates on the fly and writing de-normalised values
-  (``/max_distance_traveled * (max - min) + min``, as the reference exports).
+  compact work items (origin + step vectors, a numpy table in the layout of
+  NectbQueryItem); ``query_points`` evaluates any set of items of any requests
+  in ONE persistent launch (nectb_query_points), generating coordinates on the
+  fly and writing de-normalised values (``/max_distance_traveled * (max - min)
+  + min``, as the reference exports them).
 * ``reproject`` computes a detector view at (angle, t) with the training
   sampler (nectb_query_reproject).
 * ``QueryServer`` keeps the model on the device and serves a stream of mixed
-  requests: each request is admitted when its output and workspace fit in the
-  memory budget; admitted point requests are cut into chunk slices and packed,
-  several requests per launch, into persistent launches that are replayed from
-  CUDA graphs captured per chunk-count bucket; launches rotate over several
-  streams so new requests start while earlier ones are still running; each
-  request completes when its last launch has finished and its result has been
-  copied to pinned host memory.  Latencies are arrival-to-result.
+  requests (continuous batching): requests are admitted into preallocated
+  device/pinned slots (the memory budget is split into slots per request class
+  at start-up, so serving never allocates), slice requests are packed several
+  per launch on high-priority streams, volume exports (cut into z-slice items)
+  and re-projections run on low-priority streams with their persistent grids
+  capped at one block per SM so slice blocks always find free SMs; point
+  launches are replayed from CUDA graphs captured per chunk-count bucket.  A
+  request completes when its last launch finished and its result reached
+  pinned host memory; latency is arrival-to-result.
 """
 from __future__ import annotations
 
@@ -38,54 +41,23 @@ from .network import _HashGridModel
 
 CHUNK = 128
 
-
-class NectbQueryItem(ctypes.Structure):
-    _fields_ = [
-        ("origin", ctypes.c_float * 3),
-        ("du", ctypes.c_float * 3),
-        ("dv", ctypes.c_float * 3),
-        ("nu", ctypes.c_int32),
-        ("nv", ctypes.c_int32),
-        ("t", ctypes.c_float),
-        ("out_scale", ctypes.c_float),
-        ("out_offset", ctypes.c_float),
-        ("out", ctypes.c_void_p),
-        ("out_stride", ctypes.c_int64),
-        ("chunk_begin", ctypes.c_int64),
-    ]
-
-
-ITEM_BYTES = ctypes.sizeof(NectbQueryItem)
+ITEM_DTYPE = np.dtype({
+    "names": ["origin", "du", "dv", "nu", "nv", "t", "out_scale", "out_offset", "out", "out_stride", "chunk_begin"],
+    "formats": [("<f4", 3), ("<f4", 3), ("<f4", 3), "<i4", "<i4", "<f4", "<f4", "<f4", "<u8", "<i8", "<i8"],
+    "offsets": [0, 12, 24, 36, 40, 44, 48, 52, 56, 64, 72],
+    "itemsize": 80,
+})  # NectbQueryItem (include/nectb.h)
 
 _lib.lib.nectb_query_points.restype = ctypes.c_int32
 _lib.lib.nectb_query_points.argtypes = [ctypes.POINTER(_lib.NectbHashGrid), ctypes.POINTER(_lib.NectbMLP),
                                         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
-                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
+                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
 _lib.lib.nectb_query_reproject.restype = ctypes.c_int32
 _lib.lib.nectb_query_reproject.argtypes = [ctypes.POINTER(_lib.NectbGeometry), ctypes.POINTER(_lib.NectbHashGrid),
                                            ctypes.POINTER(_lib.NectbMLP), ctypes.c_void_p, ctypes.c_void_p,
                                            ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_float,
                                            ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-                                           ctypes.c_void_p]
-
-
-@dataclass
-class Item:
-    """Host description of one work item (an nu x nv grid of points)."""
-    origin: tuple
-    du: tuple
-    dv: tuple
-    nu: int
-    nv: int
-    t: float
-    out: int          # device address of the first output value
-    out_stride: int   # floats between rows
-    scale: float = 1.0
-    offset: float = 0.0
-
-    @property
-    def chunks(self) -> int:
-        return -(-self.nu * self.nv // CHUNK)
+                                           ctypes.c_int32, ctypes.c_void_p]
 
 
 def denormalisation(max_distance_traveled: float, minimum: float = 0.0, maximum: float = 1.0):
@@ -98,80 +70,77 @@ def centres(n: int) -> np.ndarray:
     return (np.arange(n) + 0.5) / n
 
 
-def volume_items(out: torch.Tensor, t: float, scale: float = 1.0, offset: float = 0.0,
-                 rows_per_item: int | None = None) -> list[Item]:
-    """Volume [nz, ny, nx] at voxel centres, z-slices (or slabs of rows) as items."""
-    nz, ny, nx = out.shape
-    rows = rows_per_item or ny
-    items = []
-    base = out.data_ptr()
-    for k in range(nz):
-        for r0 in range(0, ny, rows):
-            nr = min(rows, ny - r0)
-            items.append(Item(origin=((k + 0.5) / nz, (r0 + 0.5) / ny, 0.5 / nx), du=(0.0, 0.0, 1.0 / nx),
-                              dv=(0.0, 1.0 / ny, 0.0), nu=nx, nv=nr, t=t,
-                              out=base + 4 * (k * ny * nx + r0 * nx), out_stride=nx, scale=scale, offset=offset))
-    return items
+def item_chunks(items: np.ndarray) -> np.ndarray:
+    return (items["nu"].astype(np.int64) * items["nv"] + CHUNK - 1) // CHUNK
 
 
-def slice_items(out: torch.Tensor, t: float, centre=(0.5, 0.5, 0.5), u=(0.0, 0.0, 1.0), v=(0.0, 1.0, 0.0),
-                scale: float = 1.0, offset: float = 0.0, rows_per_item: int = 64) -> list[Item]:
-    """n x n plane through ``centre`` spanned by unit vectors u (columns) and v
-    (rows), sampled at cell centres over a unit-sized square (axis-aligned
-    slices reproduce create_volume's grid; oblique ones rotate it)."""
-    nv_, nu_ = out.shape
+def volume_items(out: torch.Tensor | int, shape: tuple, t: float, scale: float = 1.0,
+                 offset: float = 0.0) -> np.ndarray:
+    """Volume [nz, ny, nx] at voxel centres, one item per z-slice; out is the
+    output tensor or its device address."""
+    nz, ny, nx = shape
+    base = out.data_ptr() if isinstance(out, torch.Tensor) else int(out)
+    it = np.zeros(nz, ITEM_DTYPE)
+    it["origin"][:, 0] = (np.arange(nz) + 0.5) / nz
+    it["origin"][:, 1] = 0.5 / ny
+    it["origin"][:, 2] = 0.5 / nx
+    it["du"][:, 2] = 1.0 / nx
+    it["dv"][:, 1] = 1.0 / ny
+    it["nu"], it["nv"], it["t"] = nx, ny, t
+    it["out_scale"], it["out_offset"] = scale, offset
+    it["out"] = base + 4 * np.arange(nz, dtype=np.uint64) * np.uint64(ny * nx)
+    it["out_stride"] = nx
+    return it
+
+
+def slice_items(out: torch.Tensor | int, shape: tuple, t: float, centre=(0.5, 0.5, 0.5), u=(0.0, 0.0, 1.0),
+                v=(0.0, 1.0, 0.0), scale: float = 1.0, offset: float = 0.0, rows_per_item: int = 64) -> np.ndarray:
+    """nv x nu plane through ``centre`` spanned by unit vectors u (columns) and v
+    (rows), sampled at cell centres of a unit square (axis-aligned slices
+    reproduce create_volume's grid; oblique ones rotate it)."""
+    nv_, nu_ = shape
+    base = out.data_ptr() if isinstance(out, torch.Tensor) else int(out)
     c = np.asarray(centre, np.float64)
     u = np.asarray(u, np.float64) / np.linalg.norm(u)
     v = np.asarray(v, np.float64) / np.linalg.norm(v)
-    items = []
-    for r0 in range(0, nv_, rows_per_item):
-        nr = min(rows_per_item, nv_ - r0)
-        o = c + ((0.5 / nu_) - 0.5) * u + ((r0 + 0.5) / nv_ - 0.5) * v
-        items.append(Item(origin=tuple(o), du=tuple(u / nu_), dv=tuple(v / nv_), nu=nu_, nv=nr, t=t,
-                          out=out.data_ptr() + 4 * r0 * nu_, out_stride=nu_, scale=scale, offset=offset))
-    return items
-
-
-def pack_items(items: list[Item]) -> tuple[ctypes.Array, int]:
-    arr = (NectbQueryItem * len(items))()
-    total = 0
-    for i, it in enumerate(items):
-        a = arr[i]
-        for k in range(3):
-            a.origin[k], a.du[k], a.dv[k] = it.origin[k], it.du[k], it.dv[k]
-        a.nu, a.nv, a.t = it.nu, it.nv, it.t
-        a.out_scale, a.out_offset = it.scale, it.offset
-        a.out, a.out_stride, a.chunk_begin = it.out, it.out_stride, total
-        total += it.chunks
-    return arr, total
+    r0 = np.arange(0, nv_, rows_per_item)
+    it = np.zeros(r0.size, ITEM_DTYPE)
+    it["origin"] = c + ((0.5 / nu_) - 0.5) * u + ((r0[:, None] + 0.5) / nv_ - 0.5) * v
+    it["du"], it["dv"] = u / nu_, v / nv_
+    it["nu"], it["nv"], it["t"] = nu_, np.minimum(rows_per_item, nv_ - r0), t
+    it["out_scale"], it["out_offset"] = scale, offset
+    it["out"] = base + 4 * r0.astype(np.uint64) * np.uint64(nu_)
+    it["out_stride"] = nu_
+    return it
 
 
 def _call_points(model: _HashGridModel, items_dev: int, n_items: int, total_chunks: int, counter_dev: int,
-                 stream: int):
+                 stream: int, max_blocks: int = 0):
     rc = _lib.lib.nectb_query_points(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
                                      model.grid_table.data_ptr(), model.mlp.data_ptr(), items_dev, n_items,
-                                     total_chunks, counter_dev, stream)
+                                     total_chunks, counter_dev, max_blocks, stream)
     _lib.check(rc, "nectb_query_points")
 
 
-def query_points(model: _HashGridModel, items: list[Item], stream: torch.cuda.Stream | None = None):
-    """Evaluate the items in one launch on ``stream`` (outputs are written in place)."""
-    if not items:
+def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.Stream | None = None):
+    """Evaluate the items (any requests) in one launch (outputs written in place)."""
+    if items.size == 0:
         return
     stream = stream or torch.cuda.current_stream()
-    arr, total = pack_items(items)
+    items = items.copy()
+    ch = item_chunks(items)
+    items["chunk_begin"] = np.concatenate([[0], np.cumsum(ch)[:-1]])
     dev = model.table.device
-    buf = torch.empty(ctypes.sizeof(arr) + 16, dtype=torch.uint8, device=dev)
-    host = torch.frombuffer(bytearray(arr), dtype=torch.uint8)
+    buf = torch.empty(items.nbytes + 16, dtype=torch.uint8, device=dev)
     with torch.cuda.stream(stream):
-        buf[:ctypes.sizeof(arr)].copy_(host, non_blocking=False)
-        counter = buf[ctypes.sizeof(arr):ctypes.sizeof(arr) + 4]
-        _call_points(model, buf.data_ptr(), len(items), total, counter.data_ptr(), stream.cuda_stream)
+        buf[:items.nbytes].copy_(torch.from_numpy(items.view(np.uint8)), non_blocking=False)
+        _call_points(model, buf.data_ptr(), items.size, int(ch.sum()), buf.data_ptr() + items.nbytes,
+                     stream.cuda_stream)
 
 
 def reproject(model: _HashGridModel, geometry, angle: float, t: float = 0.0, points_per_ray: int | None = None,
               out: torch.Tensor | None = None, workspace: torch.Tensor | None = None,
-              stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+              stream: torch.cuda.Stream | None = None, max_blocks: int = 0) -> torch.Tensor:
     """Detector view [nDetector] at (angle, t): sum of sigma * distance / max_distance_traveled per ray."""
     cg = geometry.get_c_geometry()
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
@@ -188,7 +157,8 @@ def reproject(model: _HashGridModel, geometry, angle: float, t: float = 0.0, poi
                                         ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
                                         model.mlp.data_ptr(), float(angle), float(t), S,
                                         geometry.max_distance_traveled / S, geometry.max_distance_traveled,
-                                        out.data_ptr(), workspace.data_ptr(), workspace.numel(), stream.cuda_stream)
+                                        out.data_ptr(), workspace.data_ptr(), workspace.numel(), int(max_blocks),
+                                        stream.cuda_stream)
     _lib.check(rc, "nectb_query_reproject")
     return out.view(geometry.nDetector[0], geometry.nDetector[1])
 
@@ -205,6 +175,7 @@ class Request:
     v: tuple = (0.0, 1.0, 0.0)
     # filled by the server
     arrival: float = 0.0
+    launched: float = 0.0          # host time its last launch was issued
     done: float = 0.0
     result: np.ndarray | None = None
     event: threading.Event = field(default_factory=threading.Event)
@@ -219,228 +190,336 @@ class Request:
     def latency_ms(self) -> float:
         return (self.done - self.arrival) * 1e3
 
+    def wait_ms(self) -> float:
+        """Arrival to the issue of its last launch (queueing on the host)."""
+        return (self.launched - self.arrival) * 1e3
+
 
 BUCKETS = (64, 256, 1024, 4096, 16384)   # chunks per launch (128 points each)
 MAX_ITEMS = 512
 
 
-class _Lane:
-    """One stream with its graph-captured launches (one per bucket)."""
+class _Pool:
+    """Fixed device + pinned host slots of one request class."""
 
-    def __init__(self, server: "QueryServer", dev):
-        self.stream = torch.cuda.Stream(device=dev)
-        self.items_dev = torch.empty(MAX_ITEMS * ITEM_BYTES + 64, dtype=torch.uint8, device=dev)
-        self.items_host = torch.empty(MAX_ITEMS * ITEM_BYTES, dtype=torch.uint8).pin_memory()
+    def __init__(self, n: int, floats: int, dev, ws_bytes: int = 0):
+        self.dev_buf = torch.empty(n, floats, device=dev)
+        self.host_buf = torch.empty(n, floats).pin_memory()
+        self.ws = torch.empty(n, max(ws_bytes, 1), dtype=torch.uint8, device=dev) if ws_bytes else None
+        self.free = list(range(n))
+
+
+class _Lane:
+    """One stream with graph-captured point launches (one graph per bucket).
+
+    priority: CUDA stream priority (lower is higher priority); max_blocks caps
+    the persistent grid (0 = two blocks per SM)."""
+
+    def __init__(self, dev, priority: int = 0, max_blocks: int = 0):
+        self.stream = torch.cuda.Stream(device=dev, priority=priority)
+        self.max_blocks = max_blocks
+        self.items_dev = torch.empty(MAX_ITEMS * ITEM_DTYPE.itemsize + 64, dtype=torch.uint8, device=dev)
+        self.items_host = torch.empty(MAX_ITEMS * ITEM_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
+        self.table = self.items_host.numpy().view(ITEM_DTYPE)
         self.dummy = torch.empty(CHUNK * BUCKETS[-1], device=dev)   # sink for padding chunks
         self.graphs: dict[int, torch.cuda.CUDAGraph] = {}
-        self.busy_event: torch.cuda.Event | None = None
-        self.server = server
+        self.last: torch.cuda.Event | None = None
 
     def counter_ptr(self) -> int:
-        return self.items_dev.data_ptr() + MAX_ITEMS * ITEM_BYTES
+        return self.items_dev.data_ptr() + MAX_ITEMS * ITEM_DTYPE.itemsize
+
+    def idle(self) -> bool:
+        return self.last is None or self.last.query()
 
     def capture(self, model):
         for b in BUCKETS:
-            g = torch.cuda.CUDAGraph()
-            # warm up outside capture (sets kernel attributes), then capture
-            self._write_padding(b, 0, 0)
-            with torch.cuda.stream(self.stream):
-                self.items_dev[:MAX_ITEMS * ITEM_BYTES].copy_(self.items_host, non_blocking=True)
+            self._write(np.zeros(0, ITEM_DTYPE), b)
+            with torch.cuda.stream(self.stream):   # warm-up launch sets kernel attributes
+                self.items_dev[:self.items_host.numel()].copy_(self.items_host, non_blocking=True)
                 _call_points(model, self.items_dev.data_ptr(), MAX_ITEMS, b, self.counter_ptr(),
-                             self.stream.cuda_stream)
+                             self.stream.cuda_stream, self.max_blocks)
             self.stream.synchronize()
+            g = torch.cuda.CUDAGraph()
             with torch.cuda.graph(g, stream=self.stream, capture_error_mode="relaxed"):
                 _call_points(model, self.items_dev.data_ptr(), MAX_ITEMS, b, self.counter_ptr(),
-                             torch.cuda.current_stream().cuda_stream)
+                             torch.cuda.current_stream().cuda_stream, self.max_blocks)
             self.graphs[b] = g
 
-    def _write_padding(self, bucket: int, n_items: int, used_chunks: int):
-        """Fill items n_items.. with one padding item covering the unused chunks
-        of the bucket (written to the dummy sink) and empty items after it."""
-        arr = (NectbQueryItem * MAX_ITEMS).from_buffer(self.items_host.numpy())
-        pad = bucket - used_chunks
-        for i in range(n_items, MAX_ITEMS):
-            a = arr[i]
-            a.nu = CHUNK if (i == n_items and pad > 0) else 0
-            a.nv = pad if (i == n_items and pad > 0) else 0
-            a.out = self.dummy.data_ptr()
-            a.out_stride = CHUNK
-            a.t = 0.0
-            a.out_scale, a.out_offset = 1.0, 0.0
-            a.chunk_begin = used_chunks if i == n_items else bucket
-            for k in range(3):
-                a.origin[k], a.du[k], a.dv[k] = 0.5, 0.0, 0.0
+    def _write(self, items: np.ndarray, bucket: int):
+        """items, one padding item over the bucket's unused chunks (to a sink),
+        then empty items."""
+        n = items.size
+        tab = self.table
+        ch = item_chunks(items)
+        tab[:n] = items
+        begins = np.concatenate([[0], np.cumsum(ch)]).astype(np.int64)
+        tab["chunk_begin"][:n] = begins[:-1]
+        used = int(begins[-1])
+        tail = tab[n:]
+        tail[:] = np.zeros(1, ITEM_DTYPE)
+        tail["out"] = self.dummy.data_ptr()
+        tail["out_stride"] = CHUNK
+        tail["out_scale"] = 1.0
+        tail["origin"] = 0.5
+        tail["chunk_begin"] = bucket
+        if bucket > used:
+            tail["nu"][0], tail["nv"][0], tail["chunk_begin"][0] = CHUNK, bucket - used, used
 
-    def launch(self, items: list[Item]) -> torch.cuda.Event:
-        """Pack items (<= MAX_ITEMS - 1 of them, <= the largest bucket of chunks) and replay the graph."""
-        total = sum(it.chunks for it in items)
+    def launch(self, items: np.ndarray) -> torch.cuda.Event:
+        total = int(item_chunks(items).sum())
         bucket = next(b for b in BUCKETS if b >= total)
-        arr = (NectbQueryItem * MAX_ITEMS).from_buffer(self.items_host.numpy())
-        if self.busy_event is not None:
-            self.busy_event.synchronize()   # the host staging buffer of the previous launch is free
-        c = 0
-        for i, it in enumerate(items):
-            a = arr[i]
-            for k in range(3):
-                a.origin[k], a.du[k], a.dv[k] = it.origin[k], it.du[k], it.dv[k]
-            a.nu, a.nv, a.t = it.nu, it.nv, it.t
-            a.out_scale, a.out_offset = it.scale, it.offset
-            a.out, a.out_stride, a.chunk_begin = it.out, it.out_stride, c
-            c += it.chunks
-        self._write_padding(bucket, len(items), total)
+        if self.last is not None:
+            self.last.synchronize()   # this lane's staging buffer has been consumed
+        self._write(items, bucket)
         with torch.cuda.stream(self.stream):
-            self.items_dev[:MAX_ITEMS * ITEM_BYTES].copy_(self.items_host, non_blocking=True)
+            self.items_dev[:self.items_host.numel()].copy_(self.items_host, non_blocking=True)
             self.graphs[bucket].replay()
             ev = torch.cuda.Event()
             ev.record(self.stream)
-        self.busy_event = ev
+        self.last = ev
         return ev
 
 
 class QueryServer:
-    """Continuous-batching server for slice / volume / re-projection queries."""
+    """Continuous-batching server for slice / volume / re-projection queries.
 
-    def __init__(self, model: _HashGridModel, geometry, memory_budget: int = 40 << 30, n_streams: int = 3,
-                 max_chunks_per_launch: int = BUCKETS[-1], minimum: float = 0.0, maximum: float = 1.0,
-                 points_per_ray: int | None = None):
+    The memory budget is split at start-up into slots: slices up to
+    ``max_slice``^2, volumes up to ``max_volume``^3, re-projections of the
+    geometry's detector with their sampler workspace (shares in the
+    proportions ``slot_mix``).  A request waits until a slot of its class is
+    free (admission by memory); nothing is allocated while serving.
+
+    Slices run on ``n_fast`` high-priority lanes, packed several requests per
+    launch.  Volumes and re-projections share ``n_slow`` low-priority lanes
+    whose persistent grids are capped at ``slow_blocks`` (default one block
+    per SM): with one background lane an SM keeps room for a slice block while
+    background work runs, which is what keeps slice p99 near its unloaded
+    latency."""
+
+    def __init__(self, model: _HashGridModel, geometry, memory_budget: int = 40 << 30, n_fast: int = 2,
+                 n_slow: int = 1, minimum: float = 0.0, maximum: float = 1.0, points_per_ray: int | None = None,
+                 slow_blocks: int | None = None, max_slice: int = 1024, max_volume: int = 256,
+                 slot_mix=(0.25, 0.25, 0.5), max_slots: int = 64):
         self.model = model
         self.geometry = geometry
         self.dev = model.table.device
-        self.budget = memory_budget
-        self.in_use = 0
         self.scale, self.offset = denormalisation(geometry.max_distance_traveled, minimum, maximum)
         self.points_per_ray = points_per_ray
-        self.max_chunks = max_chunks_per_launch
-        self.queue: queue.Queue = queue.Queue()
-        self.lanes = [_Lane(self, self.dev) for _ in range(n_streams)]
-        for ln in self.lanes:
+        sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
+        self.slow_blocks = slow_blocks if slow_blocks is not None else sms
+        lo, hi = torch.cuda.Stream.priority_range()
+        self.fast = [_Lane(self.dev, priority=hi) for _ in range(n_fast)]
+        self.slow = [_Lane(self.dev, priority=lo, max_blocks=self.slow_blocks) for _ in range(n_slow)]
+        for ln in self.fast + self.slow:
             ln.capture(model)
         cg = geometry.get_c_geometry()
         P = geometry.nDetector[0] * geometry.nDetector[1]
-        self.reproj_ws_bytes = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct),
-                                                                    ctypes.byref(model.grid_desc),
-                                                                    ctypes.byref(model.mlp_desc), P)
-        self._stop = False
-        self._thread = threading.Thread(target=self._run, daemon=True)
+        ws = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
+                                                  ctypes.byref(model.mlp_desc), P)
+        per = {"slice": 8 * max_slice ** 2, "volume": 8 * max_volume ** 3, "reproject": 8 * P + ws}
+        nslots = {k: max(1, min(max_slots, int(memory_budget * f // per[k])))
+                  for k, f in zip(("slice", "reproject", "volume"), slot_mix)}
+        self.pools = {"slice": _Pool(nslots["slice"], max_slice ** 2, self.dev),
+                      "volume": _Pool(nslots["volume"], max_volume ** 3, self.dev),
+                      "reproject": _Pool(nslots["reproject"], P, self.dev, ws_bytes=ws)}
+        self.max_slice, self.max_volume = max_slice, max_volume
+        self.queue: queue.Queue = queue.Queue()
         self.completed: list[Request] = []
-        self._lane_rr = 0
+        self._rr = {"fast": 0, "slow": 0}
+        self._done_q: queue.Queue = queue.Queue()
+        self._free_q: queue.Queue = queue.Queue()
+        self._finisher = threading.Thread(target=self._finish_loop, daemon=True)
+        self._finisher.start()
+        self._thread = threading.Thread(target=self._run, daemon=True)
         self._thread.start()
 
     # -- client side ------------------------------------------------------
     def submit(self, req: Request) -> Request:
+        if req.kind == "slice" and req.size > self.max_slice or req.kind == "volume" and req.size > self.max_volume:
+            raise ValueError(f"{req.kind} of size {req.size} exceeds the server's slots")
         req.arrival = time.perf_counter()
         self.queue.put(req)
         return req
 
     def close(self):
-        self._stop = True
         self.queue.put(None)
         self._thread.join()
+        self._done_q.put(None)
+        self._finisher.join()
+
+    def _finish_loop(self):
+        """Copies finished results out of their pinned slots and releases the
+        slots, off the scheduler thread (a 64 MB volume copy must not stall
+        the launches of other requests)."""
+        while True:
+            st = self._done_q.get()
+            if st is None:
+                return
+            r, pool = st["req"], self.pools[st["req"].kind]
+            r.result = pool.host_buf[st["slot"], :st["n"]].numpy().reshape(st["shape"]).copy()
+            self._free_q.put((r.kind, st["slot"]))
+            self.completed.append(r)
+            r.event.set()
 
     # -- scheduler --------------------------------------------------------
-    def _bytes(self, req: Request) -> int:
-        n = int(np.prod(req.out_shape(self.geometry))) * 4
-        return 2 * n + (self.reproj_ws_bytes if req.kind == "reproject" else 0)  # device + pinned host
+    def _lane(self, kind: str, want_idle: bool = False):
+        lanes = self.fast if kind == "fast" else self.slow
+        if not want_idle:  # prefer an idle lane, so the launch never waits for a staging buffer
+            for k in range(len(lanes)):
+                ln = lanes[(self._rr[kind] + k) % len(lanes)]
+                if ln.idle():
+                    self._rr[kind] += k + 1
+                    return ln
+        for k in range(len(lanes)):
+            ln = lanes[(self._rr[kind] + k) % len(lanes)]
+            if not want_idle or ln.idle():
+                self._rr[kind] += k + 1
+                return ln
+        return None
 
-    def _next_lane(self) -> _Lane:
-        ln = self.lanes[self._lane_rr % len(self.lanes)]
-        self._lane_rr += 1
-        return ln
+    def _finish_on(self, st: dict, ln: _Lane):
+        pool, slot, n = self.pools[st["req"].kind], st["slot"], st["n"]
+        with torch.cuda.stream(ln.stream):
+            pool.host_buf[slot, :n].copy_(pool.dev_buf[slot, :n], non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(ln.stream)
+        st["events"].append(ev)
+
+    @staticmethod
+    def _pack(active: list[dict], limit_chunks: int):
+        parts, chunks, touched = [], 0, []
+        for st in active:
+            it, ch = st["items"], st["chunks"]
+            k = 0
+            while k < it.size and chunks + ch[k] <= limit_chunks and sum(p.size for p in parts) + k < MAX_ITEMS - 1:
+                chunks += int(ch[k])
+                k += 1
+            if k:
+                parts.append(it[:k])
+                st["items"], st["chunks"] = it[k:], ch[k:]
+                touched.append(st)
+            if k < it.size:
+                break
+        return (np.concatenate(parts) if parts else np.zeros(0, ITEM_DTYPE)), touched
+
+    def _admit(self, r: Request):
+        pool = self.pools[r.kind]
+        if not pool.free:
+            return None
+        slot = pool.free.pop(0)
+        shape = r.out_shape(self.geometry)
+        n = int(np.prod(shape))
+        addr = pool.dev_buf[slot].data_ptr()
+        st = {"req": r, "slot": slot, "n": n, "shape": shape, "events": []}
+        if r.kind == "slice":
+            st["items"] = slice_items(addr, shape, r.t, r.centre, r.u, r.v, self.scale, self.offset)
+        elif r.kind == "volume":
+            st["items"] = volume_items(addr, shape, r.t, self.scale, self.offset)
+        if "items" in st:
+            st["chunks"] = item_chunks(st["items"])
+        return st
 
     def _run(self):
         torch.cuda.set_device(self.dev)
         waiting: list[Request] = []
-        active: list[dict] = []       # admitted requests with their remaining work
-        flying: list[dict] = []       # requests whose work is all launched
+        slices: list[dict] = []
+        volumes: list[dict] = []
+        reprojs: list[dict] = []
+        flying: list[dict] = []
+        closing = False
         while True:
-            # take new arrivals without blocking while there is work
-            block = not (waiting or active or flying)
+            idle = not (waiting or slices or volumes or reprojs or flying)
+            if closing and idle:
+                return
+            if idle and waiting == [] and self._free_q.qsize():
+                idle = False
             try:
-                r = self.queue.get(block=block, timeout=None if block else 0.0)
-                if r is None:
-                    if not (waiting or active or flying):
-                        return
-                else:
-                    waiting.append(r)
+                r = self.queue.get(block=idle)
                 while True:
-                    r = self.queue.get_nowait()
-                    if r is not None:
+                    if r is None:
+                        closing = True
+                    else:
                         waiting.append(r)
+                    r = self.queue.get_nowait()
             except queue.Empty:
                 pass
-            # admission by memory, in arrival order
-            while waiting and self.in_use + self._bytes(waiting[0]) <= self.budget:
-                r = waiting.pop(0)
-                self.in_use += self._bytes(r)
-                out = torch.empty(r.out_shape(self.geometry), device=self.dev)
-                st = {"req": r, "out": out, "events": [], "host": torch.empty(out.shape, pin_memory=True)}
-                if r.kind == "reproject":
-                    ln = self._next_lane()
-                    with torch.cuda.stream(ln.stream):
-                        ws = torch.empty(self.reproj_ws_bytes, dtype=torch.uint8, device=self.dev)
-                        reproject(self.model, self.geometry, r.angle, r.t, self.points_per_ray, out=out.view(-1),
-                                  workspace=ws, stream=ln.stream)
-                        st["host"].copy_(out, non_blocking=True)
-                        ev = torch.cuda.Event()
-                        ev.record(ln.stream)
-                    st["ws"] = ws
-                    st["events"].append(ev)
-                    flying.append(st)
+            # slots released by the finisher thread
+            try:
+                while True:
+                    kind, slot = self._free_q.get_nowait()
+                    self.pools[kind].free.append(slot)
+            except queue.Empty:
+                pass
+            # admission: in arrival order within each class, when a slot is free
+            still = []
+            for r in waiting:
+                st = self._admit(r)
+                if st is None:
+                    still.append(r)
                 else:
-                    items = (slice_items(out, r.t, r.centre, r.u, r.v, self.scale, self.offset)
-                             if r.kind == "slice" else volume_items(out, r.t, self.scale, self.offset))
-                    st["items"] = items
-                    active.append(st)
-            # pack pending items of all active requests into launches (continuous batching)
-            while active:
-                ln = self._next_lane()
-                batch, chunks, touched = [], 0, []
-                for st in active:
-                    while st["items"] and len(batch) < MAX_ITEMS - 1:
-                        c = st["items"][0].chunks
-                        if chunks + c > self.max_chunks:
-                            break
-                        batch.append(st["items"].pop(0))
-                        chunks += c
-                        if st not in touched:
-                            touched.append(st)
-                    if chunks >= self.max_chunks or len(batch) >= MAX_ITEMS - 1:
-                        break
-                if not batch:
+                    {"slice": slices, "volume": volumes, "reproject": reprojs}[r.kind].append(st)
+            waiting = still
+            # slices: every pending slice item, packed across requests, on a fast lane
+            while slices:
+                batch, touched = self._pack(slices, BUCKETS[-1])
+                if batch.size == 0:
                     break
+                ln = self._lane("fast")
                 ev = ln.launch(batch)
                 for st in touched:
                     st["events"].append(ev)
-                    if not st["items"]:
-                        with torch.cuda.stream(ln.stream):
-                            st["host"].copy_(st["out"], non_blocking=True)
-                            e2 = torch.cuda.Event()
-                            e2.record(ln.stream)
-                        st["events"].append(e2)
-                for st in [s for s in active if not s["items"]]:
-                    active.remove(st)
+                    if st["items"].size == 0:
+                        st["req"].launched = time.perf_counter()
+                        self._finish_on(st, ln)
+                        slices.remove(st)
+                        flying.append(st)
+            # background: one launch per idle slow lane, oldest request first
+            while reprojs or volumes:
+                ln = self._lane("slow", want_idle=True)
+                if ln is None:
+                    break
+                if reprojs and (not volumes or reprojs[0]["req"].arrival <= volumes[0]["req"].arrival):
+                    st = reprojs.pop(0)
+                    r, pool = st["req"], self.pools["reproject"]
+                    with torch.cuda.stream(ln.stream):
+                        reproject(self.model, self.geometry, r.angle, r.t, self.points_per_ray,
+                                  out=pool.dev_buf[st["slot"]], workspace=pool.ws[st["slot"]], stream=ln.stream,
+                                  max_blocks=self.slow_blocks)
+                        ev = torch.cuda.Event()
+                        ev.record(ln.stream)
+                    ln.last = ev
+                    r.launched = time.perf_counter()
+                    st["events"].append(ev)
+                    self._finish_on(st, ln)
                     flying.append(st)
-                if self.queue.qsize():
-                    break   # admit newcomers between launches
+                else:
+                    batch, touched = self._pack(volumes, 4096)
+                    ev = ln.launch(batch)
+                    for st in touched:
+                        st["events"].append(ev)
+                        if st["items"].size == 0:
+                            st["req"].launched = time.perf_counter()
+                            self._finish_on(st, ln)
+                            volumes.remove(st)
+                            flying.append(st)
             # completions
             for st in list(flying):
                 if all(e.query() for e in st["events"]):
-                    r = st["req"]
-                    r.result = st["host"].numpy()
-                    r.done = time.perf_counter()
-                    self.in_use -= self._bytes(r)
+                    st["req"].done = time.perf_counter()
                     flying.remove(st)
-                    self.completed.append(r)
-                    r.event.set()
-            if not (waiting or active) and flying:
-                time.sleep(0.0002)
+                    self._done_q.put(st)
+            if self.queue.empty() and not slices and (flying or reprojs or volumes or waiting):
+                time.sleep(0.0001)
 
     # -- statistics ---------------------------------------------------------
     def latency_stats(self) -> dict:
         out = {}
         for kind in ("slice", "reproject", "volume"):
-            lat = np.array([r.latency_ms() for r in self.completed if r.kind == kind])
+            done = [r for r in self.completed if r.kind == kind]
+            lat = np.array([r.latency_ms() for r in done])
             if lat.size:
+                wait = np.array([r.wait_ms() for r in done])
                 out[kind] = {"n": int(lat.size), "p50_ms": float(np.percentile(lat, 50)),
-                             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean())}
+                             "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                             "wait_p99_ms": float(np.percentile(wait, 99))}
         return out

@@ -61,24 +61,22 @@ def test_volume_and_slices_match_oracle(cuda_device, precision):
     vol = torch.empty(12, 16, 20, device="cuda")
     sl = torch.empty(33, 47, device="cuda")
     ob = torch.empty(40, 40, device="cuda")
-    items = (serving.volume_items(vol, t) + serving.slice_items(sl, t, centre=(0.4, 0.5, 0.6)) +
-             serving.slice_items(ob, t, centre=(0.5, 0.5, 0.5), u=(0.2, 0.7, 0.3), v=(0.0, -0.3, 0.9),
-                                 rows_per_item=7))
-    serving.query_points(m, items)
+    it_sl = serving.slice_items(sl, sl.shape, t, centre=(0.4, 0.5, 0.6))
+    it_ob = serving.slice_items(ob, ob.shape, t, centre=(0.5, 0.5, 0.5), u=(0.2, 0.7, 0.3), v=(0.0, -0.3, 0.9),
+                                rows_per_item=7)
+    serving.query_points(m, np.concatenate([serving.volume_items(vol, vol.shape, t), it_sl, it_ob]))
     torch.cuda.synchronize()
     z, y, x = [serving.centres(n) for n in (12, 16, 20)]
     Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
     ref = oracle_sigma(m, levels, np.stack([Z, Y, X], -1).reshape(-1, 3), t)
     assert rel(vol.cpu(), ref) < TOL[precision]
-    for out, it_list in ((sl, serving.slice_items(sl, t, centre=(0.4, 0.5, 0.6))),
-                         (ob, serving.slice_items(ob, t, centre=(0.5, 0.5, 0.5), u=(0.2, 0.7, 0.3),
-                                                  v=(0.0, -0.3, 0.9), rows_per_item=7))):
+    for out, items in ((sl, it_sl), (ob, it_ob)):
         pts = []
-        for it in it_list:
-            for j in range(it.nv):
-                for i in range(it.nu):
-                    pts.append(np.clip(np.float32(it.origin) + np.float32(i) * np.float32(it.du) +
-                                       np.float32(j) * np.float32(it.dv), 0, 1))
+        for it in items:
+            o, du, dv = it["origin"], it["du"], it["dv"]
+            for j in range(int(it["nv"])):
+                for i in range(int(it["nu"])):
+                    pts.append(np.clip(o + np.float32(i) * du + np.float32(j) * dv, 0, 1))
         assert rel(out.cpu(), oracle_sigma(m, levels, np.array(pts, np.float32), t)) < TOL[precision]
 
 
@@ -117,7 +115,7 @@ def test_server_results_same_alone_and_in_mix(cuda_device, precision):
         reqs.append(dict(kind=kind, t=float(rng.random()), size=int(rng.choice([40, 64, 96])) if kind != "volume"
                          else 24, angle=float(rng.random() * 6.28),
                          centre=tuple(rng.random(3) * 0.4 + 0.3), u=(0.0, 0.0, 1.0), v=(0.0, 1.0, 0.0)))
-    srv = QueryServer(m, geo, memory_budget=256 << 20, n_streams=3, points_per_ray=64)
+    srv = QueryServer(m, geo, memory_budget=256 << 20, points_per_ray=64)
     alone = []
     for d in reqs:  # one at a time
         r = srv.submit(Request(**d))
