@@ -182,7 +182,10 @@ typedef struct NectbQueryItem {
  * export_video (nect/trainers/base_trainer.py:402-450,
  * nect/static_export.py:106-144, nect/dynamic_export.py:297-544), which
  * materialise coordinate grids and call the model one slice at a time.
- * counter: one device uint32 the kernel uses as its work cursor (zeroed here). */
+ * counter: two device uint32: [0] the work cursor (zeroed by every call) and
+ * [1] an error word the launch sets to non-zero when a tensor-core wait timed
+ * out (its items are then incomplete).  The library never clears [1]: the
+ * caller zeroes it once and reads it (stream-ordered) when it wants to know. */
 int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
                        const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
                        int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream);
@@ -235,6 +238,18 @@ typedef struct NectbTrainBatch {
 size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                    const NectbMLP* mlp, int32_t num_rays);
 
+/* Device address of the error word inside a training (or re-projection)
+ * workspace of num_rays rays (num_rays = detector pixels for a
+ * re-projection); workspace NULL gives the word of the static scratch of
+ * nectb_train_step_static on the current device.  Every step clears the word
+ * and sets it to non-zero when a tensor-core wait of that step timed out
+ * (results of the step are then incomplete and the call's stream stays
+ * usable).  Read it stream-ordered after the step, e.g. with cudaMemcpyAsync.
+ * Returns NULL on invalid arguments.  No reference counterpart (the reference
+ * reports only CUDA errors, ct_sampling.cu:639-644). */
+const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_t num_rays,
+                                           const void* workspace);
+
 /* Fused forward+backward.  grid_params is the table in grid->feature_dtype
  * (fp32 or fp16); mlp_params fp32.  Gradients are accumulated (+=) into
  * grid_grad (fp32, nectb_hashgrid_layout total * n_features) and mlp_grad
@@ -284,6 +299,14 @@ int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq
 #define NECTB_PROFILE_SLOTS 8
 int nectb_profile_enable(int32_t enable);
 int nectb_profile_collect(int32_t* launches, double* total_ms);
+
+/* Self-test of the bounded waits the tensor-core kernels use: one block waits
+ * on an mbarrier that nothing arrives at, polling at most max_tries times,
+ * then writes *error_word = 1 if the wait gave up (0 if it completed).  It
+ * lets a test check, on a GPU and without any fault, that a wait that runs
+ * out ends the kernel with a status the host reads and leaves the context
+ * usable.  No reference counterpart. */
+int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, void* stream);
 
 /* Version string and last error message of the calling thread. */
 const char* nectb_version(void);

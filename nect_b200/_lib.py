@@ -124,6 +124,18 @@ _SIGNATURES = {
          ctypes.POINTER(NectbTrainBatch), c_ptr, c_ptr, c_ptr, c_ptr, c_ptr],
     ),
     "nectb_train_static_scratch_bytes": (c_size, []),
+    "nectb_query_points": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_int, c_i64, c_ptr, c_int,
+         c_ptr],
+    ),
+    "nectb_query_reproject": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_f32,
+         c_f32, c_int, c_f32, c_f32, c_ptr, c_ptr, c_size, c_int, c_ptr],
+    ),
+    "nectb_train_error_word": (c_ptr, [ctypes.POINTER(NectbGeometry), c_int, c_ptr]),
+    "nectb_selftest_bounded_wait": (c_int, [c_ptr, ctypes.c_uint32, c_ptr]),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
     "nectb_adam_step": (

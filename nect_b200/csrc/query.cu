@@ -72,8 +72,11 @@ __device__ __forceinline__ uint8_t* qalign1024(uint8_t* p) {
   return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
 }
 
+// At most 128 registers so that three blocks share an SM under the 164 KB
+// shared split (a background block beside two slice blocks, or three blocks of
+// one query).
 template <int D, int F>
-__global__ void __launch_bounds__(kQThreads, 2)
+__global__ void __launch_bounds__(kQThreads, 4)
 query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W,
                    const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
                    unsigned int* __restrict__ counter, int out_act) {
@@ -216,7 +219,10 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
     tc::fence_before();
     __syncthreads();
   }
-  if (timed_out) tc::mbar_wait(bar, phase);
+  if (timed_out) {
+    tc::mbar_wait(bar, phase);  // let the MMA in flight finish before TMEM is freed
+    if (t == 0) atomicOr(counter + 1, 1u);
+  }
   tc::fence_before();
   __syncthreads();
   if (warp == 0) {
@@ -282,7 +288,7 @@ int launch_query_mixed(const GridDev& g, const void* table, const float* W, cons
   auto k = query_mixed_kernel<D, F>;
   const size_t smem = 1024 + 2 * kQWTile + 2 * kQTile + 64 * 4 + 64;
   set_smem(k, smem, true);
-  int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 2 * sm_count()));
+  int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 3 * sm_count()));
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   ProfScope ps(kProfModel, s);
   k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);

@@ -127,8 +127,19 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
   return true;
 }
 
+// Blocks of the forward per SM.  Shared memory per block is 33.5 KB (A1
+// reuses the X tile), so four blocks (16 warps, 4 x 128 TMEM columns) still
+// leave 92 KB of L1 for the coarse levels' gathers.  Measured on the 512^2
+// cone workloads: 2 / 3 / 4 blocks give 19.5 / 15.3 / 13.6 ms (3D) and
+// 34.0 / 28.0 / 26.0 ms (4D) per 2^18-ray forward.
+#ifndef NECTB_FWD_BLOCKS_PER_SM
+#define NECTB_FWD_BLOCKS_PER_SM 4
+#endif
+constexpr int kFwdBlocksPerSM = NECTB_FWD_BLOCKS_PER_SM;
+static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 128 <= 512, "TMEM holds 512 columns per SM");
+
 template <int D, int F>
-__global__ void __launch_bounds__(kMixThreads, 2)
+__global__ void __launch_bounds__(kMixThreads, kFwdBlocksPerSM)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ y_pred, float* __restrict__ loss) {
@@ -140,8 +151,11 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   uint8_t* sW0 = base;
   uint8_t* sW1 = sW0 + kWTile;
   uint8_t* sX = sW1 + kWTile;
-  uint8_t* sA = sX + kTile;
-  float* sWout = reinterpret_cast<float*>(sA + kTile);
+  // A1 overwrites X: the first MMA has finished reading X (its commit has
+  // arrived) before A1 is written, and the next X is written only after the
+  // second MMA, which reads A1, has completed.
+  uint8_t* sA = sX;
+  float* sWout = reinterpret_cast<float*>(sX + kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   float* red = reinterpret_cast<float*>(tslot + 4);
@@ -497,14 +511,18 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   (void)geo;
+  int fblocks = std::max(1, std::min<int>(kFwdBlocksPerSM * sms, (int)ceil_div(a.num_rays, 4)));
   int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
-  if (a.max_blocks > 0) blocks = std::min(blocks, a.max_blocks);
+  if (a.max_blocks > 0) {
+    fblocks = std::min(fblocks, a.max_blocks);
+    blocks = std::min(blocks, a.max_blocks);
+  }
   {
     auto k = fwd_mixed_kernel<D, F>;
-    const size_t smem = 1024 + 2 * kWTile + 2 * kTile + 64 * 4 + 64;
+    const size_t smem = 1024 + 2 * kWTile + kTile + 64 * 4 + 64;
     set_smem(k, smem, a.max_blocks > 0);
     ProfScope ps(kProfForward, s);
-    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
+    k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
   }
   if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)

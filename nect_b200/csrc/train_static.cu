@@ -21,6 +21,7 @@
 #include <mutex>
 
 #include "common.cuh"
+#include "train_common.cuh"
 
 extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                               const NectbMLP* mlp, int32_t num_rays);
@@ -74,4 +75,18 @@ extern "C" int nectb_train_step_static(const NectbGeometry* geometry, const Nect
   if (int rc = scratch_address(&scratch)) return rc;
   return nectb_train_step(geometry, grid, mlp, grid_params, mlp_params, batch, grid_grad, mlp_grad, y_pred, loss,
                           scratch, kStaticScratchBytes, stream);
+}
+
+extern "C" const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_t num_rays,
+                                                      const void* workspace) {
+  using namespace nectb;
+  clear_error();
+  if (!geometry || num_rays <= 0) {
+    set_error(NECTB_ERR_INVALID, "nectb_train_error_word: null geometry or num_rays <= 0");
+    return nullptr;
+  }
+  void* ws = const_cast<void*>(workspace);
+  if (!ws && scratch_address(&ws) != NECTB_OK) return nullptr;
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  return carve_workspace(ws, num_rays, P).counters + 2;
 }

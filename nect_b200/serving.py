@@ -48,17 +48,6 @@ ITEM_DTYPE = np.dtype({
     "itemsize": 80,
 })  # NectbQueryItem (include/nectb.h)
 
-_lib.lib.nectb_query_points.restype = ctypes.c_int32
-_lib.lib.nectb_query_points.argtypes = [ctypes.POINTER(_lib.NectbHashGrid), ctypes.POINTER(_lib.NectbMLP),
-                                        ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int32,
-                                        ctypes.c_int64, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p]
-_lib.lib.nectb_query_reproject.restype = ctypes.c_int32
-_lib.lib.nectb_query_reproject.argtypes = [ctypes.POINTER(_lib.NectbGeometry), ctypes.POINTER(_lib.NectbHashGrid),
-                                           ctypes.POINTER(_lib.NectbMLP), ctypes.c_void_p, ctypes.c_void_p,
-                                           ctypes.c_float, ctypes.c_float, ctypes.c_int32, ctypes.c_float,
-                                           ctypes.c_float, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_size_t,
-                                           ctypes.c_int32, ctypes.c_void_p]
-
 
 def denormalisation(max_distance_traveled: float, minimum: float = 0.0, maximum: float = 1.0):
     """(scale, offset) of sigma/max_distance_traveled*(max-min)+min (static_export.py:139-140)."""
@@ -133,6 +122,7 @@ def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.St
     dev = model.table.device
     buf = torch.empty(items.nbytes + 16, dtype=torch.uint8, device=dev)
     with torch.cuda.stream(stream):
+        buf[items.nbytes:].zero_()   # work cursor and error word
         buf[:items.nbytes].copy_(torch.from_numpy(items.view(np.uint8)), non_blocking=False)
         _call_points(model, buf.data_ptr(), items.size, int(ch.sum()), buf.data_ptr() + items.nbytes,
                      stream.cuda_stream)
@@ -218,7 +208,7 @@ class _Lane:
     def __init__(self, dev, priority: int = 0, max_blocks: int = 0):
         self.stream = torch.cuda.Stream(device=dev, priority=priority)
         self.max_blocks = max_blocks
-        self.items_dev = torch.empty(MAX_ITEMS * ITEM_DTYPE.itemsize + 64, dtype=torch.uint8, device=dev)
+        self.items_dev = torch.zeros(MAX_ITEMS * ITEM_DTYPE.itemsize + 64, dtype=torch.uint8, device=dev)
         self.items_host = torch.empty(MAX_ITEMS * ITEM_DTYPE.itemsize, dtype=torch.uint8).pin_memory()
         self.table = self.items_host.numpy().view(ITEM_DTYPE)
         self.dummy = torch.empty(CHUNK * BUCKETS[-1], device=dev)   # sink for padding chunks
@@ -230,6 +220,13 @@ class _Lane:
 
     def idle(self) -> bool:
         return self.last is None or self.last.query()
+
+    def error_word(self) -> int:
+        """Sticky error word of this lane's launches (non-zero if a tensor-core
+        wait timed out).  Synchronises the lane."""
+        off = MAX_ITEMS * ITEM_DTYPE.itemsize + 4
+        self.stream.synchronize()
+        return int(self.items_dev[off:off + 4].view(torch.int32).item())
 
     def capture(self, model):
         for b in BUCKETS:
@@ -510,6 +507,13 @@ class QueryServer:
                     self._done_q.put(st)
             if self.queue.empty() and not slices and (flying or reprojs or volumes or waiting):
                 time.sleep(0.0001)
+
+    def device_errors(self) -> int:
+        """OR of the error words of every lane (0 = no tensor-core wait timed out)."""
+        err = 0
+        for ln in self.fast + self.slow:
+            err |= ln.error_word()
+        return err
 
     # -- statistics ---------------------------------------------------------
     def latency_stats(self) -> dict:

@@ -55,7 +55,18 @@ class Workspace:
                                                     ctypes.byref(model.mlp_desc), num_rays)
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
+        self.num_rays = num_rays
         return self.buf.data_ptr(), self.buf.numel()
+
+    def error_word(self, c_geometry) -> int:
+        """The device error word of the last step run in this workspace (0 = every
+        tensor-core wait completed).  Synchronises the current stream."""
+        addr = _lib.lib.nectb_train_error_word(ctypes.byref(c_geometry.c_struct), int(self.num_rays),
+                                               self.buf.data_ptr())
+        if not addr:
+            raise RuntimeError("nectb_train_error_word: " + _lib.lib.nectb_last_error().decode())
+        off = addr - self.buf.data_ptr()
+        return int(self.buf[off:off + 4].view(torch.int32).item())
 
 
 def c_batch(batch: RayBatch, max_distance_traveled: float, loss: str, loss_scale: float = 1.0):
@@ -191,6 +202,10 @@ class Trainer:
         adam_step(self.model.mlp, self.mlp_grad, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas,
                   self.eps, self.weight_decay)
         return loss
+
+    def device_error(self) -> int:
+        """Error word of the last step (non-zero if a tensor-core wait timed out)."""
+        return self.workspace.error_word(self.c_geometry)
 
     def train_projection(self, projection: torch.Tensor, angle: float, t: float = 0.0) -> torch.Tensor | None:
         """All batches of one projection (flattened, min-max scaled, on device)."""
