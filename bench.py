@@ -63,7 +63,7 @@ def workload_spec(name: str, precision: str):
         enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=21, base_resolution=16,
                                 max_resolution_factor=2.0, nDetector=[512, 512], base_resolution_t=4)
         return dict(geo=geo, model=ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision),
-                    S=512, rays=1 << 18, n_angles=3600, turns=10, phantom="porous", n_dims=4)
+                    S=512, rays=1 << 18, n_angles=3600, turns=10, phantom="dynamic", n_dims=4)
     raise ValueError(name)
 
 
@@ -77,6 +77,15 @@ def make_projections(spec, geometry, n_proj: int, device, seed: int = 0):
     if spec["phantom"] == "ellipsoids":
         ph = phantoms.ellipsoid_phantom(20, seed)
         projs = torch.stack([phantoms.ellipsoid_projection(ph, geometry, float(a), device) for a in angles])
+    elif spec["phantom"] == "dynamic":
+        # each projection at its own t; Poisson noise at 1e4 incident photons on the attenuation
+        # expressed per object width (p / n), so that exp(-p) stays in the detector's range
+        ph = phantoms.dynamic_porous(geometry.nVoxel[0], seed=seed, attempts=60000)
+        projs = torch.stack([phantoms.dynamic_porous_projection(ph, geometry, float(a), float(t), device)
+                             for a, t in zip(angles, ts)])
+        gen = torch.Generator(device=projs.device).manual_seed(seed)
+        counts = torch.poisson(1e4 * torch.exp(-projs.double() / geometry.nVoxel[0]), generator=gen)
+        projs = (-torch.log(torch.clamp(counts, min=1.0) / 1e4) * geometry.nVoxel[0]).float()
     else:
         ph = phantoms.porous_phantom(geometry.nVoxel[0], seed=seed, attempts=60000)
         projs = torch.stack([phantoms.porous_projection(ph, geometry, float(a), device) for a in angles])
@@ -375,10 +384,13 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
     achieved = per_launch_bytes.get(dominant, 0.0) / (kernel_ms[dominant] / 1e3) / 1e9 if dominant in kernel_ms else None
-    traffic = None
-    tfile = ROOT / "profiles" / f"traffic_{args.workload}_{args.precision}.json"
+    traffic = None   # DRAM bytes per launch of the dominant kernel from the committed ncu capture
+    tfile = ROOT / "profiles" / "traffic_per_launch.txt"
     if tfile.exists():
-        traffic = json.loads(tfile.read_text()).get(dominant)
+        for line in tfile.read_text().splitlines():
+            f = line.split()
+            if len(f) == 4 and not line.startswith("#") and f[:3] == [args.workload, args.precision, dominant]:
+                traffic = float(f[3])
 
     # ---- end to end through the public API, host buffers (pinned projection in, loss out)
     host = projs.cpu().pin_memory()
@@ -435,6 +447,62 @@ def main():
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+def run_psnr(args):
+    """Time-to-PSNR of the mixed path against the plain fp32 path at equal
+    iterations on the static parallel-beam workload (128^3 phantom of 20
+    ellipsoids, 180 exact projections over [0, pi) on 128^2 pixels, S = 256,
+    one full projection (16,384 rays) per step, L2 loss, Adam lr 1e-3).
+    PSNR (-10 log10 MSE) and 3D SSIM of the exported volume against the
+    phantom; the untrained network and filtered back-projection (no learned
+    model) are reported beside them."""
+    from nect_b200 import phantoms
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig
+    from nect_b200.reconstruct import fbp_parallel, fit, psnr, ssim3d
+    from nect_b200.sampling import Geometry
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    geo = Geometry(nDetector=[128, 128], dDetector=[1 / 128, 1 / 128], mode="parallel", nVoxel=[128] * 3,
+                   dVoxel=[1 / 128] * 3)
+    ph = phantoms.ellipsoid_phantom(20, 0)
+    angles = np.linspace(0, math.pi, 180, endpoint=False)
+    projs = torch.stack([phantoms.ellipsoid_projection(ph, geo, float(a), dev) for a in angles])
+    truth = phantoms.ellipsoid_volume(ph, 128, dev)
+    fbp = fbp_parallel(projs, geo, angles)
+    out = {"metric": "time-to-PSNR, mixed vs plain fp32 at equal iterations", "unit": "s",
+           "higher_is_better": False, "n_gpus": 1, "steps": args.psnr_steps,
+           "config": {"workload": "c1_static_parallel: 128^3 ellipsoid phantom, 180 views over [0,pi), 128^2 "
+                                  "detector, S=256, 16,384 rays/step, hash 16x2 2^19 base 16 finest 1024, MLP 2x64, "
+                                  "L2, Adam 1e-3", "data": "synthetic (seeded phantom, exact chord-length projections)"},
+           "fbp": {"psnr": psnr(fbp, truth), "ssim": ssim3d(fbp, truth)}}
+    runs = {}
+    for precision in ("plain_fp32", "mixed"):
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=19, base_resolution=16,
+                                finest_resolution=1024)
+        cfg = ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), precision)
+
+        def evaluate(rec):
+            v = rec.volume()
+            return {"psnr": psnr(v, truth), "ssim": ssim3d(v, truth)}
+
+        rec = fit(geo, projs, angles, model_cfg=cfg, niter=args.psnr_steps, lr=1e-3, rays_per_batch=65536,
+                  points_per_ray=256, loss="l2", seed=0, device=dev, evaluate=evaluate, eval_every=args.eval_every)
+        runs[precision] = {"history": [(st, round(sec, 4), m["psnr"], m["ssim"]) for st, sec, m in rec.history],
+                           "final_psnr": rec.history[-1][2]["psnr"], "final_ssim": rec.history[-1][2]["ssim"],
+                           "untrained_psnr": rec.history[0][2]["psnr"], "train_seconds": rec.train_seconds}
+    target = runs["plain_fp32"]["final_psnr"] - 0.1
+    for precision, r in runs.items():
+        hit = next(((st, sec) for st, sec, p_, _ in r["history"] if p_ >= target), None)
+        r["time_to_target_s"] = hit[1] if hit else None
+        r["steps_to_target"] = hit[0] if hit else None
+    out["target_psnr"] = target
+    out["runs"] = runs
+    out["psnr_gap_db"] = runs["mixed"]["final_psnr"] - runs["plain_fp32"]["final_psnr"]
+    out["value"] = runs["mixed"]["time_to_target_s"]
+    out["plain_value"] = runs["plain_fp32"]["time_to_target_s"]
+    print(json.dumps(out))
 
 
 def run_serving(args):
@@ -542,7 +610,13 @@ def run_serving(args):
 
 
 if __name__ == "__main__":
-    if "--serving" in sys.argv:
+    if "--psnr" in sys.argv:
+        ap = argparse.ArgumentParser()
+        ap.add_argument("--psnr", action="store_true")
+        ap.add_argument("--psnr-steps", type=int, default=2000)
+        ap.add_argument("--eval-every", type=int, default=100)
+        run_psnr(ap.parse_args())
+    elif "--serving" in sys.argv:
         ap = argparse.ArgumentParser()
         ap.add_argument("--serving", action="store_true")
         ap.add_argument("--serve-rate", type=float, default=200.0)

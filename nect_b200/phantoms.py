@@ -247,6 +247,108 @@ def porous_volume(ph: PorousPhantom, n: int, device) -> torch.Tensor:
     return vol
 
 
+# ------------------------------------------------ dynamic porous medium (C3) ----
+@dataclass
+class DynamicPorousPhantom:
+    base: PorousPhantom
+    shrink: np.ndarray        # [G] radius loss per unit t (0 for grains that do not shrink)
+    noise: np.ndarray         # [K,K,K] value-noise lattice in [-1, 1]
+    mu_brine: float = 0.5
+    front_width: float = 4.0  # voxels
+    noise_amp: float = 12.0   # voxels of interface displacement
+
+    def radii(self, t: float) -> np.ndarray:
+        return np.maximum(self.base.radii - self.shrink * t, 0.0)
+
+    def front_z(self, t: float) -> float:
+        """Height of the unperturbed front: rises through the cylinder as t goes 0 -> 1."""
+        h = self.base.half_height
+        return -h - 2 * self.front_width + (2 * h + 4 * self.front_width) * t
+
+
+def dynamic_porous(n: int = 256, seed: int = 0, n_shrinking: int = 30, lattice: int = 9,
+                   attempts: int = 400_000) -> DynamicPorousPhantom:
+    """The porous medium plus a brine front (attenuation 0.5) rising in z as
+    sigmoid((z0(t) + noise(x) - z) / w), its interface displaced by seeded
+    trilinear value noise, and ``n_shrinking`` grains whose radii shrink
+    linearly at U[0.2, 1.0] voxels per unit t.  The brine adds
+    (0.5 - 0.2) * front over the whole cylinder (grains included), so every
+    part of the object has a closed form except the front, which is
+    ray-marched."""
+    base = porous_phantom(n, seed=seed, attempts=attempts)
+    rng = np.random.default_rng(seed + 1)
+    shrink = np.zeros(len(base.radii))
+    pick = rng.choice(len(base.radii), size=min(n_shrinking, len(base.radii)), replace=False)
+    shrink[pick] = rng.uniform(0.2, 1.0, pick.size)
+    noise = rng.uniform(-1.0, 1.0, (lattice, lattice, lattice))
+    return DynamicPorousPhantom(base, shrink, noise)
+
+
+def _front(ph: DynamicPorousPhantom, x: torch.Tensor, t: float) -> torch.Tensor:
+    """Brine fraction in [0,1] at world points x [..., 3] (x, y, z), voxel units."""
+    b = ph.base
+    K = ph.noise.shape[0]
+    lat = torch.as_tensor(ph.noise, device=x.device, dtype=x.dtype)
+    # lattice spans the cylinder's bounding box
+    g = torch.stack([(x[..., 0] + b.radius) / (2 * b.radius), (x[..., 1] + b.radius) / (2 * b.radius),
+                     (x[..., 2] + b.half_height) / (2 * b.half_height)], -1).clamp(0, 1) * (K - 1)
+    i0 = g.floor().long().clamp(max=K - 2)
+    f = g - i0
+    val = torch.zeros(x.shape[:-1], device=x.device, dtype=x.dtype)
+    for cx in (0, 1):
+        for cy in (0, 1):
+            for cz in (0, 1):
+                w = ((f[..., 0] if cx else 1 - f[..., 0]) * (f[..., 1] if cy else 1 - f[..., 1])
+                     * (f[..., 2] if cz else 1 - f[..., 2]))
+                val = val + w * lat[i0[..., 0] + cx, i0[..., 1] + cy, i0[..., 2] + cz]
+    return torch.sigmoid((ph.front_z(t) + ph.noise_amp * val - x[..., 2]) / ph.front_width)
+
+
+def dynamic_porous_projection(ph: DynamicPorousPhantom, geometry, angle: float, t: float, device,
+                              samples_per_voxel: int = 4, chunk: int = 8192) -> torch.Tensor:
+    """Line integrals at (angle, t): exact chords of the cylinder and of the
+    grains at their radii at t, plus the brine front ray-marched at
+    ``samples_per_voxel`` midpoint samples per voxel of path inside the
+    cylinder."""
+    b = ph.base
+    static = porous_projection(b, geometry, angle, device,
+                               grain_scale=np.divide(ph.radii(t), b.radii, out=np.zeros_like(b.radii),
+                                                     where=b.radii > 0)).double().reshape(-1)
+    o, d = detector_rays(geometry, angle, device)
+    # entry/exit of the cylinder's bounding box along each ray
+    lo = torch.tensor([-b.radius, -b.radius, -b.half_height], device=device, dtype=torch.float64)
+    hi = -lo
+    safe = torch.where(d.abs() > 1e-12, d, torch.full_like(d, 1e-12))
+    t0 = torch.minimum((lo - o) / safe, (hi - o) / safe).max(1).values
+    t1 = torch.maximum((lo - o) / safe, (hi - o) / safe).min(1).values
+    L = torch.clamp(t1 - t0, min=0)
+    n_s = int(math.ceil(float(L.max()) * samples_per_voxel)) if L.numel() else 0
+    brine = torch.zeros_like(L)
+    if n_s > 0:
+        u = (torch.arange(n_s, device=device, dtype=torch.float64) + 0.5) / n_s
+        for i in range(0, o.shape[0], chunk):
+            tt = t0[i:i + chunk, None] + u[None] * L[i:i + chunk, None]                   # [c, n_s]
+            pts = o[i:i + chunk, None, :] + tt[..., None] * d[i:i + chunk, None, :]       # [c, n_s, 3]
+            inside = (pts[..., 0] ** 2 + pts[..., 1] ** 2 <= b.radius ** 2) & (pts[..., 2].abs() <= b.half_height)
+            fr = _front(ph, pts, t) * inside
+            brine[i:i + chunk] = fr.sum(1) * (L[i:i + chunk] / n_s)
+    out = static + (ph.mu_brine - b.mu_cyl) * brine
+    return out.to(torch.float32).reshape(geometry.nDetector[0], geometry.nDetector[1])
+
+
+def dynamic_porous_volume(ph: DynamicPorousPhantom, n: int, t: float, device) -> torch.Tensor:
+    """Voxel-centre attenuation [z, y, x] at time t."""
+    b = ph.base
+    shrunk = PorousPhantom(b.radius, b.half_height, b.mu_cyl, b.mu_grain, b.centers, ph.radii(t), b.packing)
+    vol = porous_volume(shrunk, n, device).double()
+    c = torch.arange(n, device=device, dtype=torch.float64) - (n - 1) / 2
+    Z, Y, X = torch.meshgrid(c, c, c, indexing="ij")
+    pts = torch.stack([X, Y, Z], -1)
+    inside = (X ** 2 + Y ** 2 <= b.radius ** 2) & (Z.abs() <= b.half_height)
+    vol = vol + (ph.mu_brine - b.mu_cyl) * _front(ph, pts, t) * inside
+    return vol.float()
+
+
 def minmax_scale(projs: torch.Tensor):
     """Dataset-wide min-max scaling to [0,1] (nect/data.py:177-183)."""
     mn = projs.min()

@@ -1,0 +1,217 @@
+"""User entry point: reconstruct a volume from projections on the fused kernels.
+
+Mirrors ``nect.reconstruct`` (nect/reconstruct.py:113-131) for the hot path
+this package replaces: a hash-grid model is trained on the projections with
+the fused sample -> encode -> MLP -> line integral -> loss -> backward step
+(nectb_train_step) and the fused Adam update, then exported on a regular grid
+with create_volume's de-normalisation (nect/trainers/base_trainer.py:402-450).
+
+Scheduling follows BaseTrainer.fit (base_trainer.py:492-655) with one batch
+per projection visit: each step takes the next projection of a seeded random
+order, a device randperm of its pixels and one batch of rays.  The reference's
+progressive schedules (detector binning, points-per-ray ramp), S3IM and TV
+regularisers and its lr warm-up are not part of this path.
+"""
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .config import HashEncoderConfig, MLPNetConfig, ModelConfig, get_model
+from .network import _HashGridModel
+from .sampling import Geometry
+from .serving import denormalisation, query_points, volume_items
+from .trainer import Trainer
+
+
+@dataclass
+class Reconstruction:
+    """A trained model with the dataset scaling needed to export volumes."""
+    model: _HashGridModel
+    geometry: Geometry
+    minimum: float
+    maximum: float
+    trainer: Trainer
+    history: list = field(default_factory=list)   # (step, seconds of training, metrics dict)
+
+    def volume(self, t: float = 0.0, shape: tuple | None = None) -> torch.Tensor:
+        """Attenuation on the voxel-centre grid [z, y, x] (create_volume)."""
+        shape = tuple(shape or self.geometry.nVoxel)
+        scale, offset = denormalisation(self.geometry.max_distance_traveled, self.minimum, self.maximum)
+        out = torch.empty(shape, device=self.model.table.device)
+        query_points(self.model, volume_items(out, shape, t, scale, offset))
+        return out
+
+
+def default_model_config(geometry: Geometry, mode: str, precision: str) -> ModelConfig:
+    """The model of the static parallel-beam workload: 16 levels x 2 features,
+    2^19 entries, base 16, finest 2 x the largest detector extent, 2 x 64 ReLU
+    MLP with softplus output (temporal base 4 for dynamic scans).  The
+    reference's own preset (nect/cfg/static/hash_grid.yaml: 19 levels x 4
+    features, 6 x 64 LeakyReLU) is outside the kernel instantiations."""
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=19, base_resolution=16,
+                            max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
+                            nVoxel=list(geometry.nVoxel), base_resolution_t=4 if mode == "dynamic" else None)
+    return ModelConfig("hash_grid_4d" if mode == "dynamic" else "hash_grid", enc, MLPNetConfig(n_hidden_layers=2),
+                       precision)
+
+
+def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *, model_cfg: ModelConfig | None = None,
+        precision: str = "mixed", niter: int = 2000, lr: float = 1e-3, rays_per_batch: int = 65536,
+        points_per_ray: int | None = None, loss: str = "l2", seed: int = 0, device="cuda",
+        evaluate=None, eval_every: int = 0) -> Reconstruction:
+    """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
+    ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
+    scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
+    called every ``eval_every`` steps (and at the end) outside the training
+    time; its dict is recorded in ``history``."""
+    dev = torch.device(device)
+    proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
+    n_proj = proj.shape[0]
+    mn, mx = float(proj.min()), float(proj.max())
+    proj = ((proj - mn) / (mx - mn)).reshape(n_proj, -1).contiguous()
+    angles = [float(a) for a in angles]
+    if timesteps is None:
+        ts = [0.0] * n_proj
+    else:
+        tt = np.asarray(timesteps, np.float64)
+        ts = list(tt / tt.max()) if tt.max() > 0 else [0.0] * n_proj   # nect/data.py:78-79
+    mode = "static" if timesteps is None else "dynamic"
+    cfg = model_cfg or default_model_config(geometry, mode, precision)
+    torch.manual_seed(seed)
+    model = get_model(cfg, device=dev)
+    S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
+    trainer = Trainer(model, geometry, points_per_batch=rays_per_batch * S, points_per_ray=S, loss=loss, lr=lr,
+                      device=dev)
+    rec = Reconstruction(model, geometry, mn, mx, trainer)
+    order = np.random.default_rng(seed).permutation(n_proj)
+    P = proj.shape[1]
+    train_s = 0.0
+
+    def record(step):
+        if evaluate is not None:
+            torch.cuda.synchronize(dev)
+            rec.history.append((step, train_s, evaluate(rec)))
+
+    record(0)
+    for step in range(1, niter + 1):
+        k = int(order[(step - 1) % n_proj])
+        if (step - 1) % n_proj == n_proj - 1:
+            order = np.random.default_rng(seed + step).permutation(n_proj)
+        t0 = time.perf_counter()
+        perm = torch.randperm(P, dtype=torch.int64, device=dev)
+        batch = trainer.make_batch(perm, 0, angles[k], proj[k], ts[k])
+        trainer.step(batch)
+        if eval_every and (step % eval_every == 0 or step == niter):
+            torch.cuda.synchronize(dev)
+            train_s += time.perf_counter() - t0
+            record(step)
+        else:
+            train_s += time.perf_counter() - t0
+    torch.cuda.synchronize(dev)
+    rec.train_seconds = train_s
+    return rec
+
+
+def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=None, radians: bool = True,
+                niter: int | None = None, lr: float | None = None, timesteps=None, precision: str = "mixed",
+                **kw):
+    """``nect.reconstruct`` for arrays of projections: returns the volume
+    (np.ndarray [z, y, x]) for mode "static" and the Reconstruction (export
+    any t with ``.volume(t)``) for mode "dynamic"."""
+    if angles is None:
+        angles = geometry.angles
+    angles = np.asarray(angles, np.float64)
+    if not radians:
+        angles = np.deg2rad(angles)
+    if mode == "dynamic" and timesteps is None:
+        timesteps = getattr(geometry, "timesteps", None)
+        if timesteps is None:
+            timesteps = np.arange(len(angles), dtype=np.float64)
+    rec = fit(geometry, projections, angles, timesteps if mode == "dynamic" else None, precision=precision,
+              niter=niter or 2000, lr=lr or 1e-3, **kw)
+    if mode == "static":
+        return rec.volume().cpu().numpy()
+    return rec
+
+
+# ------------------------------------------------------------ evaluation ----
+def psnr(x: torch.Tensor, y: torch.Tensor) -> float:
+    """-10 log10(MSE), as nect/src/evaluation/evaluator.py:17-19."""
+    return float(-10 * torch.log10(torch.nn.functional.mse_loss(x.float(), y.float())))
+
+
+def ssim3d(x: torch.Tensor, y: torch.Tensor, data_range: float | None = None, win: int = 7,
+           sigma: float = 1.5) -> float:
+    """Structural similarity (Wang et al., IEEE TIP 13(4), 2004) with a
+    separable Gaussian window over three dimensions (K1 = 0.01, K2 = 0.03)."""
+    x = x.float()[None, None]
+    y = y.float()[None, None]
+    L = data_range if data_range is not None else float(y.max() - y.min())
+    g = torch.exp(-((torch.arange(win, device=x.device) - win // 2) ** 2) / (2 * sigma ** 2))
+    g = (g / g.sum()).float()
+
+    def blur(v):
+        for dim in range(3):
+            shape = [1, 1, 1, 1, 1]
+            shape[2 + dim] = win
+            v = torch.nn.functional.conv3d(v, g.view(shape))
+        return v
+
+    mx, my = blur(x), blur(y)
+    sxx = blur(x * x) - mx * mx
+    syy = blur(y * y) - my * my
+    sxy = blur(x * y) - mx * my
+    c1, c2 = (0.01 * L) ** 2, (0.03 * L) ** 2
+    s = ((2 * mx * my + c1) * (2 * sxy + c2)) / ((mx * mx + my * my + c1) * (sxx + syy + c2))
+    return float(s.mean())
+
+
+def fbp_parallel(projections: torch.Tensor, geometry: Geometry, angles) -> torch.Tensor:
+    """Filtered back-projection (Ram-Lak filter, linear interpolation) of
+    parallel-beam projections [N, rows, cols] on the geometry's voxel grid
+    [z, y, x]: the classical reconstruction without a learned model that the
+    reference runs through tigre (nect/fdk.py).  Angles must cover [0, pi)
+    evenly.  Detector conventions as the sampler (ct_sampling.cu:226-256):
+    column u maps to world -y before rotation, row v to z, so the ray of
+    pixel u at angle a is {x sin a - y cos a = u}."""
+    if geometry.mode != "parallel":
+        raise ValueError("fbp_parallel needs a parallel-beam geometry")
+    dev = projections.device
+    p = projections.double()
+    n, nr, nc = p.shape
+    du = geometry.dDetector[1]
+    # Ram-Lak kernel in the spatial domain, zero-padded linear convolution via FFT
+    m = 1 << int(math.ceil(math.log2(2 * nc)))
+    k = torch.arange(-(nc - 1), nc, device=dev, dtype=torch.float64)
+    h = torch.zeros_like(k)
+    h[k == 0] = 1.0 / (4 * du * du)
+    odd = (k.abs() % 2) == 1
+    h[odd] = -1.0 / (math.pi ** 2 * k[odd] ** 2 * du * du)
+    H = torch.fft.rfft(h, m)
+    q = torch.fft.irfft(torch.fft.rfft(p, m, dim=-1) * H, m, dim=-1)[..., nc - 1:2 * nc - 1] * du
+    nz, ny, nx = geometry.nVoxel
+    dz, dy, dx = geometry.dVoxel
+    xs = (torch.arange(nx, device=dev, dtype=torch.float64) - (nx - 1) / 2) * dx + geometry.offOrigin[2]
+    ys = (torch.arange(ny, device=dev, dtype=torch.float64) - (ny - 1) / 2) * dy + geometry.offOrigin[1]
+    Y, X = torch.meshgrid(ys, xs, indexing="ij")
+    u0 = -(nc - 1) / 2 * du + geometry.offDetector[1]
+    zs = (torch.arange(nz, device=dev, dtype=torch.float64) - (nz - 1) / 2) * dz + geometry.offOrigin[0]
+    rows = ((zs - geometry.offDetector[0]) / geometry.dDetector[0] + (nr - 1) / 2).round().long().clamp(0, nr - 1)
+    vol = torch.zeros(nz, ny, nx, device=dev, dtype=torch.float64)
+    for i, a in enumerate(angles):
+        u = X * math.sin(a) - (Y - geometry.COR) * math.cos(a)
+        f = (u - u0) / du
+        j0 = f.floor().long()
+        w = f - j0
+        ok0 = (j0 >= 0) & (j0 < nc)
+        ok1 = (j0 + 1 >= 0) & (j0 + 1 < nc)
+        qi = q[i][rows]                                   # [nz, nc]
+        v0 = qi[:, j0.clamp(0, nc - 1)] * ok0
+        v1 = qi[:, (j0 + 1).clamp(0, nc - 1)] * ok1
+        vol += v0 * (1 - w) + v1 * w
+    return (vol * math.pi / len(angles)).float()

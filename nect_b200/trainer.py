@@ -56,13 +56,14 @@ class Workspace:
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         self.num_rays = num_rays
+        self.c_geometry = c_geometry
         return self.buf.data_ptr(), self.buf.numel()
 
-    def error_word(self, c_geometry) -> int:
+    def error_word(self, c_geometry=None) -> int:
         """The device error word of the last step run in this workspace (0 = every
         tensor-core wait completed).  Synchronises the current stream."""
-        addr = _lib.lib.nectb_train_error_word(ctypes.byref(c_geometry.c_struct), int(self.num_rays),
-                                               self.buf.data_ptr())
+        cg = c_geometry if c_geometry is not None else self.c_geometry
+        addr = _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), int(self.num_rays), self.buf.data_ptr())
         if not addr:
             raise RuntimeError("nectb_train_error_word: " + _lib.lib.nectb_last_error().decode())
         off = addr - self.buf.data_ptr()

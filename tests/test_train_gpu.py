@@ -83,7 +83,7 @@ def test_model_forward_matches_oracle(cuda_device, n_dims, precision):
     assert torch.allclose(out, ref, rtol=1e-5, atol=1e-6), (out - ref).abs().max()
 
 
-def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=False):
+def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=False, ws=None):
     from nect_b200.sampling import Geometry
     from nect_b200.trainer import RayBatch, Workspace, train_step
 
@@ -110,7 +110,8 @@ def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=Fal
                      max_ray_distance_per_point=maxd, jitter=jitter, detector_offset=det_off, projection=proj, t=t)
     tg = torch.zeros_like(m.table)
     mg = torch.zeros_like(m.mlp)
-    L, y_pred = train_step(m, cg, batch, geo.max_distance_traveled, tg, mg, Workspace(), loss)
+    L, y_pred = train_step(m, cg, batch, geo.max_distance_traveled, tg, mg, ws if ws is not None else Workspace(),
+                           loss)
     torch.cuda.synchronize()
     # oracle: same samples (C oracle with the device's trig values), fp64 network
     a = torch.tensor([angle, 0.0], dtype=torch.float32, device="cuda")
@@ -164,8 +165,10 @@ def test_mixed_error_word_clear(cuda_device):
     """The bounded mbarrier waits of the tensor-core kernels never time out."""
     from nect_b200.trainer import Workspace
 
-    ws = Workspace()
-    run_train_case(3, "mixed", "l2", "cone")
+    for n_dims in (3, 4):
+        ws = Workspace()
+        run_train_case(n_dims, "mixed", "l2", "cone", ws=ws)
+        assert ws.error_word() == 0
 
 
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
