@@ -210,7 +210,7 @@ def collect_profile():
     n = (ctypes.c_int32 * 8)()
     ms = (ctypes.c_double * 8)()
     _lib.lib.nectb_profile_collect(ctypes.addressof(n), ctypes.addressof(ms))
-    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "slot6", "slot7"]
+    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "scatter", "slot7"]
     return {names[i]: (int(n[i]), float(ms[i])) for i in range(8) if n[i]}
 
 
@@ -369,13 +369,18 @@ def main():
     gather = enc.n_levels * corners * enc.n_features_per_level * feat_bytes
     scatter = enc.n_levels * corners * enc.n_features_per_level * 4
     n_params = model.table.numel() + model.mlp.numel()
-    per_launch_bytes = {
-        "backward": n_valid / args.steps * (gather + scatter),
+    staged = "scatter" in prof   # the mixed backward ran as tensor-core pass + staged scatter passes
+    stage_io = enc.n_levels * enc.n_features_per_level * 4   # staged dL/d(encoding) per sample, each way
+    step_bytes = {   # algorithmic bytes per step of each kernel kind
+        "backward": n_valid / args.steps * (gather + (stage_io if staged else scatter)),
+        "scatter": n_valid / args.steps * (scatter + stage_io),
         "forward": n_valid / args.steps * gather,
-        "adam": n_params * (32 + (2 if args.precision == "mixed" else 0)) / 2,  # two launches per step
+        "adam": n_params * (34 if args.precision == "mixed" else 32),
         "ray_prep": rays_per_step * 64.0,
     }
     kernel_ms = {k: v[1] / max(v[0], 1) for k, v in prof.items()}
+    launches_per_step = {k: v[0] / args.steps for k, v in prof.items()}
+    per_launch_bytes = {k: step_bytes[k] / launches_per_step[k] for k in prof if k in step_bytes}
     dominant = max(prof, key=lambda k: prof[k][1]) if prof else "backward"
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
@@ -435,7 +440,7 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes.get(dominant),
-                     "kernel_ms": kernel_ms},
+                     "kernel_ms": kernel_ms, "launches_per_step": launches_per_step},
         "cpu_baseline": cpu_baseline,
         "e2e": e2e,
         "gpu_launches": gpu_launches,

@@ -238,6 +238,19 @@ typedef struct NectbTrainBatch {
 size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                    const NectbMLP* mlp, int32_t num_rays);
 
+/* Recommended staging bytes for the mixed path's two-pass backward, to add to
+ * nectb_train_workspace_bytes(): with them the backward runs in 8 rounds of
+ * scheduling indices (detector pixels, or batch positions when the batch
+ * repeats a pixel); each round's tensor-core pass writes dL/d(encoding) of its
+ * samples (fp32, num_points_per_ray * n_levels * n_features per index) and
+ * scatter passes over level groups apply it to grid_grad with the gradient
+ * slice of each group resident in L2.  Less staging gives more rounds; when
+ * it would take more than 64 rounds the single-pass backward (scatter inside
+ * the tensor-core kernel) runs instead.  Returns 0 for the plain fp32 path, which does not
+ * stage.  No reference counterpart. */
+size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                 const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray);
+
 /* Device address of the error word inside a training (or re-projection)
  * workspace of num_rays rays (num_rays = detector pixels for a
  * re-projection); workspace NULL gives the word of the static scratch of
@@ -254,7 +267,9 @@ const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_
  * (fp32 or fp16); mlp_params fp32.  Gradients are accumulated (+=) into
  * grid_grad (fp32, nectb_hashgrid_layout total * n_features) and mlp_grad
  * (fp32, nectb_mlp_param_count).  y_pred[num_rays] and loss[1] are written.
- * workspace: nectb_train_workspace_bytes() bytes of device memory. */
+ * workspace: at least nectb_train_workspace_bytes() bytes of device memory;
+ * bytes beyond that are staging for the mixed path's two-pass backward
+ * (nectb_train_staging_bytes). */
 int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid,
                      const NectbMLP* mlp, const void* grid_params,
                      const float* mlp_params, const NectbTrainBatch* batch,
@@ -293,7 +308,7 @@ int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq
 /* Per-kernel timing of the library's own launches with CUDA events recorded
  * on the launch stream around each kernel (off by default).  Slots:
  * 0 ray preparation, 1 forward, 2 backward, 3 Adam, 4 sampling, 5 model
- * forward.  nectb_profile_collect waits for the recorded events, adds their
+ * forward and queries, 6 staged gradient scatter.  nectb_profile_collect waits for the recorded events, adds their
  * durations and returns per slot the launch count and total milliseconds.
  * No counterpart in the reference, which has no profiler. */
 #define NECTB_PROFILE_SLOTS 8

@@ -135,6 +135,8 @@ _SIGNATURES = {
          c_f32, c_int, c_f32, c_f32, c_ptr, c_ptr, c_size, c_int, c_ptr],
     ),
     "nectb_train_error_word": (c_ptr, [ctypes.POINTER(NectbGeometry), c_int, c_ptr]),
+    "nectb_train_staging_bytes": (
+        c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int, c_int]),
     "nectb_selftest_bounded_wait": (c_int, [c_ptr, ctypes.c_uint32, c_ptr]),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),

@@ -41,7 +41,15 @@ inline void set_smem(K k, size_t bytes, bool shares_sms) {
 
 // Records CUDA events around a kernel launch while profiling is enabled
 // (nectb_profile_enable); slots are listed in include/nectb.h.
-enum { kProfRayPrep = 0, kProfForward = 1, kProfBackward = 2, kProfAdam = 3, kProfSample = 4, kProfModel = 5 };
+enum {
+  kProfRayPrep = 0,
+  kProfForward = 1,
+  kProfBackward = 2,
+  kProfAdam = 3,
+  kProfSample = 4,
+  kProfModel = 5,
+  kProfScatter = 6
+};
 class ProfScope {
  public:
   ProfScope(int slot, cudaStream_t s);

@@ -212,17 +212,21 @@ __device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, doub
 // run's first lane, so the table sees one atomic per (cell, corner) instead of
 // one per sample.  Other levels scatter per sample.  Sums equal the
 // per-sample atomics up to fp32 reassociation.
+//
+// dL/d(feature f of level l) is read at dsrc[l * lstride + f * fstride]; only
+// levels [l0, l1) are scattered.
 template <int D, int F>
 __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict__ grad, const float* x, bool valid,
-                                             const float* dsrc, int stride, uint32_t agg_levels) {
+                                             const float* dsrc, int64_t lstride, int fstride, uint32_t agg_levels,
+                                             int l0, int l1) {
   const int lane = threadIdx.x & 31;
 #pragma unroll 1
-  for (int l = 0; l < g.n_levels; ++l) {
+  for (int l = l0; l < l1; ++l) {
     LevelCorners<D> lc;
     level_corners<D>(g, l, x, lc);
     float d[F];
 #pragma unroll
-    for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[(l * F + f) * stride] : 0.f;
+    for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[l * lstride + f * fstride] : 0.f;
     float* base = grad + g.offset[l] * F;
     if ((agg_levels >> l) & 1u) {
       // runs of lanes in the same spatial cell (t is the same for the whole

@@ -106,7 +106,7 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   a.loss_type = batch->loss_type;
   a.loss_scale = batch->loss_scale;
   a.max_blocks = 0;
-  Workspace ws = carve_workspace(workspace, a.num_rays, P);
+  Workspace ws = carve_workspace(workspace, a.num_rays, P, workspace_size);
   if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
   if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
   {
@@ -122,6 +122,17 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
                        y_pred, loss, s);
   }
   return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, a, ws, grid_grad, mlp_grad, y_pred, loss, s);
+}
+
+extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                            const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray) {
+  using namespace nectb;
+  if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0) return 0;
+  if (mlp->compute_dtype == NECTB_F32) return 0;  // the plain path scatters in its backward
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  const int64_t N = std::max<int64_t>(num_rays, P);
+  const int64_t per_round = ceil_div(N, kStagedRounds);
+  return (size_t)per_round * num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
 }
 
 extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr,

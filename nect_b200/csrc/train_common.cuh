@@ -44,22 +44,38 @@ struct TrainArgs {
 
 enum : unsigned int { kFlagDuplicatePixels = 1u };
 
+// The two-pass mixed backward: rounds the recommended staging buffer is sized
+// for (nectb_train_staging_bytes), and the most rounds a smaller staging
+// buffer may need before the fused single-pass backward is used instead.
+constexpr int kStagedRounds = 8;
+constexpr int kMaxStagedRounds = 64;
+
 // Workspace: RayRec[R] | slot[P] (int32: batch index of the ray through each
 // detector pixel, -1 if none) | 64-byte control block (scheduling cursors of
 // the forward and backward, error word, flags).
+// Any workspace bytes beyond workspace_bytes() (from a 256-byte boundary) are
+// the staging buffer of the two-pass mixed backward.
 struct Workspace {
   RayRec* rays;
   int32_t* slot;
-  unsigned int* counters;  // [0] forward cursor, [1] backward cursor, [2] error word, [3] flags
+  unsigned int* counters;  // [0] forward cursor, [1] backward cursor, [2] error word, [3] flags,
+                           // [5] scatter cursor
+  float* stage = nullptr;
+  size_t stage_bytes = 0;
 };
 
 inline size_t workspace_bytes(int R, int P) { return (size_t)R * sizeof(RayRec) + (size_t)P * 4 + 256; }
 
-inline Workspace carve_workspace(void* ws, int R, int P) {
+inline Workspace carve_workspace(void* ws, int R, int P, size_t size = 0) {
   Workspace w;
   w.rays = (RayRec*)ws;
   w.slot = (int32_t*)((char*)ws + (size_t)R * sizeof(RayRec));
   w.counters = (unsigned int*)((char*)w.slot + (((size_t)P * 4 + 63) & ~size_t(63)));
+  const size_t base = (workspace_bytes(R, P) + 255) & ~size_t(255);
+  if (size > base) {
+    w.stage = (float*)((char*)ws + base);
+    w.stage_bytes = size - base;
+  }
   return w;
 }
 
@@ -88,18 +104,23 @@ __device__ __forceinline__ RayRec load_ray(const RayRec* recs, int r) { return r
 // in detector-pixel order (neighbouring rays run together, so the blocks in
 // flight touch a compact part of the tables and the L2 keeps it), or in batch
 // order when the batch repeats a pixel.  Returns -1 when none are left.
+// The scheduling index (pixel, or batch position) of the returned ray is
+// written to *sched; only indices in [lo, hi) are handed out (a round of the
+// staged backward), the cursor counting from lo.
 __device__ __forceinline__ int next_ray(unsigned int* cursor, const int32_t* __restrict__ slot,
-                                        const RayRec* __restrict__ recs, int R, int P, bool by_pixel, int lane) {
+                                        const RayRec* __restrict__ recs, int R, int P, bool by_pixel, int lane,
+                                        int lo = 0, int hi = 0x7fffffff, int* sched = nullptr) {
+  const unsigned int end = (unsigned)min(hi, by_pixel ? P : R);
   while (true) {
     unsigned int idx = 0;
-    if (lane == 0) idx = atomicAdd(cursor, 1u);
+    if (lane == 0) idx = (unsigned)lo + atomicAdd(cursor, 1u);
     idx = __shfl_sync(0xffffffffu, idx, 0);
+    if (idx >= end) return -1;
+    if (sched) *sched = (int)idx;
     if (by_pixel) {
-      if (idx >= (unsigned)P) return -1;
       const int r = slot[idx];
       if (r >= 0) return r;
     } else {
-      if (idx >= (unsigned)R) return -1;
       if (recs[idx].count > 0) return (int)idx;
     }
   }

@@ -30,6 +30,7 @@ namespace nectb {
 namespace {
 
 constexpr int kMixThreads = 128;
+constexpr int kScatterThreads = 256;
 constexpr uint32_t kTile = 128 * 128;  // bytes of a [128][64 bf16] tile
 constexpr uint32_t kWTile = 64 * 128;  // bytes of a [64][64 bf16] tile
 
@@ -105,6 +106,7 @@ __device__ __forceinline__ void ld64(uint32_t taddr, float* v) {
 struct RayCursor {
   int ray = -1;
   int base = 0;
+  int sched = 0;  // scheduling index (detector pixel, or batch position) of the ray
   RayRec rec;
 };
 
@@ -112,10 +114,11 @@ struct RayCursor {
 // scheduler when the current one is done).  Returns false when no rays are
 // left.  Rays without samples were finalised by the preparation kernel.
 __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* cursor,
-                                           const int32_t* slot, const TrainArgs& a, bool by_pixel, int lane) {
+                                           const int32_t* slot, const TrainArgs& a, bool by_pixel, int lane,
+                                           int lo = 0, int hi = 0x7fffffff) {
   if (cur.ray >= a.num_rays) return false;
   if (cur.ray >= 0 && cur.base < cur.rec.count) return true;
-  const int r = next_ray(cursor, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane);
+  const int r = next_ray(cursor, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane, lo, hi, &cur.sched);
   if (r < 0) {
     cur.ray = a.num_rays;
     cur.rec.count = 0;
@@ -269,11 +272,16 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   }
 }
 
-template <int D, int F>
+// Staged mode (kStaged): instead of scattering, dL/d(encoding) of every sample
+// is written to the staging buffer, level-major: stage[(l * slots + s) * F + f]
+// with s = (scheduling index - lo) * S + sample, for the rays whose
+// scheduling index lies in [lo, hi); scatter_stage_kernel applies it.
+template <int D, int F, bool kStaged>
 __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad) {
+                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
+                 float* __restrict__ stage, int64_t slots) {
   constexpr int IN = 16 * F;
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   unsigned int* err = ctrl + 2;
@@ -323,7 +331,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   RayCursor cur;
   bool timed_out = false;
   while (true) {
-    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane);
+    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
@@ -459,8 +467,21 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 #pragma unroll
     for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, dx + 16 * c);
     tc::tmem_wait_ld();
-    scatter_warp<D, F>(grid, table_grad, p, valid, dx, 1,
-                       active ? run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u);
+    if constexpr (kStaged) {
+      if (valid) {
+        float* dst = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
+#pragma unroll
+        for (int l = 0; l < 16; ++l) {
+          if constexpr (F == 2) *reinterpret_cast<float2*>(dst + l * slots * F) = make_float2(dx[2 * l], dx[2 * l + 1]);
+          else
+#pragma unroll
+            for (int f = 0; f < F; ++f) dst[l * slots * F + f] = dx[l * F + f];
+        }
+      }
+    } else {
+      scatter_warp<D, F>(grid, table_grad, p, valid, dx, F, 1,
+                         active ? run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u, 0, grid.n_levels);
+    }
     tc::fence_before();
     __syncthreads();
     if (active) cur.base += 32;
@@ -503,6 +524,37 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   }
 }
 
+// Applies staged encoding gradients of the rays with scheduling index in
+// [lo, hi) to the fp32 gradient table, levels [l0, l1) only: a pass touches a
+// slice of the gradient table small enough to stay in L2.  Warp per 32
+// consecutive samples of a ray (the backward's order, so runs of equal cells
+// are merged the same way); no shared memory or TMEM, so many warps per SM
+// keep many reductions in flight.
+template <int D, int F>
+__global__ void __launch_bounds__(kScatterThreads)
+scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs, const int32_t* __restrict__ slot,
+                     unsigned int* __restrict__ ctrl, const float* __restrict__ stage, int64_t slots, int lo, int hi,
+                     int l0, int l1, float* __restrict__ table_grad) {
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  const int lane = threadIdx.x & 31;
+  RayCursor cur;
+  while (next_chunk(cur, recs, ctrl + 5, slot, a, by_pixel, lane, lo, hi)) {
+    const int i = cur.base + lane;
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
+    bool valid = false;
+    if (i < cur.rec.count) valid = sample_point(cur.rec, i, p);
+    if (D == 4) p[3] = a.t;
+    const float* dsrc = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
+    scatter_warp<D, F>(grid, table_grad, p, valid, dsrc, slots * F, 1,
+                       run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz), l0, l1);
+    cur.base += 32;
+  }
+}
+
+// Level groups of the staged scatter: consecutive levels whose fp32 gradient
+// slices add up to at most kScatterGroupBytes.
+constexpr size_t kScatterGroupBytes = size_t(48) << 20;
+
 template <int D, int F>
 int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W, const TrainArgs& a,
               Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
@@ -526,16 +578,65 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   }
   if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)
-  {
-    auto k = bwd_mixed_kernel<D, F>;
-    // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
-    const size_t smem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
-    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
+  const size_t bsmem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
+  constexpr int IN = 16 * F;
+  const int64_t per_index = (int64_t)a.S * IN * (int64_t)sizeof(float);
+  const int64_t N = std::max(a.num_rays, a.n_pixels);  // covers both scheduling orders
+  const int64_t per_round = ws.stage ? std::min<int64_t>((int64_t)(ws.stage_bytes / per_index), N) : 0;
+  if (per_round <= 0 || ceil_div(N, per_round) > kMaxStagedRounds) {
+    // fused single pass: the backward scatters its own gradients
+    auto k = bwd_mixed_kernel<D, F, false>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
-    k<<<blocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                        W_grad);
+    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+                                         W_grad, 0, 0x7fffffff, nullptr, 0);
+    return launch_status("bwd_mixed_kernel");
   }
-  return launch_status("bwd_mixed_kernel");
+  // two passes per round of scheduling indices: the tensor-core backward
+  // stages dL/d(encoding), then one scatter pass per level group
+  int group_start[NECTB_MAX_LEVELS + 1], n_groups = 0;
+  {
+    size_t acc = 0;
+    for (int l = 0; l < grid.n_levels; ++l) {
+      const int64_t next = l + 1 < grid.n_levels ? grid.offset[l + 1] : grid.total_entries;
+      const size_t bytes = (size_t)(next - grid.offset[l]) * F * sizeof(float);
+      if (l == 0 || acc + bytes > kScatterGroupBytes) {
+        group_start[n_groups++] = l;
+        acc = 0;
+      }
+      acc += bytes;
+    }
+    group_start[n_groups] = grid.n_levels;
+  }
+  auto kb = bwd_mixed_kernel<D, F, true>;
+  cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+  auto ks = scatter_stage_kernel<D, F>;
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
+  const int sblocks = sms * std::max(per_sm, 1);
+  const int64_t slots = per_round * a.S;
+  for (int64_t lo = 0; lo < N; lo += per_round) {
+    const int hi = (int)std::min<int64_t>(N, lo + per_round);
+    if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor")) return rc;
+    {
+      ProfScope ps(kProfBackward, s);
+      kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+                                            W_grad, (int)lo, hi, ws.stage, slots);
+    }
+    if (int rc = launch_status("bwd_mixed_kernel")) return rc;
+    for (int gi = 0; gi < n_groups; ++gi) {
+      if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 5, 0, sizeof(unsigned int), s), "memset cursor"))
+        return rc;
+      {
+        ProfScope ps(kProfScatter, s);
+        ks<<<sblocks, kScatterThreads, 0, s>>>(grid, a, ws.rays, ws.slot, ws.counters, ws.stage, slots, (int)lo, hi,
+                                               group_start[gi], group_start[gi + 1], table_grad);
+      }
+      if (int rc = launch_status("scatter_stage_kernel")) return rc;
+    }
+  }
+  return NECTB_OK;
 }
 
 }  // namespace
@@ -548,6 +649,8 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
   if (mlp.n_hidden_layers != 2 || mlp.activation != NECTB_ACT_RELU)
     return set_error(NECTB_ERR_INVALID, "mixed path: needs 2 hidden ReLU layers (got %d, act %d)",
                      mlp.n_hidden_layers, mlp.activation);
+  if (grid.n_levels != 16 || mlp.n_input != 16 * F || mlp.width != 64)
+    return set_error(NECTB_ERR_INVALID, "mixed path: needs 16 levels, n_input 16 x n_features and width 64");
   const __half* tab = (const __half*)table;
   const int oact = mlp.output_activation;
   if (D == 3 && F == 2) return run_mixed<3, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);

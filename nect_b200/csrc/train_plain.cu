@@ -271,7 +271,7 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
     // per-sample atomics: the SIMT path is issue-bound and the run reduction's
     // shuffles cost it more than the atomics they save (measured)
-    scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, LD, 0u);
+    scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, (int64_t)F * LD, LD, 0u, 0, grid.n_levels);
     __syncthreads();
     base += 32;
   }

@@ -45,14 +45,24 @@ class RayBatch:
 
 
 class Workspace:
-    """Caller-owned device workspace for nectb_train_step, grown on demand."""
+    """Caller-owned device workspace for nectb_train_step, grown on demand.
 
-    def __init__(self):
+    With ``staging`` (default) it also holds the recommended staging buffer of
+    the mixed path's two-pass backward; without it the mixed backward runs as
+    one fused pass."""
+
+    def __init__(self, staging: bool = True):
         self.buf = None
+        self.staging = staging
 
-    def get(self, model: _HashGridModel, c_geometry, num_rays: int, device) -> tuple[int, int]:
+    def get(self, model: _HashGridModel, c_geometry, num_rays: int, device,
+            points_per_ray: int = 0) -> tuple[int, int]:
         need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
                                                     ctypes.byref(model.mlp_desc), num_rays)
+        if self.staging and points_per_ray > 0:
+            need = ((need + 255) // 256) * 256 + _lib.lib.nectb_train_staging_bytes(
+                ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
+                num_rays, points_per_ray)
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         self.num_rays = num_rays
@@ -102,7 +112,7 @@ def train_step(model: _HashGridModel, c_geometry, batch: RayBatch, max_distance_
         _lib.require_cuda(t, name)
     y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
     loss_out = torch.empty(1, device=dev, dtype=torch.float32)
-    ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev)
+    ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev, batch.points_per_ray)
     cb = c_batch(batch, max_distance_traveled, loss, loss_scale)
     rc = _lib.lib.nectb_train_step(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
                                    ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(), model.mlp.data_ptr(),

@@ -171,6 +171,21 @@ def test_mixed_error_word_clear(cuda_device):
         assert ws.error_word() == 0
 
 
+@pytest.mark.parametrize("n_dims,duplicates", [(3, False), (4, False), (4, True)])
+def test_staged_and_fused_backward_agree(cuda_device, n_dims, duplicates):
+    """The two-pass backward (tensor-core pass staging dL/d(encoding), scatter
+    passes per level group, 8 rounds) and the single fused pass give the same
+    gradients up to fp32 reassociation of the reductions."""
+    from nect_b200.trainer import Workspace
+
+    (y1, L1, gt1, gm1), _ = run_train_case(n_dims, "mixed", "l2", "cone", duplicates, ws=Workspace(staging=True))
+    (y2, L2, gt2, gm2), _ = run_train_case(n_dims, "mixed", "l2", "cone", duplicates, ws=Workspace(staging=False))
+    assert torch.equal(y1, y2)
+    assert abs(L1 - L2) <= 1e-5 * abs(L2)   # the loss is an fp32 atomic sum over blocks
+    assert rel_max(gt1, gt2) < 1e-5, rel_max(gt1, gt2)
+    assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
+
+
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
 def test_batch_with_repeated_pixels(cuda_device, precision):
     """Every ray of the batch is processed when pixels repeat (the pixel-order
