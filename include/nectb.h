@@ -264,7 +264,8 @@ const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_
                                            const void* workspace);
 
 /* Fused forward+backward.  grid_params is the table in grid->feature_dtype
- * (fp32 or fp16); mlp_params fp32.  Gradients are accumulated (+=) into
+ * (fp32 or fp16); mlp_params fp32; grid_params and grid_grad 16-byte
+ * aligned (paired 16-byte reductions).  Gradients are accumulated (+=) into
  * grid_grad (fp32, nectb_hashgrid_layout total * n_features) and mlp_grad
  * (fp32, nectb_mlp_param_count).  y_pred[num_rays] and loss[1] are written.
  * workspace: at least nectb_train_workspace_bytes() bytes of device memory;

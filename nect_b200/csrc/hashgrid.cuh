@@ -205,13 +205,51 @@ __device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, doub
   return m;
 }
 
+// Adds the contributions of corners c and c + 1 (which differ along axis 0,
+// the axis with hash prime 1 and dense stride 1): when their entries form an
+// aligned pair (i0 even, i1 = i0 + 1) one 16-byte reduction carries both,
+// otherwise one 8-byte reduction each.  The gradient table must be 16-byte
+// aligned (level offsets are multiples of 8 entries).
+__device__ __forceinline__ void red_pair_f2(float* base, uint32_t i0, uint32_t i1, float a0, float a1, float b0,
+                                            float b1) {
+  float* dst = base + (int64_t)i0 * 2;
+  if (!(i0 & 1u) && i1 == i0 + 1u) {
+    atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a0, a1, b0, b1));
+  } else {
+    atomicAdd(reinterpret_cast<float2*>(dst), make_float2(a0, a1));
+    atomicAdd(reinterpret_cast<float2*>(base + (int64_t)i1 * 2), make_float2(b0, b1));
+  }
+}
+
+template <int F>
+__device__ __forceinline__ void red_entry(float* dst, const float* v) {
+  if constexpr (F == 2) atomicAdd(reinterpret_cast<float2*>(dst), make_float2(v[0], v[1]));
+  else if constexpr (F == 4) atomicAdd(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
+  else
+#pragma unroll
+    for (int f = 0; f < F; ++f) atomicAdd(dst + f, v[f]);
+}
+
+// Sum of v over the lanes [lane, end] of the lane's run (lanes after it in the
+// same run); valid in the run's first lane.
+__device__ __forceinline__ float run_sum(float v, int lane, int end) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const float tv = __shfl_down_sync(0xffffffffu, v, o);
+    if (lane + o <= end) v += tv;
+  }
+  return v;
+}
+
 // Warp-cooperative gradient scatter of 32 samples of one ray (all lanes call;
 // `valid` masks lanes without a sample).  On levels in agg_levels, lanes in the
 // same cell form contiguous runs along the ray; each run's contributions to
 // each corner are summed with a segmented shuffle reduction and written by the
 // run's first lane, so the table sees one atomic per (cell, corner) instead of
-// one per sample.  Other levels scatter per sample.  Sums equal the
-// per-sample atomics up to fp32 reassociation.
+// one per sample.  In 4D the time weight is the same for every sample of a
+// batch, so runs sum the 8 spatial corners and scale by the two time weights.
+// Other levels scatter per sample.  Sums equal the per-sample atomics up to
+// fp32 reassociation.
 //
 // dL/d(feature f of level l) is read at dsrc[l * lstride + f * fstride]; only
 // levels [l0, l1) are scattered.
@@ -237,39 +275,68 @@ __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict
       const uint32_t heads = __ballot_sync(0xffffffffu, head);
       const uint32_t later = heads & ~((2u << lane) - 1u);
       const int end = later ? (__ffs(later) - 2) : 31;
+      constexpr int SC = D == 4 ? 8 : (1 << D);   // corners summed along the run
+      float ws[SC];
+      float wt0 = 1.f, wt1 = 1.f;
+      if constexpr (D == 4) {
+        LevelCorners<3> ls;   // spatial weights (the 4D weights are these times the time weight)
+        level_corners<3>(g, l, x, ls);
 #pragma unroll
-      for (int c = 0; c < (1 << D); ++c) {
-        float v[F];
+        for (int c = 0; c < 8; ++c) ws[c] = ls.w[c];
+        const int r = g.res[l][3];
+        const float pt = x[3] * (float)r;
+        int ct = (int)floorf(pt);
+        ct = ct < 0 ? 0 : (ct > r - 1 ? r - 1 : ct);
+        wt1 = pt - (float)ct;
+        wt0 = 1.f - wt1;
+      } else {
 #pragma unroll
-        for (int f = 0; f < F; ++f) v[f] = lc.w[c] * d[f];
+        for (int c = 0; c < SC; ++c) ws[c] = lc.w[c];
+      }
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
+      for (int c = 0; c < SC; c += 2) {
+        float s0[F], s1[F];
 #pragma unroll
-          for (int f = 0; f < F; ++f) {
-            const float tv = __shfl_down_sync(0xffffffffu, v[f], o);
-            if (lane + o <= end) v[f] += tv;
-          }
+        for (int f = 0; f < F; ++f) {
+          s0[f] = run_sum(ws[c] * d[f], lane, end);
+          s1[f] = run_sum(ws[c + 1] * d[f], lane, end);
         }
         if (head && valid) {
-          float* dst = base + (int64_t)lc.idx[c] * F;
-          if constexpr (F == 2) atomicAdd(reinterpret_cast<float2*>(dst), make_float2(v[0], v[1]));
-          else if constexpr (F == 4) atomicAdd(reinterpret_cast<float4*>(dst), make_float4(v[0], v[1], v[2], v[3]));
-          else
 #pragma unroll
-            for (int f = 0; f < F; ++f) atomicAdd(dst + f, v[f]);
+          for (int tb = 0; tb < (D == 4 ? 2 : 1); ++tb) {
+            const float wt = D == 4 ? (tb ? wt1 : wt0) : 1.f;
+            const int c0 = c + tb * 8;
+            if constexpr (F == 2) {
+              red_pair_f2(base, lc.idx[c0], lc.idx[c0 + 1], wt * s0[0], wt * s0[1], wt * s1[0], wt * s1[1]);
+            } else {
+              float v0[F], v1[F];
+#pragma unroll
+              for (int f = 0; f < F; ++f) {
+                v0[f] = wt * s0[f];
+                v1[f] = wt * s1[f];
+              }
+              red_entry<F>(base + (int64_t)lc.idx[c0] * F, v0);
+              red_entry<F>(base + (int64_t)lc.idx[c0 + 1] * F, v1);
+            }
+          }
         }
       }
     } else if (valid) {
 #pragma unroll
-      for (int c = 0; c < (1 << D); ++c) {
-        float* dst = base + (int64_t)lc.idx[c] * F;
-        if constexpr (F == 2) atomicAdd(reinterpret_cast<float2*>(dst), make_float2(lc.w[c] * d[0], lc.w[c] * d[1]));
-        else if constexpr (F == 4)
-          atomicAdd(reinterpret_cast<float4*>(dst),
-                    make_float4(lc.w[c] * d[0], lc.w[c] * d[1], lc.w[c] * d[2], lc.w[c] * d[3]));
-        else
+      for (int c = 0; c < (1 << D); c += 2) {
+        if constexpr (F == 2) {
+          red_pair_f2(base, lc.idx[c], lc.idx[c + 1], lc.w[c] * d[0], lc.w[c] * d[1], lc.w[c + 1] * d[0],
+                      lc.w[c + 1] * d[1]);
+        } else {
+          float v0[F], v1[F];
 #pragma unroll
-          for (int f = 0; f < F; ++f) atomicAdd(dst + f, lc.w[c] * d[f]);
+          for (int f = 0; f < F; ++f) {
+            v0[f] = lc.w[c] * d[f];
+            v1[f] = lc.w[c + 1] * d[f];
+          }
+          red_entry<F>(base + (int64_t)lc.idx[c] * F, v0);
+          red_entry<F>(base + (int64_t)lc.idx[c + 1] * F, v1);
+        }
       }
     }
   }

@@ -82,6 +82,8 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   cudaStream_t s = (cudaStream_t)stream;
   if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
   if (batch->num_rays == 0) return NECTB_OK;
+  NECTB_REQUIRE(((uintptr_t)grid_grad & 15u) == 0 && ((uintptr_t)grid_params & 15u) == 0,
+                "grid_grad and grid_params must be 16-byte aligned");
   NECTB_REQUIRE(batch->random_ray_index && batch->jitter && batch->detector_offset && batch->projection,
                 "null batch input");
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
