@@ -278,6 +278,27 @@ int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid,
                      float* loss, void* workspace, size_t workspace_bytes,
                      void* stream);
 
+/* The step in two halves, for losses of y_pred that the caller computes
+ * itself (the reference composes y_pred, then loss_fn(y_pred, y), optional
+ * Poisson noise and S3IM, base_trainer.py:552-566; continuous-scan training
+ * averages y_pred over several sub-angles, continous_scanning_trainer.py:
+ * 85-140).  nectb_train_forward prepares the rays and writes y_pred[num_rays]
+ * (loss_type and loss_scale are ignored); nectb_train_backward then takes
+ * dloss_dy[num_rays] = dL/dy_pred and ADDS the gradients into grid_grad and
+ * mlp_grad.  Both get the same batch and the same workspace, which must not be
+ * used by another step in between; positions and encodings are regenerated in
+ * the backward, as in nectb_train_step. */
+int nectb_train_forward(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                        const NectbMLP* mlp, const void* grid_params,
+                        const float* mlp_params, const NectbTrainBatch* batch,
+                        float* y_pred, void* workspace, size_t workspace_bytes,
+                        void* stream);
+int nectb_train_backward(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                         const NectbMLP* mlp, const void* grid_params,
+                         const float* mlp_params, const NectbTrainBatch* batch,
+                         const float* dloss_dy, float* grid_grad, float* mlp_grad,
+                         void* workspace, size_t workspace_bytes, void* stream);
+
 /* nectb_train_step without a caller workspace, for callers that cannot
  * allocate device memory (a runtime that binds this library through its C ABI
  * and has no CUDA allocator, or a loop that must never call cudaMalloc, which

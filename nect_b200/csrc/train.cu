@@ -64,10 +64,23 @@ extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, con
   return workspace_bytes(std::max(num_rays, 1), std::max(P, 0));
 }
 
-extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
-                                const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
-                                float* grid_grad, float* mlp_grad, float* y_pred, float* loss, void* workspace,
-                                size_t workspace_size, void* stream) {
+namespace nectb {
+namespace {
+
+// dL/dsigma of every sample of ray r is dL/dy_pred[r] * scale[r] (y_pred is the
+// scaled sum of the ray's sigmas, base_trainer.py:552-554).
+__global__ void set_ray_grad_kernel(RayRec* __restrict__ recs, const float* __restrict__ dloss_dy, int R) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < R) recs[r].gsig = dloss_dy[r] * recs[r].scale;
+}
+
+// The whole step (phase forward | backward, built-in loss), its forward half
+// (y_pred only; the workspace keeps the prepared rays) or its backward half
+// (dL/dy_pred given by the caller, the workspace of the matching forward).
+int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                const float* dloss_dy, float* grid_grad, float* mlp_grad, float* y_pred, float* loss,
+                void* workspace, size_t workspace_size, void* stream, int phase) {
   clear_error();
   if (int rc = validate_geometry(geometry)) return rc;
   GridDev g;
@@ -78,9 +91,14 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   NECTB_REQUIRE(batch->num_rays >= 0 && batch->num_points_per_ray >= 1, "bad batch sizes");
   NECTB_REQUIRE(batch->loss_type == 1 || batch->loss_type == 2, "loss_type must be 1 (L1) or 2 (L2)");
   NECTB_REQUIRE(batch->max_distance_traveled > 0.f, "max_distance_traveled must be positive");
-  NECTB_REQUIRE(grid_params && mlp_params && grid_grad && mlp_grad && y_pred && loss, "null parameter/output");
+  NECTB_REQUIRE(grid_params && mlp_params, "null parameters");
+  NECTB_REQUIRE(!(phase & kPhaseForward) || y_pred, "null y_pred");
+  NECTB_REQUIRE(!(phase & kPhaseBackward) || (grid_grad && mlp_grad), "null gradient buffers");
+  NECTB_REQUIRE(phase != (kPhaseForward | kPhaseBackward) || loss, "null loss");
+  NECTB_REQUIRE(phase != kPhaseBackward || dloss_dy, "null dloss_dy");
   cudaStream_t s = (cudaStream_t)stream;
-  if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
+  if (loss)
+    if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
   if (batch->num_rays == 0) return NECTB_OK;
   NECTB_REQUIRE(((uintptr_t)grid_grad & 15u) == 0 && ((uintptr_t)grid_params & 15u) == 0,
                 "grid_grad and grid_params must be 16-byte aligned");
@@ -108,22 +126,58 @@ extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGr
   a.loss_type = batch->loss_type;
   a.loss_scale = batch->loss_scale;
   a.max_blocks = 0;
+  a.phase = phase;
   Workspace ws = carve_workspace(workspace, a.num_rays, P, workspace_size);
-  if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
-  if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
-  {
+  // the forward half has no loss output of its own: its loss sum lands in the workspace
+  if (!loss) loss = reinterpret_cast<float*>(ws.counters + 8);
+  if (phase & kPhaseForward) {
+    if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
+    if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
     ProfScope ps(kProfRayPrep, s);
     ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters,
                                                                        y_pred, loss);
+  } else {
+    // backward half: fresh backward cursor, the caller's loss gradient per ray
+    if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor"))
+      return rc;
+    set_ray_grad_kernel<<<(unsigned)ceil_div(a.num_rays, 256), 256, 0, s>>>(ws.rays, dloss_dy, a.num_rays);
   }
-  if (int rc = launch_status("ray_prep_kernel")) return rc;
+  if (int rc = launch_status(phase & kPhaseForward ? "ray_prep_kernel" : "set_ray_grad_kernel")) return rc;
   const int nW = (int)mlp_param_count(mlp);
+  float* tg = (phase & kPhaseBackward) ? grid_grad : nullptr;
+  float* mg = (phase & kPhaseBackward) ? mlp_grad : nullptr;
   if (mlp->compute_dtype == NECTB_F32) {
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F32, "plain path needs an fp32 table");
-    return train_plain(*geometry, g, *mlp, (const float*)grid_params, mlp_params, nW, a, ws, grid_grad, mlp_grad,
-                       y_pred, loss, s);
+    return train_plain(*geometry, g, *mlp, (const float*)grid_params, mlp_params, nW, a, ws, tg, mg, y_pred, loss,
+                       s);
   }
-  return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, a, ws, grid_grad, mlp_grad, y_pred, loss, s);
+  return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, a, ws, tg, mg, y_pred, loss, s);
+}
+
+}  // namespace
+}  // namespace nectb
+
+extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                                float* grid_grad, float* mlp_grad, float* y_pred, float* loss, void* workspace,
+                                size_t workspace_size, void* stream) {
+  return train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, nullptr, grid_grad, mlp_grad, y_pred, loss,
+                     workspace, workspace_size, stream, kPhaseForward | kPhaseBackward);
+}
+
+extern "C" int nectb_train_forward(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                   const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                                   float* y_pred, void* workspace, size_t workspace_size, void* stream) {
+  return train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, nullptr, nullptr, nullptr, y_pred, nullptr,
+                     workspace, workspace_size, stream, kPhaseForward);
+}
+
+extern "C" int nectb_train_backward(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                    const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                                    const float* dloss_dy, float* grid_grad, float* mlp_grad, void* workspace,
+                                    size_t workspace_size, void* stream) {
+  return train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, dloss_dy, grid_grad, mlp_grad, nullptr,
+                     nullptr, workspace, workspace_size, stream, kPhaseBackward);
 }
 
 extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,

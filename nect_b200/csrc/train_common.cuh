@@ -22,6 +22,8 @@ struct RayRec {
 };
 static_assert(sizeof(RayRec) == 64, "RayRec must be 64 bytes");
 
+enum { kPhaseForward = 1, kPhaseBackward = 2 };
+
 struct TrainArgs {
   const int64_t* perm;
   int64_t perm_len;
@@ -40,6 +42,7 @@ struct TrainArgs {
   int loss_type;
   float loss_scale;
   int max_blocks;  // > 0: cap on the persistent grids (queries); 0: default
+  int phase = kPhaseForward | kPhaseBackward;  // which half of the step to run
 };
 
 enum : unsigned int { kFlagDuplicatePixels = 1u };

@@ -569,15 +569,17 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     fblocks = std::min(fblocks, a.max_blocks);
     blocks = std::min(blocks, a.max_blocks);
   }
-  {
+  if (a.phase & kPhaseForward) {
     auto k = fwd_mixed_kernel<D, F>;
     const size_t smem = 1024 + 2 * kWTile + kTile + 64 * 4 + 64;
     set_smem(k, smem, a.max_blocks > 0);
-    ProfScope ps(kProfForward, s);
-    k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
+    {
+      ProfScope ps(kProfForward, s);
+      k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
+    }
+    if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   }
-  if (int rc = launch_status("fwd_mixed_kernel")) return rc;
-  if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)
+  if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
   // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
   const size_t bsmem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
   constexpr int IN = 16 * F;

@@ -310,12 +310,14 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, FNT, fsmem);
   int fblocks = std::max(1, std::min<int>(sms * std::max(per_sm, 1), (int)ceil_div(a.num_rays, FNT / 32)));
   if (a.max_blocks > 0) fblocks = std::min(fblocks, a.max_blocks);
-  {
-    ProfScope ps(kProfForward, s);
-    fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred, loss);
+  if (a.phase & kPhaseForward) {
+    {
+      ProfScope ps(kProfForward, s);
+      fk<<<fblocks, FNT, fsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred, loss);
+    }
+    if (int rc = launch_status("fwd_plain_kernel")) return rc;
   }
-  if (int rc = launch_status("fwd_plain_kernel")) return rc;
-  if (!table_grad) return NECTB_OK;  // forward only (re-projection queries)
+  if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
 
   constexpr int NT = 128;
   auto bk = bwd_plain_kernel<D, F, IN, H, NT>;

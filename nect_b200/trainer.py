@@ -122,6 +122,61 @@ def train_step(model: _HashGridModel, c_geometry, batch: RayBatch, max_distance_
     return loss_out, y_pred
 
 
+class RayIntegral(torch.autograd.Function):
+    """y_pred[r] = (sum of sigma over ray r's samples) * distances / max_distance_traveled
+    (base_trainer.py:552-554) as a function of (table, mlp): forward half
+    nectb_train_forward, backward half nectb_train_backward with the
+    incoming dL/dy_pred.  Any torch loss of y_pred may follow (L1/L2, Poisson
+    noise, S3IM, sub-angle averages), as in the reference's composition
+    (base_trainer.py:552-566).  The workspace passed in belongs to this
+    forward until its backward has run."""
+
+    @staticmethod
+    def forward(ctx, table, mlp, model, c_geometry, batch, max_distance_traveled, workspace):
+        dev = batch.perm.device
+        for name, t in (("perm", batch.perm), ("jitter", batch.jitter), ("detector_offset", batch.detector_offset),
+                        ("projection", batch.projection)):
+            _lib.require_cuda(t, name)
+        y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
+        ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev, batch.points_per_ray)
+        cb = c_batch(batch, max_distance_traveled, "l2")
+        rc = _lib.lib.nectb_train_forward(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                          ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                          model.mlp.data_ptr(), ctypes.byref(cb), y_pred.data_ptr(), ws_ptr, ws_size,
+                                          _lib.stream_ptr(dev))
+        _lib.check(rc, "nectb_train_forward")
+        # everything the backward half reads: the batch's tensors, the C batch and this workspace buffer
+        ctx.model, ctx.c_geometry, ctx.batch, ctx.cb = model, c_geometry, batch, cb
+        ctx.ws_buf, ctx.ws = workspace.buf, (ws_ptr, ws_size)
+        return y_pred
+
+    @staticmethod
+    def backward(ctx, grad_y):
+        model, dev = ctx.model, ctx.batch.perm.device
+        g = grad_y.detach().to(torch.float32).contiguous()
+        tg = torch.zeros_like(model.table)
+        mg = torch.zeros_like(model.mlp)
+        rc = _lib.lib.nectb_train_backward(ctypes.byref(ctx.c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                           ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                           model.mlp.data_ptr(), ctypes.byref(ctx.cb), g.data_ptr(), tg.data_ptr(),
+                                           mg.data_ptr(), ctx.ws[0], ctx.ws[1], _lib.stream_ptr(dev))
+        _lib.check(rc, "nectb_train_backward")
+        return tg, mg, None, None, None, None, None
+
+
+def ray_integral(model: _HashGridModel, c_geometry, batch: RayBatch, max_distance_traveled: float,
+                 workspace: Workspace) -> torch.Tensor:
+    """Differentiable y_pred [R] of one batch (see RayIntegral)."""
+    return RayIntegral.apply(model.table, model.mlp, model, c_geometry, batch, max_distance_traveled, workspace)
+
+
+def projection_loss(y_pred: torch.Tensor, y: torch.Tensor, loss: str) -> torch.Tensor:
+    """L1 or L2 (mean over rays), nect/config.py:481-497."""
+    if loss.lower() == "l1":
+        return torch.nn.functional.l1_loss(y_pred, y)
+    return torch.nn.functional.mse_loss(y_pred, y)
+
+
 class FusedRayLoss(torch.autograd.Function):
     """loss = L(y_pred(table, mlp), y) with the hand-written fused backward."""
 
@@ -213,6 +268,41 @@ class Trainer:
         adam_step(self.model.mlp, self.mlp_grad, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas,
                   self.eps, self.weight_decay)
         return loss
+
+    def continuous_step(self, perm: torch.Tensor, batch_num: int, angle_start: float, angle_stop: float,
+                        projection: torch.Tensor, t: float = 0.0, accumulation_steps: int = 4,
+                        add_poisson: bool = False) -> torch.Tensor | None:
+        """One continuous-rotation step (continous_scanning_trainer.py:85-140):
+        the detector integrates while the object turns from angle_start to
+        angle_stop, so y_pred is the mean of ``accumulation_steps`` forwards at
+        the mid-angles of equal sub-intervals (same pixels and t, a fresh
+        jitter draw per sub-angle), optionally with the reference's Poisson
+        noise term; then the loss, the hand-written backward of every
+        sub-angle forward and the Adam update."""
+        import numpy as np
+
+        edges = np.linspace(angle_start, angle_stop, accumulation_steps + 1)
+        if not hasattr(self, "_scan_ws") or len(self._scan_ws) < accumulation_steps:
+            self._scan_ws = [Workspace() for _ in range(accumulation_steps)]
+        y_pred, batch = None, None
+        for j in range(accumulation_steps):
+            batch = self.make_batch(perm, batch_num, float((edges[j] + edges[j + 1]) / 2), projection, t)
+            if batch is None:
+                return None
+            yj = ray_integral(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
+                              self._scan_ws[j]) / accumulation_steps
+            y_pred = yj if y_pred is None else y_pred + yj
+        if add_poisson:   # base_trainer.py:555-556; the Poisson draw carries no gradient
+            y_pred = (y_pred + torch.poisson(y_pred.detach() * 1e5) / 1e5) / 2
+        y = projection[perm[batch.start:batch.start + batch.num_rays]]
+        loss = projection_loss(y_pred, y, self.loss)
+        g_table, g_mlp = torch.autograd.grad(loss, [self.model.table, self.model.mlp])
+        self.step_count += 1
+        adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
+                  self.eps, self.weight_decay, half=self.model.table_half)
+        adam_step(self.model.mlp, g_mlp, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas, self.eps,
+                  self.weight_decay)
+        return loss.detach()
 
     def device_error(self) -> int:
         """Error word of the last step (non-zero if a tensor-core wait timed out)."""

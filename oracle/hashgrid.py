@@ -145,6 +145,32 @@ def split_mlp_params(flat: torch.Tensor, n_input: int, width: int, n_hidden: int
     return out
 
 
+def line_integrals(points: np.ndarray, distances: np.ndarray, tab: torch.Tensor, wf: torch.Tensor, levels,
+                   log2_T: int, n_input: int, width: int, n_hidden: int, max_distance_traveled: float,
+                   act: str = "relu", out_act: str = "softplus", t: float | None = None):
+    """y_pred [R] of one batch of sampled rays, differentiable in (tab, wf):
+    clamp (projector.py:127), drop all-zero points (base_trainer.py:523),
+    sigma = MLP(encode(x)), y_pred = sum * distances / max_distance_traveled
+    (base_trainer.py:552-554)."""
+    R, S, _ = points.shape
+    pts = torch.from_numpy(points).clamp(0, 1)
+    keep = ~torch.all(pts.view(-1, 3) == 0, dim=-1)
+    x = pts.view(-1, 3)[keep]
+    if t is not None:
+        x = torch.cat([x, torch.full((x.shape[0], 1), float(t), dtype=torch.float32)], 1)
+    Ws = split_mlp_params(wf, n_input, width, n_hidden)
+    sig = mlp(encode(x, tab, levels, log2_T), Ws, act, out_act).squeeze(-1)
+    full = torch.zeros(R * S, dtype=tab.dtype).masked_scatter(keep, sig)
+    scale = torch.from_numpy(distances).to(tab.dtype) / max_distance_traveled
+    return full.view(R, S).sum(1) * scale
+
+
+def _loss(y_pred, y, loss):
+    if loss.lower() == "l2":
+        return torch.nn.functional.mse_loss(y_pred, y)
+    return torch.nn.functional.l1_loss(y_pred, y)
+
+
 def train_step(points: np.ndarray, counts: np.ndarray, distances: np.ndarray, measured: np.ndarray,
                table: torch.Tensor, mlp_flat: torch.Tensor, levels, log2_T: int, n_input: int, width: int,
                n_hidden: int, max_distance_traveled: float, loss: str = "l2", act: str = "relu",
@@ -152,21 +178,28 @@ def train_step(points: np.ndarray, counts: np.ndarray, distances: np.ndarray, me
     """Forward + backward of one batch (points from the sampling oracle).
 
     Returns (y_pred [R], loss scalar, grad_table, grad_mlp) as float64 tensors."""
-    R, S, _ = points.shape
-    pts = torch.from_numpy(points).clamp(0, 1)                 # projector.py:127
-    keep = ~torch.all(pts.view(-1, 3) == 0, dim=-1)            # base_trainer.py:523
-    x = pts.view(-1, 3)[keep]
-    if t is not None:
-        x = torch.cat([x, torch.full((x.shape[0], 1), float(t), dtype=torch.float32)], 1)
     tab = table.detach().to(dtype).requires_grad_(True)
     wf = mlp_flat.detach().to(dtype).requires_grad_(True)
-    Ws = split_mlp_params(wf, n_input, width, n_hidden)
-    sig = mlp(encode(x, tab, levels, log2_T), Ws, act, out_act).squeeze(-1)
-    full = torch.zeros(R * S, dtype=dtype)
-    full = full.masked_scatter(keep, sig)
-    scale = torch.from_numpy(distances).to(dtype) / max_distance_traveled
-    y_pred = full.view(R, S).sum(1) * scale                    # base_trainer.py:552-554
-    y = torch.from_numpy(measured).to(dtype)
-    L = torch.nn.functional.mse_loss(y_pred, y) if loss.lower() == "l2" else torch.nn.functional.l1_loss(y_pred, y)
+    y_pred = line_integrals(points, distances, tab, wf, levels, log2_T, n_input, width, n_hidden,
+                            max_distance_traveled, act, out_act, t)
+    L = _loss(y_pred, torch.from_numpy(measured).to(dtype), loss)
+    L.backward()
+    return y_pred.detach(), L.detach(), tab.grad.detach(), wf.grad.detach()
+
+
+def averaged_step(samples: list, measured: np.ndarray, table: torch.Tensor, mlp_flat: torch.Tensor, levels,
+                  log2_T: int, n_input: int, width: int, n_hidden: int, max_distance_traveled: float,
+                  loss: str = "l2", act: str = "relu", out_act: str = "softplus", t: float | None = None,
+                  dtype=torch.float64):
+    """Continuous-rotation step (nect/trainers/continous_scanning_trainer.py:85-140):
+    y_pred is the mean of the line integrals of the same pixels at several
+    sub-angles; samples = [(points, distances), ...] one entry per sub-angle.
+
+    Returns (y_pred [R], loss scalar, grad_table, grad_mlp) as float64 tensors."""
+    tab = table.detach().to(dtype).requires_grad_(True)
+    wf = mlp_flat.detach().to(dtype).requires_grad_(True)
+    y_pred = sum(line_integrals(p, d, tab, wf, levels, log2_T, n_input, width, n_hidden, max_distance_traveled,
+                                act, out_act, t) for p, d in samples) / len(samples)
+    L = _loss(y_pred, torch.from_numpy(measured).to(dtype), loss)
     L.backward()
     return y_pred.detach(), L.detach(), tab.grad.detach(), wf.grad.detach()
