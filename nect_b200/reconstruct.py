@@ -24,6 +24,7 @@ import torch
 from .config import HashEncoderConfig, MLPNetConfig, ModelConfig, get_model
 from .network import _HashGridModel
 from .sampling import Geometry
+from .schedule import bin_projection, s3im_patch_size
 from .serving import denormalisation, query_points, volume_items
 from .trainer import Trainer
 
@@ -63,12 +64,21 @@ def default_model_config(geometry: Geometry, mode: str, precision: str) -> Model
 def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *, model_cfg: ModelConfig | None = None,
         precision: str = "mixed", niter: int = 2000, lr: float = 1e-3, rays_per_batch: int = 65536,
         points_per_ray: int | None = None, loss: str = "l2", seed: int = 0, device="cuda",
-        evaluate=None, eval_every: int = 0) -> Reconstruction:
+        evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
+        add_poisson: bool = False) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
     called every ``eval_every`` steps (and at the end) outside the training
-    time; its dict is recorded in ``history``."""
+    time; its dict is recorded in ``history``.
+
+    With a ``schedule`` (nect_b200.schedule.Schedule) each step takes that
+    projection's detector binning (pooled projection, binned geometry, random
+    detector offset while binned), points per ray and learning rate, for
+    min(niter, schedule.total_projections) steps.  ``s3im`` adds the S3IM
+    term after the schedule's warm-up (base_trainer.py:557-566) and
+    ``add_poisson`` the reference's Poisson term; both run the step as
+    forward half, torch loss, backward half."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -97,15 +107,39 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
             torch.cuda.synchronize(dev)
             rec.history.append((step, train_s, evaluate(rec)))
 
+    settings = iter(schedule.steps()) if schedule is not None else None
+    if schedule is not None:
+        niter = min(niter, schedule.total_projections)
+        rows, cols = geometry.nDetector
+        raw = proj.view(n_proj, rows, cols)
+        ppb = trainer.points_per_batch
+    binning = 1
     record(0)
     for step in range(1, niter + 1):
         k = int(order[(step - 1) % n_proj])
         if (step - 1) % n_proj == n_proj - 1:
             order = np.random.default_rng(seed + step).permutation(n_proj)
         t0 = time.perf_counter()
-        perm = torch.randperm(P, dtype=torch.int64, device=dev)
-        batch = trainer.make_batch(perm, 0, angles[k], proj[k], ts[k])
-        trainer.step(batch)
+        target = proj[k]
+        if settings is not None:
+            st = next(settings)
+            if st.detector_binning != binning:
+                binning = st.detector_binning
+                geometry.set_detector_binning(binning)
+                trainer.c_geometry = geometry.get_c_geometry()
+            target = bin_projection(raw[k], binning).reshape(-1).contiguous()
+            trainer.points_per_ray = st.points_per_ray
+            trainer.points_per_batch = ppb
+            trainer.random_offset_detector = st.random_offset_detector
+            trainer.lr = st.lr
+        perm = torch.randperm(target.numel(), dtype=torch.int64, device=dev)
+        batch = trainer.make_batch(perm, 0, angles[k], target, ts[k])
+        if s3im or add_poisson:
+            warm = schedule.warmup[0] if schedule is not None else 0
+            patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
+            trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch)
+        else:
+            trainer.step(batch)
         if eval_every and (step % eval_every == 0 or step == niter):
             torch.cuda.synchronize(dev)
             train_s += time.perf_counter() - t0
@@ -113,6 +147,9 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         else:
             train_s += time.perf_counter() - t0
     torch.cuda.synchronize(dev)
+    if binning != 1:
+        geometry.set_detector_binning(1)
+        trainer.c_geometry = geometry.get_c_geometry()
     rec.train_seconds = train_s
     return rec
 

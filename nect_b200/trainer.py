@@ -292,10 +292,27 @@ class Trainer:
             yj = ray_integral(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
                               self._scan_ws[j]) / accumulation_steps
             y_pred = yj if y_pred is None else y_pred + yj
+        y = projection[perm[batch.start:batch.start + batch.num_rays]]
+        return self._loss_and_update(y_pred, y, add_poisson)
+
+    def split_step(self, batch: RayBatch, add_poisson: bool = False, s3im_patch: int = 0) -> torch.Tensor:
+        """One step with the loss composed in torch on y_pred (base_trainer.py:552-566):
+        the L1/L2 loss, optionally the Poisson noise term and the S3IM term
+        over ``s3im_patch``-sized patches; forward and backward are the fused
+        halves (RayIntegral)."""
+        y_pred = ray_integral(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
+                              self.workspace)
+        y = batch.projection[batch.perm[batch.start:batch.start + batch.num_rays]]
+        return self._loss_and_update(y_pred, y, add_poisson, s3im_patch)
+
+    def _loss_and_update(self, y_pred, y, add_poisson=False, s3im_patch=0):
         if add_poisson:   # base_trainer.py:555-556; the Poisson draw carries no gradient
             y_pred = (y_pred + torch.poisson(y_pred.detach() * 1e5) / 1e5) / 2
-        y = projection[perm[batch.start:batch.start + batch.num_rays]]
         loss = projection_loss(y_pred, y, self.loss)
+        if s3im_patch:
+            from .schedule import s3im_loss
+
+            loss = loss + s3im_loss(y_pred, y, s3im_patch)
         g_table, g_mlp = torch.autograd.grad(loss, [self.model.table, self.model.mlp])
         self.step_count += 1
         adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
