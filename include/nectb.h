@@ -154,6 +154,18 @@ int nectb_model_forward(const NectbHashGrid* grid, const NectbMLP* mlp,
                         const float* x, int64_t n, float t, float* sigma,
                         void* stream);
 
+/* Backward of nectb_model_forward: for n points x[n*3] ((z,y,x); t broadcast
+ * in 4D) and dsigma[n] = dL/dsigma(x_i), ADDS dL/d(table) into grid_grad
+ * (fp32, 16-byte aligned, layout of the fp32 table) and dL/d(weights) into
+ * mlp_grad.  Replaces the tiny-cuda-nn backward of direct model calls in the
+ * reference's losses on model outputs (the total-variation term on a random
+ * 100^3 sub-grid, nect/trainers/base_trainer.py:615-649, nect/utils.py:
+ * 64-80).  fp32 SIMT arithmetic for both table precisions. */
+int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp,
+                         const void* grid_params, const float* mlp_params,
+                         const float* x, int64_t n, float t, const float* dsigma,
+                         float* grid_grad, float* mlp_grad, void* stream);
+
 /* ---- queries -------------------------------------------------------------- */
 /* One work item of a query: an nu x nv grid of points
  * x(i, j) = origin + i*du + j*dv (normalised (z,y,x) coordinates, i fast),

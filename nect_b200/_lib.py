@@ -111,6 +111,11 @@ _SIGNATURES = {
         c_int,
         [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_ptr, c_ptr],
     ),
+    "nectb_model_backward": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_ptr, c_ptr,
+         c_ptr, c_ptr],
+    ),
     "nectb_train_workspace_bytes": (
         c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int]),
     "nectb_train_step": (

@@ -16,6 +16,10 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
                 const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
                 float* y_pred, float* loss, cudaStream_t s);
 
+int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void* table, const float* W,
+                   const float* x, int64_t n, float tval, const float* dsigma, float* table_grad, float* W_grad,
+                   cudaStream_t s);
+
 namespace {
 
 // torch.optim.Adam (no amsgrad, not maximize), one element per thread.
@@ -189,6 +193,22 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   const int64_t N = std::max<int64_t>(num_rays, P);
   const int64_t per_round = ceil_div(N, kStagedRounds);
   return (size_t)per_round * num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
+}
+
+extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                    const float* mlp_params, const float* x, int64_t n, float t, const float* dsigma,
+                                    float* grid_grad, float* mlp_grad, void* stream) {
+  clear_error();
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  if (int rc = validate_mlp(mlp, g)) return rc;
+  NECTB_REQUIRE(g.n_levels == 16, "model backward needs n_levels == 16 (got %d)", g.n_levels);
+  NECTB_REQUIRE(n >= 0, "n must be >= 0");
+  if (n == 0) return NECTB_OK;
+  NECTB_REQUIRE(grid_params && mlp_params && x && dsigma && grid_grad && mlp_grad, "null pointer argument");
+  NECTB_REQUIRE(((uintptr_t)grid_grad & 15u) == 0, "grid_grad must be 16-byte aligned");
+  return model_backward(g, *mlp, grid->feature_dtype, grid_params, mlp_params, x, n, t, dsigma, grid_grad, mlp_grad,
+                        (cudaStream_t)stream);
 }
 
 extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr,

@@ -292,6 +292,116 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   }
 }
 
+// Backward of the model at n independent points (nectb_model_backward):
+// gradients of sum_i dsigma[i] * sigma(x_i) added to the table and weight
+// gradients.  The pipeline of bwd_plain_kernel (fp32 SIMT MLP, register tile
+// weight gradients, per-sample table reductions) with points read from x
+// (n x 3, (z, y, x); t broadcast in 4D) instead of regenerated along rays
+// and a per-point dL/dsigma.  Tables of either precision are gathered.
+template <int D, int F, int IN, int H, int NT, typename T>
+__global__ void __launch_bounds__(NT, 1)
+model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restrict__ W, const float* __restrict__ x,
+                 int64_t n, float tval, const float* __restrict__ dsigma, int act, int out_act,
+                 float* __restrict__ table_grad, float* __restrict__ W_grad) {
+  constexpr int LD = NT + 4;
+  extern __shared__ float4 smem4[];
+  float* smem = reinterpret_cast<float*>(smem4);
+  const SimtWeights sw = stage_weights<IN, H, true>(W, smem);
+  float* cols = smem + simt_weight_floats<IN, H, true>();
+  float* sX = cols;                      // [IN][LD]
+  float* sA = sX + IN * LD;              // [H][64][LD]
+  float* sG = sA + H * kWidth * LD;      // [64][LD]
+  float* sG2 = sG + kWidth * LD;         // [64][LD]
+  const int t = threadIdx.x;
+  const int lane = t & 31;
+  WGrad<IN, NT, LD> g0;
+  g0.zero();
+  WGrad<kWidth, NT, LD> gh[H > 1 ? H - 1 : 1];
+#pragma unroll
+  for (int k = 0; k < H - 1; ++k) gh[k].zero();
+  float dwout[2] = {0.f, 0.f};
+  __syncthreads();
+  for (int64_t c0 = (int64_t)blockIdx.x * NT; c0 < n; c0 += (int64_t)gridDim.x * NT) {  // block-uniform
+    const int64_t i = c0 + t;
+    const bool valid = i < n;
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
+    if (valid) {
+#pragma unroll
+      for (int k = 0; k < 3; ++k) p[k] = x[i * 3 + k];
+    }
+    if (D == 4) p[3] = tval;
+    if (valid) {
+      encode_point<D, F, T>(grid, table, p, sX + t, LD);
+    } else {
+      for (int k = 0; k < IN; ++k) sX[k * LD + t] = 0.f;
+    }
+    gemv_cols<IN, kWidth, LD>(sw.WT[0], sX + t, sA + t, act);
+#pragma unroll
+    for (int k = 1; k < H; ++k)
+      gemv_cols<kWidth, kWidth, LD>(sw.WT[k], sA + (k - 1) * kWidth * LD + t, sA + k * kWidth * LD + t, act);
+    const float* aH = sA + (H - 1) * kWidth * LD + t;
+    const float z = dot_col<kWidth, LD>(sw.wout, aH);
+    const float dz = valid ? dsigma[i] * act_grad_z(z, out_act) : 0.f;
+#pragma unroll 4
+    for (int j = 0; j < kWidth; ++j) {
+      const float aj = aH[j * LD];
+      const float v = warp_sum(dz * aj);
+      if ((j & 31) == lane) dwout[j >> 5] += v;
+      sG[j * LD + t] = dz * sw.wout[j] * act_grad_a(aj, act);
+    }
+    float* G = sG;
+    float* G2 = sG2;
+#pragma unroll
+    for (int k = H - 1; k >= 1; --k) {
+      __syncthreads();
+      gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      gemv_cols<kWidth, kWidth, LD>(sw.W[k], G + t, G2 + t, NECTB_ACT_NONE);
+      const float* ak = sA + (k - 1) * kWidth * LD + t;
+      for (int j = 0; j < kWidth; ++j) G2[j * LD + t] *= act_grad_a(ak[j * LD], act);
+      float* tmp = G;
+      G = G2;
+      G2 = tmp;
+    }
+    __syncthreads();
+    g0.add(G, sX);
+    gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
+    scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, (int64_t)F * LD, LD, 0u, 0, grid.n_levels);
+    __syncthreads();
+  }
+  g0.flush(W_grad);
+#pragma unroll
+  for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+  const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
+  __syncthreads();
+  float* red = sG;  // [NT/32][64]
+  red[(t >> 5) * kWidth + lane] = dwout[0];
+  red[(t >> 5) * kWidth + lane + 32] = dwout[1];
+  __syncthreads();
+  if (t < kWidth) {
+    float s = 0.f;
+    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + t];
+    atomicAdd(W_grad + nHidden + t, s);
+  }
+}
+
+template <int D, int F, int H, typename T>
+int launch_model_bwd(const GridDev& grid, const void* table, const float* W, const float* x, int64_t n, float tval,
+                     const float* dsigma, int act, int out_act, float* table_grad, float* W_grad, cudaStream_t s) {
+  constexpr int IN = 16 * F;
+  constexpr int NT = 128;
+  auto k = model_bwd_kernel<D, F, IN, H, NT, T>;
+  const size_t smem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
+  if (smem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "model backward needs %zu B of shared memory", smem);
+  cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(sms, ceil_div(n, NT)));
+  ProfScope ps(kProfModel, s);
+  k<<<blocks, NT, smem, s>>>(grid, (const T*)table, W, x, n, tval, dsigma, act, out_act, table_grad, W_grad);
+  return launch_status("model_bwd_kernel");
+}
+
 template <int D, int F, int H>
 int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table, const float* W, const TrainArgs& a,
               Workspace ws, int act, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
@@ -334,6 +444,22 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
 }
 
 }  // namespace
+
+int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void* table, const float* W,
+                   const float* x, int64_t n, float tval, const float* dsigma, float* table_grad, float* W_grad,
+                   cudaStream_t s) {
+  const bool h = dtype == NECTB_F16;
+  const int D = g.n_dims, F = g.n_features, H = mlp.n_hidden_layers;
+  const int act = mlp.activation, oact = mlp.output_activation;
+  if (D == 3 && F == 2 && H == 2)
+    return h ? launch_model_bwd<3, 2, 2, __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s)
+             : launch_model_bwd<3, 2, 2, float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s);
+  if (D == 4 && F == 2 && H == 2)
+    return h ? launch_model_bwd<4, 2, 2, __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s)
+             : launch_model_bwd<4, 2, 2, float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s);
+  return set_error(NECTB_ERR_INVALID, "model backward: unsupported configuration (n_dims %d, n_features %d, "
+                   "hidden %d)", D, F, H);
+}
 
 int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const float* table,
                 const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,

@@ -65,7 +65,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         precision: str = "mixed", niter: int = 2000, lr: float = 1e-3, rays_per_batch: int = 65536,
         points_per_ray: int | None = None, loss: str = "l2", seed: int = 0, device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
-        add_poisson: bool = False) -> Reconstruction:
+        add_poisson: bool = False, tv: float = 0.0) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -77,8 +77,10 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     detector offset while binned), points per ray and learning rate, for
     min(niter, schedule.total_projections) steps.  ``s3im`` adds the S3IM
     term after the schedule's warm-up (base_trainer.py:557-566) and
-    ``add_poisson`` the reference's Poisson term; both run the step as
-    forward half, torch loss, backward half."""
+    ``add_poisson`` the reference's Poisson term and ``tv`` > 0 the
+    total-variation term of a static model on a random 100^3 sub-grid after
+    the warm-up (base_trainer.py:615-649); these run the step as forward
+    half, torch loss, backward half."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -114,6 +116,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         raw = proj.view(n_proj, rows, cols)
         ppb = trainer.points_per_batch
     binning = 1
+    tv_rng = np.random.default_rng(seed + 7)
     record(0)
     for step in range(1, niter + 1):
         k = int(order[(step - 1) % n_proj])
@@ -134,10 +137,12 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
             trainer.lr = st.lr
         perm = torch.randperm(target.numel(), dtype=torch.int64, device=dev)
         batch = trainer.make_batch(perm, 0, angles[k], target, ts[k])
-        if s3im or add_poisson:
+        if s3im or add_poisson or tv > 0:
             warm = schedule.warmup[0] if schedule is not None else 0
             patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
-            trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch)
+            tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
+            trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
+                               tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
         else:
             trainer.step(batch)
         if eval_every and (step % eval_every == 0 or step == niter):

@@ -170,6 +170,58 @@ def ray_integral(model: _HashGridModel, c_geometry, batch: RayBatch, max_distanc
     return RayIntegral.apply(model.table, model.mlp, model, c_geometry, batch, max_distance_traveled, workspace)
 
 
+class ModelPoints(torch.autograd.Function):
+    """sigma(x) at n points, differentiable in (table, mlp): forward
+    nectb_model_forward, backward nectb_model_backward.  For losses on model
+    outputs, such as the total-variation term (base_trainer.py:615-649)."""
+
+    @staticmethod
+    def forward(ctx, table, mlp, model, x, t):
+        x = x.detach().to(torch.float32).contiguous()
+        _lib.require_cuda(x, "x")
+        sigma = torch.empty(x.shape[0], device=x.device, dtype=torch.float32)
+        rc = _lib.lib.nectb_model_forward(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
+                                          model.grid_table.data_ptr(), model.mlp.data_ptr(), x.data_ptr(),
+                                          x.shape[0], float(t), sigma.data_ptr(), _lib.stream_ptr(x.device))
+        _lib.check(rc, "nectb_model_forward")
+        ctx.model, ctx.x, ctx.t = model, x, float(t)
+        return sigma
+
+    @staticmethod
+    def backward(ctx, dsigma):
+        model, x = ctx.model, ctx.x
+        g = dsigma.detach().to(torch.float32).contiguous()
+        tg, mg = torch.zeros_like(model.table), torch.zeros_like(model.mlp)
+        rc = _lib.lib.nectb_model_backward(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
+                                           model.grid_table.data_ptr(), model.mlp.data_ptr(), x.data_ptr(),
+                                           x.shape[0], ctx.t, g.data_ptr(), tg.data_ptr(), mg.data_ptr(),
+                                           _lib.stream_ptr(x.device))
+        _lib.check(rc, "nectb_model_backward")
+        return tg, mg, None, None, None
+
+
+def model_points(model: _HashGridModel, x: torch.Tensor, t: float = 0.0) -> torch.Tensor:
+    """Differentiable sigma [n] of the model at points x [n, 3] ((z, y, x) in [0, 1])."""
+    return ModelPoints.apply(model.table, model.mlp, model, x, t)
+
+
+def total_variation_3d(volume: torch.Tensor, weight: float = 1.0) -> torch.Tensor:
+    """Sum of absolute neighbour differences along the three axes over the
+    voxel count, times weight (nect/utils.py:64-80)."""
+    di = (volume[1:] - volume[:-1]).abs().sum()
+    dj = (volume[:, 1:] - volume[:, :-1]).abs().sum()
+    dk = (volume[:, :, 1:] - volume[:, :, :-1]).abs().sum()
+    return (di + dj + dk) / (volume.shape[0] * volume.shape[1] * volume.shape[2]) * weight
+
+
+def tv_points(origin, n: int = 100, extent: float = 0.2, device="cuda") -> torch.Tensor:
+    """The n^3 grid [origin, origin + extent] per axis, (z, y, x) order, as
+    base_trainer.py:620-640 builds it for the total-variation term."""
+    axes = [torch.linspace(float(o), float(o) + extent, n, device=device) for o in origin]
+    z, y, x = torch.meshgrid(axes, indexing="ij")
+    return torch.stack((z.flatten(), y.flatten(), x.flatten()), 1)
+
+
 def projection_loss(y_pred: torch.Tensor, y: torch.Tensor, loss: str) -> torch.Tensor:
     """L1 or L2 (mean over rays), nect/config.py:481-497."""
     if loss.lower() == "l1":
@@ -295,17 +347,23 @@ class Trainer:
         y = projection[perm[batch.start:batch.start + batch.num_rays]]
         return self._loss_and_update(y_pred, y, add_poisson)
 
-    def split_step(self, batch: RayBatch, add_poisson: bool = False, s3im_patch: int = 0) -> torch.Tensor:
+    def split_step(self, batch: RayBatch, add_poisson: bool = False, s3im_patch: int = 0,
+                   tv_weight: float = 0.0, tv_origin=None) -> torch.Tensor:
         """One step with the loss composed in torch on y_pred (base_trainer.py:552-566):
-        the L1/L2 loss, optionally the Poisson noise term and the S3IM term
-        over ``s3im_patch``-sized patches; forward and backward are the fused
-        halves (RayIntegral)."""
+        the L1/L2 loss, optionally the Poisson noise term, the S3IM term over
+        ``s3im_patch``-sized patches and the total-variation term of the model
+        on a 100^3 grid of side 0.2 at ``tv_origin`` (base_trainer.py:615-649);
+        forward and backward are the fused halves (RayIntegral, ModelPoints)."""
         y_pred = ray_integral(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
                               self.workspace)
         y = batch.projection[batch.perm[batch.start:batch.start + batch.num_rays]]
-        return self._loss_and_update(y_pred, y, add_poisson, s3im_patch)
+        extra = None
+        if tv_weight > 0:
+            pts = tv_points(tv_origin, device=y_pred.device)
+            extra = total_variation_3d(model_points(self.model, pts).view(100, 100, 100), tv_weight)
+        return self._loss_and_update(y_pred, y, add_poisson, s3im_patch, extra)
 
-    def _loss_and_update(self, y_pred, y, add_poisson=False, s3im_patch=0):
+    def _loss_and_update(self, y_pred, y, add_poisson=False, s3im_patch=0, extra=None):
         if add_poisson:   # base_trainer.py:555-556; the Poisson draw carries no gradient
             y_pred = (y_pred + torch.poisson(y_pred.detach() * 1e5) / 1e5) / 2
         loss = projection_loss(y_pred, y, self.loss)
@@ -313,6 +371,8 @@ class Trainer:
             from .schedule import s3im_loss
 
             loss = loss + s3im_loss(y_pred, y, s3im_patch)
+        if extra is not None:
+            loss = loss + extra
         g_table, g_mlp = torch.autograd.grad(loss, [self.model.table, self.model.mlp])
         self.step_count += 1
         adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
