@@ -256,6 +256,23 @@ def adam_step(param: torch.Tensor, grad: torch.Tensor, m: torch.Tensor, v: torch
     _lib.check(rc, "nectb_adam_step")
 
 
+def reduce_gradients(grads, group=None) -> None:
+    """Average gradients over the ranks of ``group`` in place, as the
+    reference's Fabric DDP does (base_trainer.py:106-112): one all-reduce per
+    gradient tensor (the table gradient is one contiguous buffer; NCCL over
+    NVLink/NVSwitch on GPUs), then division by the world size."""
+    import torch.distributed as dist
+
+    if not dist.is_available() or not dist.is_initialized():
+        return
+    world = dist.get_world_size(group)
+    if world == 1:
+        return
+    for g in grads:
+        dist.all_reduce(g, op=dist.ReduceOp.SUM, group=group)
+        g.div_(world)
+
+
 class Trainer:
     """Per-projection training loop on the fused kernels.
 
@@ -267,7 +284,7 @@ class Trainer:
     def __init__(self, model: _HashGridModel, geometry: Geometry, points_per_batch: int, points_per_ray: int,
                  loss: str = "l2", lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8,
                  weight_decay: float = 0.0, batch_per_proj: int = 1, random_offset_detector: float = 0.0,
-                 uniform_ray_spacing: bool = True, device="cuda"):
+                 uniform_ray_spacing: bool = True, device="cuda", data_parallel: bool = False, process_group=None):
         self.model = model
         self.geometry = geometry
         self.c_geometry = geometry.get_c_geometry()
@@ -290,6 +307,9 @@ class Trainer:
         self.v_mlp = torch.zeros_like(model.mlp)
         self.step_count = 0
         self.workspace = Workspace()
+        # data parallel: every rank trains on its own rays, gradients are averaged before Adam
+        self.data_parallel = data_parallel
+        self.process_group = process_group
 
     @property
     def batch_size(self) -> int:
@@ -314,6 +334,8 @@ class Trainer:
     def step(self, batch: RayBatch) -> torch.Tensor:
         loss, _ = train_step(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
                              self.table_grad, self.mlp_grad, self.workspace, self.loss)
+        if self.data_parallel:
+            reduce_gradients([self.table_grad, self.mlp_grad], self.process_group)
         self.step_count += 1
         adam_step(self.model.table, self.table_grad, self.m_table, self.v_table, self.step_count, self.lr,
                   self.betas, self.eps, self.weight_decay, half=self.model.table_half)
@@ -374,6 +396,8 @@ class Trainer:
         if extra is not None:
             loss = loss + extra
         g_table, g_mlp = torch.autograd.grad(loss, [self.model.table, self.model.mlp])
+        if self.data_parallel:
+            reduce_gradients([g_table, g_mlp], self.process_group)
         self.step_count += 1
         adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
                   self.eps, self.weight_decay, half=self.model.table_half)
