@@ -64,6 +64,14 @@ def workload_spec(name: str, precision: str):
                                 max_resolution_factor=2.0, nDetector=[512, 512], base_resolution_t=4)
         return dict(geo=geo, model=ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision),
                     S=512, rays=1 << 18, n_angles=3600, turns=10, phantom="dynamic", n_dims=4)
+    if name == "c5_large_cone":
+        # 2048^2 detector, object 1024 voxels across at magnification 2, cylindrical clipping
+        geo = dict(nDetector=[2048, 2048], dDetector=[1.0, 1.0], mode="cone", DSD=4000.0, DSO=2000.0,
+                   nVoxel=[1024, 1024, 1024], dVoxel=[1.0, 1.0, 1.0], reconstruction_mode="cylindrical")
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=4, log2_hashmap_size=22, base_resolution=16,
+                                finest_resolution=4096, base_resolution_t=4)
+        return dict(geo=geo, model=ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=3), precision),
+                    S=1024, rays=1 << 20, n_angles=7200, turns=20, phantom="ellipsoids", n_dims=4)
     raise ValueError(name)
 
 
@@ -75,7 +83,7 @@ def make_projections(spec, geometry, n_proj: int, device, seed: int = 0):
     angles = angles_all[idx]
     ts = idx / max(spec["n_angles"] - 1, 1)
     if spec["phantom"] == "ellipsoids":
-        ph = phantoms.ellipsoid_phantom(20, seed)
+        ph = phantoms.ellipsoid_phantom(20, seed, size=geometry.sVoxel[0])   # the large 4D workload: 1024 voxels
         projs = torch.stack([phantoms.ellipsoid_projection(ph, geometry, float(a), device) for a in angles])
     elif spec["phantom"] == "dynamic":
         # each projection at its own t; Poisson noise at 1e4 incident photons on the attenuation
@@ -176,7 +184,7 @@ def cpu_port_step(spec, geometry, model_cfg, table, mlp_flat, proj_flat_cpu, ang
     loss = torch.nn.functional.mse_loss(y_pred, y)
     loss.backward()
     opt.step()
-    return float(loss)
+    return float(loss.detach())
 
 
 def run_cpu(spec, geometry, model, projs, angles, ts, steps: int, warmup: int, rays: int):
@@ -236,7 +244,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c2_static_cone",
-                    choices=["c2_static_cone", "c1_static_parallel", "c3_dynamic_cone"])
+                    choices=["c2_static_cone", "c1_static_parallel", "c3_dynamic_cone", "c5_large_cone"])
     ap.add_argument("--precision", default=os.environ.get("NECTB_PRECISION", "mixed"),
                     choices=["mixed", "plain_fp32"])
     ap.add_argument("--cpu-rays", type=int, default=2048)

@@ -256,9 +256,9 @@ size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHas
  * repeats a pixel); each round's tensor-core pass writes dL/d(encoding) of its
  * samples (fp32, num_points_per_ray * n_levels * n_features per index) and
  * scatter passes over level groups apply it to grid_grad with the gradient
- * slice of each group resident in L2.  Less staging gives more rounds; when
- * it would take more than 64 rounds the single-pass backward (scatter inside
- * the tensor-core kernel) runs instead.  Returns 0 for the plain fp32 path, which does not
+ * slice of each group resident in L2.  The recommendation is capped at 4 GiB.
+ * Less staging gives more rounds; when it would take more than 64 rounds the
+ * single-pass backward (scatter inside the tensor-core kernel) runs instead.  Returns 0 for the plain fp32 path, which does not
  * stage.  No reference counterpart. */
 size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                  const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray);

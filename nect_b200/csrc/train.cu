@@ -96,14 +96,14 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
   NECTB_REQUIRE(batch->loss_type == 1 || batch->loss_type == 2, "loss_type must be 1 (L1) or 2 (L2)");
   NECTB_REQUIRE(batch->max_distance_traveled > 0.f, "max_distance_traveled must be positive");
   NECTB_REQUIRE(grid_params && mlp_params, "null parameters");
-  NECTB_REQUIRE(!(phase & kPhaseForward) || y_pred, "null y_pred");
   NECTB_REQUIRE(!(phase & kPhaseBackward) || (grid_grad && mlp_grad), "null gradient buffers");
   NECTB_REQUIRE(phase != (kPhaseForward | kPhaseBackward) || loss, "null loss");
-  NECTB_REQUIRE(phase != kPhaseBackward || dloss_dy, "null dloss_dy");
   cudaStream_t s = (cudaStream_t)stream;
   if (loss)
     if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
-  if (batch->num_rays == 0) return NECTB_OK;
+  if (batch->num_rays == 0) return NECTB_OK;  // per-ray arrays may be null
+  NECTB_REQUIRE(!(phase & kPhaseForward) || y_pred, "null y_pred");
+  NECTB_REQUIRE(phase != kPhaseBackward || dloss_dy, "null dloss_dy");
   NECTB_REQUIRE(((uintptr_t)grid_grad & 15u) == 0 && ((uintptr_t)grid_params & 15u) == 0,
                 "grid_grad and grid_params must be 16-byte aligned");
   NECTB_REQUIRE(batch->random_ray_index && batch->jitter && batch->detector_offset && batch->projection,
@@ -192,7 +192,8 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
   const int64_t N = std::max<int64_t>(num_rays, P);
   const int64_t per_round = ceil_div(N, kStagedRounds);
-  return (size_t)per_round * num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
+  const size_t per_index = (size_t)num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
+  return std::min((size_t)per_round * per_index, kStagingCap / per_index * per_index);
 }
 
 extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,

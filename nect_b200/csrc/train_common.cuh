@@ -52,6 +52,7 @@ enum : unsigned int { kFlagDuplicatePixels = 1u };
 // buffer may need before the fused single-pass backward is used instead.
 constexpr int kStagedRounds = 8;
 constexpr int kMaxStagedRounds = 64;
+constexpr size_t kStagingCap = size_t(4) << 30;  // largest staging buffer recommended
 
 // Workspace: RayRec[R] | slot[P] (int32: batch index of the ray through each
 // detector pixel, -1 if none) | 64-byte control block (scheduling cursors of

@@ -39,26 +39,47 @@ __device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
 }
 
 // fp32 weights (PyTorch layout) -> bf16 swizzled tiles: W0 rows o (IN used
-// columns), W1 rows o (64 columns); w_out stays fp32.
-template <int IN>
-__device__ __forceinline__ void stage_mixed_weights(const float* __restrict__ W, uint8_t* sW0, uint8_t* sW1,
-                                                    float* sWout) {
+// columns), W1..W_{H-1} rows o (64 columns) in consecutive 8 KB tiles after
+// W0; w_out stays fp32.
+template <int IN, int H>
+__device__ __forceinline__ void stage_mixed_weights(const float* __restrict__ W, uint8_t* sW, float* sWout) {
   for (int e = threadIdx.x; e < 64 * (IN / 8); e += blockDim.x) {
     const int o = e / (IN / 8), j = e % (IN / 8);
     float v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
-    tc::st_chunk_bf16(sW0, o, j, v);
+    tc::st_chunk_bf16(sW, o, j, v);
   }
-  const float* W1 = W + 64 * IN;
-  for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
-    const int o = e / 8, j = e % 8;
+#pragma unroll 1
+  for (int k = 1; k < H; ++k) {
+    const float* Wk = W + 64 * IN + (k - 1) * 64 * 64;
+    for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
+      const int o = e / 8, j = e % 8;
+      float v[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) v[q] = Wk[o * 64 + 8 * j + q];
+      tc::st_chunk_bf16(sW + k * kWTile, o, j, v);
+    }
+  }
+  for (int e = threadIdx.x; e < 64; e += blockDim.x) sWout[e] = W[64 * IN + (H - 1) * 64 * 64 + e];
+}
+
+// ReLU of 64 accumulator values into row r of a bf16 tile; bit j of m = (x_j > 0).
+__device__ __forceinline__ void relu_row(const float* h, uint8_t* tile, int r, uint32_t& mlo, uint32_t& mhi) {
+  mlo = 0;
+  mhi = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
     float v[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = W1[o * 64 + 8 * j + q];
-    tc::st_chunk_bf16(sW1, o, j, v);
+    for (int q = 0; q < 8; ++q) {
+      const float x = h[8 * j + q];
+      v[q] = fmaxf(x, 0.f);
+      const uint32_t bit = x > 0.f ? 1u : 0u;
+      if (8 * j + q < 32) mlo |= bit << (8 * j + q); else mhi |= bit << (8 * j + q - 32);
+    }
+    tc::st_chunk_bf16(tile, r, j, v);
   }
-  for (int e = threadIdx.x; e < 64; e += blockDim.x) sWout[e] = W[64 * IN + 64 * 64 + e];
 }
 
 // Encodes one sample into row r of the swizzled X tile (bf16), 8 features
@@ -141,7 +162,7 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
 constexpr int kFwdBlocksPerSM = NECTB_FWD_BLOCKS_PER_SM;
 static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 128 <= 512, "TMEM holds 512 columns per SM");
 
-template <int D, int F>
+template <int D, int F, int H>
 __global__ void __launch_bounds__(kMixThreads, kFwdBlocksPerSM)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
@@ -151,12 +172,11 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
-  uint8_t* sW0 = base;
-  uint8_t* sW1 = sW0 + kWTile;
-  uint8_t* sX = sW1 + kWTile;
-  // A1 overwrites X: the first MMA has finished reading X (its commit has
-  // arrived) before A1 is written, and the next X is written only after the
-  // second MMA, which reads A1, has completed.
+  uint8_t* sW = base;  // H weight tiles
+  uint8_t* sX = sW + H * kWTile;
+  // Each hidden layer's activations overwrite X: the MMA that read the tile has
+  // finished (its commit has arrived) before the next activations are written,
+  // and the next X is written only after the last MMA has completed.
   uint8_t* sA = sX;
   float* sWout = reinterpret_cast<float*>(sX + kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
@@ -164,7 +184,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   float* red = reinterpret_cast<float*>(tslot + 4);
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  stage_mixed_weights<IN>(W, sW0, sW1, sWout);
+  stage_mixed_weights<IN, H>(W, sW, sWout);
   if (warp == 0) {
     tc::tmem_alloc(tslot, 128);
     tc::tmem_relinquish();
@@ -176,8 +196,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   tc::fence_after();
   const uint32_t tm = *tslot;
   const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
-  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA);
-  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
   constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
 
   uint32_t phase = 0;
@@ -194,48 +213,40 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
     encode_row<D, F>(grid, table, p, valid, sX, t);
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-#pragma unroll
-      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), idesc, k > 0);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
     float h[64];
-    ld64(my_lanes, h);
+    // layer k (0-based) writes TMEM columns 64 * (k & 1); its input is X for
+    // k = 0, else the previous layer's activations in sA
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float v[8];
+    for (int k = 0; k < H; ++k) {
+      if (k > 0) {
+        uint32_t mlo, mhi;
+        relu_row(h, sA, t, mlo, mhi);
+      }
+      tc::fence_async_smem();
+      tc::fence_before();
+      __syncthreads();
+      if (t == 0) {
+        tc::fence_after();
+        if (k == 0) {
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = fmaxf(h[8 * j + q], 0.f);
-      tc::st_chunk_bf16(sA, t, j, v);
-    }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
+          for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sX_a, q), tc::desc_k(sW_a, q), idesc, q > 0);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, q), tc::desc_k(sW_a + k * kWTile, q), idesc, q > 0);
+        }
+        tc::commit(bar);
+      }
+      timed_out = !tc::mbar_wait(bar, phase);
+      phase ^= 1;
+      if (__syncthreads_or(timed_out)) {
+        timed_out = true;
+        break;
+      }
       tc::fence_after();
-#pragma unroll
-      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), idesc, k > 0);
-      tc::commit(bar);
+      ld64(my_lanes + 64 * (k & 1), h);
     }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
-    ld64(my_lanes + 64, h);
+    if (timed_out) break;
     float z = 0.f;
 #pragma unroll
     for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
@@ -276,32 +287,33 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 // is written to the staging buffer, level-major: stage[(l * slots + s) * F + f]
 // with s = (scheduling index - lo) * S + sample, for the rays whose
 // scheduling index lies in [lo, hi); scatter_stage_kernel applies it.
-template <int D, int F, bool kStaged>
+template <int D, int F, int H, bool kStaged>
 __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
                  float* __restrict__ stage, int64_t slots) {
   constexpr int IN = 16 * F;
+  static_assert(IN <= 64 && H >= 2 && H <= 3, "TMEM plan: 64 transient + (H - 1) x 64 + IN columns <= 256");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
-  // Tile order matters: the padded (M = 128) weight-gradient operands read a
-  // second 16 KB block right after their tile, so sG is followed by sA and sA
-  // by sX, all inside this block's allocation.
-  uint8_t* sW0 = base;
-  uint8_t* sW1 = sW0 + kWTile;
-  uint8_t* sG = sW1 + kWTile;  // G2
-  uint8_t* sA = sG + kTile;    // A1, later G1
-  uint8_t* sX = sA + kTile;
+  // Tiles: sG (G_H), then A_{H-1} ... A_1 (each later replaced by G_k), then
+  // X.  Order matters: the padded (M = 128) weight-gradient products read a
+  // second 16 KB block right after their G tile, which is always the next
+  // tile of this list, inside this block's allocation.
+  uint8_t* sW = base;  // H weight tiles
+  uint8_t* sG = sW + H * kWTile;
+  uint8_t* sX = sG + H * kTile;
   float* sWout = reinterpret_cast<float*>(sX + kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
+  auto sAk = [&](int k) { return sG + (H - k) * kTile; };   // A_k (k = 1..H-1), later G_k
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  stage_mixed_weights<IN>(W, sW0, sW1, sWout);
+  stage_mixed_weights<IN, H>(W, sW, sWout);
   if (warp == 0) {
     tc::tmem_alloc(tslot, 256);
     tc::tmem_relinquish();
@@ -313,14 +325,14 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   tc::fence_after();
   const uint32_t tm = *tslot;
   const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
-  // TMEM columns: [0,64) acc0, [64,128) acc1, [128,192) dW1, [192,192+IN) dW0
-  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sG_a = tc::smem_u32(sG);
-  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  // TMEM columns: [0,64) every layer's and every gradient product's transient
+  // result, [192 - 64k, 256 - 64k) dW_k for k = 1..H-1, [192, 192 + IN) dW0.
+  const uint32_t sX_a = tc::smem_u32(sX), sG_a = tc::smem_u32(sG), sW_a = tc::smem_u32(sW);
   // M = 128 weight-gradient products: rows 64..127 of A come from the tile kTile further on.
   const uint32_t pad_lbo = kTile;
   constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
   constexpr uint32_t id_dA = tc::idesc_bf16(128, 64, false, true);
-  constexpr uint32_t id_dW1 = tc::idesc_bf16(128, 64, true, true);
+  constexpr uint32_t id_dW = tc::idesc_bf16(128, 64, true, true);
   constexpr uint32_t id_dX = tc::idesc_bf16(128, IN, false, true);
   constexpr uint32_t id_dW0 = tc::idesc_bf16(128, IN, true, true);
 
@@ -330,6 +342,22 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   int j0_out = 0;
   RayCursor cur;
   bool timed_out = false;
+  // Issues the MMAs of one phase (thread 0), waits for them; false on time-out.
+  auto run_phase = [&](auto issue) -> bool {
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+      issue();
+      tc::commit(bar);
+    }
+    const bool to = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(to)) return false;
+    tc::fence_after();
+    return true;
+  };
   while (true) {
     const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi);
     if (!__syncthreads_or(active)) break;
@@ -339,59 +367,34 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
     encode_row<D, F>(grid, table, p, valid, sX, t);
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-#pragma unroll
-      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), id_fwd, k > 0);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
+    // forward recompute: layer 0 from X, layer k from A_k (stored with its ReLU mask)
     float h[64];
-    ld64(my_lanes, h);
-    uint32_t m1lo = 0, m1hi = 0;  // relu masks of A1
+    uint32_t mlo[H], mhi[H];
+    bool ok = run_phase([&] {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float v[8];
+      for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sX_a, q), tc::desc_k(sW_a, q), id_fwd, q > 0);
+    });
+    if (ok) ld64(my_lanes, h);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const float x = h[8 * j + q];
-        v[q] = fmaxf(x, 0.f);
-        const uint32_t bit = x > 0.f ? 1u : 0u;
-        if (8 * j + q < 32) m1lo |= bit << (8 * j + q); else m1hi |= bit << (8 * j + q - 32);
-      }
-      tc::st_chunk_bf16(sA, t, j, v);
+    for (int k = 1; k < H && ok; ++k) {
+      relu_row(h, sAk(k), t, mlo[k], mhi[k]);
+      const uint32_t a_k = tc::smem_u32(sAk(k));
+      ok = run_phase([&] {
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          tc::mma(tm, tc::desc_k(a_k, q), tc::desc_k(sW_a + k * kWTile, q), id_fwd, q > 0);
+      });
+      if (ok) ld64(my_lanes, h);
     }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-#pragma unroll
-      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), id_fwd, k > 0);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
+    if (!ok) {
       timed_out = true;
       break;
     }
-    tc::fence_after();
-    ld64(my_lanes + 64, h);
     float z = 0.f;
 #pragma unroll
     for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
     const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
-    // w_out gradient over the warp's samples; G2 = dz * w_out * 1[a2 > 0]
+    // w_out gradient over the warp's samples; G_H = dz * w_out * 1[a_H > 0]
     {
       float v[64];
 #pragma unroll
@@ -408,71 +411,66 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
       for (int q = 0; q < 8; ++q) v[q] = h[8 * j + q] > 0.f ? dz * sWout[8 * j + q] : 0.f;
       tc::st_chunk_bf16(sG, t, j, v);
     }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-      // dA1 = G2 W1 (A = G2 K-major, B = W1 MN-major)
+    // backward through the hidden layers: G_{k+1} (tile gt) gives
+    //   dA_k = G_{k+1} W_k        (A = G K-major, B = W_k MN-major) -> transient columns
+    //   dW_k += G_{k+1}^T A_k     (A = G MN-major, M = 128 padded; B = A_k MN-major; K = 128 samples)
+    // and G_k = dA_k * 1[a_k > 0] replaces A_k once the dW_k product has completed.
+    uint32_t gt = sG_a;
 #pragma unroll
-      for (int k = 0; k < 4; ++k) tc::mma(tm, tc::desc_k(sG_a, k), tc::desc_mn(sW1_a, k, kWTile), id_dA, k > 0);
-      // dW1 += G2^T A1 (A = G2 MN-major, M = 128 padded; B = A1 MN-major; K = 128 samples)
+    for (int k = H - 1; k >= 1 && ok; --k) {
+      const uint32_t a_k = tc::smem_u32(sAk(k));
+      const uint32_t wk = sW_a + k * kWTile;
+      const uint32_t dwk = tm + 192 - 64 * k;
+      ok = run_phase([&] {
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
-        tc::mma(tm + 128, tc::desc_mn(sG_a, k, pad_lbo), tc::desc_mn(sA_a, k, kTile), id_dW1, (k > 0) | wacc);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
-    ld64(my_lanes, h);
+        for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(gt, q), tc::desc_mn(wk, q, kWTile), id_dA, q > 0);
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float v[8];
+        for (int q = 0; q < 8; ++q)
+          tc::mma(dwk, tc::desc_mn(gt, q, pad_lbo), tc::desc_mn(a_k, q, kTile), id_dW, (q > 0) | wacc);
+      });
+      if (!ok) break;
+      ld64(my_lanes, h);
 #pragma unroll
-      for (int q = 0; q < 8; ++q) {
-        const int c = 8 * j + q;
-        const uint32_t bit = c < 32 ? (m1lo >> c) & 1u : (m1hi >> (c - 32)) & 1u;
-        v[q] = bit ? h[c] : 0.f;
+      for (int j = 0; j < 8; ++j) {
+        float v[8];
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int c = 8 * j + q;
+          const uint32_t bit = c < 32 ? (mlo[k] >> c) & 1u : (mhi[k] >> (c - 32)) & 1u;
+          v[q] = bit ? h[c] : 0.f;
+        }
+        tc::st_chunk_bf16(sAk(k), t, j, v);
       }
-      tc::st_chunk_bf16(sA, t, j, v);  // G1 replaces A1 (the dW1 product has completed)
+      gt = a_k;
     }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-      // dX = G1 W0 (A = G1 K-major, B = W0 MN-major, N = IN)
+    // dX = G_1 W0 (A = G_1 K-major, B = W0 MN-major, N = IN); dW0 += G_1^T X
+    if (ok)
+      ok = run_phase([&] {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_mn(sW0_a, k, kWTile), id_dX, k > 0);
-      // dW0 += G1^T X (A = G1 MN-major, M = 128 padded; B = X MN-major; K = 128 samples)
+        for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(gt, q), tc::desc_mn(sW_a, q, kWTile), id_dX, q > 0);
 #pragma unroll
-      for (int k = 0; k < 8; ++k)
-        tc::mma(tm + 192, tc::desc_mn(sA_a, k, pad_lbo), tc::desc_mn(sX_a, k, kTile), id_dW0, (k > 0) | wacc);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
+        for (int q = 0; q < 8; ++q)
+          tc::mma(tm + 192, tc::desc_mn(gt, q, pad_lbo), tc::desc_mn(sX_a, q, kTile), id_dW0, (q > 0) | wacc);
+      });
+    if (!ok) {
       timed_out = true;
       break;
     }
     wacc = 1;
-    tc::fence_after();
     float dx[IN];
 #pragma unroll
-    for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, dx + 16 * c);
+    for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 16 * c, dx + 16 * c);
     tc::tmem_wait_ld();
     if constexpr (kStaged) {
       if (valid) {
         float* dst = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
 #pragma unroll
         for (int l = 0; l < 16; ++l) {
-          if constexpr (F == 2) *reinterpret_cast<float2*>(dst + l * slots * F) = make_float2(dx[2 * l], dx[2 * l + 1]);
+          if constexpr (F == 2)
+            *reinterpret_cast<float2*>(dst + l * slots * F) = make_float2(dx[2 * l], dx[2 * l + 1]);
+          else if constexpr (F == 4)
+            *reinterpret_cast<float4*>(dst + l * slots * F) =
+                make_float4(dx[4 * l], dx[4 * l + 1], dx[4 * l + 2], dx[4 * l + 3]);
           else
 #pragma unroll
             for (int f = 0; f < F; ++f) dst[l * slots * F + f] = dx[l * F + f];
@@ -480,7 +478,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
       }
     } else {
       scatter_warp<D, F>(grid, table_grad, p, valid, dx, F, 1,
-                         active ? run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u, 0, grid.n_levels);
+                         active ? run_levels<D>(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u, 0, grid.n_levels);
     }
     tc::fence_before();
     __syncthreads();
@@ -494,10 +492,14 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     tc::fence_after();
     if (warp < 2) {
       const int o = t;
-      float v[64];
-      ld64(my_lanes + 128, v);
+#pragma unroll 1
+      for (int k = 1; k < H; ++k) {
+        float v[64];
+        ld64(my_lanes + 192 - 64 * k, v);
+        float* dst = W_grad + 64 * IN + (k - 1) * 64 * 64 + o * 64;
 #pragma unroll
-      for (int i2 = 0; i2 < 64; ++i2) atomicAdd(W_grad + 64 * IN + o * 64 + i2, v[i2]);
+        for (int i2 = 0; i2 < 64; ++i2) atomicAdd(dst + i2, v[i2]);
+      }
       float w0[IN];
 #pragma unroll
       for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 192 + 16 * c, w0 + 16 * c);
@@ -517,7 +519,8 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   red[warp * 64 + j0_out + 1] = dwout1;
   tc::fence_before();
   __syncthreads();
-  if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
+  if (t < 64)
+    atomicAdd(W_grad + 64 * IN + (H - 1) * 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
   if (warp == 0) {
     tc::fence_after();
     tc::tmem_dealloc(tm, 256);
@@ -546,7 +549,7 @@ scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs,
     if (D == 4) p[3] = a.t;
     const float* dsrc = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
     scatter_warp<D, F>(grid, table_grad, p, valid, dsrc, slots * F, 1,
-                       run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz), l0, l1);
+                       run_levels<D>(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz), l0, l1);
     cur.base += 32;
   }
 }
@@ -555,7 +558,7 @@ scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs,
 // slices add up to at most kScatterGroupBytes.
 constexpr size_t kScatterGroupBytes = size_t(48) << 20;
 
-template <int D, int F>
+template <int D, int F, int H>
 int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W, const TrainArgs& a,
               Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
               cudaStream_t s) {
@@ -570,8 +573,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     blocks = std::min(blocks, a.max_blocks);
   }
   if (a.phase & kPhaseForward) {
-    auto k = fwd_mixed_kernel<D, F>;
-    const size_t smem = 1024 + 2 * kWTile + kTile + 64 * 4 + 64;
+    auto k = fwd_mixed_kernel<D, F, H>;
+    const size_t smem = 1024 + H * kWTile + kTile + 64 * 4 + 64;
     set_smem(k, smem, a.max_blocks > 0);
     {
       ProfScope ps(kProfForward, s);
@@ -580,15 +583,16 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   }
   if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
-  // 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
-  const size_t bsmem = std::max<size_t>(1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
+  // at least 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
+  const size_t bsmem =
+      std::max<size_t>(1024 + H * kWTile + (H + 1) * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
   constexpr int IN = 16 * F;
   const int64_t per_index = (int64_t)a.S * IN * (int64_t)sizeof(float);
   const int64_t N = std::max(a.num_rays, a.n_pixels);  // covers both scheduling orders
   const int64_t per_round = ws.stage ? std::min<int64_t>((int64_t)(ws.stage_bytes / per_index), N) : 0;
   if (per_round <= 0 || ceil_div(N, per_round) > kMaxStagedRounds) {
     // fused single pass: the backward scatters its own gradients
-    auto k = bwd_mixed_kernel<D, F, false>;
+    auto k = bwd_mixed_kernel<D, F, H, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
     k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
@@ -611,7 +615,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     }
     group_start[n_groups] = grid.n_levels;
   }
-  auto kb = bwd_mixed_kernel<D, F, true>;
+  auto kb = bwd_mixed_kernel<D, F, H, true>;
   cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
@@ -648,16 +652,21 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
                 float* y_pred, float* loss, cudaStream_t s) {
   (void)nW;
   const int D = grid.n_dims, F = grid.n_features;
-  if (mlp.n_hidden_layers != 2 || mlp.activation != NECTB_ACT_RELU)
-    return set_error(NECTB_ERR_INVALID, "mixed path: needs 2 hidden ReLU layers (got %d, act %d)",
-                     mlp.n_hidden_layers, mlp.activation);
+  const int H = mlp.n_hidden_layers;
+  if ((H != 2 && H != 3) || mlp.activation != NECTB_ACT_RELU)
+    return set_error(NECTB_ERR_INVALID, "mixed path: needs 2 or 3 hidden ReLU layers (got %d, act %d)", H,
+                     mlp.activation);
   if (grid.n_levels != 16 || mlp.n_input != 16 * F || mlp.width != 64)
     return set_error(NECTB_ERR_INVALID, "mixed path: needs 16 levels, n_input 16 x n_features and width 64");
   const __half* tab = (const __half*)table;
   const int oact = mlp.output_activation;
-  if (D == 3 && F == 2) return run_mixed<3, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
-  if (D == 4 && F == 2) return run_mixed<4, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
-  return set_error(NECTB_ERR_INVALID, "mixed path: unsupported grid (n_dims %d, n_features %d)", D, F);
+  if (D == 3 && F == 2 && H == 2)
+    return run_mixed<3, 2, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  if (D == 4 && F == 2 && H == 2)
+    return run_mixed<4, 2, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  if (D == 4 && F == 4 && H == 3)  // the large 4D workload: 16 x 4 features, 3 x 64 MLP
+    return run_mixed<4, 4, 3>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  return set_error(NECTB_ERR_INVALID, "mixed path: unsupported grid (n_dims %d, n_features %d, hidden %d)", D, F, H);
 }
 
 }  // namespace nectb

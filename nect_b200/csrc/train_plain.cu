@@ -429,7 +429,9 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   }
   if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
 
-  constexpr int NT = 128;
+  // 64-thread tiles when 128 would not fit shared memory (3 hidden layers over 64 inputs)
+  constexpr int NT = (IN + (H + 2) * kWidth) * (128 + 4) * 4 + simt_weight_floats<IN, H, true>() * 4 > 227 * 1024
+                         ? 64 : 128;
   auto bk = bwd_plain_kernel<D, F, IN, H, NT>;
   const size_t bsmem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
   if (bsmem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "plain backward needs %zu B of shared memory", bsmem);
@@ -471,8 +473,10 @@ int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
     return run_plain<3, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
   if (D == 4 && F == 2 && H == 2)
     return run_plain<4, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
-  return set_error(NECTB_ERR_INVALID, "plain path supports 16x2 grids with 2 hidden layers (got n_dims %d, "
-                   "n_features %d, hidden %d)", D, F, H);
+  if (D == 4 && F == 4 && H == 3)  // the large 4D workload: 16 x 4 features, 3 x 64 MLP
+    return run_plain<4, 4, 3>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+  return set_error(NECTB_ERR_INVALID, "plain path supports 16x2 grids with 2 hidden layers and 16x4 4D grids with "
+                   "3 (got n_dims %d, n_features %d, hidden %d)", D, F, H);
 }
 
 }  // namespace nectb

@@ -111,14 +111,14 @@ class EllipsoidPhantom:
     mu: np.ndarray        # [E]
 
 
-def ellipsoid_phantom(n: int = 20, seed: int = 0) -> EllipsoidPhantom:
-    """Centres U[-0.6,0.6]^3 in the cube [-1,1]^3 scaled to the unit cube
-    (i.e. U[-0.3,0.3] in world units), semi-axes U[0.05,0.35] of the [-1,1]
-    cube (world U[0.025,0.175]), uniform random rotations, attenuation
-    U[0.1,1.0]."""
+def ellipsoid_phantom(n: int = 20, seed: int = 0, size: float = 1.0) -> EllipsoidPhantom:
+    """Centres U[-0.6,0.6]^3 in the cube [-1,1]^3 scaled to a cube of side
+    ``size`` (unit cube: U[-0.3,0.3] in world units), semi-axes U[0.05,0.35]
+    of the [-1,1] cube (unit cube: U[0.025,0.175]), uniform random rotations,
+    attenuation U[0.1,1.0] per unit of the cube."""
     rng = np.random.default_rng(seed)
-    centers = rng.uniform(-0.6, 0.6, (n, 3)) * 0.5
-    axes = rng.uniform(0.05, 0.35, (n, 3)) * 0.5
+    centers = rng.uniform(-0.6, 0.6, (n, 3)) * 0.5 * size
+    axes = rng.uniform(0.05, 0.35, (n, 3)) * 0.5 * size
     q = rng.normal(size=(n, 4))
     q /= np.linalg.norm(q, axis=1, keepdims=True)
     w, x, y, z = q.T

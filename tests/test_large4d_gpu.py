@@ -1,0 +1,102 @@
+"""The large 4D workload's model shape (16 levels x 4 features, 3 x 64 MLP)
+on a cone beam with cylindrical clipping: fused training steps of both paths
+against the fp64 oracle, and the two-pass mixed backward against the single
+pass.  Tolerances as the 2-feature parity tests: plain y_pred and loss 1e-4,
+gradients 1e-3 of the largest entry; mixed y_pred 2e-2, loss 5e-2, gradient
+cosine > 0.99 and max deviation < 5e-2."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import hashgrid as ohg
+from oracle import sampling as osamp
+
+pytestmark = pytest.mark.gpu
+
+
+def make_model(precision, seed=0):
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig
+    from nect_b200.network import HashGrid4D
+
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=4, log2_hashmap_size=12, base_resolution=4,
+                            finest_resolution=128, base_resolution_t=2)
+    net = MLPNetConfig(n_hidden_layers=3, n_neurons=64, activation="ReLU", output_activation="Softplus")
+    m = HashGrid4D(enc, net, precision=precision, device="cuda", seed=seed)
+    with torch.no_grad():
+        g = torch.Generator(device="cpu").manual_seed(seed + 1)
+        m.table.copy_((torch.rand(m.table.shape, generator=g) * 2 - 1) * 0.5)
+        m.refresh_half()
+    return m, enc
+
+
+def run_case(precision, ws=None, duplicates=False):
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import RayBatch, Workspace, train_step
+
+    torch.manual_seed(13)
+    geo = Geometry(nDetector=[40, 48], dDetector=[1.5, 1.5], mode="cone", DSD=300.0, DSO=200.0, nVoxel=[32] * 3,
+                   dVoxel=[1.0] * 3, reconstruction_mode="cylindrical")
+    m, enc = make_model(precision)
+    cg = geo.get_c_geometry()
+    P = 40 * 48
+    S, R, start = 64, 600, 80
+    perm = torch.randperm(P, device="cuda")
+    if duplicates:
+        perm[start + 1:start + 30] = perm[start]
+    jitter = torch.rand(R, device="cuda") - 0.5
+    det_off = torch.zeros(R, 2, device="cuda")
+    proj = torch.rand(P, device="cuda")
+    angle, t = 2.1, 0.3
+    maxd = geo.max_distance_traveled / S
+    batch = RayBatch(perm=perm, start=start, num_rays=R, points_per_ray=S, angle=angle,
+                     max_ray_distance_per_point=maxd, jitter=jitter, detector_offset=det_off, projection=proj, t=t)
+    tg, mg = torch.zeros_like(m.table), torch.zeros_like(m.mlp)
+    L, y = train_step(m, cg, batch, geo.max_distance_traveled, tg, mg, ws if ws is not None else Workspace(), "l2")
+    torch.cuda.synchronize()
+    ang = torch.tensor([angle, 0.0], dtype=torch.float32, device="cuda")
+    c, s = torch.cos(ang).cpu().numpy(), torch.sin(ang).cpu().numpy()
+    trig = np.array([c[0], s[0], c[1], c[1], c[1], s[1], s[1], s[1]], np.float32)
+    pts, dist, counts = osamp.oracle_sample(osamp.to_struct(cg), perm.cpu().numpy(), start, R, S, angle, maxd, True,
+                                            jitter.cpu().numpy(), det_off.cpu().numpy(), trig=trig)
+    levels, _ = ohg.layout(4, 16, enc.log2_hashmap_size, float(enc.base_resolution), float(enc.per_level_scale),
+                           float(enc.base_resolution_t))
+    meas = proj.cpu().numpy()[perm.cpu().numpy()[start:start + R]]
+    yo, Lo, gto, gmo = ohg.train_step(pts, counts, dist, meas, m.grid_table.detach().cpu(), m.mlp.detach().cpu(),
+                                      levels, enc.log2_hashmap_size, 64, 64, 3, geo.max_distance_traveled, t=t)
+    return (y.cpu().double(), float(L), tg.cpu().double(), mg.cpu().double()), (yo, float(Lo), gto, gmo)
+
+
+def rel_max(a, b):
+    return float((a - b).abs().max() / b.abs().max().clamp(min=1e-30))
+
+
+def cosine(a, b):
+    a, b = a.flatten(), b.flatten()
+    return float((a @ b) / (a.norm() * b.norm()).clamp(min=1e-30))
+
+
+def test_plain_step_matches_oracle(cuda_device):
+    (y, L, gt, gm), (yo, Lo, gto, gmo) = run_case("plain_fp32")
+    assert (y != 0).sum() > 100
+    assert rel_max(y, yo) < 1e-4
+    assert abs(L - Lo) <= 1e-4 * abs(Lo)
+    assert rel_max(gm, gmo) < 1e-3, rel_max(gm, gmo)
+    assert rel_max(gt, gto) < 1e-3, rel_max(gt, gto)
+
+
+def test_mixed_step_matches_oracle(cuda_device):
+    (y, L, gt, gm), (yo, Lo, gto, gmo) = run_case("mixed")
+    assert rel_max(y, yo) < 2e-2, rel_max(y, yo)
+    assert abs(L - Lo) <= 5e-2 * abs(Lo)
+    assert cosine(gm, gmo) > 0.99 and cosine(gt, gto) > 0.99, (cosine(gm, gmo), cosine(gt, gto))
+    assert rel_max(gm, gmo) < 5e-2 and rel_max(gt, gto) < 5e-2, (rel_max(gm, gmo), rel_max(gt, gto))
+
+
+@pytest.mark.parametrize("duplicates", [False, True])
+def test_mixed_staged_and_fused_agree(cuda_device, duplicates):
+    from nect_b200.trainer import Workspace
+
+    (y1, L1, gt1, gm1), _ = run_case("mixed", Workspace(staging=True), duplicates)
+    (y2, L2, gt2, gm2), _ = run_case("mixed", Workspace(staging=False), duplicates)
+    assert torch.equal(y1, y2)
+    assert rel_max(gt1, gt2) < 1e-5 and rel_max(gm1, gm2) < 1e-5

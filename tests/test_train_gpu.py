@@ -194,3 +194,42 @@ def test_batch_with_repeated_pixels(cuda_device, precision):
     tol = 1e-4 if precision == "plain_fp32" else 2e-2
     assert rel_max(y, yo) < tol
     assert cosine(gt, gto) > 0.99
+
+
+@pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
+def test_edge_batches(cuda_device, precision):
+    """Empty batch; a batch whose rays all miss the object (detector shifted
+    off the volume: no samples, y_pred 0, loss from the measured values only,
+    no gradient); one sample per ray."""
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import RayBatch, Workspace, train_step
+
+    m, enc = make_model(3, precision=precision)
+    P = 32 * 32
+    perm = torch.randperm(P, device="cuda")
+    proj = torch.rand(P, device="cuda")
+
+    def step(geo, R, S):
+        batch = RayBatch(perm=perm, start=0, num_rays=R, points_per_ray=S, angle=0.3,
+                         max_ray_distance_per_point=geo.max_distance_traveled / S,
+                         jitter=torch.zeros(max(R, 1), device="cuda"),
+                         detector_offset=torch.zeros(max(R, 1), 2, device="cuda"), projection=proj)
+        tg, mg = torch.zeros_like(m.table), torch.zeros_like(m.mlp)
+        L, y = train_step(m, geo.get_c_geometry(), batch, geo.max_distance_traveled, tg, mg, Workspace(), "l2")
+        torch.cuda.synchronize()
+        return float(L), y, tg, mg
+
+    geo = Geometry(nDetector=[32, 32], dDetector=[1 / 32, 1 / 32], mode="parallel", nVoxel=[32] * 3,
+                   dVoxel=[1 / 32] * 3)
+    L, y, tg, mg = step(geo, 0, 16)
+    assert L == 0.0 and y.numel() == 0 and not tg.any() and not mg.any()
+
+    off = Geometry(nDetector=[32, 32], dDetector=[1 / 32, 1 / 32], mode="parallel", nVoxel=[32] * 3,
+                   dVoxel=[1 / 32] * 3, offDetector=(5.0, 5.0))
+    L, y, tg, mg = step(off, 300, 16)
+    meas = proj[perm[:300]]
+    assert not y.any() and not tg.any() and not mg.any()
+    assert abs(L - float((meas * meas).mean())) <= 1e-6 * float((meas * meas).mean())
+
+    L, y, tg, mg = step(geo, 300, 1)
+    assert math.isfinite(L) and (y != 0).sum() > 100 and tg.abs().sum() > 0
