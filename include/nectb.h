@@ -251,12 +251,13 @@ size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHas
                                    const NectbMLP* mlp, int32_t num_rays);
 
 /* Recommended staging bytes for the mixed path's two-pass backward, to add to
- * nectb_train_workspace_bytes(): with them the backward runs in 8 rounds of
- * scheduling indices (detector pixels, or batch positions when the batch
- * repeats a pixel); each round's tensor-core pass writes dL/d(encoding) of its
- * samples (fp32, num_points_per_ray * n_levels * n_features per index) and
- * scatter passes over level groups apply it to grid_grad with the gradient
- * slice of each group resident in L2.  The recommendation is capped at 4 GiB.
+ * nectb_train_workspace_bytes(): the rays with samples are listed in
+ * scheduling order (detector pixels, or batch positions when the batch
+ * repeats a pixel) and the backward runs in 8 rounds of equal ray counts;
+ * each round's tensor-core pass writes dL/d(encoding) of its samples (fp32,
+ * num_points_per_ray * n_levels * n_features per ray) and scatter passes over
+ * level groups apply it to grid_grad with the gradient slice of each group
+ * resident in L2.  The recommendation is capped at 16 GiB (plus the ray list).
  * Less staging gives more rounds; when it would take more than 64 rounds the
  * single-pass backward (scatter inside the tensor-core kernel) runs instead.  Returns 0 for the plain fp32 path, which does not
  * stage.  No reference counterpart. */
@@ -342,7 +343,8 @@ int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq
 /* Per-kernel timing of the library's own launches with CUDA events recorded
  * on the launch stream around each kernel (off by default).  Slots:
  * 0 ray preparation, 1 forward, 2 backward, 3 Adam, 4 sampling, 5 model
- * forward and queries, 6 staged gradient scatter.  nectb_profile_collect waits for the recorded events, adds their
+ * forward and queries, 6 staged gradient scatter, 7 ray ordering of the
+ * staged backward (three launches timed as one).  nectb_profile_collect waits for the recorded events, adds their
  * durations and returns per slot the launch count and total milliseconds.
  * No counterpart in the reference, which has no profiler. */
 #define NECTB_PROFILE_SLOTS 8

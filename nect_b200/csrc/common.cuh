@@ -48,7 +48,8 @@ enum {
   kProfAdam = 3,
   kProfSample = 4,
   kProfModel = 5,
-  kProfScatter = 6
+  kProfScatter = 6,
+  kProfOrder = 7
 };
 class ProfScope {
  public:

@@ -2,6 +2,7 @@
 // training kernels: per-ray records, the ray-preparation kernel, the ray
 // scheduler, sample regeneration and the workspace layout.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 
 #include "common.cuh"
@@ -52,7 +53,14 @@ enum : unsigned int { kFlagDuplicatePixels = 1u };
 // buffer may need before the fused single-pass backward is used instead.
 constexpr int kStagedRounds = 8;
 constexpr int kMaxStagedRounds = 64;
-constexpr size_t kStagingCap = size_t(4) << 30;  // largest staging buffer recommended
+constexpr size_t kStagingCap = size_t(16) << 30;  // largest staging buffer recommended
+constexpr int kOrderBlock = 1024;                  // threads of the ray-order kernels
+
+// Bytes at the front of the staging region for the ray order and its block sums.
+inline size_t order_bytes(int R, int P) {
+  const size_t n_blocks = (size_t)(std::max(R, P) + kOrderBlock - 1) / kOrderBlock;
+  return (((size_t)R * 4 + 255) & ~size_t(255)) + (((n_blocks + 1) * 4 + 255) & ~size_t(255));
+}
 
 // Workspace: RayRec[R] | slot[P] (int32: batch index of the ray through each
 // detector pixel, -1 if none) | 64-byte control block (scheduling cursors of
@@ -128,6 +136,31 @@ __device__ __forceinline__ int next_ray(unsigned int* cursor, const int32_t* __r
       if (recs[idx].count > 0) return (int)idx;
     }
   }
+}
+
+// The rays with samples in scheduling order, for the two-pass backward's
+// rounds of equal ray counts: order[rank] = ray, ranks 0..ctrl[6]-1.  Three
+// launches over the scheduling indices (pixels, or batch positions when the
+// batch repeats a pixel): per-block counts, one block scanning them, and the
+// per-block compaction, so pixel order is kept.
+__global__ void order_count_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
+                                   const unsigned int* __restrict__ ctrl, int R, int P,
+                                   unsigned int* __restrict__ block_sums);
+__global__ void order_scan_kernel(unsigned int* __restrict__ block_sums, int n_blocks, unsigned int* __restrict__ ctrl);
+__global__ void order_compact_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
+                                     const unsigned int* __restrict__ ctrl, int R, int P,
+                                     const unsigned int* __restrict__ block_sums, int32_t* __restrict__ order);
+
+// Scheduler over ranks [lo, hi) of the ordered rays (one round); the rank of
+// the returned ray is written to *sched.  Returns -1 when none are left.
+__device__ __forceinline__ int next_ray_ranked(unsigned int* cursor, const int32_t* __restrict__ order,
+                                               unsigned int n_valid, int lo, int hi, int lane, int* sched) {
+  unsigned int idx = 0;
+  if (lane == 0) idx = (unsigned)lo + atomicAdd(cursor, 1u);
+  idx = __shfl_sync(0xffffffffu, idx, 0);
+  if (idx >= min((unsigned)hi, n_valid)) return -1;
+  *sched = (int)idx;
+  return order[idx];
 }
 
 // Loss gradient dL/dy_pred for one ray (mean over rays, nect/config.py:481-497),

@@ -134,12 +134,16 @@ struct RayCursor {
 // Advances the warp to its next chunk of 32 samples (a new ray from the
 // scheduler when the current one is done).  Returns false when no rays are
 // left.  Rays without samples were finalised by the preparation kernel.
+// With ``order`` the rays come from the ordered list, ranks [lo, hi) (one
+// round of the two-pass backward), else from the scheduling indices [lo, hi).
 __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* cursor,
                                            const int32_t* slot, const TrainArgs& a, bool by_pixel, int lane,
-                                           int lo = 0, int hi = 0x7fffffff) {
+                                           int lo = 0, int hi = 0x7fffffff, const int32_t* order = nullptr,
+                                           unsigned int n_valid = 0) {
   if (cur.ray >= a.num_rays) return false;
   if (cur.ray >= 0 && cur.base < cur.rec.count) return true;
-  const int r = next_ray(cursor, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane, lo, hi, &cur.sched);
+  const int r = order ? next_ray_ranked(cursor, order, n_valid, lo, hi, lane, &cur.sched)
+                      : next_ray(cursor, slot, recs, a.num_rays, a.n_pixels, by_pixel, lane, lo, hi, &cur.sched);
   if (r < 0) {
     cur.ray = a.num_rays;
     cur.rec.count = 0;
@@ -292,10 +296,11 @@ __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
-                 float* __restrict__ stage, int64_t slots) {
+                 float* __restrict__ stage, int64_t slots, const int32_t* __restrict__ order) {
   constexpr int IN = 16 * F;
   static_assert(IN <= 64 && H >= 2 && H <= 3, "TMEM plan: 64 transient + (H - 1) x 64 + IN columns <= 256");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  const unsigned int n_valid = order ? ctrl[6] : 0u;
   unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
@@ -359,7 +364,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     return true;
   };
   while (true) {
-    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi);
+    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi, order, n_valid);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
@@ -537,11 +542,12 @@ template <int D, int F>
 __global__ void __launch_bounds__(kScatterThreads)
 scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs, const int32_t* __restrict__ slot,
                      unsigned int* __restrict__ ctrl, const float* __restrict__ stage, int64_t slots, int lo, int hi,
-                     int l0, int l1, float* __restrict__ table_grad) {
+                     int l0, int l1, float* __restrict__ table_grad, const int32_t* __restrict__ order) {
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  const unsigned int n_valid = ctrl[6];
   const int lane = threadIdx.x & 31;
   RayCursor cur;
-  while (next_chunk(cur, recs, ctrl + 5, slot, a, by_pixel, lane, lo, hi)) {
+  while (next_chunk(cur, recs, ctrl + 5, slot, a, by_pixel, lane, lo, hi, order, n_valid)) {
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
@@ -588,19 +594,35 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
       std::max<size_t>(1024 + H * kWTile + (H + 1) * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
   constexpr int IN = 16 * F;
   const int64_t per_index = (int64_t)a.S * IN * (int64_t)sizeof(float);
-  const int64_t N = std::max(a.num_rays, a.n_pixels);  // covers both scheduling orders
-  const int64_t per_round = ws.stage ? std::min<int64_t>((int64_t)(ws.stage_bytes / per_index), N) : 0;
-  if (per_round <= 0 || ceil_div(N, per_round) > kMaxStagedRounds) {
+  const int R = a.num_rays;
+  // staging region: ray order and its block sums, then dL/d(encoding) of one round of Q rays
+  const size_t ob = order_bytes(R, a.n_pixels);
+  const int64_t per_round =
+      ws.stage && ws.stage_bytes > ob ? std::min<int64_t>((int64_t)((ws.stage_bytes - ob) / per_index), R) : 0;
+  if (per_round <= 0 || ceil_div(R, per_round) > kMaxStagedRounds) {
     // fused single pass: the backward scatters its own gradients
     auto k = bwd_mixed_kernel<D, F, H, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
     k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                         W_grad, 0, 0x7fffffff, nullptr, 0);
+                                         W_grad, 0, 0x7fffffff, nullptr, 0, nullptr);
     return launch_status("bwd_mixed_kernel");
   }
-  // two passes per round of scheduling indices: the tensor-core backward
-  // stages dL/d(encoding), then one scatter pass per level group
+  int32_t* order = reinterpret_cast<int32_t*>(ws.stage);
+  unsigned int* block_sums = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(ws.stage) +
+                                                             (((size_t)R * 4 + 255) & ~size_t(255)));
+  float* stage = reinterpret_cast<float*>(reinterpret_cast<char*>(ws.stage) + ob);
+  {
+    ProfScope ps(kProfOrder, s);
+    const int n_blocks = (int)ceil_div(std::max(R, a.n_pixels), kOrderBlock);
+    order_count_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, block_sums);
+    order_scan_kernel<<<1, kOrderBlock, 0, s>>>(block_sums, n_blocks, ws.counters);
+    order_compact_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, block_sums,
+                                                          order);
+    if (int rc = launch_status("order kernels")) return rc;
+  }
+  // two passes per round of Q ordered rays: the tensor-core backward stages
+  // dL/d(encoding), then one scatter pass per level group
   int group_start[NECTB_MAX_LEVELS + 1], n_groups = 0;
   {
     size_t acc = 0;
@@ -622,13 +644,13 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
   const int sblocks = sms * std::max(per_sm, 1);
   const int64_t slots = per_round * a.S;
-  for (int64_t lo = 0; lo < N; lo += per_round) {
-    const int hi = (int)std::min<int64_t>(N, lo + per_round);
+  for (int64_t lo = 0; lo < R; lo += per_round) {
+    const int hi = (int)std::min<int64_t>(R, lo + per_round);
     if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor")) return rc;
     {
       ProfScope ps(kProfBackward, s);
       kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                            W_grad, (int)lo, hi, ws.stage, slots);
+                                            W_grad, (int)lo, hi, stage, slots, order);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
@@ -636,8 +658,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
         return rc;
       {
         ProfScope ps(kProfScatter, s);
-        ks<<<sblocks, kScatterThreads, 0, s>>>(grid, a, ws.rays, ws.slot, ws.counters, ws.stage, slots, (int)lo, hi,
-                                               group_start[gi], group_start[gi + 1], table_grad);
+        ks<<<sblocks, kScatterThreads, 0, s>>>(grid, a, ws.rays, ws.slot, ws.counters, stage, slots, (int)lo, hi,
+                                               group_start[gi], group_start[gi + 1], table_grad, order);
       }
       if (int rc = launch_status("scatter_stage_kernel")) return rc;
     }
