@@ -359,6 +359,29 @@ int nectb_profile_collect(int32_t* launches, double* total_ms);
  * usable.  No reference counterpart. */
 int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, void* stream);
 
+/* Launch shapes and scheduling of the mixed training path, process-wide:
+ * blocks per SM of the forward (1..4) and of the tensor-core backward (1..2),
+ * of the gradient scatter (0 = as many as fit), the rounds the recommended
+ * staging is sized for (nectb_train_staging_bytes, 1..64), the largest fp32
+ * gradient slice one scatter pass covers, and the samples-per-cell
+ * thresholds above which runs of samples along a ray are merged before their
+ * reductions (3D and 4D grids).  Results do not depend on these beyond fp32
+ * reassociation; the Python autotuner (nect_b200.autotune) picks them per
+ * workload.  nectb_set_tuning validates and applies to steps issued after it
+ * returns; defaults: 4, 2, 0, 8, 48 MiB, 0.75, 1.5.  No reference
+ * counterpart. */
+typedef struct NectbTuning {
+  int32_t forward_blocks_per_sm;
+  int32_t backward_blocks_per_sm;
+  int32_t scatter_blocks_per_sm;
+  int32_t staged_rounds;
+  int64_t scatter_group_bytes;
+  float run_threshold_3d;
+  float run_threshold_4d;
+} NectbTuning;
+int nectb_get_tuning(NectbTuning* tuning);
+int nectb_set_tuning(const NectbTuning* tuning);
+
 /* Version string and last error message of the calling thread. */
 const char* nectb_version(void);
 const char* nectb_last_error(void);

@@ -93,6 +93,18 @@ class NectbTrainBatch(ctypes.Structure):
     ]
 
 
+class NectbTuning(ctypes.Structure):
+    _fields_ = [
+        ("forward_blocks_per_sm", c_int),
+        ("backward_blocks_per_sm", c_int),
+        ("scatter_blocks_per_sm", c_int),
+        ("staged_rounds", c_int),
+        ("scatter_group_bytes", c_i64),
+        ("run_threshold_3d", c_f32),
+        ("run_threshold_4d", c_f32),
+    ]
+
+
 # name -> (restype, argtypes)
 _SIGNATURES = {
     "nectb_version": (ctypes.c_char_p, []),
@@ -153,6 +165,8 @@ _SIGNATURES = {
     "nectb_train_staging_bytes": (
         c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int, c_int]),
     "nectb_selftest_bounded_wait": (c_int, [c_ptr, ctypes.c_uint32, c_ptr]),
+    "nectb_get_tuning": (c_int, [ctypes.POINTER(NectbTuning)]),
+    "nectb_set_tuning": (c_int, [ctypes.POINTER(NectbTuning)]),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
     "nectb_adam_step": (

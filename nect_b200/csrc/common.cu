@@ -97,3 +97,40 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
   }
   return NECTB_OK;
 }
+
+namespace nectb {
+namespace {
+std::mutex g_tuning_mu;
+NectbTuning g_tuning = {4, 2, 0, 8, int64_t(48) << 20, 0.75f, 1.5f};
+}  // namespace
+
+NectbTuning current_tuning() {
+  std::lock_guard<std::mutex> lk(g_tuning_mu);
+  return g_tuning;
+}
+}  // namespace nectb
+
+extern "C" int nectb_get_tuning(NectbTuning* tuning) {
+  using namespace nectb;
+  clear_error();
+  NECTB_REQUIRE(tuning, "null tuning");
+  *tuning = current_tuning();
+  return NECTB_OK;
+}
+
+extern "C" int nectb_set_tuning(const NectbTuning* t) {
+  using namespace nectb;
+  clear_error();
+  NECTB_REQUIRE(t, "null tuning");
+  NECTB_REQUIRE(t->forward_blocks_per_sm >= 1 && t->forward_blocks_per_sm <= 4, "forward_blocks_per_sm must be 1..4");
+  NECTB_REQUIRE(t->backward_blocks_per_sm >= 1 && t->backward_blocks_per_sm <= 2, "backward_blocks_per_sm must be 1..2");
+  NECTB_REQUIRE(t->scatter_blocks_per_sm >= 0 && t->scatter_blocks_per_sm <= 8, "scatter_blocks_per_sm must be 0..8");
+  NECTB_REQUIRE(t->staged_rounds >= 1 && t->staged_rounds <= 64, "staged_rounds must be 1..64");
+  NECTB_REQUIRE(t->scatter_group_bytes >= (int64_t(1) << 20), "scatter_group_bytes must be at least 1 MiB");
+  NECTB_REQUIRE(t->run_threshold_3d >= 0.f && t->run_threshold_3d <= 64.f && t->run_threshold_4d >= 0.f &&
+                    t->run_threshold_4d <= 64.f,
+                "run thresholds must be in [0, 64]");
+  std::lock_guard<std::mutex> lk(g_tuning_mu);
+  g_tuning = *t;
+  return NECTB_OK;
+}

@@ -24,6 +24,9 @@ inline int launch_status(const char* what) { return cuda_status(cudaGetLastError
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// The current launch shapes and scheduling (nectb_set_tuning), copied under a lock.
+NectbTuning current_tuning();
+
 // Sets a kernel's dynamic shared memory and its L1/shared split.  An SM keeps
 // one split while any block is resident, so a kernel that shares SMs with
 // other launches (a capped background grid, serving queries) asks for a split

@@ -196,18 +196,17 @@ __device__ __forceinline__ void scatter_point(const GridDev& g, float* __restric
 
 // Levels on which the 32 consecutive samples a warp holds of one ray share
 // cells: expected samples per cell = 1 / (res * (|dx| + |dy| + |dz|)) in
-// normalised coordinates.  Bit l is set when that exceeds ~1.3 samples in 3D
-// and ~0.7 in 4D, where merging a run costs half the shuffles (separable time
-// weights).  Measured on the 512^2 cone workloads: thresholds 0.25 / 0.5 /
-// 0.75 / 1.0 / 1.5 give 1.98 / 1.87 / 1.89 / 1.92 / 1.94 ms (3D) and
-// 1.72 / 1.52 / 1.45 / 1.40 / 1.39 ms (4D) per scatter pass.
-template <int D>
-__device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, double dy, double dz) {
-  constexpr float kThreshold = D == 4 ? 1.5f : 0.75f;
+// normalised coordinates.  Bit l is set when res * (|dx| + |dy| + |dz|) is
+// below the threshold.  Defaults (NectbTuning): 0.75 (3D), 1.5 (4D, where
+// merging a run costs half the shuffles: separable time weights).  Measured
+// on the 512^2 cone workloads: 0.25 / 0.5 / 0.75 / 1.0 / 1.5 give 1.98 / 1.87 /
+// 1.89 / 1.92 / 1.94 ms (3D) and 1.72 / 1.52 / 1.45 / 1.40 / 1.39 ms (4D) per
+// scatter pass.
+__device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, double dy, double dz, float threshold) {
   const float cross = (float)(fabs(dx) + fabs(dy) + fabs(dz));
   uint32_t m = 0;
   for (int l = 0; l < g.n_levels; ++l)
-    if ((float)g.res[l][0] * cross < kThreshold) m |= 1u << l;
+    if ((float)g.res[l][0] * cross < threshold) m |= 1u << l;
   return m;
 }
 

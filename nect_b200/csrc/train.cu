@@ -190,7 +190,7 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0) return 0;
   if (mlp->compute_dtype == NECTB_F32) return 0;  // the plain path scatters in its backward
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
-  const int64_t per_round = ceil_div(num_rays, kStagedRounds);
+  const int64_t per_round = ceil_div(num_rays, current_tuning().staged_rounds);
   const size_t per_ray = (size_t)num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
   return order_bytes(num_rays, P) + std::min((size_t)per_round * per_ray, kStagingCap / per_ray * per_ray);
 }

@@ -44,14 +44,14 @@ struct TrainArgs {
   float loss_scale;
   int max_blocks;  // > 0: cap on the persistent grids (queries); 0: default
   int phase = kPhaseForward | kPhaseBackward;  // which half of the step to run
+  float run_threshold = 0.75f;                 // run merging of the scatter (set from the tuning)
 };
 
 enum : unsigned int { kFlagDuplicatePixels = 1u };
 
-// The two-pass mixed backward: rounds the recommended staging buffer is sized
-// for (nectb_train_staging_bytes), and the most rounds a smaller staging
-// buffer may need before the fused single-pass backward is used instead.
-constexpr int kStagedRounds = 8;
+// The two-pass mixed backward: the most rounds a staging buffer may need
+// before the fused single-pass backward is used instead (the recommended
+// staging is sized for NectbTuning::staged_rounds, 8 by default).
 constexpr int kMaxStagedRounds = 64;
 constexpr size_t kStagingCap = size_t(16) << 30;  // largest staging buffer recommended
 constexpr int kOrderBlock = 1024;                  // threads of the ray-order kernels

@@ -482,8 +482,8 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         }
       }
     } else {
-      scatter_warp<D, F>(grid, table_grad, p, valid, dx, F, 1,
-                         active ? run_levels<D>(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz) : 0u, 0, grid.n_levels);
+      const uint32_t agg = active ? run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz, a.run_threshold) : 0u;
+      scatter_warp<D, F>(grid, table_grad, p, valid, dx, F, 1, agg, 0, grid.n_levels);
     }
     tc::fence_before();
     __syncthreads();
@@ -555,25 +555,28 @@ scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs,
     if (D == 4) p[3] = a.t;
     const float* dsrc = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
     scatter_warp<D, F>(grid, table_grad, p, valid, dsrc, slots * F, 1,
-                       run_levels<D>(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz), l0, l1);
+                       run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz, a.run_threshold), l0, l1);
     cur.base += 32;
   }
 }
 
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
-// slices add up to at most kScatterGroupBytes.
-constexpr size_t kScatterGroupBytes = size_t(48) << 20;
-
+// slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
 template <int D, int F, int H>
-int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W, const TrainArgs& a,
-              Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
-              cudaStream_t s) {
+int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W,
+              const TrainArgs& args, Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred,
+              float* loss, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   (void)geo;
-  int fblocks = std::max(1, std::min<int>(kFwdBlocksPerSM * sms, (int)ceil_div(a.num_rays, 4)));
-  int blocks = std::max(1, std::min<int>(2 * sms, (int)ceil_div(a.num_rays, 4)));
+  const NectbTuning tune = current_tuning();
+  TrainArgs a = args;
+  a.run_threshold = D == 4 ? tune.run_threshold_4d : tune.run_threshold_3d;
+  const size_t group_bytes = (size_t)tune.scatter_group_bytes;
+  int fblocks = std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
+                                          (int)ceil_div(a.num_rays, 4)));
+  int blocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if (a.max_blocks > 0) {
     fblocks = std::min(fblocks, a.max_blocks);
     blocks = std::min(blocks, a.max_blocks);
@@ -629,7 +632,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     for (int l = 0; l < grid.n_levels; ++l) {
       const int64_t next = l + 1 < grid.n_levels ? grid.offset[l + 1] : grid.total_entries;
       const size_t bytes = (size_t)(next - grid.offset[l]) * F * sizeof(float);
-      if (l == 0 || acc + bytes > kScatterGroupBytes) {
+      if (l == 0 || acc + bytes > group_bytes) {
         group_start[n_groups++] = l;
         acc = 0;
       }
@@ -642,6 +645,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
+  if (tune.scatter_blocks_per_sm > 0) per_sm = std::min(per_sm, tune.scatter_blocks_per_sm);
   const int sblocks = sms * std::max(per_sm, 1);
   const int64_t slots = per_round * a.S;
   for (int64_t lo = 0; lo < R; lo += per_round) {

@@ -1,0 +1,20 @@
+"""The process-wide tuning interface (CPU): round trip and validation."""
+import pytest
+
+
+def test_tuning_round_trip_and_validation():
+    from nect_b200 import autotune
+
+    before = autotune.get_tuning()
+    try:
+        assert before["forward_blocks_per_sm"] == 4 and before["staged_rounds"] == 8
+        autotune.set_tuning({"staged_rounds": 16, "run_threshold_3d": 0.5, "scatter_group_bytes": 8 << 20})
+        now = autotune.get_tuning()
+        assert now["staged_rounds"] == 16 and now["run_threshold_3d"] == 0.5 and now["scatter_group_bytes"] == 8 << 20
+        for bad in ({"forward_blocks_per_sm": 0}, {"backward_blocks_per_sm": 3}, {"staged_rounds": 65},
+                    {"scatter_group_bytes": 1000}, {"run_threshold_4d": -1.0}):
+            with pytest.raises(RuntimeError):
+                autotune.set_tuning(bad)
+        assert autotune.get_tuning() == now   # a rejected setting changes nothing
+    finally:
+        autotune.set_tuning(before)
