@@ -253,7 +253,8 @@ size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHas
 /* Recommended staging bytes for the mixed path's two-pass backward, to add to
  * nectb_train_workspace_bytes(): the rays with samples are listed in
  * scheduling order (detector pixels, or batch positions when the batch
- * repeats a pixel) and the backward runs in 8 rounds of equal ray counts;
+ * repeats a pixel) and the backward runs in rounds of equal ray counts
+ * (NectbTuning::staged_rounds, 4 by default);
  * each round's tensor-core pass writes dL/d(encoding) of its samples (fp32,
  * num_points_per_ray * n_levels * n_features per ray) and scatter passes over
  * level groups apply it to grid_grad with the gradient slice of each group
@@ -368,7 +369,7 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * reductions (3D and 4D grids).  Results do not depend on these beyond fp32
  * reassociation; the Python autotuner (nect_b200.autotune) picks them per
  * workload.  nectb_set_tuning validates and applies to steps issued after it
- * returns; defaults: 4, 2, 0, 8, 48 MiB, 0.75, 1.5.  No reference
+ * returns; defaults: 4, 2, 0, 4, 48 MiB, 1.0, 3.0.  No reference
  * counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;

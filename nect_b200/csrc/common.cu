@@ -101,7 +101,7 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
 namespace nectb {
 namespace {
 std::mutex g_tuning_mu;
-NectbTuning g_tuning = {4, 2, 0, 8, int64_t(48) << 20, 0.75f, 1.5f};
+NectbTuning g_tuning = {4, 2, 0, 4, int64_t(48) << 20, 1.0f, 3.0f};
 }  // namespace
 
 NectbTuning current_tuning() {

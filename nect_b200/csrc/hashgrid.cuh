@@ -197,11 +197,9 @@ __device__ __forceinline__ void scatter_point(const GridDev& g, float* __restric
 // Levels on which the 32 consecutive samples a warp holds of one ray share
 // cells: expected samples per cell = 1 / (res * (|dx| + |dy| + |dz|)) in
 // normalised coordinates.  Bit l is set when res * (|dx| + |dy| + |dz|) is
-// below the threshold.  Defaults (NectbTuning): 0.75 (3D), 1.5 (4D, where
-// merging a run costs half the shuffles: separable time weights).  Measured
-// on the 512^2 cone workloads: 0.25 / 0.5 / 0.75 / 1.0 / 1.5 give 1.98 / 1.87 /
-// 1.89 / 1.92 / 1.94 ms (3D) and 1.72 / 1.52 / 1.45 / 1.40 / 1.39 ms (4D) per
-// scatter pass.
+// below the threshold.  Defaults (NectbTuning): 1.0 (3D) and 3.0 (4D, where
+// merging a run costs half the shuffles: separable time weights), the values
+// the autotuner picked on the 512^2 cone workloads.
 __device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, double dy, double dz, float threshold) {
   const float cross = (float)(fabs(dx) + fabs(dy) + fabs(dz));
   uint32_t m = 0;

@@ -51,7 +51,7 @@ enum : unsigned int { kFlagDuplicatePixels = 1u };
 
 // The two-pass mixed backward: the most rounds a staging buffer may need
 // before the fused single-pass backward is used instead (the recommended
-// staging is sized for NectbTuning::staged_rounds, 8 by default).
+// staging is sized for NectbTuning::staged_rounds, 4 by default).
 constexpr int kMaxStagedRounds = 64;
 constexpr size_t kStagingCap = size_t(16) << 30;  // largest staging buffer recommended
 constexpr int kOrderBlock = 1024;                  // threads of the ray-order kernels
