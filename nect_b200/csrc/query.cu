@@ -75,7 +75,7 @@ __device__ __forceinline__ uint8_t* qalign1024(uint8_t* p) {
 // At most 128 registers so that three blocks share an SM under the 164 KB
 // shared split (a background block beside two slice blocks, or three blocks of
 // one query).
-template <int D, int F>
+template <int D, int F, int H>
 __global__ void __launch_bounds__(kQThreads, 4)
 query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W,
                    const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
@@ -83,10 +83,9 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
   constexpr int IN = 16 * F;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = qalign1024(smem_raw);
-  uint8_t* sW0 = base;
-  uint8_t* sW1 = sW0 + kQWTile;
-  uint8_t* sX = sW1 + kQWTile;
-  uint8_t* sA = sX + kQTile;
+  uint8_t* sW = base;                // H weight tiles
+  uint8_t* sX = sW + H * kQWTile;
+  uint8_t* sA = sX + kQTile;         // every hidden layer's activations in turn
   float* sWout = reinterpret_cast<float*>(sA + kQTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
@@ -100,16 +99,20 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
     float v[8];
 #pragma unroll
     for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
-    tc::st_chunk_bf16(sW0, o, j, v);
+    tc::st_chunk_bf16(sW, o, j, v);
   }
-  for (int e = t; e < 64 * 8; e += kQThreads) {
-    const int o = e / 8, j = e % 8;
-    float v[8];
+#pragma unroll 1
+  for (int k = 1; k < H; ++k) {
+    const float* Wk = W + 64 * IN + (k - 1) * 64 * 64;
+    for (int e = t; e < 64 * 8; e += kQThreads) {
+      const int o = e / 8, j = e % 8;
+      float v[8];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = W[64 * IN + o * 64 + 8 * j + q];
-    tc::st_chunk_bf16(sW1, o, j, v);
+      for (int q = 0; q < 8; ++q) v[q] = Wk[o * 64 + 8 * j + q];
+      tc::st_chunk_bf16(sW + k * kQWTile, o, j, v);
+    }
   }
-  for (int e = t; e < 64; e += kQThreads) sWout[e] = W[64 * IN + 64 * 64 + e];
+  for (int e = t; e < 64; e += kQThreads) sWout[e] = W[64 * IN + (H - 1) * 64 * 64 + e];
   if (warp == 0) {
     tc::tmem_alloc(tslot, 128);
     tc::tmem_relinquish();
@@ -121,8 +124,7 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
   tc::fence_after();
   const uint32_t tm = *tslot;
   const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
-  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA);
-  const uint32_t sW0_a = tc::smem_u32(sW0), sW1_a = tc::smem_u32(sW1);
+  const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
   constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
   uint32_t phase = 0;
   bool timed_out = false;
@@ -166,52 +168,48 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
         tc::st_chunk_bf16(sX, t, j, v);
       }
     }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
-      tc::fence_after();
-#pragma unroll
-      for (int k = 0; k < IN / 16; ++k) tc::mma(tm, tc::desc_k(sX_a, k), tc::desc_k(sW0_a, k), idesc, k > 0);
-      tc::commit(bar);
-    }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
+    // layer k writes TMEM columns 64 * (k & 1); its input is X for k = 0, else
+    // the previous layer's activations in sA (written once the MMA that read
+    // sA before has completed)
     float h[64];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) tc::tmem_ld16(my_lanes + 16 * c, h + 16 * c);
-    tc::tmem_wait_ld();
+    for (int k = 0; k < H; ++k) {
+      if (k > 0) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      float v[8];
+        for (int j = 0; j < 8; ++j) {
+          float v[8];
 #pragma unroll
-      for (int qq = 0; qq < 8; ++qq) v[qq] = fmaxf(h[8 * j + qq], 0.f);
-      tc::st_chunk_bf16(sA, t, j, v);
-    }
-    tc::fence_async_smem();
-    tc::fence_before();
-    __syncthreads();
-    if (t == 0) {
+          for (int qq = 0; qq < 8; ++qq) v[qq] = fmaxf(h[8 * j + qq], 0.f);
+          tc::st_chunk_bf16(sA, t, j, v);
+        }
+      }
+      tc::fence_async_smem();
+      tc::fence_before();
+      __syncthreads();
+      if (t == 0) {
+        tc::fence_after();
+        if (k == 0) {
+#pragma unroll
+          for (int c = 0; c < IN / 16; ++c) tc::mma(tm, tc::desc_k(sX_a, c), tc::desc_k(sW_a, c), idesc, c > 0);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, c), tc::desc_k(sW_a + k * kQWTile, c), idesc, c > 0);
+        }
+        tc::commit(bar);
+      }
+      timed_out = !tc::mbar_wait(bar, phase);
+      phase ^= 1;
+      if (__syncthreads_or(timed_out)) {
+        timed_out = true;
+        break;
+      }
       tc::fence_after();
 #pragma unroll
-      for (int k = 0; k < 4; ++k) tc::mma(tm + 64, tc::desc_k(sA_a, k), tc::desc_k(sW1_a, k), idesc, k > 0);
-      tc::commit(bar);
+      for (int c = 0; c < 4; ++c) tc::tmem_ld16(my_lanes + 64 * (k & 1) + 16 * c, h + 16 * c);
+      tc::tmem_wait_ld();
     }
-    timed_out = !tc::mbar_wait(bar, phase);
-    phase ^= 1;
-    if (__syncthreads_or(timed_out)) {
-      timed_out = true;
-      break;
-    }
-    tc::fence_after();
-#pragma unroll
-    for (int c = 0; c < 4; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, h + 16 * c);
-    tc::tmem_wait_ld();
+    if (timed_out) break;
     float z = 0.f;
 #pragma unroll
     for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
@@ -282,11 +280,11 @@ int sm_count() {
   return sms;
 }
 
-template <int D, int F>
+template <int D, int F, int H>
 int launch_query_mixed(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
                        int64_t chunks, unsigned int* counter, int oact, int max_blocks, cudaStream_t s) {
-  auto k = query_mixed_kernel<D, F>;
-  const size_t smem = 1024 + 2 * kQWTile + 2 * kQTile + 64 * 4 + 64;
+  auto k = query_mixed_kernel<D, F, H>;
+  const size_t smem = 1024 + H * kQWTile + 2 * kQTile + 64 * 4 + 64;
   set_smem(k, smem, true);
   int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 3 * sm_count()));
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
@@ -334,13 +332,16 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
   const bool mixed = mlp->compute_dtype != NECTB_F32;
   if (mixed) {
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
-    NECTB_REQUIRE(H == 2 && mlp->activation == NECTB_ACT_RELU, "mixed queries need 2 hidden ReLU layers");
-    if (D == 3 && F == 2)
-      return launch_query_mixed<3, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                      mlp->output_activation, max_blocks, s);
-    if (D == 4 && F == 2)
-      return launch_query_mixed<4, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                      mlp->output_activation, max_blocks, s);
+    NECTB_REQUIRE(mlp->activation == NECTB_ACT_RELU, "mixed queries need ReLU hidden layers");
+    if (D == 3 && F == 2 && H == 2)
+      return launch_query_mixed<3, 2, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                         mlp->output_activation, max_blocks, s);
+    if (D == 4 && F == 2 && H == 2)
+      return launch_query_mixed<4, 2, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                         mlp->output_activation, max_blocks, s);
+    if (D == 4 && F == 4 && H == 3)
+      return launch_query_mixed<4, 4, 3>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                         mlp->output_activation, max_blocks, s);
   } else {
     const int act = mlp->activation, oact = mlp->output_activation;
     const bool h = grid->feature_dtype == NECTB_F16;
@@ -354,6 +355,9 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
                                                      counter, act, oact, max_blocks, s)
                : launch_query_plain<4, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
                                                     counter, act, oact, max_blocks, s);
+    if (D == 4 && F == 4 && H == 3 && !h)
+      return launch_query_plain<4, 4, float, 3>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                                act, oact, max_blocks, s);
   }
   return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, hidden %d)", D,
                    F, H);

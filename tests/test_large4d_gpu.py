@@ -100,3 +100,42 @@ def test_mixed_staged_and_fused_agree(cuda_device, duplicates):
     (y2, L2, gt2, gm2), _ = run_case("mixed", Workspace(staging=False), duplicates)
     assert torch.equal(y1, y2)
     assert rel_max(gt1, gt2) < 1e-5 and rel_max(gm1, gm2) < 1e-5
+
+
+@pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
+def test_queries_and_model_forward_match_oracle(cuda_device, precision):
+    """Slices through nectb_query_points and the module forward of the
+    16 x 4 / 3-layer model against the fp64 oracle (1e-5 plain; 2e-2 mixed,
+    whose query MLP runs in bf16 on the tensor cores)."""
+    from nect_b200.serving import query_points, slice_items
+
+    m, enc = make_model(precision)
+    levels, _ = ohg.layout(4, 16, enc.log2_hashmap_size, float(enc.base_resolution), float(enc.per_level_scale),
+                           float(enc.base_resolution_t))
+    Ws = ohg.split_mlp_params(m.mlp.detach().cpu().double(), 64, 64, 3)
+    table = m.grid_table.detach().cpu().double()
+    t = 0.55
+    out = torch.empty(48, 40, device="cuda")
+    query_points(m, slice_items(out, out.shape, t, centre=(0.45, 0.5, 0.55), u=(0.2, 0.3, 0.9), v=(0.0, 1.0, -0.3)))
+    g = torch.Generator(device="cpu").manual_seed(2)
+    x = torch.rand(2000, 3, generator=g)
+    sig = m(x.cuda(), t).squeeze(-1).cpu().double()
+    torch.cuda.synchronize()
+    ref = ohg.mlp(ohg.encode(torch.cat([x, torch.full((2000, 1), t)], 1), table, levels, enc.log2_hashmap_size),
+                  Ws).squeeze(-1)
+    assert rel_max(sig, ref) < 1e-5   # the module forward is fp32 SIMT for both table precisions
+    # oracle of the slice: the same points as slice_items generates them (cell centres of the plane)
+    import numpy as np
+
+    items = slice_items(0, (48, 40), t, centre=(0.45, 0.5, 0.55), u=(0.2, 0.3, 0.9), v=(0.0, 1.0, -0.3))
+    pts = []
+    for it in items:
+        i, j = np.meshgrid(np.arange(it["nu"]), np.arange(it["nv"]), indexing="xy")
+        p = (it["origin"][None, None, :].astype(np.float32) + i[..., None].astype(np.float32) * it["du"]
+             + j[..., None].astype(np.float32) * it["dv"])
+        pts.append(np.clip(p.reshape(-1, 3), 0, 1))
+    xs = torch.from_numpy(np.concatenate(pts)).float()
+    ref_s = ohg.mlp(ohg.encode(torch.cat([xs, torch.full((xs.shape[0], 1), t)], 1), table, levels,
+                               enc.log2_hashmap_size), Ws).squeeze(-1)
+    got = out.cpu().double().flatten()
+    assert rel_max(got, ref_s) < (1e-5 if precision == "plain_fp32" else 2e-2), rel_max(got, ref_s)

@@ -118,7 +118,7 @@ def test_continuous_scan_step_matches_oracle(cuda_device, n_dims, precision):
     y, gt, gm = y.detach().cpu().double(), gt.cpu().double(), gm.cpu().double()
     if precision == "plain_fp32":
         assert rel_max(y, yo) < 1e-4
-        assert abs(float(L) - float(Lo)) <= 1e-4 * abs(float(Lo))
+        assert abs(float(L.detach()) - float(Lo)) <= 1e-4 * abs(float(Lo))
         assert rel_max(gt, gto) < 1e-3, rel_max(gt, gto)
         assert rel_max(gm, gmo) < 1e-3, rel_max(gm, gmo)
     else:
