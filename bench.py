@@ -408,13 +408,13 @@ def main():
     peak = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
     achieved = per_launch_bytes.get(dominant, 0.0) / (kernel_ms[dominant] / 1e3) / 1e9 if dominant in kernel_ms else None
-    traffic = None   # DRAM bytes per launch of the dominant kernel from the committed ncu capture
-    tfile = ROOT / "profiles" / "traffic_per_launch.txt"
+    traffic = None   # DRAM bytes per launch of the dominant kernel: the committed ncu capture's bytes per step
+    tfile = ROOT / "profiles" / "dram_bytes_per_step.txt"   # divided by this run's launches per step
     if tfile.exists():
         for line in tfile.read_text().splitlines():
             f = line.split()
             if len(f) == 4 and not line.startswith("#") and f[:3] == [args.workload, args.precision, dominant]:
-                traffic = float(f[3])
+                traffic = float(f[3]) / max(launches_per_step.get(dominant, 1.0), 1.0)
 
     # ---- end to end through the public API, host buffers (pinned projection in, loss out)
     host = projs.cpu().pin_memory()
