@@ -390,10 +390,14 @@ def main():
     n_params = model.table.numel() + model.mlp.numel()
     staged = "scatter" in prof   # the mixed backward ran as tensor-core pass + staged scatter passes
     stage_io = enc.n_levels * enc.n_features_per_level * 4   # staged dL/d(encoding) per sample, each way
+    row = enc.n_levels * enc.n_features_per_level * 2        # stored bf16 encoding row per sample
+    stored = 0.0   # share of samples whose rows the forward stores (recommended workspace: min(R*S, 48 GiB) rows)
+    if staged:
+        stored = min(1.0, min(rays_per_step * S, (48 << 30) // row) / max(n_valid / args.steps, 1.0))
     step_bytes = {   # algorithmic bytes per step of each kernel kind
-        "backward": n_valid / args.steps * (gather + (stage_io if staged else scatter)),
+        "backward": n_valid / args.steps * (stored * row + (1 - stored) * gather + (stage_io if staged else scatter)),
         "scatter": n_valid / args.steps * (scatter + stage_io),
-        "forward": n_valid / args.steps * gather,
+        "forward": n_valid / args.steps * (gather + stored * row),
         "adam": n_params * (34 if args.precision == "mixed" else 32),
         "ray_prep": rays_per_step * 64.0,
     }
@@ -461,7 +465,8 @@ def main():
         "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
                      "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes.get(dominant),
-                     "kernel_ms": kernel_ms, "launches_per_step": launches_per_step},
+                     "kernel_ms": kernel_ms, "launches_per_step": launches_per_step,
+                     "encoding_store_share": stored},
         "cpu_baseline": cpu_baseline,
         "e2e": e2e,
         "gpu_launches": gpu_launches,

@@ -119,12 +119,22 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// Writes 8 consecutive values (chunk j of row r) as bf16 into a swizzled tile.
-__device__ __forceinline__ void st_chunk_bf16(uint8_t* tile, int r, int j, const float* v) {
+// 8 values rounded to bf16 (round to nearest even), packed into 16 bytes.
+__device__ __forceinline__ uint4 pack_bf16x8(const float* v) {
   __nv_bfloat162 h[4];
 #pragma unroll
   for (int q = 0; q < 4; ++q) h[q] = __floats2bfloat162_rn(v[2 * q], v[2 * q + 1]);
-  *reinterpret_cast<uint4*>(tile + sw128(r, j)) = *reinterpret_cast<const uint4*>(h);
+  return *reinterpret_cast<const uint4*>(h);
+}
+
+// Stores 16 packed bytes as chunk j of row r of a swizzled tile.
+__device__ __forceinline__ void st_chunk_raw(uint8_t* tile, int r, int j, uint4 v) {
+  *reinterpret_cast<uint4*>(tile + sw128(r, j)) = v;
+}
+
+// Writes 8 consecutive values (chunk j of row r) as bf16 into a swizzled tile.
+__device__ __forceinline__ void st_chunk_bf16(uint8_t* tile, int r, int j, const float* v) {
+  st_chunk_raw(tile, r, j, pack_bf16x8(v));
 }
 
 }  // namespace tc

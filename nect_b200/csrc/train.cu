@@ -190,9 +190,14 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0) return 0;
   if (mlp->compute_dtype == NECTB_F32) return 0;  // the plain path scatters in its backward
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
-  const int64_t per_round = ceil_div(num_rays, current_tuning().staged_rounds);
   const size_t per_ray = (size_t)num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
-  return order_bytes(num_rays, P) + std::min((size_t)per_round * per_ray, kStagingCap / per_ray * per_ray);
+  // order and offsets, the staged rounds, and an encoding store for every
+  // sample slot of the batch (bf16 rows of n_levels x n_features), capped
+  const size_t row_bytes = (size_t)grid->n_levels * grid->n_features * 2;
+  const size_t rows = std::min<size_t>({(size_t)num_rays * num_points_per_ray, kEncodingStoreCap / row_bytes,
+                                        (size_t)0xffffffffu});
+  return order_bytes(num_rays, P) + staged_round_bytes(num_rays, current_tuning().staged_rounds, per_ray) + 256 +
+         align256(rows * row_bytes);
 }
 
 extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,

@@ -56,10 +56,19 @@ constexpr int kMaxStagedRounds = 64;
 constexpr size_t kStagingCap = size_t(16) << 30;  // largest staging buffer recommended
 constexpr int kOrderBlock = 1024;                  // threads of the ray-order kernels
 
-// Bytes at the front of the staging region for the ray order and its block sums.
+// Stored encodings: the forward writes each sample's bf16 MLP input row, which
+// the backward reads back instead of gathering the tables again.  Largest
+// store the recommended staging size includes.
+constexpr size_t kEncodingStoreCap = size_t(48) << 30;
+
+inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
+inline int order_blocks(int R, int P) { return (std::max(R, P) + kOrderBlock - 1) / kOrderBlock; }
+
+// Bytes at the front of the staging region: the ray order, its block sums,
+// the sample offset of every ranked ray and their block sums.
 inline size_t order_bytes(int R, int P) {
-  const size_t n_blocks = (size_t)(std::max(R, P) + kOrderBlock - 1) / kOrderBlock;
-  return (((size_t)R * 4 + 255) & ~size_t(255)) + (((n_blocks + 1) * 4 + 255) & ~size_t(255));
+  const size_t nb = (size_t)order_blocks(R, P) + 1;
+  return align256((size_t)R * 4) + align256(nb * 4) + align256((size_t)R * 8) + align256(nb * 8);
 }
 
 // Workspace: RayRec[R] | slot[P] (int32: batch index of the ray through each
@@ -71,7 +80,8 @@ struct Workspace {
   RayRec* rays;
   int32_t* slot;
   unsigned int* counters;  // [0] forward cursor, [1] backward cursor, [2] error word, [3] flags,
-                           // [5] scatter cursor
+                           // [5] scatter cursor, [6] rays with samples, [7] encoding-store rows
+                           // the forward filled, [8] forward loss sum (split step)
   float* stage = nullptr;
   size_t stage_bytes = 0;
 };
@@ -89,6 +99,65 @@ inline Workspace carve_workspace(void* ws, int R, int P, size_t size = 0) {
     w.stage_bytes = size - base;
   }
   return w;
+}
+
+// Split of the staging region of the two-pass mixed backward:
+//   order[R] int32 | block sums | offs[R] uint64 (first stored row of each
+//   ranked ray) | block sums | encoding store [xcap rows of row_bytes] |
+//   staged dL/d(encoding) of one round of per_round rays (per_ray bytes each).
+// The staged rounds take the recommended size for `rounds` rounds (capped at
+// kStagingCap) and the encoding store the rest, up to R * S rows; when that
+// leaves less than one ray's rows there is no store and the rounds take the
+// whole region.  per_round == 0: no staging (the fused single-pass backward).
+// The store starts at the same address whatever the split, so a backward half
+// reading rows [0, min(its xcap, the forward's)) never reads its own staging.
+struct StageLayout {
+  int32_t* order = nullptr;
+  unsigned int* block_sums = nullptr;
+  uint64_t* offs = nullptr;
+  unsigned long long* block_samples = nullptr;
+  uint4* xstore = nullptr;
+  uint32_t xcap = 0;  // rows of the encoding store
+  float* stage = nullptr;
+  int64_t per_round = 0;
+};
+
+inline size_t staged_round_bytes(int R, int rounds, size_t per_ray) {
+  const int64_t per_round = (R + rounds - 1) / rounds;
+  return std::min((size_t)per_round * per_ray, kStagingCap / per_ray * per_ray);
+}
+
+inline StageLayout stage_layout(const Workspace& ws, int R, int P, int S, size_t row_bytes, size_t per_ray,
+                                int rounds) {
+  StageLayout L;
+  const size_t ob = order_bytes(R, P);
+  if (!ws.stage || ws.stage_bytes <= ob || R <= 0) return L;
+  char* p = reinterpret_cast<char*>(ws.stage);
+  const size_t nb = (size_t)order_blocks(R, P) + 1;
+  L.order = reinterpret_cast<int32_t*>(p);
+  L.block_sums = reinterpret_cast<unsigned int*>(p + align256((size_t)R * 4));
+  L.offs = reinterpret_cast<uint64_t*>(p + align256((size_t)R * 4) + align256(nb * 4));
+  L.block_samples = reinterpret_cast<unsigned long long*>(p + align256((size_t)R * 4) + align256(nb * 4) +
+                                                          align256((size_t)R * 8));
+  const size_t avail = ws.stage_bytes - ob;
+  const size_t want = staged_round_bytes(R, rounds, per_ray);
+  size_t xbytes = 0;
+  if (avail >= want + (size_t)S * row_bytes + 256) {
+    const size_t rows = std::min<size_t>({(avail - want - 256) / row_bytes, (size_t)R * S, 0xffffffffu});
+    if (rows >= (size_t)S) {
+      L.xcap = (uint32_t)rows;
+      xbytes = align256(rows * row_bytes);
+      L.xstore = reinterpret_cast<uint4*>(p + ob);
+    }
+  }
+  L.stage = reinterpret_cast<float*>(p + ob + xbytes);
+  L.per_round = std::min<int64_t>((int64_t)((avail - xbytes) / per_ray), R);
+  if (L.per_round <= 0 || (R + L.per_round - 1) / L.per_round > kMaxStagedRounds) {
+    L.per_round = 0;
+    L.xstore = nullptr;
+    L.xcap = 0;
+  }
+  return L;
 }
 
 // Warp per ray: set-up, sample count (warp ballot), measured value, scale;
@@ -139,17 +208,22 @@ __device__ __forceinline__ int next_ray(unsigned int* cursor, const int32_t* __r
 }
 
 // The rays with samples in scheduling order, for the two-pass backward's
-// rounds of equal ray counts: order[rank] = ray, ranks 0..ctrl[6]-1.  Three
-// launches over the scheduling indices (pixels, or batch positions when the
-// batch repeats a pixel): per-block counts, one block scanning them, and the
-// per-block compaction, so pixel order is kept.
+// rounds of equal ray counts: order[rank] = ray, ranks 0..ctrl[6]-1, and
+// offs[rank] = samples of the rays ranked before it (the ray's first row in
+// the encoding store).  Three launches over the scheduling indices (pixels,
+// or batch positions when the batch repeats a pixel): per-block counts, one
+// block scanning them, and the per-block compaction, so pixel order is kept.
 __global__ void order_count_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
                                    const unsigned int* __restrict__ ctrl, int R, int P,
-                                   unsigned int* __restrict__ block_sums);
-__global__ void order_scan_kernel(unsigned int* __restrict__ block_sums, int n_blocks, unsigned int* __restrict__ ctrl);
+                                   unsigned int* __restrict__ block_sums,
+                                   unsigned long long* __restrict__ block_samples);
+__global__ void order_scan_kernel(unsigned int* __restrict__ block_sums, unsigned long long* __restrict__ block_samples,
+                                  int n_blocks, unsigned int* __restrict__ ctrl);
 __global__ void order_compact_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
                                      const unsigned int* __restrict__ ctrl, int R, int P,
-                                     const unsigned int* __restrict__ block_sums, int32_t* __restrict__ order);
+                                     const unsigned int* __restrict__ block_sums,
+                                     const unsigned long long* __restrict__ block_samples,
+                                     int32_t* __restrict__ order, uint64_t* __restrict__ offs);
 
 // Scheduler over ranks [lo, hi) of the ordered rays (one round); the rank of
 // the returned ray is written to *sched.  Returns -1 when none are left.

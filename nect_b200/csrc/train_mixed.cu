@@ -83,10 +83,12 @@ __device__ __forceinline__ void relu_row(const float* h, uint8_t* tile, int r, u
 }
 
 // Encodes one sample into row r of the swizzled X tile (bf16), 8 features
-// (one 16-byte chunk) at a time; invalid samples write zeros.
+// (one 16-byte chunk) at a time; invalid samples write zeros.  With xdst the
+// row is also written there (evict-first: the store streams past the L2 that
+// holds the tables).
 template <int D, int F>
 __device__ __forceinline__ void encode_row(const GridDev& g, const __half* __restrict__ table, const float* p,
-                                           bool valid, uint8_t* sX, int r) {
+                                           bool valid, uint8_t* sX, int r, uint4* __restrict__ xdst = nullptr) {
   constexpr int LPC = 8 / F;  // levels per 16-byte chunk
 #pragma unroll 1
   for (int j = 0; j < 16 / LPC; ++j) {
@@ -112,7 +114,9 @@ __device__ __forceinline__ void encode_row(const GridDev& g, const __half* __res
 #pragma unroll
       for (int q = 0; q < 8; ++q) v[q] = 0.f;
     }
-    tc::st_chunk_bf16(sX, r, j, v);
+    const uint4 packed = tc::pack_bf16x8(v);
+    tc::st_chunk_raw(sX, r, j, packed);
+    if (xdst) __stcs(xdst + j, packed);
   }
 }
 
@@ -127,7 +131,8 @@ __device__ __forceinline__ void ld64(uint32_t taddr, float* v) {
 struct RayCursor {
   int ray = -1;
   int base = 0;
-  int sched = 0;  // scheduling index (detector pixel, or batch position) of the ray
+  int sched = 0;      // scheduling index (detector pixel, or batch position; rank with an order) of the ray
+  int64_t xrow = -1;  // encoding-store row of the ray's sample 0, -1 if its rows are not stored
   RayRec rec;
 };
 
@@ -136,10 +141,12 @@ struct RayCursor {
 // left.  Rays without samples were finalised by the preparation kernel.
 // With ``order`` the rays come from the ordered list, ranks [lo, hi) (one
 // round of the two-pass backward), else from the scheduling indices [lo, hi).
+// With ``offs`` a ray whose rows all lie below xcap gets its store row.
 __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, unsigned int* cursor,
                                            const int32_t* slot, const TrainArgs& a, bool by_pixel, int lane,
                                            int lo = 0, int hi = 0x7fffffff, const int32_t* order = nullptr,
-                                           unsigned int n_valid = 0) {
+                                           unsigned int n_valid = 0, const uint64_t* offs = nullptr,
+                                           uint32_t xcap = 0) {
   if (cur.ray >= a.num_rays) return false;
   if (cur.ray >= 0 && cur.base < cur.rec.count) return true;
   const int r = order ? next_ray_ranked(cursor, order, n_valid, lo, hi, lane, &cur.sched)
@@ -147,11 +154,17 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
   if (r < 0) {
     cur.ray = a.num_rays;
     cur.rec.count = 0;
+    cur.xrow = -1;
     return false;
   }
   cur.rec = load_ray(recs, r);
   cur.ray = r;
   cur.base = 0;
+  cur.xrow = -1;
+  if (order && offs) {
+    const uint64_t o = offs[cur.sched];
+    if (o + (uint64_t)cur.rec.count <= (uint64_t)xcap) cur.xrow = (int64_t)o;
+  }
   return true;
 }
 
@@ -170,9 +183,11 @@ template <int D, int F, int H>
 __global__ void __launch_bounds__(kMixThreads, kFwdBlocksPerSM)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int out_act, float* __restrict__ y_pred, float* __restrict__ loss) {
+                 int out_act, float* __restrict__ y_pred, float* __restrict__ loss, const int32_t* __restrict__ order,
+                 const uint64_t* __restrict__ offs, uint4* __restrict__ xstore, uint32_t xcap) {
   constexpr int IN = 16 * F;
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  const unsigned int n_valid = order ? ctrl[6] : 0u;
   unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
@@ -188,6 +203,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   float* red = reinterpret_cast<float*>(tslot + 4);
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (xstore && blockIdx.x == 0 && t == 0) ctrl[7] = xcap;  // rows this forward fills, for the backward
   stage_mixed_weights<IN, H>(W, sW, sWout);
   if (warp == 0) {
     tc::tmem_alloc(tslot, 128);
@@ -209,14 +225,16 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   RayCursor cur;
   bool timed_out = false;
   while (true) {
-    const bool active = next_chunk(cur, recs, ctrl, slot, a, by_pixel, lane);
+    const bool active =
+        next_chunk(cur, recs, ctrl, slot, a, by_pixel, lane, 0, 0x7fffffff, order, n_valid, offs, xcap);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
-    encode_row<D, F>(grid, table, p, valid, sX, t);
+    encode_row<D, F>(grid, table, p, valid, sX, t,
+                     valid && cur.xrow >= 0 ? xstore + (size_t)(cur.xrow + i) * (IN / 8) : nullptr);
     float h[64];
     // layer k (0-based) writes TMEM columns 64 * (k & 1); its input is X for
     // k = 0, else the previous layer's activations in sA
@@ -296,11 +314,14 @@ __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
-                 float* __restrict__ stage, int64_t slots, const int32_t* __restrict__ order) {
+                 float* __restrict__ stage, int64_t slots, const int32_t* __restrict__ order,
+                 const uint64_t* __restrict__ offs, const uint4* __restrict__ xstore, uint32_t xcap) {
   constexpr int IN = 16 * F;
   static_assert(IN <= 64 && H >= 2 && H <= 3, "TMEM plan: 64 transient + (H - 1) x 64 + IN columns <= 256");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
+  // rows below both this launch's store size and the forward's are valid
+  const uint32_t xrows = xstore ? min(xcap, ctrl[7]) : 0u;
   unsigned int* err = ctrl + 2;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
@@ -364,14 +385,22 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     return true;
   };
   while (true) {
-    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi, order, n_valid);
+    const bool active =
+        next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi, order, n_valid, offs, xrows);
     if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
-    encode_row<D, F>(grid, table, p, valid, sX, t);
+    if (cur.xrow >= 0) {  // the forward stored this ray's rows: stream them back (warp-uniform branch)
+      const uint4* src = xstore + (size_t)(cur.xrow + i) * (IN / 8);
+#pragma unroll
+      for (int j = 0; j < IN / 8; ++j)
+        tc::st_chunk_raw(sX, t, j, valid ? __ldcs(src + j) : make_uint4(0u, 0u, 0u, 0u));
+    } else {
+      encode_row<D, F>(grid, table, p, valid, sX, t);
+    }
     // forward recompute: layer 0 from X, layer k from A_k (stored with its ReLU mask)
     float h[64];
     uint32_t mlo[H], mhi[H];
@@ -581,13 +610,33 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     fblocks = std::min(fblocks, a.max_blocks);
     blocks = std::min(blocks, a.max_blocks);
   }
+  constexpr int IN = 16 * F;
+  const int R = a.num_rays;
+  // staging region: ray order and sample offsets, the encoding store, then
+  // dL/d(encoding) of one round of per_round rays
+  const StageLayout L = stage_layout(ws, R, a.n_pixels, a.S, IN * sizeof(__nv_bfloat16),
+                                     (size_t)a.S * IN * sizeof(float), tune.staged_rounds);
+  auto run_order = [&]() -> int {
+    ProfScope ps(kProfOrder, s);
+    const int n_blocks = order_blocks(R, a.n_pixels);
+    order_count_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, L.block_sums,
+                                                        L.block_samples);
+    order_scan_kernel<<<1, kOrderBlock, 0, s>>>(L.block_sums, L.block_samples, n_blocks, ws.counters);
+    order_compact_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, L.block_sums,
+                                                          L.block_samples, L.order, L.offs);
+    return launch_status("order kernels");
+  };
   if (a.phase & kPhaseForward) {
+    // with an encoding store the forward runs the rays in rank order and keeps their rows
+    if (L.xstore)
+      if (int rc = run_order()) return rc;
     auto k = fwd_mixed_kernel<D, F, H>;
     const size_t smem = 1024 + H * kWTile + kTile + 64 * 4 + 64;
     set_smem(k, smem, a.max_blocks > 0);
     {
       ProfScope ps(kProfForward, s);
-      k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss);
+      k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
+                                           L.xstore ? L.order : nullptr, L.offs, L.xstore, L.xcap);
     }
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   }
@@ -595,35 +644,22 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // at least 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
   const size_t bsmem =
       std::max<size_t>(1024 + H * kWTile + (H + 1) * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
-  constexpr int IN = 16 * F;
-  const int64_t per_index = (int64_t)a.S * IN * (int64_t)sizeof(float);
-  const int R = a.num_rays;
-  // staging region: ray order and its block sums, then dL/d(encoding) of one round of Q rays
-  const size_t ob = order_bytes(R, a.n_pixels);
-  const int64_t per_round =
-      ws.stage && ws.stage_bytes > ob ? std::min<int64_t>((int64_t)((ws.stage_bytes - ob) / per_index), R) : 0;
-  if (per_round <= 0 || ceil_div(R, per_round) > kMaxStagedRounds) {
+  if (L.per_round <= 0) {
     // fused single pass: the backward scatters its own gradients
     auto k = bwd_mixed_kernel<D, F, H, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
     k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                         W_grad, 0, 0x7fffffff, nullptr, 0, nullptr);
+                                         W_grad, 0, 0x7fffffff, nullptr, 0, nullptr, nullptr, nullptr, 0u);
     return launch_status("bwd_mixed_kernel");
   }
-  int32_t* order = reinterpret_cast<int32_t*>(ws.stage);
-  unsigned int* block_sums = reinterpret_cast<unsigned int*>(reinterpret_cast<char*>(ws.stage) +
-                                                             (((size_t)R * 4 + 255) & ~size_t(255)));
-  float* stage = reinterpret_cast<float*>(reinterpret_cast<char*>(ws.stage) + ob);
-  {
-    ProfScope ps(kProfOrder, s);
-    const int n_blocks = (int)ceil_div(std::max(R, a.n_pixels), kOrderBlock);
-    order_count_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, block_sums);
-    order_scan_kernel<<<1, kOrderBlock, 0, s>>>(block_sums, n_blocks, ws.counters);
-    order_compact_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, block_sums,
-                                                          order);
-    if (int rc = launch_status("order kernels")) return rc;
-  }
+  // the order is a function of the prepared rays alone: computed again unless
+  // this call's forward just did
+  if (!((a.phase & kPhaseForward) && L.xstore))
+    if (int rc = run_order()) return rc;
+  const int64_t per_round = L.per_round;
+  float* stage = L.stage;
+  const int32_t* order = L.order;
   // two passes per round of Q ordered rays: the tensor-core backward stages
   // dL/d(encoding), then one scatter pass per level group
   int group_start[NECTB_MAX_LEVELS + 1], n_groups = 0;
@@ -654,7 +690,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     {
       ProfScope ps(kProfBackward, s);
       kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                            W_grad, (int)lo, hi, stage, slots, order);
+                                            W_grad, (int)lo, hi, stage, slots, order, L.offs, L.xstore, L.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {

@@ -78,89 +78,99 @@ __device__ __forceinline__ bool ordered_valid(const int32_t* __restrict__ slot, 
   return r >= 0 && recs[r].count > 0;
 }
 
-// Exclusive block scan of one flag per thread (kOrderBlock threads); returns
-// the thread's rank among the block's set flags, *total the block's count.
-__device__ __forceinline__ unsigned int block_rank(bool flag, unsigned int* warp_sums, unsigned int* total) {
+// Exclusive scan of one value per thread over a block of kOrderBlock threads
+// (32 warps); returns the thread's prefix, *total the block's sum.  Callers
+// that scan again into the same warp_sums synchronise first.
+template <typename T>
+__device__ __forceinline__ T block_scan(T v, T* warp_sums, T* total) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned int ballot = __ballot_sync(0xffffffffu, flag);
-  const unsigned int in_warp = __popc(ballot & ((1u << lane) - 1u));
-  if (lane == 0) warp_sums[warp] = __popc(ballot);
+  T x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const T y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) warp_sums[warp] = x;
   __syncthreads();
   if (warp == 0) {
-    const unsigned int v = warp_sums[lane];   // kOrderBlock / 32 == 32 warps
-    unsigned int x = v;
+    const T w = warp_sums[lane];
+    T z = w;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
-      const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+      const T y = __shfl_up_sync(0xffffffffu, z, o);
+      if (lane >= o) z += y;
     }
-    warp_sums[lane] = x - v;                  // exclusive
-    if (lane == 31) warp_sums[32] = x;
+    warp_sums[lane] = z - w;  // exclusive over warps
+    if (lane == 31) warp_sums[32] = z;
   }
   __syncthreads();
   *total = warp_sums[32];
-  return warp_sums[warp] + in_warp;
+  return warp_sums[warp] + x - v;
 }
 
 __global__ void __launch_bounds__(kOrderBlock)
 order_count_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
-                   const unsigned int* __restrict__ ctrl, int R, int P, unsigned int* __restrict__ block_sums) {
+                   const unsigned int* __restrict__ ctrl, int R, int P, unsigned int* __restrict__ block_sums,
+                   unsigned long long* __restrict__ block_samples) {
   __shared__ unsigned int ws[33];
+  __shared__ unsigned long long ws64[33];
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
-  int ray;
+  int ray = -1;
   const bool v = ordered_valid(slot, recs, by_pixel, blockIdx.x * kOrderBlock + threadIdx.x, by_pixel ? P : R, &ray);
   unsigned int total;
-  block_rank(v, ws, &total);
-  if (threadIdx.x == 0) block_sums[blockIdx.x] = total;
+  unsigned long long samples;
+  block_scan<unsigned int>(v ? 1u : 0u, ws, &total);
+  block_scan<unsigned long long>(v ? (unsigned long long)recs[ray].count : 0ull, ws64, &samples);
+  if (threadIdx.x == 0) {
+    block_sums[blockIdx.x] = total;
+    block_samples[blockIdx.x] = samples;
+  }
 }
 
 __global__ void __launch_bounds__(kOrderBlock)
-order_scan_kernel(unsigned int* __restrict__ block_sums, int n_blocks, unsigned int* __restrict__ ctrl) {
+order_scan_kernel(unsigned int* __restrict__ block_sums, unsigned long long* __restrict__ block_samples, int n_blocks,
+                  unsigned int* __restrict__ ctrl) {
   __shared__ unsigned int ws[33];
+  __shared__ unsigned long long ws64[33];
   unsigned int carry = 0;
-  for (int b0 = 0; b0 < n_blocks; b0 += kOrderBlock) {   // block-uniform loop
+  unsigned long long carry64 = 0;
+  for (int b0 = 0; b0 < n_blocks; b0 += kOrderBlock) {  // block-uniform loop
     const int b = b0 + threadIdx.x;
-    const unsigned int v = b < n_blocks ? block_sums[b] : 0u;
-    // exclusive scan of v over the block (ranks of a count, not of a flag)
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    unsigned int x = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const unsigned int y = __shfl_up_sync(0xffffffffu, x, o);
-      if (lane >= o) x += y;
+    unsigned int total;
+    unsigned long long total64;
+    const unsigned int x = block_scan<unsigned int>(b < n_blocks ? block_sums[b] : 0u, ws, &total);
+    const unsigned long long x64 = block_scan<unsigned long long>(b < n_blocks ? block_samples[b] : 0ull, ws64,
+                                                                  &total64);
+    if (b < n_blocks) {
+      block_sums[b] = carry + x;
+      block_samples[b] = carry64 + x64;
     }
-    if (lane == 31) ws[warp] = x;
-    __syncthreads();
-    if (warp == 0) {
-      const unsigned int w = ws[lane];
-      unsigned int z = w;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const unsigned int y = __shfl_up_sync(0xffffffffu, z, o);
-        if (lane >= o) z += y;
-      }
-      ws[lane] = z - w;
-      if (lane == 31) ws[32] = z;
-    }
-    __syncthreads();
-    if (b < n_blocks) block_sums[b] = carry + ws[warp] + x - v;
-    carry += ws[32];
+    carry += total;
+    carry64 += total64;
     __syncthreads();
   }
-  if (threadIdx.x == 0) ctrl[6] = carry;   // rays with samples
+  if (threadIdx.x == 0) ctrl[6] = carry;  // rays with samples
 }
 
 __global__ void __launch_bounds__(kOrderBlock)
 order_compact_kernel(const int32_t* __restrict__ slot, const RayRec* __restrict__ recs,
                      const unsigned int* __restrict__ ctrl, int R, int P, const unsigned int* __restrict__ block_sums,
-                     int32_t* __restrict__ order) {
+                     const unsigned long long* __restrict__ block_samples, int32_t* __restrict__ order,
+                     uint64_t* __restrict__ offs) {
   __shared__ unsigned int ws[33];
+  __shared__ unsigned long long ws64[33];
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   int ray = -1;
   const bool v = ordered_valid(slot, recs, by_pixel, blockIdx.x * kOrderBlock + threadIdx.x, by_pixel ? P : R, &ray);
   unsigned int total;
-  const unsigned int rank = block_rank(v, ws, &total);
-  if (v) order[block_sums[blockIdx.x] + rank] = ray;
+  unsigned long long samples;
+  const unsigned int rank = block_scan<unsigned int>(v ? 1u : 0u, ws, &total);
+  const unsigned long long off =
+      block_scan<unsigned long long>(v ? (unsigned long long)recs[ray].count : 0ull, ws64, &samples);
+  if (v) {
+    order[block_sums[blockIdx.x] + rank] = ray;
+    offs[block_sums[blockIdx.x] + rank] = block_samples[blockIdx.x] + off;
+  }
 }
 
 namespace {

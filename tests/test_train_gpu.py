@@ -186,6 +186,33 @@ def test_staged_and_fused_backward_agree(cuda_device, n_dims, duplicates):
     assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
 
 
+@pytest.mark.parametrize("n_dims,duplicates,store_rows", [(3, False, 5600), (4, True, 5600), (3, False, 0),
+                                                           (4, False, 0)])
+def test_encoding_store_partial_and_absent(cuda_device, n_dims, duplicates, store_rows):
+    """The staged backward reads the rows the forward stored and gathers the
+    rest: a store smaller than the batch's samples (rays beyond it recompute)
+    and no store at all give the single fused pass's results."""
+    from nect_b200.trainer import Workspace
+
+    R, S, row_bytes = 700, 64, 32 * 2
+
+    class Trimmed(Workspace):
+        # passes the C ABI a workspace smaller than the recommended one by the
+        # store rows it should not have
+        def get(self, model, c_geometry, num_rays, device, points_per_ray=0):
+            ptr, n = super().get(model, c_geometry, num_rays, device, points_per_ray)
+            return ptr, n - (R * S - store_rows) * row_bytes - (256 if store_rows == 0 else 0)
+
+    ws = Trimmed(staging=True)
+    (y1, L1, gt1, gm1), _ = run_train_case(n_dims, "mixed", "l2", "cone", duplicates, ws=ws)
+    assert ws.error_word() == 0
+    (y2, L2, gt2, gm2), _ = run_train_case(n_dims, "mixed", "l2", "cone", duplicates, ws=Workspace(staging=False))
+    assert torch.equal(y1, y2)
+    assert abs(L1 - L2) <= 1e-5 * abs(L2)
+    assert rel_max(gt1, gt2) < 1e-5, rel_max(gt1, gt2)
+    assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
+
+
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
 def test_batch_with_repeated_pixels(cuda_device, precision):
     """Every ray of the batch is processed when pixels repeat (the pixel-order
