@@ -255,8 +255,11 @@ __device__ __forceinline__ float run_sum(float v, int lane, int end) {
 // fp32 reassociation.
 //
 // dL/d(feature f of level l) is read at dsrc[l * lstride + f * fstride]; only
-// levels [l0, l1) are scattered.
-template <int D, int F>
+// levels [l0, l1) are scattered.  kStreamSrc: dsrc is global memory read once
+// (the staging buffer, fstride 1, rows aligned to F floats): one vector load
+// per level, evict-first, so the streamed rows do not push the gradient slice
+// out of L2.
+template <int D, int F, bool kStreamSrc = false>
 __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict__ grad, const float* x, bool valid,
                                              const float* dsrc, int64_t lstride, int fstride, uint32_t agg_levels,
                                              int l0, int l1) {
@@ -266,8 +269,21 @@ __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict
     LevelCorners<D> lc;
     level_corners<D>(g, l, x, lc);
     float d[F];
+    if constexpr (kStreamSrc && F == 2) {
+      const float2 v = valid ? __ldcs(reinterpret_cast<const float2*>(dsrc + l * lstride)) : make_float2(0.f, 0.f);
+      d[0] = v.x;
+      d[1] = v.y;
+    } else if constexpr (kStreamSrc && F == 4) {
+      const float4 v =
+          valid ? __ldcs(reinterpret_cast<const float4*>(dsrc + l * lstride)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      d[0] = v.x;
+      d[1] = v.y;
+      d[2] = v.z;
+      d[3] = v.w;
+    } else {
 #pragma unroll
-    for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[l * lstride + f * fstride] : 0.f;
+      for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[l * lstride + f * fstride] : 0.f;
+    }
     float* base = grad + g.offset[l] * F;
     if ((agg_levels >> l) & 1u) {
       // runs of lanes in the same spatial cell (t is the same for the whole

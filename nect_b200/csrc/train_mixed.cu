@@ -500,11 +500,12 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         float* dst = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
 #pragma unroll
         for (int l = 0; l < 16; ++l) {
+          // evict-first: each staged value is read once, by the scatter pass
           if constexpr (F == 2)
-            *reinterpret_cast<float2*>(dst + l * slots * F) = make_float2(dx[2 * l], dx[2 * l + 1]);
+            __stcs(reinterpret_cast<float2*>(dst + l * slots * F), make_float2(dx[2 * l], dx[2 * l + 1]));
           else if constexpr (F == 4)
-            *reinterpret_cast<float4*>(dst + l * slots * F) =
-                make_float4(dx[4 * l], dx[4 * l + 1], dx[4 * l + 2], dx[4 * l + 3]);
+            __stcs(reinterpret_cast<float4*>(dst + l * slots * F),
+                   make_float4(dx[4 * l], dx[4 * l + 1], dx[4 * l + 2], dx[4 * l + 3]));
           else
 #pragma unroll
             for (int f = 0; f < F; ++f) dst[l * slots * F + f] = dx[l * F + f];
@@ -583,8 +584,8 @@ scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs,
     if (i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
     const float* dsrc = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
-    scatter_warp<D, F>(grid, table_grad, p, valid, dsrc, slots * F, 1,
-                       run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz, a.run_threshold), l0, l1);
+    scatter_warp<D, F, true>(grid, table_grad, p, valid, dsrc, slots * F, 1,
+                             run_levels(grid, cur.rec.dx, cur.rec.dy, cur.rec.dz, a.run_threshold), l0, l1);
     cur.base += 32;
   }
 }
