@@ -368,6 +368,8 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   int j0_out = 0;
   RayCursor cur;
   bool timed_out = false;
+  uint4 xrow[IN / 8];    // stored rows of the current chunk (this thread's sample)
+  bool pre_ok = false;   // xrow already holds them (prefetched during the previous tile)
   // Issues the MMAs of one phase (thread 0), waits for them; false on time-out.
   auto run_phase = [&](auto issue) -> bool {
     tc::fence_async_smem();
@@ -395,10 +397,22 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (D == 4) p[3] = a.t;
     if (cur.xrow >= 0) {  // the forward stored this ray's rows: stream them back (warp-uniform branch)
       const uint4* src = xstore + (size_t)(cur.xrow + i) * (IN / 8);
+      if (!pre_ok && valid) {  // not prefetched: the first chunk of a ray
 #pragma unroll
-      for (int j = 0; j < IN / 8; ++j)
-        tc::st_chunk_raw(sX, t, j, valid ? __ldcs(src + j) : make_uint4(0u, 0u, 0u, 0u));
+        for (int j = 0; j < IN / 8; ++j) xrow[j] = __ldcs(src + j);
+      }
+#pragma unroll
+      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sX, t, j, valid ? xrow[j] : make_uint4(0u, 0u, 0u, 0u));
+      // prefetch the rows of the warp's next chunk of this ray; they arrive
+      // while this tile's MMAs run (rows below the ray's count lie in its
+      // stored range)
+      pre_ok = cur.base + 32 < cur.rec.count;
+      if (pre_ok && i + 32 < cur.rec.count) {
+#pragma unroll
+        for (int j = 0; j < IN / 8; ++j) xrow[j] = __ldcs(src + 32 * (IN / 8) + j);
+      }
     } else {
+      pre_ok = false;
       encode_row<D, F>(grid, table, p, valid, sX, t);
     }
     // forward recompute: layer 0 from X, layer k from A_k (stored with its ReLU mask)
