@@ -74,11 +74,18 @@ def _time_steps(trainer, make_batch, steps: int, warmup: int) -> float:
     return e0.elapsed_time(e1) / steps
 
 
+def _best_of(trainer, make_batch, steps: int, warmup: int, reps: int) -> float:
+    return min(_time_steps(trainer, make_batch, steps, warmup) for _ in range(reps))
+
+
 def tune(trainer, make_batch, steps: int = 3, warmup: int = 2, space: dict | None = None,
-         cache: str | Path | None = None) -> dict:
+         cache: str | Path | None = None, reps: int = 2, margin: float = 0.01) -> dict:
     """Pick the fastest tuning for this trainer's workload.  ``make_batch(k)``
     returns the k-th RayBatch of a representative stream (it is called for
-    warm-up and timed steps of every candidate)."""
+    warm-up and timed steps of every candidate).  Each candidate is timed as
+    the best of ``reps`` runs and replaces the incumbent only when faster by
+    more than ``margin``; the result is checked once more against the tuning
+    the search started from, so timing noise cannot leave a slower choice."""
     space = space or SPACE
     probe = make_batch(0)
     key = workload_key(trainer, probe.num_rays)
@@ -91,19 +98,27 @@ def tune(trainer, make_batch, steps: int = 3, warmup: int = 2, space: dict | Non
     saved = [t.detach().clone() for t in (model.table, model.mlp, trainer.m_table, trainer.v_table, trainer.m_mlp,
                                           trainer.v_mlp)]
     saved_step = trainer.step_count
-    best = get_tuning()
+    start = get_tuning()
+    best = dict(start)
     try:
         set_tuning(best)
-        best_ms = _time_steps(trainer, make_batch, steps, warmup)
+        best_ms = _best_of(trainer, make_batch, steps, warmup, reps)
         for name, values in space.items():
             for v in values:
                 if v == best[name]:
                     continue
                 cand = dict(best, **{name: v})
                 set_tuning(cand)
-                ms = _time_steps(trainer, make_batch, steps, warmup)
-                if ms < best_ms:
+                ms = _best_of(trainer, make_batch, steps, warmup, reps)
+                if ms < best_ms * (1.0 - margin):
                     best, best_ms = cand, ms
+        if best != start:   # confirm against the starting point with fresh timings
+            set_tuning(start)
+            start_ms = _best_of(trainer, make_batch, steps, warmup, reps)
+            set_tuning(best)
+            best_ms = _best_of(trainer, make_batch, steps, warmup, reps)
+            if start_ms <= best_ms * (1.0 + margin / 2):
+                best, best_ms = start, start_ms
         set_tuning(best)
     finally:
         with torch.no_grad():
