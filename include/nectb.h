@@ -258,10 +258,19 @@ size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHas
  * each round's tensor-core pass writes dL/d(encoding) of its samples (fp32,
  * num_points_per_ray * n_levels * n_features per ray) and scatter passes over
  * level groups apply it to grid_grad with the gradient slice of each group
- * resident in L2.  The recommendation is capped at 16 GiB (plus the ray list).
- * Less staging gives more rounds; when it would take more than 64 rounds the
- * single-pass backward (scatter inside the tensor-core kernel) runs instead.  Returns 0 for the plain fp32 path, which does not
- * stage.  No reference counterpart. */
+ * resident in L2.  The rounds' part is capped at 16 GiB (plus the ray list).
+ * It also includes an encoding store: the forward writes each sample's bf16
+ * MLP input row (n_levels * n_features * 2 bytes) there and the backward
+ * reads it back instead of gathering the tables a second time (identical
+ * values); the store has a row for every sample slot (num_rays *
+ * num_points_per_ray), capped at 48 GiB, and rays whose rows do not fit
+ * gather again.  A smaller buffer gets fewer store rows, then no store, then
+ * more rounds; when it would take more than 64 rounds the single-pass
+ * backward (scatter inside the tensor-core kernel) runs instead.  The split
+ * between store and rounds follows the buffer size and staged_rounds, so a
+ * split step's two halves take the same workspace size with the tuning
+ * unchanged between them.  Returns 0 for the plain fp32 path, which does
+ * not stage.  No reference counterpart. */
 size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                  const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray);
 
