@@ -168,19 +168,37 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
   return true;
 }
 
-// Blocks of the forward per SM.  Shared memory per block is 33.5 KB (A1
-// reuses the X tile), so four blocks (16 warps, 4 x 128 TMEM columns) still
-// leave 92 KB of L1 for the coarse levels' gathers.  Measured on the 512^2
-// cone workloads: 2 / 3 / 4 blocks give 19.5 / 15.3 / 13.6 ms (3D) and
-// 34.0 / 28.0 / 26.0 ms (4D) per 2^18-ray forward.
+// Warpgroups of the forward per SM.  A block is one to four independent
+// warpgroups (128 threads each, one 128-sample tile, its own TMEM quarter,
+// mbarrier and named barrier) that share one copy of the weight tiles: with
+// four, shared memory is 82 KB per SM instead of four blocks' 136 KB, and the
+// L1 that the gathers hit (neighbouring rays reuse table entries) grows from
+// 92 to 156 KB.  Re-projection queries, which share SMs with serving
+// kernels, run one warpgroup per block.
 #ifndef NECTB_FWD_BLOCKS_PER_SM
 #define NECTB_FWD_BLOCKS_PER_SM 4
 #endif
 constexpr int kFwdBlocksPerSM = NECTB_FWD_BLOCKS_PER_SM;
 static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 128 <= 512, "TMEM holds 512 columns per SM");
 
+// Barrier over the 128 threads of warpgroup wg (named barrier wg + 1; 0 is
+// __syncthreads'), and its OR-reduction form.
+__device__ __forceinline__ void wg_sync(int wg) { asm volatile("bar.sync %0, 128;" ::"r"(wg + 1) : "memory"); }
+__device__ __forceinline__ bool wg_or(int wg, bool p) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred pi, po;\n\t"
+      "setp.ne.u32 pi, %1, 0;\n\t"
+      "bar.red.or.pred po, %2, 128, pi;\n\t"
+      "selp.u32 %0, 1, 0, po;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)p), "r"(wg + 1)
+      : "memory");
+  return r != 0;
+}
+
 template <int D, int F, int H>
-__global__ void __launch_bounds__(kMixThreads, kFwdBlocksPerSM)
+__global__ void __launch_bounds__(kFwdBlocksPerSM * kMixThreads, 1)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ y_pred, float* __restrict__ loss, const int32_t* __restrict__ order,
@@ -189,33 +207,37 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
   unsigned int* err = ctrl + 2;
+  const int n_wg = blockDim.x / kMixThreads;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
-  uint8_t* sW = base;  // H weight tiles
-  uint8_t* sX = sW + H * kWTile;
+  uint8_t* sW = base;  // H weight tiles, shared by the warpgroups
+  float* sWout = reinterpret_cast<float*>(sW + H * kWTile + n_wg * kTile);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sWout + 64);       // [n_wg]
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kFwdBlocksPerSM);
+  float* red = reinterpret_cast<float*>(tslot + 4);                 // [warps]
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int wg = t / kMixThreads, r = t % kMixThreads;  // warpgroup, and this thread's row of its tile
   // Each hidden layer's activations overwrite X: the MMA that read the tile has
   // finished (its commit has arrived) before the next activations are written,
   // and the next X is written only after the last MMA has completed.
+  uint8_t* sX = sW + H * kWTile + wg * kTile;
   uint8_t* sA = sX;
-  float* sWout = reinterpret_cast<float*>(sX + kTile);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
-  float* red = reinterpret_cast<float*>(tslot + 4);
-
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  uint64_t* bar = bars + wg;
   if (xstore && blockIdx.x == 0 && t == 0) ctrl[7] = xcap;  // rows this forward fills, for the backward
   stage_mixed_weights<IN, H>(W, sW, sWout);
+  const uint32_t ncols = n_wg == 1 ? 128u : (n_wg == 2 ? 256u : 512u);
   if (warp == 0) {
-    tc::tmem_alloc(tslot, 128);
+    tc::tmem_alloc(tslot, ncols);
     tc::tmem_relinquish();
   }
-  if (t == 0) tc::mbar_init(bar, 1);
+  if (r == 0) tc::mbar_init(bar, 1);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
-  const uint32_t tm = *tslot;
-  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
+  const uint32_t tm = *tslot + 128u * wg;  // this warpgroup's 128 columns
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * (warp & 3)) << 16);
   const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
   constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
 
@@ -227,27 +249,28 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   while (true) {
     const bool active =
         next_chunk(cur, recs, ctrl, slot, a, by_pixel, lane, 0, 0x7fffffff, order, n_valid, offs, xcap);
-    if (!__syncthreads_or(active)) break;
+    if (!wg_or(wg, active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
-    encode_row<D, F>(grid, table, p, valid, sX, t,
+    encode_row<D, F>(grid, table, p, valid, sX, r,
                      valid && cur.xrow >= 0 ? xstore + (size_t)(cur.xrow + i) * (IN / 8) : nullptr);
     float h[64];
-    // layer k (0-based) writes TMEM columns 64 * (k & 1); its input is X for
-    // k = 0, else the previous layer's activations in sA
+    // layer k (0-based) writes TMEM columns 64 * (k & 1) of the warpgroup's
+    // quarter; its input is X for k = 0, else the previous layer's
+    // activations in sA
 #pragma unroll
     for (int k = 0; k < H; ++k) {
       if (k > 0) {
         uint32_t mlo, mhi;
-        relu_row(h, sA, t, mlo, mhi);
+        relu_row(h, sA, r, mlo, mhi);
       }
       tc::fence_async_smem();
       tc::fence_before();
-      __syncthreads();
-      if (t == 0) {
+      wg_sync(wg);
+      if (r == 0) {
         tc::fence_after();
         if (k == 0) {
 #pragma unroll
@@ -261,7 +284,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
       }
       timed_out = !tc::mbar_wait(bar, phase);
       phase ^= 1;
-      if (__syncthreads_or(timed_out)) {
+      if (wg_or(wg, timed_out)) {
         timed_out = true;
         break;
       }
@@ -294,14 +317,18 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
       }
     }
   }
-  if (timed_out && t == 0) atomicOr(err, 1u);
+  if (timed_out && r == 0) atomicOr(err, 1u);
   if (lane == 0) red[warp] = loss_acc;
   tc::fence_before();
   __syncthreads();
-  if (t == 0) atomicAdd(loss, (red[0] + red[1] + red[2] + red[3]) / (float)a.num_rays);
+  if (t == 0) {
+    float sum = 0.f;
+    for (int w = 0; w < (int)(blockDim.x / 32); ++w) sum += red[w];
+    atomicAdd(loss, sum / (float)a.num_rays);
+  }
   if (warp == 0) {
     tc::fence_after();
-    tc::tmem_dealloc(tm, 128);
+    tc::tmem_dealloc(*tslot, ncols);
   }
 }
 
@@ -618,8 +645,13 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   TrainArgs a = args;
   a.run_threshold = D == 4 ? tune.run_threshold_4d : tune.run_threshold_3d;
   const size_t group_bytes = (size_t)tune.scatter_group_bytes;
-  int fblocks = std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
-                                          (int)ceil_div(a.num_rays, 4)));
+  // forward: one block of `wgs` warpgroups per SM when training; queries
+  // (which share SMs with serving kernels) one warpgroup per block
+  const int wgs = a.max_blocks > 0 ? 1 : std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM);
+  int fblocks = a.max_blocks > 0
+                    ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
+                                                (int)ceil_div(a.num_rays, 4)))
+                    : std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * wgs)));
   int blocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if (a.max_blocks > 0) {
     fblocks = std::min(fblocks, a.max_blocks);
@@ -646,11 +678,11 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     if (L.xstore)
       if (int rc = run_order()) return rc;
     auto k = fwd_mixed_kernel<D, F, H>;
-    const size_t smem = 1024 + H * kWTile + kTile + 64 * 4 + 64;
+    const size_t smem = 1024 + H * kWTile + wgs * kTile + 64 * 4 + kFwdBlocksPerSM * 8 + 16 + 4 * kFwdBlocksPerSM * 4;
     set_smem(k, smem, a.max_blocks > 0);
     {
       ProfScope ps(kProfForward, s);
-      k<<<fblocks, kMixThreads, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
+      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
                                            L.xstore ? L.order : nullptr, L.offs, L.xstore, L.xcap);
     }
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
