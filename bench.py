@@ -391,9 +391,9 @@ def main():
     staged = "scatter" in prof   # the mixed backward ran as tensor-core pass + staged scatter passes
     stage_io = enc.n_levels * enc.n_features_per_level * 4   # staged dL/d(encoding) per sample, each way
     row = enc.n_levels * enc.n_features_per_level * 2        # stored bf16 encoding row per sample
-    stored = 0.0   # share of samples whose rows the forward stores (recommended workspace: min(R*S, 48 GiB) rows)
+    stored = 0.0   # share of samples whose rows the forward stores (recommended workspace: min(R*S, 80 GiB) rows)
     if staged:
-        stored = min(1.0, min(rays_per_step * S, (48 << 30) // row) / max(n_valid / args.steps, 1.0))
+        stored = min(1.0, min(rays_per_step * S, (80 << 30) // row) / max(n_valid / args.steps, 1.0))
     step_bytes = {   # algorithmic bytes per step of each kernel kind
         "backward": n_valid / args.steps * (stored * row + (1 - stored) * gather + (stage_io if staged else scatter)),
         "scatter": n_valid / args.steps * (scatter + stage_io),

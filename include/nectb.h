@@ -263,7 +263,7 @@ size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, const NectbHas
  * MLP input row (n_levels * n_features * 2 bytes) there and the backward
  * reads it back instead of gathering the tables a second time (identical
  * values); the store has a row for every sample slot (num_rays *
- * num_points_per_ray), capped at 48 GiB, and rays whose rows do not fit
+ * num_points_per_ray), capped at 80 GiB, and rays whose rows do not fit
  * gather again.  A smaller buffer gets fewer store rows, then no store, then
  * more rounds; when it would take more than 64 rounds the single-pass
  * backward (scatter inside the tensor-core kernel) runs instead.  The split

@@ -59,7 +59,7 @@ constexpr int kOrderBlock = 1024;                  // threads of the ray-order k
 // Stored encodings: the forward writes each sample's bf16 MLP input row, which
 // the backward reads back instead of gathering the tables again.  Largest
 // store the recommended staging size includes.
-constexpr size_t kEncodingStoreCap = size_t(48) << 30;
+constexpr size_t kEncodingStoreCap = size_t(80) << 30;
 
 inline size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
 inline int order_blocks(int R, int P) { return (std::max(R, P) + kOrderBlock - 1) / kOrderBlock; }
