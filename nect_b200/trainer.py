@@ -48,21 +48,26 @@ class Workspace:
     """Caller-owned device workspace for nectb_train_step, grown on demand.
 
     With ``staging`` (default) it also holds the recommended staging buffer of
-    the mixed path's two-pass backward; without it the mixed backward runs as
-    one fused pass."""
+    the mixed path's two-pass backward (ray order, the encoding store and one
+    round of staged gradients); without it the mixed backward runs as one
+    fused pass.  ``staging_fraction`` < 1 takes that share of the
+    recommendation: the library then keeps fewer rows in the encoding store
+    (rays beyond it gather again), then none, then runs more rounds; results
+    do not change."""
 
-    def __init__(self, staging: bool = True):
+    def __init__(self, staging: bool = True, staging_fraction: float = 1.0):
         self.buf = None
         self.staging = staging
+        self.staging_fraction = staging_fraction
 
     def get(self, model: _HashGridModel, c_geometry, num_rays: int, device,
             points_per_ray: int = 0) -> tuple[int, int]:
         need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
                                                     ctypes.byref(model.mlp_desc), num_rays)
         if self.staging and points_per_ray > 0:
-            need = ((need + 255) // 256) * 256 + _lib.lib.nectb_train_staging_bytes(
+            need = ((need + 255) // 256) * 256 + int(self.staging_fraction * _lib.lib.nectb_train_staging_bytes(
                 ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
-                num_rays, points_per_ray)
+                num_rays, points_per_ray))
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         self.num_rays = num_rays
@@ -356,8 +361,10 @@ class Trainer:
         import numpy as np
 
         edges = np.linspace(angle_start, angle_stop, accumulation_steps + 1)
-        if not hasattr(self, "_scan_ws") or len(self._scan_ws) < accumulation_steps:
-            self._scan_ws = [Workspace() for _ in range(accumulation_steps)]
+        if not hasattr(self, "_scan_ws") or len(self._scan_ws) != accumulation_steps:
+            # every sub-angle forward keeps its workspace until the backward:
+            # together they take one step's recommended staging
+            self._scan_ws = [Workspace(staging_fraction=1.0 / accumulation_steps) for _ in range(accumulation_steps)]
         y_pred, batch = None, None
         for j in range(accumulation_steps):
             batch = self.make_batch(perm, batch_num, float((edges[j] + edges[j + 1]) / 2), projection, t)

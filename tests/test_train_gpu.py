@@ -213,6 +213,19 @@ def test_encoding_store_partial_and_absent(cuda_device, n_dims, duplicates, stor
     assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
 
 
+@pytest.mark.parametrize("fraction", [0.3, 0.05])
+def test_partial_staging_budget(cuda_device, fraction):
+    """A workspace with a share of the recommended staging (fewer store rows,
+    or no store and more rounds) gives the single fused pass's results."""
+    from nect_b200.trainer import Workspace
+
+    (y1, L1, gt1, gm1), _ = run_train_case(3, "mixed", "l2", "cone", ws=Workspace(staging_fraction=fraction))
+    (y2, L2, gt2, gm2), _ = run_train_case(3, "mixed", "l2", "cone", ws=Workspace(staging=False))
+    assert torch.equal(y1, y2)
+    assert rel_max(gt1, gt2) < 1e-5, rel_max(gt1, gt2)
+    assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
+
+
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
 def test_batch_with_repeated_pixels(cuda_device, precision):
     """Every ray of the batch is processed when pixels repeat (the pixel-order
