@@ -370,7 +370,8 @@ int nectb_profile_collect(int32_t* launches, double* total_ms);
 int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, void* stream);
 
 /* Launch shapes and scheduling of the mixed training path, process-wide:
- * blocks per SM of the forward (1..4) and of the tensor-core backward (1..2),
+ * warpgroups per SM of the forward (1..4), blocks per SM of the tensor-core
+ * backward (1..3; the three-layer model's kernel takes at most 2),
  * of the gradient scatter (0 = as many as fit), the rounds the recommended
  * staging is sized for (nectb_train_staging_bytes, 1..64), the largest fp32
  * gradient slice one scatter pass covers, and the samples-per-cell
@@ -378,7 +379,7 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * reductions (3D and 4D grids).  Results do not depend on these beyond fp32
  * reassociation; the Python autotuner (nect_b200.autotune) picks them per
  * workload.  nectb_set_tuning validates and applies to steps issued after it
- * returns; defaults: 4, 2, 0, 4, 48 MiB, 1.0, 3.0.  No reference
+ * returns; defaults: 4, 3, 0, 4, 48 MiB, 1.0, 3.0.  No reference
  * counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;

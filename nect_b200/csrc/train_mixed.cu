@@ -603,6 +603,292 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   }
 }
 
+// Lean staged backward for two hidden layers: 128 TMEM columns and 66 KB of
+// shared memory per block, so three blocks (12 warps) share an SM.
+//   TMEM: [0, 64) the transient result of every phase; [64, 128) the weight
+//   gradients, dW1 in lanes 0..63 and dW0 in lanes 64..127.  Both products
+//   are M = 128 MMAs whose A operand is a G tile and a zero tile: dW1 =
+//   [G2; 0]^T A1 writes its rows to lanes 0..63 and adds exactly 0 to lanes
+//   64..127, dW0 = [0; G1]^T X the reverse.  The first tile's dW1 product
+//   (accumulate off) clears the whole region before dW0 first adds to it.
+//   Shared memory: W0, W1 | G2 slot | zero tile | A1 slot.  X is written to
+//   the A1 slot for layer 0, read back into registers before A1 replaces it,
+//   and written to the G2 slot (free once dW1 is done) for the last phase.
+//   Accumulator rows are read 16 columns at a time; the w_out gradient is a
+//   16-column butterfly reduce-scatter per chunk.
+template <int D, int F>
+__global__ void __launch_bounds__(kMixThreads, 3)
+bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
+                const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
+                int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage, int64_t slots,
+                const int32_t* __restrict__ order, const uint64_t* __restrict__ offs, const uint4* __restrict__ xstore,
+                uint32_t xcap) {
+  constexpr int IN = 16 * F;
+  constexpr int H = 2;
+  static_assert(IN <= 64, "dW0 shares the 64 weight-gradient columns");
+  const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
+  const unsigned int n_valid = ctrl[6];
+  unsigned int* err = ctrl + 2;
+  const uint32_t xrows = xstore ? min(xcap, ctrl[7]) : 0u;
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* base = align1024(smem_raw);
+  uint8_t* sW = base;                 // W0, W1
+  uint8_t* sG = sW + H * kWTile;      // G2, later X
+  uint8_t* sZ = sG + kTile;           // zeros
+  uint8_t* sA = sZ + kTile;           // X, then A1, then G1
+  float* sWout = reinterpret_cast<float*>(sA + kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
+
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  stage_mixed_weights<IN, H>(W, sW, sWout);
+  {
+    uint4* z = reinterpret_cast<uint4*>(sZ);
+    for (int e = t; e < (int)(kTile / 16); e += kMixThreads) z[e] = make_uint4(0u, 0u, 0u, 0u);
+  }
+  if (warp == 0) {
+    tc::tmem_alloc(tslot, 128);
+    tc::tmem_relinquish();
+  }
+  if (t == 0) tc::mbar_init(bar, 1);
+  tc::fence_async_smem();
+  tc::fence_before();
+  __syncthreads();
+  tc::fence_after();
+  const uint32_t tm = *tslot;
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
+  const uint32_t sG_a = tc::smem_u32(sG), sZ_a = tc::smem_u32(sZ), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
+  constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
+  constexpr uint32_t id_dA = tc::idesc_bf16(128, 64, false, true);
+  constexpr uint32_t id_dW = tc::idesc_bf16(128, 64, true, true);
+  constexpr uint32_t id_dX = tc::idesc_bf16(128, IN, false, true);
+  constexpr uint32_t id_dW0 = tc::idesc_bf16(128, IN, true, true);
+
+  uint32_t phase = 0;
+  uint32_t wacc = 0;  // the first tile's dW1 product starts the accumulators
+  float dwacc[4] = {0.f, 0.f, 0.f, 0.f};  // w_out gradient, column 16c + (lane >> 1) of chunk c
+  uint4 xr[IN / 8];                       // this thread's X row (current tile)
+  uint4 xn[IN / 8];                       // the next chunk's stored row, prefetched
+  bool pre_ok = false;
+  RayCursor cur;
+  bool timed_out = false;
+  auto run_phase = [&](auto issue) -> bool {
+    tc::fence_async_smem();
+    tc::fence_before();
+    __syncthreads();
+    if (t == 0) {
+      tc::fence_after();
+      issue();
+      tc::commit(bar);
+    }
+    const bool to = !tc::mbar_wait(bar, phase);
+    phase ^= 1;
+    if (__syncthreads_or(to)) return false;
+    tc::fence_after();
+    return true;
+  };
+  while (true) {
+    const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi, order, n_valid, offs, xrows);
+    if (!__syncthreads_or(active)) break;
+    const int i = cur.base + lane;
+    float p[4] = {0.f, 0.f, 0.f, 0.f};
+    bool valid = false;
+    if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
+    if (D == 4) p[3] = a.t;
+    if (cur.xrow >= 0) {  // stored rows (warp-uniform branch)
+      const uint4* src = xstore + (size_t)(cur.xrow + i) * (IN / 8);
+      if (pre_ok) {
+#pragma unroll
+        for (int j = 0; j < IN / 8; ++j) xr[j] = xn[j];
+      } else if (valid) {
+#pragma unroll
+        for (int j = 0; j < IN / 8; ++j) xr[j] = __ldcs(src + j);
+      }
+#pragma unroll
+      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sA, t, j, valid ? xr[j] : make_uint4(0u, 0u, 0u, 0u));
+      pre_ok = cur.base + 32 < cur.rec.count;
+      if (pre_ok && i + 32 < cur.rec.count) {
+#pragma unroll
+        for (int j = 0; j < IN / 8; ++j) xn[j] = __ldcs(src + 32 * (IN / 8) + j);
+      }
+    } else {
+      pre_ok = false;
+      encode_row<D, F>(grid, table, p, valid, sA, t);
+    }
+    // layer 0: h1 = X W0^T
+    bool ok = run_phase([&] {
+#pragma unroll
+      for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_k(sW_a, q), id_fwd, q > 0);
+    });
+    if (!ok) {
+      timed_out = true;
+      break;
+    }
+    // keep the X row for the last phase, then A1 = relu(h1) replaces it
+#pragma unroll
+    for (int j = 0; j < IN / 8; ++j) xr[j] = *reinterpret_cast<const uint4*>(sA + tc::sw128(t, j));
+    uint32_t m1lo = 0, m1hi = 0;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(my_lanes + 16 * c, h);
+      tc::tmem_wait_ld();
+      float v[8], u[8];
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        v[q] = fmaxf(h[q], 0.f);
+        u[q] = fmaxf(h[8 + q], 0.f);
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const uint32_t bit = h[q] > 0.f ? 1u : 0u;
+        const int col = 16 * c + q;
+        if (col < 32) m1lo |= bit << col; else m1hi |= bit << (col - 32);
+      }
+      tc::st_chunk_bf16(sA, t, 2 * c, v);
+      tc::st_chunk_bf16(sA, t, 2 * c + 1, u);
+    }
+    // layer 1: h2 = A1 W1^T
+    ok = run_phase([&] {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_k(sW_a + kWTile, q), id_fwd, q > 0);
+    });
+    if (!ok) {
+      timed_out = true;
+      break;
+    }
+    float z = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(my_lanes + 16 * c, h);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int q = 0; q < 16; ++q) z = fmaf(sWout[16 * c + q], fmaxf(h[q], 0.f), z);
+    }
+    const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
+    // second pass over h2: the w_out gradient and G2 = dz * w_out * 1[h2 > 0]
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(my_lanes + 16 * c, h);
+      tc::tmem_wait_ld();
+      float v[16], g[16];
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        v[q] = dz * fmaxf(h[q], 0.f);
+        g[q] = h[q] > 0.f ? dz * sWout[16 * c + q] : 0.f;
+      }
+      tc::st_chunk_bf16(sG, t, 2 * c, g);
+      tc::st_chunk_bf16(sG, t, 2 * c + 1, g + 8);
+      float r8[8], r4[4], r2[2], r1[1];
+      detail::rs_step<8>(v, r8, lane, 16);
+      detail::rs_step<4>(r8, r4, lane, 8);
+      detail::rs_step<2>(r4, r2, lane, 4);
+      detail::rs_step<1>(r2, r1, lane, 2);
+      dwacc[c] += r1[0] + __shfl_xor_sync(0xffffffffu, r1[0], 1);
+    }
+    // dA1 = G2 W1 (transient); dW1 += [G2; 0]^T A1 (lanes 0..63 of [64, 128))
+    ok = run_phase([&] {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(sG_a, q), tc::desc_mn(sW_a + kWTile, q, kWTile), id_dA, q > 0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        tc::mma(tm + 64, tc::desc_mn(sG_a, q, sZ_a - sG_a), tc::desc_mn(sA_a, q, kTile), id_dW, (q > 0) | wacc);
+    });
+    if (!ok) {
+      timed_out = true;
+      break;
+    }
+    wacc = 1;
+    // G1 = dA1 * 1[h1 > 0] replaces A1; X goes to the G2 slot
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+      float h[16];
+      tc::tmem_ld16(my_lanes + 16 * c, h);
+      tc::tmem_wait_ld();
+#pragma unroll
+      for (int q = 0; q < 16; ++q) {
+        const int col = 16 * c + q;
+        const uint32_t bit = col < 32 ? (m1lo >> col) & 1u : (m1hi >> (col - 32)) & 1u;
+        h[q] = bit ? h[q] : 0.f;
+      }
+      tc::st_chunk_bf16(sA, t, 2 * c, h);
+      tc::st_chunk_bf16(sA, t, 2 * c + 1, h + 8);
+    }
+#pragma unroll
+    for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sG, t, j, xr[j]);
+    // dX = G1 W0 (transient); dW0 += [0; G1]^T X (lanes 64..127 of [64, 64 + IN))
+    ok = run_phase([&] {
+#pragma unroll
+      for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_mn(sW_a, q, kWTile), id_dX, q > 0);
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        tc::mma(tm + 64, tc::desc_mn(sZ_a, q, sA_a - sZ_a), tc::desc_mn(sG_a, q, kTile), id_dW0, 1u);
+    });
+    if (!ok) {
+      timed_out = true;
+      break;
+    }
+    {
+      float* dst = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
+#pragma unroll
+      for (int c = 0; c < IN / 16; ++c) {
+        float dx[16];
+        tc::tmem_ld16(my_lanes + 16 * c, dx);  // warp-collective: every lane loads
+        tc::tmem_wait_ld();
+        if (valid) {
+#pragma unroll
+          for (int k = 0; k < 16 / F; ++k) {
+            const int l = c * (16 / F) + k;  // level
+            if constexpr (F == 2)
+              __stcs(reinterpret_cast<float2*>(dst + l * slots * F), make_float2(dx[2 * k], dx[2 * k + 1]));
+            else
+              __stcs(reinterpret_cast<float4*>(dst + l * slots * F),
+                     make_float4(dx[4 * k], dx[4 * k + 1], dx[4 * k + 2], dx[4 * k + 3]));
+          }
+        }
+      }
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (active) cur.base += 32;
+  }
+  if (timed_out) {
+    if (t == 0) atomicOr(err, 2u);
+    tc::mbar_wait(bar, phase);  // let the MMAs in flight retire (bounded) before freeing TMEM
+  } else if (wacc) {
+    tc::fence_after();
+    if (warp < 2) {  // dW1 rows o = t in lanes 0..63
+      float v[64];
+      ld64(my_lanes + 64, v);
+      float* dst = W_grad + 64 * IN + t * 64;
+#pragma unroll
+      for (int j = 0; j < 64; ++j) atomicAdd(dst + j, v[j]);
+    } else {  // dW0 rows o = t - 64 in lanes 64..127
+      float v[IN];
+#pragma unroll
+      for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, v + 16 * c);
+      tc::tmem_wait_ld();
+      float* dst = W_grad + (t - 64) * IN;
+#pragma unroll
+      for (int j = 0; j < IN; ++j) atomicAdd(dst + j, v[j]);
+    }
+  }
+  if (!(lane & 1)) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) red[warp * 64 + 16 * c + (lane >> 1)] = dwacc[c];
+  }
+  tc::fence_before();
+  __syncthreads();
+  if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
+  if (warp == 0) {
+    tc::fence_after();
+    tc::tmem_dealloc(tm, 128);
+  }
+}
+
 // Applies staged encoding gradients of the rays with scheduling index in
 // [lo, hi) to the fp32 gradient table, levels [l0, l1) only: a pass touches a
 // slice of the gradient table small enough to stay in L2.  Warp per 32
@@ -652,7 +938,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
                     ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
                                                 (int)ceil_div(a.num_rays, 4)))
                     : std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * wgs)));
-  int blocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
+  int blocks = std::max(1, std::min<int>(std::min(tune.backward_blocks_per_sm, 2) * sms, (int)ceil_div(a.num_rays, 4)));
   if (a.max_blocks > 0) {
     fblocks = std::min(fblocks, a.max_blocks);
     blocks = std::min(blocks, a.max_blocks);
@@ -725,6 +1011,11 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   }
   auto kb = bwd_mixed_kernel<D, F, H, true>;
   cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+  // two hidden layers: the lean kernel, up to three blocks per SM
+  constexpr bool kLean = H == 2;
+  const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4;
+  const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
+  if constexpr (kLean) set_smem(bwd_lean_kernel<D, F>, lsmem, false);
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
@@ -736,8 +1027,13 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor")) return rc;
     {
       ProfScope ps(kProfBackward, s);
-      kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                            W_grad, (int)lo, hi, stage, slots, order, L.offs, L.xstore, L.xcap);
+      if constexpr (kLean)
+        bwd_lean_kernel<D, F><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters,
+                                                                  out_act, W_grad, (int)lo, hi, stage, slots, order,
+                                                                  L.offs, L.xstore, L.xcap);
+      else
+        kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+                                              W_grad, (int)lo, hi, stage, slots, order, L.offs, L.xstore, L.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
