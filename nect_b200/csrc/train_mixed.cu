@@ -603,17 +603,17 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   }
 }
 
-// Lean staged backward for two hidden layers: 128 TMEM columns and 66 KB of
+// Lean staged backward for two hidden layers: 128 TMEM columns and 68 KB of
 // shared memory per block, so three blocks (12 warps) share an SM.
 //   TMEM: [0, 64) the transient result of every phase; [64, 128) the weight
 //   gradients, dW1 in lanes 0..63 and dW0 in lanes 64..127.  Both products
-//   are M = 128 MMAs whose A operand is a G tile and a zero tile: dW1 =
-//   [G2; 0]^T A1 writes its rows to lanes 0..63 and adds exactly 0 to lanes
-//   64..127, dW0 = [0; G1]^T X the reverse.  The first tile's dW1 product
-//   (accumulate off) clears the whole region before dW0 first adds to it.
-//   Shared memory: W0, W1 | G2 slot | zero tile | A1 slot.  X is written to
-//   the A1 slot for layer 0, read back into registers before A1 replaces it,
-//   and written to the G2 slot (free once dW1 is done) for the last phase.
+//   are M = 128 MMAs whose A operand is a G tile and zeros: dW1 = [G2; 0]^T
+//   A1 writes its rows to lanes 0..63 and adds exactly 0 to lanes 64..127,
+//   dW0 = [0; G1]^T X the reverse.  The first tile's dW1 product (accumulate
+//   off) clears the whole region before dW0 first adds to it.  The zero half
+//   of every K step (16 rows of 64 bf16, 2 KB) is one 2 KB zero block, which
+//   each step reaches through its own leading-byte offset.
+//   Shared memory: W0, W1 | G2 | zero block | A1, then G1 | X.
 //   Accumulator rows are read 16 columns at a time; the w_out gradient is a
 //   16-column butterfly reduce-scatter per chunk.
 template <int D, int F>
@@ -632,11 +632,13 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   const uint32_t xrows = xstore ? min(xcap, ctrl[7]) : 0u;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
+  constexpr uint32_t kZero = 2048;    // one K step of a 64-element MN block
   uint8_t* sW = base;                 // W0, W1
-  uint8_t* sG = sW + H * kWTile;      // G2, later X
-  uint8_t* sZ = sG + kTile;           // zeros
-  uint8_t* sA = sZ + kTile;           // X, then A1, then G1
-  float* sWout = reinterpret_cast<float*>(sA + kTile);
+  uint8_t* sG = sW + H * kWTile;      // G2
+  uint8_t* sZ = sG + kTile;           // zeros (1024-aligned)
+  uint8_t* sA = sZ + kZero;           // A1, then G1
+  uint8_t* sX = sA + kTile;           // X
+  float* sWout = reinterpret_cast<float*>(sX + kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
@@ -645,7 +647,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   stage_mixed_weights<IN, H>(W, sW, sWout);
   {
     uint4* z = reinterpret_cast<uint4*>(sZ);
-    for (int e = t; e < (int)(kTile / 16); e += kMixThreads) z[e] = make_uint4(0u, 0u, 0u, 0u);
+    for (int e = t; e < (int)(kZero / 16); e += kMixThreads) z[e] = make_uint4(0u, 0u, 0u, 0u);
   }
   if (warp == 0) {
     tc::tmem_alloc(tslot, 128);
@@ -659,6 +661,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   const uint32_t tm = *tslot;
   const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
   const uint32_t sG_a = tc::smem_u32(sG), sZ_a = tc::smem_u32(sZ), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
+  const uint32_t sX_a = tc::smem_u32(sX);
   constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
   constexpr uint32_t id_dA = tc::idesc_bf16(128, 64, false, true);
   constexpr uint32_t id_dW = tc::idesc_bf16(128, 64, true, true);
@@ -668,8 +671,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   uint32_t phase = 0;
   uint32_t wacc = 0;  // the first tile's dW1 product starts the accumulators
   float dwacc[4] = {0.f, 0.f, 0.f, 0.f};  // w_out gradient, column 16c + (lane >> 1) of chunk c
-  uint4 xr[IN / 8];                       // this thread's X row (current tile)
-  uint4 xn[IN / 8];                       // the next chunk's stored row, prefetched
+  uint4 xn[IN / 8];                       // the stored row of this thread's sample (prefetched a tile ahead)
   bool pre_ok = false;
   RayCursor cur;
   bool timed_out = false;
@@ -698,15 +700,12 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
     if (D == 4) p[3] = a.t;
     if (cur.xrow >= 0) {  // stored rows (warp-uniform branch)
       const uint4* src = xstore + (size_t)(cur.xrow + i) * (IN / 8);
-      if (pre_ok) {
+      if (!pre_ok && valid) {
 #pragma unroll
-        for (int j = 0; j < IN / 8; ++j) xr[j] = xn[j];
-      } else if (valid) {
-#pragma unroll
-        for (int j = 0; j < IN / 8; ++j) xr[j] = __ldcs(src + j);
+        for (int j = 0; j < IN / 8; ++j) xn[j] = __ldcs(src + j);
       }
 #pragma unroll
-      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sA, t, j, valid ? xr[j] : make_uint4(0u, 0u, 0u, 0u));
+      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sX, t, j, valid ? xn[j] : make_uint4(0u, 0u, 0u, 0u));
       pre_ok = cur.base + 32 < cur.rec.count;
       if (pre_ok && i + 32 < cur.rec.count) {
 #pragma unroll
@@ -714,20 +713,17 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       }
     } else {
       pre_ok = false;
-      encode_row<D, F>(grid, table, p, valid, sA, t);
+      encode_row<D, F>(grid, table, p, valid, sX, t);
     }
     // layer 0: h1 = X W0^T
     bool ok = run_phase([&] {
 #pragma unroll
-      for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_k(sW_a, q), id_fwd, q > 0);
+      for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sX_a, q), tc::desc_k(sW_a, q), id_fwd, q > 0);
     });
     if (!ok) {
       timed_out = true;
       break;
     }
-    // keep the X row for the last phase, then A1 = relu(h1) replaces it
-#pragma unroll
-    for (int j = 0; j < IN / 8; ++j) xr[j] = *reinterpret_cast<const uint4*>(sA + tc::sw128(t, j));
     uint32_t m1lo = 0, m1hi = 0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
@@ -794,15 +790,16 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
 #pragma unroll
       for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(sG_a, q), tc::desc_mn(sW_a + kWTile, q, kWTile), id_dA, q > 0);
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
-        tc::mma(tm + 64, tc::desc_mn(sG_a, q, sZ_a - sG_a), tc::desc_mn(sA_a, q, kTile), id_dW, (q > 0) | wacc);
+      for (int q = 0; q < 8; ++q)  // second M block: the zero block, for every K step
+        tc::mma(tm + 64, tc::desc_mn(sG_a, q, sZ_a - (sG_a + 2048u * q)), tc::desc_mn(sA_a, q, kTile), id_dW,
+                (q > 0) | wacc);
     });
     if (!ok) {
       timed_out = true;
       break;
     }
     wacc = 1;
-    // G1 = dA1 * 1[h1 > 0] replaces A1; X goes to the G2 slot
+    // G1 = dA1 * 1[h1 > 0] replaces A1
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
       float h[16];
@@ -817,15 +814,14 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       tc::st_chunk_bf16(sA, t, 2 * c, h);
       tc::st_chunk_bf16(sA, t, 2 * c + 1, h + 8);
     }
-#pragma unroll
-    for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sG, t, j, xr[j]);
     // dX = G1 W0 (transient); dW0 += [0; G1]^T X (lanes 64..127 of [64, 64 + IN))
     ok = run_phase([&] {
 #pragma unroll
       for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_mn(sW_a, q, kWTile), id_dX, q > 0);
 #pragma unroll
-      for (int q = 0; q < 8; ++q)
-        tc::mma(tm + 64, tc::desc_mn(sZ_a, q, sA_a - sZ_a), tc::desc_mn(sG_a, q, kTile), id_dW0, 1u);
+      for (int q = 0; q < 8; ++q)  // first M block: the zero block; second: K step q of G1
+        tc::mma(tm + 64, tc::desc_sw128(sZ_a, sA_a + 2048u * q - sZ_a, 1024u), tc::desc_mn(sX_a, q, kTile), id_dW0,
+                1u);
     });
     if (!ok) {
       timed_out = true;
@@ -1013,7 +1009,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   // two hidden layers: the lean kernel, up to three blocks per SM
   constexpr bool kLean = H == 2;
-  const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 64 * 4 + 64 + 4 * 64 * 4;
+  const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 2048 + 64 * 4 + 64 + 4 * 64 * 4;
   const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if constexpr (kLean) set_smem(bwd_lean_kernel<D, F>, lsmem, false);
   auto ks = scatter_stage_kernel<D, F>;
