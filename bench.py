@@ -336,7 +336,19 @@ def main():
     if not args.no_autotune and args.precision == "mixed":   # the tunables belong to the mixed path
         from nect_b200 import autotune
 
+        # every rank tunes on its own GPU without the gradient all-reduce (the
+        # search may take different numbers of steps on different ranks, and a
+        # collective needs all of them), then all ranks take rank 0's choice
+        trainer.data_parallel = False
         tuning = autotune.tune(trainer, make_step_batch, steps=3, warmup=2)
+        trainer.data_parallel = world > 1
+        if world > 1:
+            import torch.distributed as dist
+
+            chosen = [tuning]
+            dist.broadcast_object_list(chosen, src=0)
+            tuning = chosen[0]
+            autotune.set_tuning(tuning)
     for k in range(args.warmup):
         trainer.step(make_step_batch(k))
     torch.cuda.synchronize()
