@@ -215,11 +215,12 @@ def collect_profile():
     from nect_b200 import _lib
     import ctypes
 
-    n = (ctypes.c_int32 * 8)()
-    ms = (ctypes.c_double * 8)()
+    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "scatter", "ray_order",
+             "time_slice"]
+    n = (ctypes.c_int32 * len(names))()
+    ms = (ctypes.c_double * len(names))()
     _lib.lib.nectb_profile_collect(ctypes.addressof(n), ctypes.addressof(ms))
-    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "scatter", "ray_order"]
-    return {names[i]: (int(n[i]), float(ms[i])) for i in range(8) if n[i]}
+    return {names[i]: (int(n[i]), float(ms[i])) for i in range(len(names)) if n[i]}
 
 
 def valid_samples(trainer, batches) -> int:

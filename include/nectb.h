@@ -354,10 +354,12 @@ int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq
  * on the launch stream around each kernel (off by default).  Slots:
  * 0 ray preparation, 1 forward, 2 backward, 3 Adam, 4 sampling, 5 model
  * forward and queries, 6 staged gradient scatter, 7 ray ordering of the
- * staged backward (three launches timed as one).  nectb_profile_collect waits for the recorded events, adds their
- * durations and returns per slot the launch count and total milliseconds.
- * No counterpart in the reference, which has no profiler. */
-#define NECTB_PROFILE_SLOTS 8
+ * staged backward (three launches timed as one), 8 time slice of a 4D grid
+ * and the spread of its gradient.  nectb_profile_collect waits for the
+ * recorded events, adds their durations and returns per slot the launch
+ * count and total milliseconds.  No counterpart in the reference, which has
+ * no profiler. */
+#define NECTB_PROFILE_SLOTS 9
 int nectb_profile_enable(int32_t enable);
 int nectb_profile_collect(int32_t* launches, double* total_ms);
 
@@ -376,11 +378,15 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * staging is sized for (nectb_train_staging_bytes, 1..64), the largest fp32
  * gradient slice one scatter pass covers, and the samples-per-cell
  * thresholds above which runs of samples along a ray are merged before their
- * reductions (3D and 4D grids).  Results do not depend on these beyond fp32
- * reassociation; the Python autotuner (nect_b200.autotune) picks them per
- * workload.  nectb_set_tuning validates and applies to steps issued after it
- * returns; defaults: 4, 3, 0, 4, 48 MiB, 1.0, 3.0.  No reference
- * counterpart. */
+ * reductions (3D and 4D grids), and time_slice: 1 lets a mixed 4D training
+ * step with staging interpolate the fp16 table at the batch's t once (a 3D
+ * slice per level, fp16) and run the 3D kernels on it, the gradient being
+ * spread back to the two time vertices afterwards; the slice's fp16 rounding
+ * lies below the bf16 rounding of the MLP input.  The other settings change
+ * results by fp32 reassociation only; the Python autotuner
+ * (nect_b200.autotune) picks them per workload.  nectb_set_tuning validates
+ * and applies to steps issued after it returns; defaults: 4, 3, 0, 4,
+ * 48 MiB, 1.0, 3.0, 1.  No reference counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;
   int32_t backward_blocks_per_sm;
@@ -389,6 +395,7 @@ typedef struct NectbTuning {
   int64_t scatter_group_bytes;
   float run_threshold_3d;
   float run_threshold_4d;
+  int32_t time_slice;
 } NectbTuning;
 int nectb_get_tuning(NectbTuning* tuning);
 int nectb_set_tuning(const NectbTuning* tuning);

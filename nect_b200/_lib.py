@@ -102,6 +102,7 @@ class NectbTuning(ctypes.Structure):
         ("scatter_group_bytes", c_i64),
         ("run_threshold_3d", c_f32),
         ("run_threshold_4d", c_f32),
+        ("time_slice", c_int),
     ]
 
 

@@ -101,7 +101,7 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
 namespace nectb {
 namespace {
 std::mutex g_tuning_mu;
-NectbTuning g_tuning = {4, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f};
+NectbTuning g_tuning = {4, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1};
 }  // namespace
 
 NectbTuning current_tuning() {
@@ -130,6 +130,7 @@ extern "C" int nectb_set_tuning(const NectbTuning* t) {
   NECTB_REQUIRE(t->run_threshold_3d >= 0.f && t->run_threshold_3d <= 64.f && t->run_threshold_4d >= 0.f &&
                     t->run_threshold_4d <= 64.f,
                 "run thresholds must be in [0, 64]");
+  NECTB_REQUIRE(t->time_slice == 0 || t->time_slice == 1, "time_slice must be 0 or 1");
   std::lock_guard<std::mutex> lk(g_tuning_mu);
   g_tuning = *t;
   return NECTB_OK;

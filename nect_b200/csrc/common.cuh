@@ -52,7 +52,8 @@ enum {
   kProfSample = 4,
   kProfModel = 5,
   kProfScatter = 6,
-  kProfOrder = 7
+  kProfOrder = 7,
+  kProfSlice = 8
 };
 class ProfScope {
  public:

@@ -196,8 +196,13 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   const size_t row_bytes = (size_t)grid->n_levels * grid->n_features * 2;
   const size_t rows = std::min<size_t>({(size_t)num_rays * num_points_per_ray, kEncodingStoreCap / row_bytes,
                                         (size_t)0xffffffffu});
-  return order_bytes(num_rays, P) + staged_round_bytes(num_rays, current_tuning().staged_rounds, per_ray) + 256 +
-         align256(rows * row_bytes);
+  const NectbTuning tune = current_tuning();
+  size_t bytes = order_bytes(num_rays, P) + staged_round_bytes(num_rays, tune.staged_rounds, per_ray) + 256 +
+                 align256(rows * row_bytes);
+  GridDev g;
+  if (tune.time_slice && grid->n_dims == 4 && make_grid_dev(grid, &g))
+    bytes += slice_bytes(g) + 256;  // the time slice and its gradient
+  return bytes;
 }
 
 extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,

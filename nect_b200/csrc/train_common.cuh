@@ -3,6 +3,7 @@
 // scheduler, sample regeneration and the workspace layout.
 #pragma once
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 
 #include "common.cuh"
@@ -158,6 +159,67 @@ inline StageLayout stage_layout(const Workspace& ws, int R, int P, int S, size_t
     L.xcap = 0;
   }
   return L;
+}
+
+// Time slice of a 4D grid at the batch's t (mixed training).  Along t a
+// level's 16-corner interpolation is a blend of two time vertices with the
+// same weights for every sample of the batch, and the vertices' entries are
+// the 3D vertex's entry XOR a per-level constant (hashed levels: the hash is
+// an XOR of per-axis terms, masked) or plus a per-level offset (dense levels:
+// t is the outermost stride).  So per level
+//   slice[k] = w0 * table[k ^ c0] + w1 * table[k ^ c1]   (hashed)
+//   slice[k] = w0 * table[k + c0] + w1 * table[k + c1]   (dense, k < x*y*z vertices)
+// and the 3D view g3 of the grid (same resolutions, strides and hash, slice
+// offsets) indexes it: the 3D kernels then gather 8 corners instead of 16.
+// Gradients reduced into a slice-shaped table g are spread back by
+//   dtable[e] += w0 * g[e ^ c0] + w1 * g[e ^ c1]          (hashed; conflict-free)
+//   dtable[k + c0] += w0 * g[k], dtable[k + c1] += w1 * g[k]  (dense)
+struct TimeSlice {
+  GridDev g3;
+  int64_t off4[NECTB_MAX_LEVELS];    // the 4D level offsets
+  int64_t n_real[NECTB_MAX_LEVELS];  // slice entries that exist (T, or the dense x*y*z vertices)
+  int64_t c0[NECTB_MAX_LEVELS], c1[NECTB_MAX_LEVELS];
+  float w0[NECTB_MAX_LEVELS], w1[NECTB_MAX_LEVELS];
+};
+
+// t -> vertex and weights exactly as level_corners computes them for axis 3.
+inline TimeSlice make_time_slice(const GridDev& g, float t) {
+  TimeSlice s;
+  s.g3 = g;
+  s.g3.n_dims = 3;
+  int64_t off = 0;
+  for (int l = 0; l < g.n_levels; ++l) {
+    s.off4[l] = g.offset[l];
+    const int r = g.res[l][3];
+    const float p = t * (float)r;
+    int ci = (int)std::floor(p);
+    ci = ci < 0 ? 0 : (ci > r - 1 ? r - 1 : ci);
+    const float f = p - (float)ci;
+    s.w0[l] = 1.f - f;
+    s.w1[l] = f;
+    const bool hashed = (g.hashed_bits >> l) & 1u;
+    if (hashed) {
+      const uint32_t term = (uint32_t)ci * kPrime3;
+      s.c0[l] = (int64_t)(term & g.hash_mask);
+      s.c1[l] = (int64_t)((term + kPrime3) & g.hash_mask);
+      s.n_real[l] = (int64_t)g.hash_mask + 1;
+    } else {
+      const int64_t s3 = g.stride[l][3];
+      s.c0[l] = (int64_t)ci * s3;
+      s.c1[l] = (int64_t)(ci + 1) * s3;
+      s.n_real[l] = s3;
+    }
+    s.g3.offset[l] = off;
+    off += hashed ? s.n_real[l] : (s.n_real[l] + 7) / 8 * 8;
+  }
+  s.g3.total_entries = off;
+  return s;
+}
+
+// Bytes of a 4D grid's time slice (fp16) and its fp32 gradient, for one step.
+inline size_t slice_bytes(const GridDev& g) {
+  const int64_t n3 = make_time_slice(g, 0.f).g3.total_entries;
+  return align256((size_t)n3 * g.n_features * 2) + align256((size_t)n3 * g.n_features * 4);
 }
 
 // Warp per ray: set-up, sample count (warp ballot), measured value, scale;

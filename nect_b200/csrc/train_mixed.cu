@@ -913,6 +913,60 @@ scatter_stage_kernel(GridDev grid, TrainArgs a, const RayRec* __restrict__ recs,
   }
 }
 
+// Builds the fp16 time slice of every level (grid y = level): slice entry k
+// blends the entries of the two time vertices; dense levels' padding is zero.
+template <int F>
+__global__ void time_slice_kernel(TimeSlice s, const __half* __restrict__ t4, __half* __restrict__ t3) {
+  const int l = blockIdx.y;
+  const bool hashed = (s.g3.hashed_bits >> l) & 1u;
+  const int64_t n = (l + 1 < s.g3.n_levels ? s.g3.offset[l + 1] : s.g3.total_entries) - s.g3.offset[l];
+  const float w0 = s.w0[l], w1 = s.w1[l];
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    __half* dst = t3 + (s.g3.offset[l] + k) * F;
+    if (k >= s.n_real[l]) {
+#pragma unroll
+      for (int f = 0; f < F; ++f) dst[f] = __float2half_rn(0.f);
+      continue;
+    }
+    const int64_t e0 = hashed ? (int64_t)((uint64_t)k ^ (uint64_t)s.c0[l]) : k + s.c0[l];
+    const int64_t e1 = hashed ? (int64_t)((uint64_t)k ^ (uint64_t)s.c1[l]) : k + s.c1[l];
+    const __half* a = t4 + (s.off4[l] + e0) * F;
+    const __half* b = t4 + (s.off4[l] + e1) * F;
+#pragma unroll
+    for (int f = 0; f < F; ++f) dst[f] = __float2half_rn(fmaf(w0, __half2float(a[f]), w1 * __half2float(b[f])));
+  }
+}
+
+// Adds the slice-shaped gradient g3 to the 4D gradient table at the two time
+// vertices (grid y = level).  Hashed levels: one thread per 4D entry gathers
+// its two slice entries (an XOR is its own inverse, so no two threads write
+// the same entry); dense levels: one thread per slice entry writes its two
+// vertices, which lie in different t slabs.
+template <int F>
+__global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, float* __restrict__ g4) {
+  const int l = blockIdx.y;
+  const bool hashed = (s.g3.hashed_bits >> l) & 1u;
+  const int64_t n = s.n_real[l];
+  const float w0 = s.w0[l], w1 = s.w1[l];
+  const float* src = g3 + s.g3.offset[l] * F;
+  float* dst = g4 + s.off4[l] * F;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    if (hashed) {
+      const float* a = src + (int64_t)((uint64_t)k ^ (uint64_t)s.c0[l]) * F;
+      const float* b = src + (int64_t)((uint64_t)k ^ (uint64_t)s.c1[l]) * F;
+#pragma unroll
+      for (int f = 0; f < F; ++f) dst[k * F + f] += fmaf(w0, a[f], w1 * b[f]);
+    } else {
+#pragma unroll
+      for (int f = 0; f < F; ++f) {
+        const float v = src[k * F + f];
+        dst[(k + s.c0[l]) * F + f] += w0 * v;
+        dst[(k + s.c1[l]) * F + f] += w1 * v;
+      }
+    }
+  }
+}
+
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
 // slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
 template <int D, int F, int H>
@@ -922,8 +976,48 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  (void)geo;
   const NectbTuning tune = current_tuning();
+  if constexpr (D == 4) {
+    // Training with staging: the 3D kernels on the time slice at the batch's t
+    // (queries and steps without staging room keep the 4D kernels).  The slice
+    // and its gradient sit at the end of the staging region.
+    const size_t sb = slice_bytes(grid);
+    if (tune.time_slice && args.max_blocks == 0 && ws.stage &&
+        ws.stage_bytes >= sb + order_bytes(args.num_rays, args.n_pixels) + (size_t(1) << 20)) {
+      const TimeSlice ts = make_time_slice(grid, args.t);
+      const int64_t n3 = ts.g3.total_entries;
+      Workspace ws3 = ws;
+      ws3.stage_bytes = (ws.stage_bytes - sb) & ~size_t(255);
+      __half* t3 = reinterpret_cast<__half*>(reinterpret_cast<char*>(ws.stage) + ws3.stage_bytes);
+      float* g3 = reinterpret_cast<float*>(reinterpret_cast<char*>(t3) + align256((size_t)n3 * F * 2));
+      int64_t max_level = 0;
+      for (int l = 0; l < grid.n_levels; ++l) max_level = std::max(max_level, ts.n_real[l] + 8);
+      const dim3 sgrid((unsigned)std::min<int64_t>(ceil_div(max_level, 256), 1024), (unsigned)grid.n_levels);
+      if (args.phase & kPhaseForward) {
+        {
+          ProfScope ps(kProfSlice, s);
+          time_slice_kernel<F><<<sgrid, 256, 0, s>>>(ts, table, t3);
+        }
+        if (int rc = launch_status("time_slice_kernel")) return rc;
+      }
+      const bool bwd = table_grad && (args.phase & kPhaseBackward);
+      if (bwd)
+        if (int rc = cuda_status(cudaMemsetAsync(g3, 0, (size_t)n3 * F * sizeof(float), s), "memset slice gradient"))
+          return rc;
+      if (int rc = run_mixed<3, F, H>(geo, ts.g3, t3, W, args, ws3, out_act, bwd ? g3 : nullptr, W_grad, y_pred,
+                                      loss, s))
+        return rc;
+      if (bwd) {
+        {
+          ProfScope ps(kProfSlice, s);
+          time_spread_kernel<F><<<sgrid, 256, 0, s>>>(ts, g3, table_grad);
+        }
+        if (int rc = launch_status("time_spread_kernel")) return rc;
+      }
+      return NECTB_OK;
+    }
+  }
+  (void)geo;
   TrainArgs a = args;
   a.run_threshold = D == 4 ? tune.run_threshold_4d : tune.run_threshold_3d;
   const size_t group_bytes = (size_t)tune.scatter_group_bytes;
