@@ -97,7 +97,7 @@ def test_model_forward_matches_oracle(cuda_device, n_dims, precision):
     assert torch.allclose(out, ref, rtol=1e-5, atol=1e-6), (out - ref).abs().max()
 
 
-def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=False, ws=None):
+def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=False, ws=None, t=0.45):
     from nect_b200.sampling import Geometry
     from nect_b200.trainer import RayBatch, Workspace, train_step
 
@@ -118,7 +118,7 @@ def run_train_case(n_dims, precision, loss, geom_kind="parallel", duplicates=Fal
     jitter = torch.rand(R, device="cuda") - 0.5
     det_off = torch.zeros(R, 2, device="cuda")
     proj = torch.rand(P, device="cuda")
-    angle, t = 0.7, 0.45
+    angle = 0.7
     maxd = geo.max_distance_traveled / S
     batch = RayBatch(perm=perm, start=start, num_rays=R, points_per_ray=S, angle=angle,
                      max_ray_distance_per_point=maxd, jitter=jitter, detector_offset=det_off, projection=proj, t=t)
@@ -230,8 +230,8 @@ def test_encoding_store_partial_and_absent(cuda_device, n_dims, duplicates, stor
     assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
 
 
-@pytest.mark.parametrize("duplicates", [False, True])
-def test_time_slice_matches_4d_kernels(cuda_device, duplicates):
+@pytest.mark.parametrize("duplicates,t", [(False, 0.45), (True, 0.45), (False, 0.0), (False, 1.0)])
+def test_time_slice_matches_4d_kernels(cuda_device, duplicates, t):
     """A 4D mixed step on the time slice at the batch's t (8-corner 3D
     kernels, gradients spread back to the two time vertices) against the same
     step on the 16-corner 4D kernels.  The slice is fp16, so its values carry
@@ -242,9 +242,11 @@ def test_time_slice_matches_4d_kernels(cuda_device, duplicates):
     oracle is test_fused_mixed_step_matches_oracle (4D, default tuning)."""
     from nect_b200.trainer import Workspace
 
-    (y1, L1, gt1, gm1), _ = run_train_case(4, "mixed", "l2", "cone", duplicates, ws=Workspace())
+    (y1, L1, gt1, gm1), (yo, Lo, gto, gmo) = run_train_case(4, "mixed", "l2", "cone", duplicates, ws=Workspace(), t=t)
     with tuning(time_slice=0):
-        (y2, L2, gt2, gm2), _ = run_train_case(4, "mixed", "l2", "cone", duplicates, ws=Workspace())
+        (y2, L2, gt2, gm2), _ = run_train_case(4, "mixed", "l2", "cone", duplicates, ws=Workspace(), t=t)
+    # t = 0 and t = 1 put the blend on the first and the last time vertex
+    assert cosine(gt1, gto) > 0.99 and rel_max(y1, yo) < 2e-2, (cosine(gt1, gto), rel_max(y1, yo))
     assert rel_max(y1, y2) < 1e-2, rel_max(y1, y2)
     assert abs(L1 - L2) <= 1e-2 * abs(L2)
     assert cosine(gt1, gt2) > 0.999 and cosine(gm1, gm2) > 0.999, (cosine(gt1, gt2), cosine(gm1, gm2))
