@@ -1099,13 +1099,15 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     }
     group_start[n_groups] = grid.n_levels;
   }
-  auto kb = bwd_mixed_kernel<D, F, H, true>;
-  cudaFuncSetAttribute(kb, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
-  // two hidden layers: the lean kernel, up to three blocks per SM
+  // tensor-core pass of a round: the lean kernel for two hidden layers (up to
+  // three blocks per SM), else the general one (two)
   constexpr bool kLean = H == 2;
   const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 2048 + 64 * 4 + 64 + 4 * 64 * 4;
   const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
-  if constexpr (kLean) set_smem(bwd_lean_kernel<D, F>, lsmem, false);
+  if constexpr (kLean)
+    set_smem(bwd_lean_kernel<D, F>, lsmem, false);
+  else
+    cudaFuncSetAttribute(bwd_mixed_kernel<D, F, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
@@ -1122,8 +1124,9 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
                                                                   out_act, W_grad, (int)lo, hi, stage, slots, order,
                                                                   L.offs, L.xstore, L.xcap);
       else
-        kb<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
-                                              W_grad, (int)lo, hi, stage, slots, order, L.offs, L.xstore, L.xcap);
+        bwd_mixed_kernel<D, F, H, true><<<blocks, kMixThreads, bsmem, s>>>(
+            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
+            order, L.offs, L.xstore, L.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
