@@ -2,7 +2,7 @@
 
 Stand-ins for the reference's data (its demo data sets are downloaded from
 Zenodo and its porous phantoms need porespy, neither available here), built to
-the shapes, sizes and value ranges of the BASELINE workloads:
+the shapes, sizes and value ranges of the benchmark workloads:
 
 * ``ellipsoid_phantom``: additive sum of seeded random ellipsoids in the unit
   cube (static parallel-beam workload, 128^3, 20 ellipsoids).

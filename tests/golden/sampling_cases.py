@@ -2,7 +2,7 @@
 
 Each case names one of the reference's four geometry structs with its
 constructor keywords (nect/sampling/ct_sampling.cu:650-749) and one call of
-``sample`` (:756-807).  They cover the BASELINE geometries (parallel unit
+``sample`` (:756-807).  They cover the benchmark geometries (parallel unit
 cube with a 128x128 detector; cone beam DSO 500 / DSD 1000 on a 512x512
 detector over a 256^3 volume), detector offsets and tilt, centre-of-rotation
 shifts, cylindrical clipping with top/bottom removal, non-uniform spacing,

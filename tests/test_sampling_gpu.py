@@ -61,7 +61,7 @@ def test_kernel_matches_reference_kernel(ref_module, mine, cuda_device, case):
 @pytest.mark.parametrize("geom,angles,S", [(CONE_C2, [0.0, 0.8, 2.6, 4.4], 512), (PAR_C1, [0.0, 1.0, 2.5], 256)],
                          ids=["cone_c2_full_projection", "parallel_c1_full_projection"])
 def test_full_projection_bit_exact(ref_module, mine, cuda_device, geom, angles, S):
-    """Every pixel of a BASELINE-size projection in one batch (R = P)."""
+    """Every pixel of a full-size benchmark projection in one batch (R = P)."""
     n = geom["nDetector"][0] * geom["nDetector"][1]
     perm = torch.randperm(n, device=cuda_device)
     for j, ang in enumerate(angles):
