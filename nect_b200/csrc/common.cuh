@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdint>
 #include <cstdio>
+#include <type_traits>
 #include <cuda_runtime.h>
 
 #include "../../include/nectb.h"
@@ -23,6 +24,22 @@ inline int cuda_status(cudaError_t e, const char* what) {
 inline int launch_status(const char* what) { return cuda_status(cudaGetLastError(), what); }
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
+
+// The model shapes the fused kernels are instantiated for: 16 levels of F = 2
+// or 4 features over D = 3 or 4 inputs, H = 2 or 3 hidden layers of 64.
+// Calls fn(integral_constant D, F, H) for a supported shape and returns its
+// result, else kUnsupportedShape.
+constexpr int kUnsupportedShape = -1000;
+template <typename Fn>
+inline int dispatch_shape(int D, int F, int H, Fn&& fn) {
+  using std::integral_constant;
+#define NECTB_SHAPE(d, f, h) \
+  if (D == d && F == f && H == h) return fn(integral_constant<int, d>{}, integral_constant<int, f>{}, integral_constant<int, h>{});
+  NECTB_SHAPE(3, 2, 2) NECTB_SHAPE(3, 2, 3) NECTB_SHAPE(3, 4, 2) NECTB_SHAPE(3, 4, 3)
+  NECTB_SHAPE(4, 2, 2) NECTB_SHAPE(4, 2, 3) NECTB_SHAPE(4, 4, 2) NECTB_SHAPE(4, 4, 3)
+#undef NECTB_SHAPE
+  return kUnsupportedShape;
+}
 
 // The current launch shapes and scheduling (nectb_set_tuning), copied under a lock.
 NectbTuning current_tuning();

@@ -143,23 +143,18 @@ int dispatch_encode(const GridDev& g, int dtype, const void* params, const float
   return set_error(NECTB_ERR_INVALID, "unsupported grid (n_dims %d, n_features %d)", g.n_dims, g.n_features);
 }
 
-// Instantiated for the configurations of the benchmark workloads: 16 levels of
-// 2 features with 2 hidden layers (3D and 4D) and 16 levels of 4 features with
-// 3 hidden layers (4D), fp32 or fp16 tables.
+// Instantiated for 16 levels of 2 or 4 features over 3 or 4 inputs with 2 or 3
+// hidden layers of 64 (dispatch_shape), fp32 or fp16 tables.
 int dispatch_model(const GridDev& g, int dtype, int H, const void* p, const float* W, const float* x, int64_t n,
                    float t, int act, int oact, float* sigma, cudaStream_t s) {
   const bool h = dtype == NECTB_F16;
   if (g.n_levels != 16) return set_error(NECTB_ERR_INVALID, "fused model paths need n_levels == 16");
   const int D = g.n_dims, F = g.n_features;
-  if (D == 3 && F == 2 && H == 2)
-    return h ? launch_model<3, 2, __half, 2>(g, p, W, x, n, t, act, oact, sigma, s)
-             : launch_model<3, 2, float, 2>(g, p, W, x, n, t, act, oact, sigma, s);
-  if (D == 4 && F == 2 && H == 2)
-    return h ? launch_model<4, 2, __half, 2>(g, p, W, x, n, t, act, oact, sigma, s)
-             : launch_model<4, 2, float, 2>(g, p, W, x, n, t, act, oact, sigma, s);
-  if (D == 4 && F == 4 && H == 3)
-    return h ? launch_model<4, 4, __half, 3>(g, p, W, x, n, t, act, oact, sigma, s)
-             : launch_model<4, 4, float, 3>(g, p, W, x, n, t, act, oact, sigma, s);
+  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
+    return h ? launch_model<d(), f(), __half, hl()>(g, p, W, x, n, t, act, oact, sigma, s)
+             : launch_model<d(), f(), float, hl()>(g, p, W, x, n, t, act, oact, sigma, s);
+  });
+  if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model forward: unsupported configuration (n_dims %d, n_features %d, "
                    "hidden %d, %s table)", D, F, H, h ? "fp16" : "fp32");
 }

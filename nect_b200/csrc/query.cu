@@ -333,31 +333,21 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
   if (mixed) {
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
     NECTB_REQUIRE(mlp->activation == NECTB_ACT_RELU, "mixed queries need ReLU hidden layers");
-    if (D == 3 && F == 2 && H == 2)
-      return launch_query_mixed<3, 2, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                         mlp->output_activation, max_blocks, s);
-    if (D == 4 && F == 2 && H == 2)
-      return launch_query_mixed<4, 2, 2>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                         mlp->output_activation, max_blocks, s);
-    if (D == 4 && F == 4 && H == 3)
-      return launch_query_mixed<4, 4, 3>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                         mlp->output_activation, max_blocks, s);
+    const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
+      return launch_query_mixed<d(), f(), h()>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                               mlp->output_activation, max_blocks, s);
+    });
+    if (rc != kUnsupportedShape) return rc;
   } else {
     const int act = mlp->activation, oact = mlp->output_activation;
     const bool h = grid->feature_dtype == NECTB_F16;
-    if (D == 3 && F == 2 && H == 2)
-      return h ? launch_query_plain<3, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                     counter, act, oact, max_blocks, s)
-               : launch_query_plain<3, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                    counter, act, oact, max_blocks, s);
-    if (D == 4 && F == 2 && H == 2)
-      return h ? launch_query_plain<4, 2, __half, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                     counter, act, oact, max_blocks, s)
-               : launch_query_plain<4, 2, float, 2>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                    counter, act, oact, max_blocks, s);
-    if (D == 4 && F == 4 && H == 3 && !h)
-      return launch_query_plain<4, 4, float, 3>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                                act, oact, max_blocks, s);
+    const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
+      return h ? launch_query_plain<d(), f(), __half, hl()>(g, grid_params, mlp_params, items, n_items,
+                                                            total_chunks, counter, act, oact, max_blocks, s)
+               : launch_query_plain<d(), f(), float, hl()>(g, grid_params, mlp_params, items, n_items, total_chunks,
+                                                           counter, act, oact, max_blocks, s);
+    });
+    if (rc != kUnsupportedShape) return rc;
   }
   return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, hidden %d)", D,
                    F, H);

@@ -1158,12 +1158,10 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
     return set_error(NECTB_ERR_INVALID, "mixed path: needs 16 levels, n_input 16 x n_features and width 64");
   const __half* tab = (const __half*)table;
   const int oact = mlp.output_activation;
-  if (D == 3 && F == 2 && H == 2)
-    return run_mixed<3, 2, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
-  if (D == 4 && F == 2 && H == 2)
-    return run_mixed<4, 2, 2>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
-  if (D == 4 && F == 4 && H == 3)  // the large 4D workload: 16 x 4 features, 3 x 64 MLP
-    return run_mixed<4, 4, 3>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
+    return run_mixed<d(), f(), h()>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  });
+  if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "mixed path: unsupported grid (n_dims %d, n_features %d, hidden %d)", D, F, H);
 }
 

@@ -255,7 +255,7 @@ struct WGrad {
   }
   __device__ __forceinline__ void add(const float* __restrict__ G, const float* __restrict__ A) {
     const int jb = threadIdx.x / IBLK, ib = threadIdx.x % IBLK;
-#pragma unroll 2
+#pragma unroll 1
     for (int t = 0; t < NT; t += 4) {
       float4 g[4], v[IB];
 #pragma unroll
@@ -281,6 +281,18 @@ struct WGrad {
       for (int b = 0; b < IB; ++b) atomicAdd(dst + (4 * jb + a) * K + ib * IB + b, acc[a][b]);
   }
 };
+
+// Whether the layer-0 weight-gradient tile stays in registers across the
+// sample-tile loop.  A thread carries 4 * (IN + (H - 1) * 64) / (NT / 16)
+// accumulators when every tile stays; the 3-layer MLP over 64 inputs (192 of
+// them, the kernel at the 255-register limit) measured wrong first-layer and
+// table gradients on B200 in that form, and exact ones when its layer-0 tile
+// is added to W_grad after every sample tile (4096 atomics per tile of NT
+// samples, about 64 per sample) and only the hidden-layer tiles stay.
+template <int IN, int H, int NT>
+__host__ __device__ constexpr bool carry_layer0() {
+  return 4 * (IN + (H - 1) * kWidth) / (NT / 16) <= 160;
+}
 
 template <int D, int F, int IN, int H, int NT>
 __global__ void __launch_bounds__(NT, 1)
@@ -370,6 +382,10 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     }
     __syncthreads();
     g0.add(G, sX);
+    if constexpr (!carry_layer0<IN, H, NT>()) {
+      g0.flush(W_grad);
+      g0.zero();
+    }
     // dX = W_0^T G_1 (W_0 is [64][IN] = M[j][i]) into G2, then scatter
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
     // per-sample atomics: the SIMT path is issue-bound and the run reduction's
@@ -378,7 +394,7 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     __syncthreads();
     base += 32;
   }
-  g0.flush(W_grad);
+  if constexpr (carry_layer0<IN, H, NT>()) g0.flush(W_grad);
 #pragma unroll
   for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
   const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
@@ -467,11 +483,15 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
     }
     __syncthreads();
     g0.add(G, sX);
+    if constexpr (!carry_layer0<IN, H, NT>()) {
+      g0.flush(W_grad);
+      g0.zero();
+    }
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
     scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, (int64_t)F * LD, LD, 0u, 0, grid.n_levels);
     __syncthreads();
   }
-  g0.flush(W_grad);
+  if constexpr (carry_layer0<IN, H, NT>()) g0.flush(W_grad);
 #pragma unroll
   for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
   const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
@@ -491,7 +511,9 @@ template <int D, int F, int H, typename T>
 int launch_model_bwd(const GridDev& grid, const void* table, const float* W, const float* x, int64_t n, float tval,
                      const float* dsigma, int act, int out_act, float* table_grad, float* W_grad, cudaStream_t s) {
   constexpr int IN = 16 * F;
-  constexpr int NT = 128;
+  // 64-thread tiles when 128 would not fit shared memory (3 hidden layers over 64 inputs)
+  constexpr int NT = (IN + (H + 2) * kWidth) * (128 + 4) * 4 + simt_weight_floats<IN, H, true>() * 4 > 227 * 1024
+                         ? 64 : 128;
   auto k = model_bwd_kernel<D, F, IN, H, NT, T>;
   const size_t smem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
   if (smem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "model backward needs %zu B of shared memory", smem);
@@ -556,12 +578,13 @@ int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void*
   const bool h = dtype == NECTB_F16;
   const int D = g.n_dims, F = g.n_features, H = mlp.n_hidden_layers;
   const int act = mlp.activation, oact = mlp.output_activation;
-  if (D == 3 && F == 2 && H == 2)
-    return h ? launch_model_bwd<3, 2, 2, __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s)
-             : launch_model_bwd<3, 2, 2, float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s);
-  if (D == 4 && F == 2 && H == 2)
-    return h ? launch_model_bwd<4, 2, 2, __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s)
-             : launch_model_bwd<4, 2, 2, float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad, W_grad, s);
+  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
+    return h ? launch_model_bwd<d(), f(), hl(), __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad,
+                                                        W_grad, s)
+             : launch_model_bwd<d(), f(), hl(), float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad,
+                                                       W_grad, s);
+  });
+  if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model backward: unsupported configuration (n_dims %d, n_features %d, "
                    "hidden %d)", D, F, H);
 }
@@ -572,14 +595,12 @@ int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
   (void)nW;
   const int D = grid.n_dims, F = grid.n_features, H = mlp.n_hidden_layers;
   const int act = mlp.activation, oact = mlp.output_activation;
-  if (D == 3 && F == 2 && H == 2)
-    return run_plain<3, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
-  if (D == 4 && F == 2 && H == 2)
-    return run_plain<4, 2, 2>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
-  if (D == 4 && F == 4 && H == 3)  // the large 4D workload: 16 x 4 features, 3 x 64 MLP
-    return run_plain<4, 4, 3>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
-  return set_error(NECTB_ERR_INVALID, "plain path supports 16x2 grids with 2 hidden layers and 16x4 4D grids with "
-                   "3 (got n_dims %d, n_features %d, hidden %d)", D, F, H);
+  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
+    return run_plain<d(), f(), h()>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+  });
+  if (rc != kUnsupportedShape) return rc;
+  return set_error(NECTB_ERR_INVALID, "plain path supports 16 levels of 2 or 4 features with 2 or 3 hidden layers "
+                   "(got n_dims %d, n_features %d, hidden %d)", D, F, H);
 }
 
 }  // namespace nectb
