@@ -114,7 +114,11 @@ typedef struct NectbHashGrid {
  * 115-135).  Weights are one fp32 buffer in PyTorch Linear layout
  * ([out][in]): W0 [width x n_input], W1..W_{H-1} [width x width],
  * W_out [1 x width].  compute_dtype NECTB_F32 runs the plain SIMT path;
- * NECTB_BF16 runs the tensor-core path (bf16 operands, fp32 accumulation). */
+ * NECTB_BF16 runs the tensor-core path (bf16 operands, fp32 accumulation).
+ * The fused model, training and query calls take width 64 and 2 or 3 hidden
+ * layers over a grid of 16 levels of 2 or 4 features (n_input 32 or 64) in
+ * 3D or 4D; hidden activation ReLU on the tensor-core path, ReLU, LeakyReLU
+ * or none on the SIMT path.  Other shapes return NECTB_ERR_INVALID. */
 typedef struct NectbMLP {
   int32_t n_input;
   int32_t n_hidden_layers;
