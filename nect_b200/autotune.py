@@ -86,6 +86,9 @@ def tune(trainer, make_batch, steps: int = 3, warmup: int = 2, space: dict | Non
     the best of ``reps`` runs and replaces the incumbent only when faster by
     more than ``margin``; the result is checked once more against the tuning
     the search started from, so timing noise cannot leave a slower choice."""
+    if getattr(trainer, "sharded", None) is not None:
+        raise ValueError("tune a trainer without the sharded optimizer: its steps are collectives, and the "
+                         "search takes a different number of steps on each rank")
     space = space or SPACE
     probe = make_batch(0)
     key = workload_key(trainer, probe.num_rays)

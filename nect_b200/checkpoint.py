@@ -35,7 +35,7 @@ from .trainer import Trainer
 
 def _adam_state(trainer: Trainer) -> dict:
     state = {}
-    for i, (m, v) in enumerate(((trainer.m_table, trainer.v_table), (trainer.m_mlp, trainer.v_mlp))):
+    for i, (m, v) in enumerate(trainer.optimizer_moments()):
         state[i] = {"step": torch.tensor(float(trainer.step_count)), "exp_avg": m.detach().clone(),
                     "exp_avg_sq": v.detach().clone()}
     group = {"lr": trainer.lr, "betas": tuple(trainer.betas), "eps": trainer.eps,
@@ -65,7 +65,13 @@ def _geometry_dict(geometry) -> dict:
 
 def save(run_dir: str | Path, model: _HashGridModel, trainer: Trainer | None = None, geometry=None,
          epoch: int = 0, angle: int = 0) -> Path:
-    """Write ``run_dir/model/{config.yaml, geometry.yaml, checkpoints/last.ckpt}``."""
+    """Write ``run_dir/model/{config.yaml, geometry.yaml, checkpoints/last.ckpt}``.
+
+    With a trainer whose optimizer is sharded over data-parallel ranks every
+    rank calls this (the Adam moments are gathered); rank 0 writes."""
+    adam = _adam_state(trainer) if trainer is not None else None
+    if trainer is not None and trainer.sharded is not None and trainer.sharded.rank != 0:
+        return Path(run_dir) / "model" / "checkpoints" / "last.ckpt"
     base = Path(run_dir) / "model"
     (base / "checkpoints").mkdir(parents=True, exist_ok=True)
     with open(base / "config.yaml", "w") as f:
@@ -76,8 +82,8 @@ def save(run_dir: str | Path, model: _HashGridModel, trainer: Trainer | None = N
     state = {"model": {k: v.detach().cpu() for k, v in model.state_dict().items()}, "epoch": epoch, "angle": angle}
     if trainer is not None:
         state["optim"] = {"state": {i: {k: (v.cpu() if torch.is_tensor(v) else v) for k, v in s.items()}
-                                    for i, s in _adam_state(trainer)["state"].items()},
-                          "param_groups": _adam_state(trainer)["param_groups"]}
+                                    for i, s in adam["state"].items()},
+                          "param_groups": adam["param_groups"]}
         state["lr_scheduler"] = {"lr": trainer.lr}
     path = base / "checkpoints" / "last.ckpt"
     torch.save(state, path)
@@ -119,10 +125,6 @@ def resume(path: str | Path, model: _HashGridModel, trainer: Trainer | None = No
     model.load_state_dict(data["model"])
     if trainer is not None and "optim" in data:
         st = data["optim"]["state"]
-        with torch.no_grad():
-            trainer.m_table.copy_(st[0]["exp_avg"])
-            trainer.v_table.copy_(st[0]["exp_avg_sq"])
-            trainer.m_mlp.copy_(st[1]["exp_avg"])
-            trainer.v_mlp.copy_(st[1]["exp_avg_sq"])
+        trainer.load_optimizer_moments([(st[i]["exp_avg"], st[i]["exp_avg_sq"]) for i in (0, 1)])
         trainer.step_count = int(float(st[0]["step"]))
     return {"epoch": data.get("epoch", 0), "angle": data.get("angle", 0)}

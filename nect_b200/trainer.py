@@ -254,6 +254,10 @@ class FusedRayLoss(torch.autograd.Function):
 def adam_step(param: torch.Tensor, grad: torch.Tensor, m: torch.Tensor, v: torch.Tensor, step: int, lr: float,
               betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0, half: torch.Tensor | None = None,
               zero_grad: bool = True):
+    n = param.numel()
+    if grad.numel() != n or m.numel() != n or v.numel() != n or (half is not None and half.numel() != n):
+        raise ValueError(f"adam_step: parameter, gradient and moments differ in size ({n}, {grad.numel()}, "
+                         f"{m.numel()}, {v.numel()})")
     rc = _lib.lib.nectb_adam_step(param.data_ptr(), grad.data_ptr(), m.data_ptr(), v.data_ptr(), param.numel(),
                                   float(lr), float(betas[0]), float(betas[1]), float(eps), float(weight_decay),
                                   int(step), half.data_ptr() if half is not None else None, 1 if zero_grad else 0,
@@ -278,6 +282,104 @@ def reduce_gradients(grads, group=None) -> None:
         g.div_(world)
 
 
+class ShardedAdam:
+    """Data-parallel Adam with the optimizer state sharded over the ranks.
+
+    The reference averages gradients with one DDP all-reduce and runs the full
+    Adam step on every rank (base_trainer.py:106-112).  Here each parameter
+    buffer is cut into ``world`` contiguous shards of ``chunk`` elements (the
+    last padded):
+
+    1. the gradient buffer (padded, ``world * chunk``) is reduce-scattered, so
+       rank r receives the summed shard r, which is divided by the world size;
+    2. rank r runs Adam on shard r only, with moments held for that shard;
+    3. the updated shards are all-gathered into every rank's parameters (and
+       the fp16 table copy refreshed from them).
+
+    The collectives move the bytes of one all-reduce; Adam's HBM traffic and
+    the moment memory per rank fall by the world size.  Results equal the
+    all-reduce step's: the sums are the same per element and Adam is
+    elementwise.  ``adam`` is the update applied to each shard (the CUDA
+    kernel behind ``adam_step`` unless a caller passes another)."""
+
+    ALIGN = 8  # shard starts on 32-byte boundaries
+
+    def __init__(self, params, group=None, adam=None):
+        import torch.distributed as dist
+
+        if not dist.is_available() or not dist.is_initialized():
+            raise RuntimeError("ShardedAdam needs an initialised torch.distributed process group")
+        self.group = group
+        self.world = dist.get_world_size(group)
+        self.rank = dist.get_rank(group)
+        self.params = list(params)
+        self.adam = adam or adam_step
+        self.shards = []  # (n, chunk, lo, valid)
+        self.grad_pad, self.grads, self.shard_grad, self.m, self.v, self.send, self.gathered = ([] for _ in range(7))
+        for p in self.params:
+            n = p.numel()
+            chunk = -(-n // self.world)
+            chunk = -(-chunk // self.ALIGN) * self.ALIGN
+            lo = self.rank * chunk
+            valid = max(0, min(n - lo, chunk))
+            self.shards.append((n, chunk, lo, valid))
+            gp = torch.zeros(self.world * chunk, dtype=p.dtype, device=p.device)
+            self.grad_pad.append(gp)
+            self.grads.append(gp[:n].view_as(p))
+            self.shard_grad.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
+            self.m.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
+            self.v.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
+            self.send.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
+            self.gathered.append(torch.empty(self.world * chunk, dtype=p.dtype, device=p.device))
+
+    @torch.no_grad()
+    def step(self, step: int, lr: float, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0,
+             halves=None) -> None:
+        """One update from the gradients accumulated in ``self.grads`` (zeroed
+        afterwards).  ``halves[i]``, when given, is an fp16 copy of params[i]
+        that is rewritten from the updated parameters."""
+        import torch.distributed as dist
+
+        halves = halves or [None] * len(self.params)
+        for i, p in enumerate(self.params):
+            n, chunk, lo, valid = self.shards[i]
+            dist.reduce_scatter_tensor(self.shard_grad[i], self.grad_pad[i], op=dist.ReduceOp.SUM, group=self.group)
+            self.shard_grad[i].div_(self.world)
+            self.grad_pad[i].zero_()
+            flat = p.view(-1)
+            if valid > 0:
+                self.adam(flat[lo:lo + valid], self.shard_grad[i][:valid], self.m[i][:valid], self.v[i][:valid],
+                          step, lr, betas, eps, weight_decay)
+                self.send[i][:valid].copy_(flat[lo:lo + valid])
+            dist.all_gather_into_tensor(self.gathered[i], self.send[i], group=self.group)
+            flat.copy_(self.gathered[i][:n])
+            if halves[i] is not None:
+                halves[i].view(-1).copy_(flat)
+
+    @torch.no_grad()
+    def full_moments(self, i: int):
+        """(exp_avg, exp_avg_sq) of params[i] at full size on every rank (a
+        collective: all ranks call it)."""
+        import torch.distributed as dist
+
+        n = self.shards[i][0]
+        out = []
+        for s in (self.m[i], self.v[i]):
+            full = torch.empty(self.world * s.numel(), dtype=s.dtype, device=s.device)
+            dist.all_gather_into_tensor(full, s.contiguous(), group=self.group)
+            out.append(full[:n].view_as(self.params[i]))
+        return tuple(out)
+
+    @torch.no_grad()
+    def load_moments(self, i: int, exp_avg: torch.Tensor, exp_avg_sq: torch.Tensor) -> None:
+        """Take this rank's shard of full-size moments of params[i]."""
+        n, chunk, lo, valid = self.shards[i]
+        for dst, src in ((self.m[i], exp_avg), (self.v[i], exp_avg_sq)):
+            dst.zero_()
+            if valid > 0:
+                dst[:valid].copy_(src.reshape(-1)[lo:lo + valid])
+
+
 class Trainer:
     """Per-projection training loop on the fused kernels.
 
@@ -289,7 +391,8 @@ class Trainer:
     def __init__(self, model: _HashGridModel, geometry: Geometry, points_per_batch: int, points_per_ray: int,
                  loss: str = "l2", lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8,
                  weight_decay: float = 0.0, batch_per_proj: int = 1, random_offset_detector: float = 0.0,
-                 uniform_ray_spacing: bool = True, device="cuda", data_parallel: bool = False, process_group=None):
+                 uniform_ray_spacing: bool = True, device="cuda", data_parallel: bool = False, process_group=None,
+                 shard_optimizer: bool = False):
         self.model = model
         self.geometry = geometry
         self.c_geometry = geometry.get_c_geometry()
@@ -304,17 +407,27 @@ class Trainer:
         self.batch_per_proj = batch_per_proj
         self.random_offset_detector = random_offset_detector
         self.uniform_ray_spacing = uniform_ray_spacing
-        self.table_grad = torch.zeros_like(model.table)
-        self.mlp_grad = torch.zeros_like(model.mlp)
-        self.m_table = torch.zeros_like(model.table)
-        self.v_table = torch.zeros_like(model.table)
-        self.m_mlp = torch.zeros_like(model.mlp)
-        self.v_mlp = torch.zeros_like(model.mlp)
         self.step_count = 0
         self.workspace = Workspace()
         # data parallel: every rank trains on its own rays, gradients are averaged before Adam
         self.data_parallel = data_parallel
         self.process_group = process_group
+        # shard_optimizer: Adam state and update split over the ranks (ShardedAdam); the
+        # gradient buffers are views of its padded reduce-scatter buffers
+        self.sharded = None
+        if shard_optimizer:
+            if not data_parallel:
+                raise ValueError("shard_optimizer splits Adam over the data-parallel ranks: pass data_parallel=True")
+            self.sharded = ShardedAdam([model.table, model.mlp], process_group)
+            self.table_grad, self.mlp_grad = self.sharded.grads
+            self.m_table = self.v_table = self.m_mlp = self.v_mlp = None
+        else:
+            self.table_grad = torch.zeros_like(model.table)
+            self.mlp_grad = torch.zeros_like(model.mlp)
+            self.m_table = torch.zeros_like(model.table)
+            self.v_table = torch.zeros_like(model.table)
+            self.m_mlp = torch.zeros_like(model.mlp)
+            self.v_mlp = torch.zeros_like(model.mlp)
 
     @property
     def batch_size(self) -> int:
@@ -339,14 +452,44 @@ class Trainer:
     def step(self, batch: RayBatch) -> torch.Tensor:
         loss, _ = train_step(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,
                              self.table_grad, self.mlp_grad, self.workspace, self.loss)
-        if self.data_parallel:
-            reduce_gradients([self.table_grad, self.mlp_grad], self.process_group)
-        self.step_count += 1
-        adam_step(self.model.table, self.table_grad, self.m_table, self.v_table, self.step_count, self.lr,
-                  self.betas, self.eps, self.weight_decay, half=self.model.table_half)
-        adam_step(self.model.mlp, self.mlp_grad, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas,
-                  self.eps, self.weight_decay)
+        self._update(self.table_grad, self.mlp_grad)
         return loss
+
+    def _update(self, g_table: torch.Tensor, g_mlp: torch.Tensor) -> None:
+        """Gradient averaging over the ranks (data parallel) and the Adam step;
+        the gradients are zeroed."""
+        self.step_count += 1
+        if self.sharded is not None:
+            if g_table is not self.table_grad:  # gradients from autograd
+                self.table_grad.add_(g_table)
+                self.mlp_grad.add_(g_mlp)
+            self.sharded.step(self.step_count, self.lr, self.betas, self.eps, self.weight_decay,
+                              halves=[self.model.table_half, None])
+            return
+        if self.data_parallel:
+            reduce_gradients([g_table, g_mlp], self.process_group)
+        adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
+                  self.eps, self.weight_decay, half=self.model.table_half)
+        adam_step(self.model.mlp, g_mlp, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas, self.eps,
+                  self.weight_decay)
+
+    def optimizer_moments(self):
+        """[(exp_avg, exp_avg_sq) of the table, the same of the MLP] at full
+        size.  With the sharded optimizer this gathers them: every rank calls."""
+        if self.sharded is not None:
+            return [self.sharded.full_moments(0), self.sharded.full_moments(1)]
+        return [(self.m_table, self.v_table), (self.m_mlp, self.v_mlp)]
+
+    @torch.no_grad()
+    def load_optimizer_moments(self, moments) -> None:
+        """Inverse of optimizer_moments (full-size tensors, any device)."""
+        if self.sharded is not None:
+            for i, (m, v) in enumerate(moments):
+                self.sharded.load_moments(i, m.to(self.model.table.device), v.to(self.model.table.device))
+            return
+        for (dm, dv), (m, v) in zip(self.optimizer_moments(), moments):
+            dm.copy_(m)
+            dv.copy_(v)
 
     def continuous_step(self, perm: torch.Tensor, batch_num: int, angle_start: float, angle_stop: float,
                         projection: torch.Tensor, t: float = 0.0, accumulation_steps: int = 4,
@@ -403,13 +546,7 @@ class Trainer:
         if extra is not None:
             loss = loss + extra
         g_table, g_mlp = torch.autograd.grad(loss, [self.model.table, self.model.mlp])
-        if self.data_parallel:
-            reduce_gradients([g_table, g_mlp], self.process_group)
-        self.step_count += 1
-        adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
-                  self.eps, self.weight_decay, half=self.model.table_half)
-        adam_step(self.model.mlp, g_mlp, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas, self.eps,
-                  self.weight_decay)
+        self._update(g_table, g_mlp)
         return loss.detach()
 
     def device_error(self) -> int:
