@@ -330,7 +330,9 @@ class ShardedAdam:
             self.m.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
             self.v.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
             self.send.append(torch.zeros(chunk, dtype=p.dtype, device=p.device))
-            self.gathered.append(torch.empty(self.world * chunk, dtype=p.dtype, device=p.device))
+            # the all-gather lands in the parameter itself unless the buffer pads
+            padded = self.world * chunk != n
+            self.gathered.append(torch.empty(self.world * chunk, dtype=p.dtype, device=p.device) if padded else None)
 
     @torch.no_grad()
     def step(self, step: int, lr: float, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0,
@@ -351,8 +353,11 @@ class ShardedAdam:
                 self.adam(flat[lo:lo + valid], self.shard_grad[i][:valid], self.m[i][:valid], self.v[i][:valid],
                           step, lr, betas, eps, weight_decay)
                 self.send[i][:valid].copy_(flat[lo:lo + valid])
-            dist.all_gather_into_tensor(self.gathered[i], self.send[i], group=self.group)
-            flat.copy_(self.gathered[i][:n])
+            if self.gathered[i] is None:
+                dist.all_gather_into_tensor(flat, self.send[i], group=self.group)
+            else:
+                dist.all_gather_into_tensor(self.gathered[i], self.send[i], group=self.group)
+                flat.copy_(self.gathered[i][:n])
             if halves[i] is not None:
                 halves[i].view(-1).copy_(flat)
 

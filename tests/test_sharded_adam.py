@@ -1,9 +1,9 @@
 """Adam sharded over data-parallel ranks (trainer.ShardedAdam) on three gloo
 ranks on CPU: the parameters, moments and fp16 table copy equal those of the
-gradient all-reduce followed by the full Adam step, with a shard that pads and
-a rank that holds no element of a small buffer; then the Trainer's update with
-the sharded optimizer, the checkpoint of its gathered moments (rank 0 writes)
-and resume into every rank's shard.  The per-shard update here is
+gradient all-reduce followed by the full Adam step, with buffers that pad, a
+rank that holds no element of a small buffer and a buffer gathered in place;
+then the Trainer's update with the sharded optimizer, the checkpoint of its
+gathered moments (rank 0 writes) and resume into every rank's shard.  The per-shard update here is
 torch.optim.Adam's rule written in torch (the CUDA Adam kernel is the default
 and needs a GPU); both arms use it, so the test checks the sharding."""
 import math
@@ -67,7 +67,7 @@ def _rank(rank, world, port, run_dir, out):
     try:
         # ShardedAdam against all-reduce + full Adam
         g = torch.Generator().manual_seed(0)
-        params = [torch.rand(1003, 2, generator=g), torch.rand(10, generator=g)]
+        params = [torch.rand(1003, 2, generator=g), torch.rand(10, generator=g), torch.rand(6, 8, generator=g)]
         ref = [p.clone() for p in params]
         ref_m, ref_v = [torch.zeros_like(p) for p in ref], [torch.zeros_like(p) for p in ref]
         half = params[0].half()
@@ -78,14 +78,15 @@ def _rank(rank, world, port, run_dir, out):
             grads = [torch.randn(p.shape, generator=gr) for p in ref]
             avg = [x.clone() for x in grads]
             reduce_gradients(avg)
-            for i in range(2):
+            for i in range(3):
                 cpu_adam(ref[i], avg[i], ref_m[i], ref_v[i], step, LR, weight_decay=WD)
                 sa.grads[i].add_(grads[i])
-            sa.step(step, LR, weight_decay=WD, halves=[half, None])
-        res["param"] = max(rel(params[i], ref[i]) for i in range(2))
+            sa.step(step, LR, weight_decay=WD, halves=[half, None, None])
+        res["param"] = max(rel(params[i], ref[i]) for i in range(3))
+        res["padded"] = [g is not None for g in sa.gathered]
         res["half"] = bool(torch.equal(half, params[0].half()))
-        mom = [sa.full_moments(i) for i in range(2)]
-        res["moments"] = max(max(rel(mom[i][0], ref_m[i]), rel(mom[i][1], ref_v[i])) for i in range(2))
+        mom = [sa.full_moments(i) for i in range(3)]
+        res["moments"] = max(max(rel(mom[i][0], ref_m[i]), rel(mom[i][1], ref_v[i])) for i in range(3))
         res["grads_zeroed"] = all(float(gp.abs().max()) == 0.0 for gp in sa.grad_pad)
 
         # Trainer update (gradients from autograd), checkpoint, resume
@@ -132,6 +133,7 @@ def test_sharded_adam_matches_all_reduce_adam(tmp_path):
             p.join(300)
             assert p.exitcode == 0
         assert [out[r]["valid"][1] for r in range(world)] == [8, 2, 0]  # 10 elements, shards of 8
+        assert out[0]["padded"] == [True, True, False]  # 48 elements in 3 shards of 16 gather in place
         for r in range(world):
             res = out[r]
             assert res["param"] < 1e-6 and res["moments"] < 1e-6, res
