@@ -9,7 +9,6 @@ bf16 tensor-core MLP) against the finite differences of the fp64 network on
 the same fp16 table values, cosine similarity > 0.99 and every entry within
 5e-2 of the largest.  The reference's own gradient (tiny-cuda-nn) cannot be
 computed here: tiny-cuda-nn is not part of the reference tree."""
-import math
 
 import numpy as np
 import pytest

@@ -6,7 +6,6 @@ served alone (bit for bit).
 Tolerances vs the fp64 oracle: plain fp32 model 1e-5 relative to the largest
 value; mixed model (bf16 tensor-core MLP) 2e-2.
 """
-import math
 
 import numpy as np
 import pytest

@@ -2,7 +2,6 @@
 reference's own kernel (compiled from nect/sampling/ct_sampling.cu into
 oracle/_ref) and against the C oracle: bit-exact points, distances and
 per-ray counts."""
-import math
 
 import numpy as np
 import pytest
