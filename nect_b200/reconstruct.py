@@ -8,9 +8,10 @@ with create_volume's de-normalisation (nect/trainers/base_trainer.py:402-450).
 
 Scheduling follows BaseTrainer.fit (base_trainer.py:492-655) with one batch
 per projection visit: each step takes the next projection of a seeded random
-order, a device randperm of its pixels and one batch of rays.  The reference's
-progressive schedules (detector binning, points-per-ray ramp), S3IM and TV
-regularisers and its lr warm-up are not part of this path.
+order, a device randperm of its pixels and one batch of rays.  ``fit`` takes
+the reference's per-projection schedules (detector binning, points-per-ray
+ramp, lr warm-up and decay: schedule.Schedule), its S3IM, Poisson and TV
+terms; ``reconstruct`` resolves the reference's quality presets into them.
 """
 from __future__ import annotations
 
@@ -24,7 +25,7 @@ import torch
 from .config import HashEncoderConfig, MLPNetConfig, ModelConfig, get_model
 from .network import _HashGridModel
 from .sampling import Geometry
-from .schedule import bin_projection, s3im_patch_size
+from .schedule import Schedule, bin_projection, s3im_patch_size
 from .serving import denormalisation, query_points, volume_items
 from .trainer import Trainer
 
@@ -48,22 +49,104 @@ class Reconstruction:
         return out
 
 
-def default_model_config(geometry: Geometry, mode: str, precision: str) -> ModelConfig:
+def default_model_config(geometry: Geometry, mode: str, precision: str, log2_hashmap_size: int = 19) -> ModelConfig:
     """The model of the static parallel-beam workload: 16 levels x 2 features,
-    2^19 entries, base 16, finest 2 x the largest detector extent, 2 x 64 ReLU
-    MLP with softplus output (temporal base 4 for dynamic scans).  The
-    reference's own preset (nect/cfg/static/hash_grid.yaml: 19 levels x 4
-    features, 6 x 64 LeakyReLU) is outside the kernel instantiations."""
-    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=19, base_resolution=16,
-                            max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
+    2^19 entries (unless given), base 16, finest 2 x the largest detector
+    extent, 2 x 64 ReLU MLP with softplus output (temporal base 4 for dynamic
+    scans).  The reference's own preset (nect/cfg/static/hash_grid.yaml: 19
+    levels x 4 features, 6 x 64 LeakyReLU) is outside the kernel
+    instantiations."""
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_hashmap_size,
+                            base_resolution=16, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
                             nVoxel=list(geometry.nVoxel), base_resolution_t=4 if mode == "dynamic" else None)
     return ModelConfig("hash_grid_4d" if mode == "dynamic" else "hash_grid", enc, MLPNetConfig(n_hidden_layers=2),
                        precision)
 
 
+# ---------------------------------------------------------- quality presets ----
+# The fields the quality presets change, as the reference's configuration
+# starts them: nect/cfg/default.yaml (loss L1, base_lr 1e-3, warm-up 500 steps
+# from lr0 1e-3, epochs / lrf / points_per_ray.end "auto") overlaid by the
+# model preset of each mode (nect/cfg/static/hash_grid.yaml: 2^21 entries;
+# nect/cfg/dynamic/quadcubes.yaml: 2^23 entries, base_lr 2e-4, warm-up 2000
+# steps from lr0 1e-4).
+_BASE_CONFIG = {
+    "static": {"loss": "l1", "base_lr": 1e-3, "warmup_steps": 500, "warmup_lr0": 1e-3, "epochs": "auto",
+               "lrf": "auto", "points_end": "auto", "log2_hashmap_size": 21},
+    "dynamic": {"loss": "l1", "base_lr": 2e-4, "warmup_steps": 2000, "warmup_lr0": 1e-4, "epochs": "auto",
+                "lrf": "auto", "points_end": "auto", "log2_hashmap_size": 23},
+}
+
+# nect/reconstruct.py:173-204: per quality, the fields set and the factor the
+# base learning rate is multiplied ("mul") or divided ("div") by.
+QUALITY_PRESETS = {
+    "poor": {"set": {"loss": "l2", "log2_hashmap_size": 19, "epochs": "0.02x"}, "lr": ("mul", 10)},
+    "low": {"set": {"loss": "l2", "log2_hashmap_size": 19, "epochs": "0.1x"}, "lr": ("mul", 5)},
+    "medium": {"set": {"epochs": "0.3x"}, "lr": ("mul", 2)},
+    "high": {"set": {"epochs": "1x", "warmup_steps": 500}, "lr": ("div", 2)},
+    "higher": {"set": {"epochs": "2x", "warmup_steps": 3000, "lrf": 0.05, "points_end": "1.5x"}, "lr": ("div", 2)},
+    "highest": {"set": {"epochs": "4x", "warmup_steps": 5000, "lrf": 0.01, "points_end": "1.5x",
+                        "log2_hashmap_size": 23}, "lr": ("div", 5)},
+}
+
+# points_per_batch "auto" fills free device memory up to this cap
+# (nect/config.py:380-388); a B200's 180 GB always reaches it.
+AUTO_POINTS_PER_BATCH = 5_000_000
+
+
+def preset_config(mode: str, quality: str = "high", niter=None, lr: float | None = None) -> dict:
+    """The configuration fields of ``reconstruct(mode, quality, niter, lr)``:
+    the preset applied to the mode's defaults, then ``niter`` replacing the
+    epochs and ``lr`` the base learning rate (nect/reconstruct.py:205-208)."""
+    if quality not in QUALITY_PRESETS:
+        raise ValueError(f"quality must be one of {list(QUALITY_PRESETS)} (got {quality!r})")
+    cfg = dict(_BASE_CONFIG[mode])
+    preset = QUALITY_PRESETS[quality]
+    cfg.update(preset["set"])
+    op, k = preset["lr"]
+    cfg["base_lr"] = cfg["base_lr"] * k if op == "mul" else cfg["base_lr"] / k
+    if niter is not None:
+        cfg["epochs"] = niter
+    if lr is not None:
+        cfg["base_lr"] = lr
+    return cfg
+
+
+def learning_rate(base_lr: float, points_per_batch: int, n_gpus: int = 1) -> float:
+    """base_lr * sqrt(points_per_batch * n_gpus / 10^6) (nect/config.py:398-399)."""
+    return base_lr * math.sqrt(points_per_batch * n_gpus / 1_000_000)
+
+
+@dataclass
+class ReconstructionPlan:
+    """What ``reconstruct`` trains with: the model configuration, the
+    per-projection schedule, the loss and the points per batch the trainer
+    samples (half the configured number, base_trainer.py:141-143)."""
+    model_cfg: ModelConfig
+    schedule: Schedule
+    loss: str
+    points_per_batch: int
+    config: dict
+
+
+def plan_reconstruction(geometry: Geometry, mode: str, n_projections: int, quality: str = "high", niter=None,
+                        lr: float | None = None, precision: str = "mixed", points_per_batch: int | None = None,
+                        n_gpus: int = 1) -> ReconstructionPlan:
+    """The quality preset resolved for this geometry and projection count."""
+    cfg = preset_config(mode, quality, niter, lr)
+    ppb = int(points_per_batch or AUTO_POINTS_PER_BATCH)
+    schedule = Schedule(list(geometry.nDetector), n_projections, epochs=cfg["epochs"],
+                        base_lr=learning_rate(cfg["base_lr"], ppb, n_gpus), points_end=cfg["points_end"],
+                        warmup_steps=cfg["warmup_steps"], warmup_lr0=cfg["warmup_lr0"], lrf=cfg["lrf"],
+                        n_gpus=n_gpus)
+    return ReconstructionPlan(default_model_config(geometry, mode, precision, cfg["log2_hashmap_size"]), schedule,
+                              cfg["loss"], ppb // 2, cfg)
+
+
 def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *, model_cfg: ModelConfig | None = None,
         precision: str = "mixed", niter: int = 2000, lr: float = 1e-3, rays_per_batch: int = 65536,
-        points_per_ray: int | None = None, loss: str = "l2", seed: int = 0, device="cuda",
+        points_per_ray: int | None = None, points_per_batch: int | None = None, loss: str = "l2", seed: int = 0,
+        device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
         add_poisson: bool = False, tv: float = 0.0) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
@@ -97,8 +180,8 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     torch.manual_seed(seed)
     model = get_model(cfg, device=dev)
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
-    trainer = Trainer(model, geometry, points_per_batch=rays_per_batch * S, points_per_ray=S, loss=loss, lr=lr,
-                      device=dev)
+    trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
+                      loss=loss, lr=lr, device=dev)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
     order = np.random.default_rng(seed).permutation(n_proj)
     P = proj.shape[1]
@@ -160,11 +243,18 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
 
 
 def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=None, radians: bool = True,
-                niter: int | None = None, lr: float | None = None, timesteps=None, precision: str = "mixed",
-                **kw):
+                quality: str = "high", niter: int | None = None, lr: float | None = None, timesteps=None,
+                precision: str = "mixed", points_per_batch: int | None = None, **kw):
     """``nect.reconstruct`` for arrays of projections: returns the volume
     (np.ndarray [z, y, x]) for mode "static" and the Reconstruction (export
-    any t with ``.volume(t)``) for mode "dynamic"."""
+    any t with ``.volume(t)``) for mode "dynamic".
+
+    As in the reference, ``quality`` picks the preset (epochs, learning rate,
+    warm-up, final lr fraction, points per ray, hash-table size and loss),
+    ``niter`` replaces the preset's epochs and ``lr`` its base learning rate;
+    training follows the per-projection schedules (detector binning,
+    points-per-ray ramp, warm-up and cosine decay) for epochs x projections
+    steps (plan_reconstruction)."""
     if angles is None:
         angles = geometry.angles
     angles = np.asarray(angles, np.float64)
@@ -174,8 +264,10 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
         timesteps = getattr(geometry, "timesteps", None)
         if timesteps is None:
             timesteps = np.arange(len(angles), dtype=np.float64)
-    rec = fit(geometry, projections, angles, timesteps if mode == "dynamic" else None, precision=precision,
-              niter=niter or 2000, lr=lr or 1e-3, **kw)
+    plan = plan_reconstruction(geometry, mode, len(angles), quality, niter, lr, precision, points_per_batch)
+    rec = fit(geometry, projections, angles, timesteps if mode == "dynamic" else None, model_cfg=plan.model_cfg,
+              precision=precision, niter=plan.schedule.total_projections, lr=plan.schedule.lr[0],
+              points_per_batch=plan.points_per_batch, loss=plan.loss, schedule=plan.schedule, **kw)
     if mode == "static":
         return rec.volume().cpu().numpy()
     return rec
