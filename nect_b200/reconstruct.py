@@ -246,8 +246,9 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
                 quality: str = "high", niter: int | None = None, lr: float | None = None, timesteps=None,
                 precision: str = "mixed", points_per_batch: int | None = None, **kw):
     """``nect.reconstruct`` for arrays of projections: returns the volume
-    (np.ndarray [z, y, x]) for mode "static" and the Reconstruction (export
-    any t with ``.volume(t)``) for mode "dynamic".
+    (np.ndarray [z, y, x], turned by 180 degrees in (y, x) as the reference
+    returns it) for mode "static" and the Reconstruction (export any t with
+    ``.volume(t)``) for mode "dynamic".
 
     As in the reference, ``quality`` picks the preset (epochs, learning rate,
     warm-up, final lr fraction, points per ray, hash-table size and loss),
@@ -269,7 +270,9 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
               precision=precision, niter=plan.schedule.total_projections, lr=plan.schedule.lr[0],
               points_per_batch=plan.points_per_batch, loss=plan.loss, schedule=plan.schedule, **kw)
     if mode == "static":
-        return rec.volume().cpu().numpy()
+        # the reference returns create_volume turned by 180 degrees in (y, x)
+        # (nect/reconstruct.py:246-247)
+        return torch.rot90(rec.volume(), 2, (1, 2)).contiguous().cpu().numpy()
     return rec
 
 

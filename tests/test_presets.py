@@ -81,3 +81,34 @@ def test_plan_with_niter_and_points_per_batch():
     assert plan.schedule.total_projections == 90 and plan.points_per_batch == 500_000
     assert plan.schedule.lr[0] == pytest.approx(2e-3)
     assert plan.model_cfg.model == "hash_grid_4d" and plan.model_cfg.encoder.log2_hashmap_size == 19
+
+
+def test_reconstruct_resolves_the_preset_and_turns_the_static_volume(monkeypatch):
+    """reconstruct() with fit() stubbed (fit itself runs on the GPU): the preset
+    reaches fit, and the static volume comes back turned by 180 degrees in
+    (y, x), as nect/reconstruct.py:246-247 returns create_volume."""
+    import numpy as np
+    import torch
+
+    from nect_b200 import reconstruct as rc
+
+    seen = {}
+    vol = torch.arange(2 * 3 * 4, dtype=torch.float32).reshape(2, 3, 4)
+
+    class Rec:
+        def volume(self):
+            return vol
+
+    def fake_fit(geometry, projections, angles, timesteps=None, **kw):
+        seen.update(kw, angles=angles, timesteps=timesteps)
+        return Rec()
+
+    monkeypatch.setattr(rc, "fit", fake_fit)
+    geo = geometry(32)
+    out = rc.reconstruct(geo, np.zeros((10, 32, 32), np.float32), angles=np.arange(10) * 18.0, radians=False,
+                         quality="medium", lr=1e-3)
+    assert np.array_equal(out, vol.flip(1).flip(2).numpy())
+    assert seen["loss"] == "l1" and seen["points_per_batch"] == 2_500_000
+    assert seen["niter"] == seen["schedule"].total_projections == math.ceil(0.3 * math.ceil(49 / 10 * 32)) * 10
+    assert seen["lr"] == pytest.approx(1e-3 * math.sqrt(5))
+    assert np.allclose(seen["angles"], np.deg2rad(np.arange(10) * 18.0)) and seen["timesteps"] is None
