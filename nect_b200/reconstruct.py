@@ -18,6 +18,7 @@ from __future__ import annotations
 import math
 import time
 from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 import torch
@@ -70,11 +71,27 @@ def default_model_config(geometry: Geometry, mode: str, precision: str, log2_has
 # model preset of each mode (nect/cfg/static/hash_grid.yaml: 2^21 entries;
 # nect/cfg/dynamic/quadcubes.yaml: 2^23 entries, base_lr 2e-4, warm-up 2000
 # steps from lr0 1e-4).
+_COMMON_CONFIG = {"loss": "l1", "epochs": "auto", "lrf": "auto", "lr_otype": "cosine", "warmup_otype": "exponential",
+                  "points_start": 100, "points_end": "auto", "points_update_interval": "auto", "points_linear": True,
+                  "downsampling_start": 2, "downsampling_end": 1, "downsampling_update_interval": 1000,
+                  "points_per_batch": "auto", "s3im": False, "add_poisson": False}
 _BASE_CONFIG = {
-    "static": {"loss": "l1", "base_lr": 1e-3, "warmup_steps": 500, "warmup_lr0": 1e-3, "epochs": "auto",
-               "lrf": "auto", "points_end": "auto", "log2_hashmap_size": 21},
-    "dynamic": {"loss": "l1", "base_lr": 2e-4, "warmup_steps": 2000, "warmup_lr0": 1e-4, "epochs": "auto",
-                "lrf": "auto", "points_end": "auto", "log2_hashmap_size": 23},
+    "static": dict(_COMMON_CONFIG, base_lr=1e-3, warmup_steps=500, warmup_lr0=1e-3, log2_hashmap_size=21),
+    "dynamic": dict(_COMMON_CONFIG, base_lr=2e-4, warmup_steps=2000, warmup_lr0=1e-4, log2_hashmap_size=23),
+}
+
+# config_override keys (the reference's configuration schema, nect/config.py)
+# -> the fields above; nested sections map key by key.
+_OVERRIDE_KEYS = {
+    "epochs": "epochs", "base_lr": "base_lr", "loss": "loss", "points_per_batch": "points_per_batch",
+    "s3im": "s3im", "add_poisson": "add_poisson",
+    ("warmup", "steps"): "warmup_steps", ("warmup", "lr0"): "warmup_lr0", ("warmup", "otype"): "warmup_otype",
+    ("lr_scheduler", "otype"): "lr_otype", ("lr_scheduler", "lrf"): "lrf",
+    ("points_per_ray", "start"): "points_start", ("points_per_ray", "end"): "points_end",
+    ("points_per_ray", "update_interval"): "points_update_interval", ("points_per_ray", "linear"): "points_linear",
+    ("downsampling_detector", "start"): "downsampling_start", ("downsampling_detector", "end"): "downsampling_end",
+    ("downsampling_detector", "update_interval"): "downsampling_update_interval",
+    ("encoder", "log2_hashmap_size"): "log2_hashmap_size",
 }
 
 # nect/reconstruct.py:173-204: per quality, the fields set and the factor the
@@ -94,10 +111,32 @@ QUALITY_PRESETS = {
 AUTO_POINTS_PER_BATCH = 5_000_000
 
 
-def preset_config(mode: str, quality: str = "high", niter=None, lr: float | None = None) -> dict:
-    """The configuration fields of ``reconstruct(mode, quality, niter, lr)``:
-    the preset applied to the mode's defaults, then ``niter`` replacing the
-    epochs and ``lr`` the base learning rate (nect/reconstruct.py:205-208)."""
+def apply_override(cfg: dict, override: dict) -> dict:
+    """``config_override`` (keys of the reference's configuration, e.g.
+    {"epochs": 3, "warmup": {"steps": 10}}) applied to the fields; keys this
+    path has no use for raise ValueError."""
+    out = dict(cfg)
+    for key, value in override.items():
+        if isinstance(value, dict):
+            for sub, v in value.items():
+                if (key, sub) not in _OVERRIDE_KEYS:
+                    raise ValueError(f"config_override: {key}.{sub} is not supported here")
+                out[_OVERRIDE_KEYS[(key, sub)]] = v
+        elif key in _OVERRIDE_KEYS:
+            out[_OVERRIDE_KEYS[key]] = value
+        else:
+            raise ValueError(f"config_override: {key} is not supported here")
+    if isinstance(out["loss"], str):
+        out["loss"] = out["loss"].lower()
+    return out
+
+
+def preset_config(mode: str, quality: str = "high", niter=None, lr: float | None = None,
+                  config_override: dict | None = None) -> dict:
+    """The configuration fields of ``reconstruct(mode, quality, niter, lr,
+    config_override)``: the preset applied to the mode's defaults, then
+    ``niter`` replacing the epochs and ``lr`` the base learning rate, then the
+    override (nect/reconstruct.py:205-216)."""
     if quality not in QUALITY_PRESETS:
         raise ValueError(f"quality must be one of {list(QUALITY_PRESETS)} (got {quality!r})")
     cfg = dict(_BASE_CONFIG[mode])
@@ -109,6 +148,8 @@ def preset_config(mode: str, quality: str = "high", niter=None, lr: float | None
         cfg["epochs"] = niter
     if lr is not None:
         cfg["base_lr"] = lr
+    if config_override:
+        cfg = apply_override(cfg, config_override)
     return cfg
 
 
@@ -131,14 +172,21 @@ class ReconstructionPlan:
 
 def plan_reconstruction(geometry: Geometry, mode: str, n_projections: int, quality: str = "high", niter=None,
                         lr: float | None = None, precision: str = "mixed", points_per_batch: int | None = None,
-                        n_gpus: int = 1) -> ReconstructionPlan:
+                        n_gpus: int = 1, config_override: dict | None = None) -> ReconstructionPlan:
     """The quality preset resolved for this geometry and projection count."""
-    cfg = preset_config(mode, quality, niter, lr)
-    ppb = int(points_per_batch or AUTO_POINTS_PER_BATCH)
+    cfg = preset_config(mode, quality, niter, lr, config_override)
+    if points_per_batch is None:
+        points_per_batch = AUTO_POINTS_PER_BATCH if cfg["points_per_batch"] == "auto" else cfg["points_per_batch"]
+    ppb = int(points_per_batch)
     schedule = Schedule(list(geometry.nDetector), n_projections, epochs=cfg["epochs"],
-                        base_lr=learning_rate(cfg["base_lr"], ppb, n_gpus), points_end=cfg["points_end"],
-                        warmup_steps=cfg["warmup_steps"], warmup_lr0=cfg["warmup_lr0"], lrf=cfg["lrf"],
-                        n_gpus=n_gpus)
+                        base_lr=learning_rate(cfg["base_lr"], ppb, n_gpus),
+                        downsampling_start=cfg["downsampling_start"], downsampling_end=cfg["downsampling_end"],
+                        downsampling_update_interval=cfg["downsampling_update_interval"],
+                        points_start=cfg["points_start"], points_end=cfg["points_end"],
+                        points_update_interval=cfg["points_update_interval"], points_linear=cfg["points_linear"],
+                        warmup_steps=cfg["warmup_steps"], warmup_lr0=cfg["warmup_lr0"],
+                        warmup_otype=cfg["warmup_otype"] or "exponential", lr_otype=cfg["lr_otype"],
+                        lrf=cfg["lrf"], n_gpus=n_gpus)
     return ReconstructionPlan(default_model_config(geometry, mode, precision, cfg["log2_hashmap_size"]), schedule,
                               cfg["loss"], ppb // 2, cfg)
 
@@ -244,18 +292,31 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
 
 def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=None, radians: bool = True,
                 quality: str = "high", niter: int | None = None, lr: float | None = None, timesteps=None,
-                precision: str = "mixed", points_per_batch: int | None = None, **kw):
-    """``nect.reconstruct`` for arrays of projections: returns the volume
-    (np.ndarray [z, y, x], turned by 180 degrees in (y, x) as the reference
-    returns it) for mode "static" and the Reconstruction (export any t with
-    ``.volume(t)``) for mode "dynamic".
+                verbose: bool = True, log: bool = False, exp_name: str | None = None,
+                flip_projections: bool = False, channel_order: str | None = None,
+                config_override: dict | None = None, save_ckpt: bool = False, precision: str = "mixed",
+                points_per_batch: int | None = None, **kw):
+    """``nect.reconstruct`` (nect/reconstruct.py:113-250) for arrays of
+    projections [N, rows, cols]: returns the volume (np.ndarray [z, y, x],
+    turned by 180 degrees in (y, x) as the reference returns it) for mode
+    "static" and the Reconstruction (export any t with ``.volume(t)``) for
+    mode "dynamic".
 
     As in the reference, ``quality`` picks the preset (epochs, learning rate,
     warm-up, final lr fraction, points per ray, hash-table size and loss),
-    ``niter`` replaces the preset's epochs and ``lr`` its base learning rate;
+    ``niter`` replaces the preset's epochs, ``lr`` its base learning rate and
+    ``config_override`` any field this path uses (ValueError for others);
     training follows the per-projection schedules (detector binning,
-    points-per-ray ramp, warm-up and cosine decay) for epochs x projections
-    steps (plan_reconstruction)."""
+    points-per-ray ramp, warm-up and decay) for epochs x projections steps
+    (plan_reconstruction).  ``flip_projections`` and ``channel_order`` act on
+    projections read from files, which the reference's in-memory path leaves
+    as given, and so do nothing here; ``save_ckpt`` writes the checkpoint and
+    its pruned copy under outputs/<exp_name> (checkpoint.save / prune);
+    ``verbose`` prints the plan and the training time; ``log`` has no
+    effect."""
+    if isinstance(projections, (str, bytes)) or hasattr(projections, "__fspath__"):
+        raise ValueError("projections must be an array [N, rows, cols]: reading projection files is not part "
+                         "of this package")
     if angles is None:
         angles = geometry.angles
     angles = np.asarray(angles, np.float64)
@@ -265,10 +326,26 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
         timesteps = getattr(geometry, "timesteps", None)
         if timesteps is None:
             timesteps = np.arange(len(angles), dtype=np.float64)
-    plan = plan_reconstruction(geometry, mode, len(angles), quality, niter, lr, precision, points_per_batch)
+    plan = plan_reconstruction(geometry, mode, len(angles), quality, niter, lr, precision, points_per_batch,
+                               config_override=config_override)
+    kw.setdefault("s3im", bool(plan.config["s3im"]))
+    kw.setdefault("add_poisson", bool(plan.config["add_poisson"]))
+    if verbose:
+        sch = plan.schedule
+        print(f"nect_b200.reconstruct: {mode}, quality {quality}: {sch.total_projections} steps "
+              f"({sch.epochs} epochs x {len(angles)} projections), lr {sch.lr[0]:.3g}, loss {plan.loss}, "
+              f"{plan.points_per_batch} points per batch, 2^{plan.model_cfg.encoder.log2_hashmap_size} entries")
     rec = fit(geometry, projections, angles, timesteps if mode == "dynamic" else None, model_cfg=plan.model_cfg,
               precision=precision, niter=plan.schedule.total_projections, lr=plan.schedule.lr[0],
               points_per_batch=plan.points_per_batch, loss=plan.loss, schedule=plan.schedule, **kw)
+    if verbose:
+        print(f"nect_b200.reconstruct: trained in {rec.train_seconds:.1f} s")
+    if save_ckpt:
+        from . import checkpoint
+
+        run = Path("outputs") / (exp_name or "reconstruction")
+        checkpoint.save(run, rec.model, rec.trainer, geometry)
+        checkpoint.prune(run)
     if mode == "static":
         # the reference returns create_volume turned by 180 degrees in (y, x)
         # (nect/reconstruct.py:246-247)

@@ -106,9 +106,35 @@ def test_reconstruct_resolves_the_preset_and_turns_the_static_volume(monkeypatch
     monkeypatch.setattr(rc, "fit", fake_fit)
     geo = geometry(32)
     out = rc.reconstruct(geo, np.zeros((10, 32, 32), np.float32), angles=np.arange(10) * 18.0, radians=False,
-                         quality="medium", lr=1e-3)
+                         quality="medium", lr=1e-3, verbose=False, flip_projections=True, channel_order="NHW")
     assert np.array_equal(out, vol.flip(1).flip(2).numpy())
     assert seen["loss"] == "l1" and seen["points_per_batch"] == 2_500_000
     assert seen["niter"] == seen["schedule"].total_projections == math.ceil(0.3 * math.ceil(49 / 10 * 32)) * 10
     assert seen["lr"] == pytest.approx(1e-3 * math.sqrt(5))
     assert np.allclose(seen["angles"], np.deg2rad(np.arange(10) * 18.0)) and seen["timesteps"] is None
+    assert seen["s3im"] is False and seen["add_poisson"] is False
+
+    seen.clear()
+    rc.reconstruct(geo, np.zeros((10, 32, 32), np.float32), angles=np.arange(10) * 0.3, quality="high",
+                   verbose=False, config_override={"epochs": 2, "s3im": True, "points_per_batch": 400_000,
+                                                   "warmup": {"steps": 7}})
+    assert seen["niter"] == 20 and seen["s3im"] is True and seen["points_per_batch"] == 200_000
+    assert seen["schedule"].warmup[0] == 7
+    with pytest.raises(ValueError, match="array"):
+        rc.reconstruct(geo, "projections.npy", angles=np.arange(10) * 0.3, verbose=False)
+
+
+def test_config_override_mapping():
+    from nect_b200.reconstruct import preset_config
+
+    cfg = preset_config("static", "high", niter=5, lr=1e-2, config_override={
+        "epochs": 9, "base_lr": 3e-3, "loss": "L2", "lr_scheduler": {"otype": "exponential", "lrf": 0.1},
+        "points_per_ray": {"start": 64, "end": 512, "linear": False}, "encoder": {"log2_hashmap_size": 18},
+        "downsampling_detector": {"start": 4, "update_interval": 50}})
+    assert cfg["epochs"] == 9 and cfg["base_lr"] == 3e-3 and cfg["loss"] == "l2"   # the override comes last
+    assert (cfg["lr_otype"], cfg["lrf"]) == ("exponential", 0.1)
+    assert (cfg["points_start"], cfg["points_end"], cfg["points_linear"]) == (64, 512, False)
+    assert cfg["log2_hashmap_size"] == 18 and (cfg["downsampling_start"], cfg["downsampling_update_interval"]) == (4, 50)
+    for bad in ({"optimizer": {"otype": "Lion"}}, {"model": "kplanes"}):
+        with pytest.raises(ValueError, match="not supported"):
+            preset_config("static", "high", config_override=bad)
