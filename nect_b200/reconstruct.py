@@ -191,12 +191,29 @@ def plan_reconstruction(geometry: Geometry, mode: str, n_projections: int, quali
                               cfg["loss"], ppb // 2, cfg)
 
 
+def step_plan(n_proj: int, seed: int, niter: int, schedule=None, start: int = 0):
+    """(step, projection index, schedule settings or None) for steps
+    start + 1 .. niter.  Each epoch visits the projections in a seeded random
+    order, drawn anew at the end of every epoch (epoch e uses seed + e * n_proj,
+    epoch 0 the seed), so a run resumed after ``start`` steps takes the steps
+    an uninterrupted run would."""
+    settings = iter(schedule.steps(start)) if schedule is not None else None
+    epoch = start // n_proj
+    order = np.random.default_rng(seed if epoch == 0 else seed + epoch * n_proj).permutation(n_proj)
+    for step in range(start + 1, niter + 1):
+        k = int(order[(step - 1) % n_proj])
+        if (step - 1) % n_proj == n_proj - 1:
+            order = np.random.default_rng(seed + step).permutation(n_proj)
+        yield step, k, (next(settings) if settings is not None else None)
+
+
 def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *, model_cfg: ModelConfig | None = None,
         precision: str = "mixed", niter: int = 2000, lr: float = 1e-3, rays_per_batch: int = 65536,
         points_per_ray: int | None = None, points_per_batch: int | None = None, loss: str = "l2", seed: int = 0,
         device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
-        add_poisson: bool = False, tv: float = 0.0) -> Reconstruction:
+        add_poisson: bool = False, tv: float = 0.0, resume_from=None, checkpoint_dir=None,
+        checkpoint_interval: float | None = None) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -211,7 +228,15 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     ``add_poisson`` the reference's Poisson term and ``tv`` > 0 the
     total-variation term of a static model on a random 100^3 sub-grid after
     the warm-up (base_trainer.py:615-649); these run the step as forward
-    half, torch loss, backward half."""
+    half, torch loss, backward half.
+
+    ``checkpoint_dir`` gets the run's checkpoint (checkpoint.save: model,
+    Adam state, epoch and angle) at the start, every ``checkpoint_interval``
+    seconds and at the end (base_trainer.py:297-299, 452-478).
+    ``resume_from`` (a last.ckpt) restores the model, the Adam state and the
+    position, and training continues from the next projection with the
+    schedule's settings at that point (base_trainer.py:189-212).  Random
+    draws (ray permutations, jitter, TV sub-grids) are not replayed."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -231,8 +256,12 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
                       loss=loss, lr=lr, device=dev)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
-    order = np.random.default_rng(seed).permutation(n_proj)
-    P = proj.shape[1]
+    start = 0
+    if resume_from is not None:
+        from . import checkpoint
+
+        pos = checkpoint.resume(resume_from, model, trainer)
+        start = int(pos["epoch"]) * n_proj + int(pos["angle"])
     train_s = 0.0
 
     def record(step):
@@ -240,7 +269,12 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
             torch.cuda.synchronize(dev)
             rec.history.append((step, train_s, evaluate(rec)))
 
-    settings = iter(schedule.steps()) if schedule is not None else None
+    def save(step, with_geometry=False):
+        from . import checkpoint
+
+        checkpoint.save(checkpoint_dir, model, trainer, geometry if with_geometry else None,
+                        epoch=step // n_proj, angle=step % n_proj)
+
     if schedule is not None:
         niter = min(niter, schedule.total_projections)
         rows, cols = geometry.nDetector
@@ -248,15 +282,14 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         ppb = trainer.points_per_batch
     binning = 1
     tv_rng = np.random.default_rng(seed + 7)
-    record(0)
-    for step in range(1, niter + 1):
-        k = int(order[(step - 1) % n_proj])
-        if (step - 1) % n_proj == n_proj - 1:
-            order = np.random.default_rng(seed + step).permutation(n_proj)
+    if checkpoint_dir is not None:
+        save(start, with_geometry=True)   # config and geometry before any detector binning
+    last_save = time.perf_counter()
+    record(start)
+    for step, k, st in step_plan(n_proj, seed, niter, schedule, start):
         t0 = time.perf_counter()
         target = proj[k]
-        if settings is not None:
-            st = next(settings)
+        if st is not None:
             if st.detector_binning != binning:
                 binning = st.detector_binning
                 geometry.set_detector_binning(binning)
@@ -282,10 +315,16 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
             record(step)
         else:
             train_s += time.perf_counter() - t0
+        if checkpoint_interval is not None and checkpoint_dir is not None and \
+                time.perf_counter() - last_save >= checkpoint_interval:
+            save(step)
+            last_save = time.perf_counter()
     torch.cuda.synchronize(dev)
     if binning != 1:
         geometry.set_detector_binning(1)
         trainer.c_geometry = geometry.get_c_geometry()
+    if checkpoint_dir is not None and niter > start:
+        save(niter)
     rec.train_seconds = train_s
     return rec
 

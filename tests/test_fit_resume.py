@@ -1,0 +1,57 @@
+"""fit()'s checkpoints and resume (CPU, with the fused step replaced by a stub
+that counts steps and moves the table): a run stopped after 12 steps and
+resumed from its checkpoint takes the projections an uninterrupted 20-step
+run takes at steps 13-20, with the model, Adam step count and position
+restored (base_trainer.py:189-212, 297-299)."""
+import numpy as np
+import torch
+
+
+def run(tmp_path, monkeypatch, niter, **kw):
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig
+    from nect_b200.reconstruct import fit
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import Trainer
+
+    seen = []
+
+    def fake_step(self, batch):
+        self.step_count += 1
+        seen.append((self.step_count, round(batch.angle, 6)))
+        with torch.no_grad():
+            self.model.table.add_(1.0)
+        return torch.zeros(1)
+
+    monkeypatch.setattr(Trainer, "step", fake_step)
+    monkeypatch.setattr(torch.cuda, "synchronize", lambda *a, **k: None)
+    geo = Geometry(nDetector=[16, 16], dDetector=[1 / 16] * 2, mode="parallel", nVoxel=[16] * 3, dVoxel=[1 / 16] * 3)
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=10, base_resolution=4,
+                            finest_resolution=32)
+    cfg = ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), "plain_fp32")
+    angles = np.linspace(0, np.pi, 7, endpoint=False)
+    projs = torch.rand(7, 16, 16, generator=torch.Generator().manual_seed(0))
+    rec = fit(geo, projs, angles, model_cfg=cfg, niter=niter, points_per_ray=8, rays_per_batch=32, seed=5,
+              device="cpu", **kw)
+    return rec, seen
+
+
+def test_resumed_fit_continues_the_uninterrupted_run(tmp_path, monkeypatch):
+    from nect_b200 import checkpoint
+
+    full, seen_full = run(tmp_path, monkeypatch, 20)
+    part, seen_part = run(tmp_path, monkeypatch, 12, checkpoint_dir=tmp_path / "a", checkpoint_interval=1e9)
+    ckpt = tmp_path / "a" / "model" / "checkpoints" / "last.ckpt"
+    data = torch.load(ckpt, map_location="cpu", weights_only=False)
+    assert (data["epoch"], data["angle"]) == (1, 5)          # 12 steps of 7 projections
+    assert (tmp_path / "a" / "model" / "geometry.yaml").exists()
+    assert seen_part == seen_full[:12]
+
+    resumed, seen_res = run(tmp_path, monkeypatch, 20, resume_from=ckpt, checkpoint_dir=tmp_path / "b")
+    assert seen_res == seen_full[12:]                          # steps 13..20, same projections
+    assert resumed.trainer.step_count == 20
+    assert torch.equal(resumed.model.table, full.model.table)
+    data = torch.load(tmp_path / "b" / "model" / "checkpoints" / "last.ckpt", map_location="cpu",
+                      weights_only=False)
+    assert (data["epoch"], data["angle"]) == (2, 6)
+    assert checkpoint.resume(tmp_path / "b" / "model" / "checkpoints" / "last.ckpt", resumed.model) == \
+        {"epoch": 2, "angle": 6}

@@ -48,3 +48,47 @@ def test_s3im_is_zero_for_identical_rays_and_grows_with_noise():
     assert float(s3im_loss(y, y, 64)) < 1e-6
     assert float(s3im_loss(y + 0.3 * torch.rand(4096), y, 64)) > 0.05
     assert float(s3im_loss(y, y, 4)) == 0.0
+
+
+def _old_loop_order(n_proj, seed, niter):
+    """The projection order of fit's loop as first written (inline)."""
+    import numpy as np
+
+    order = np.random.default_rng(seed).permutation(n_proj)
+    out = []
+    for step in range(1, niter + 1):
+        out.append(int(order[(step - 1) % n_proj]))
+        if (step - 1) % n_proj == n_proj - 1:
+            order = np.random.default_rng(seed + step).permutation(n_proj)
+    return out
+
+
+def test_step_plan_keeps_the_order_and_resumes_exactly():
+    from nect_b200.reconstruct import step_plan
+    from nect_b200.schedule import Schedule
+
+    n_proj, seed, niter = 7, 3, 40
+    full = list(step_plan(n_proj, seed, niter))
+    assert [k for _, k, _ in full] == _old_loop_order(n_proj, seed, niter)
+    assert [s for s, _, _ in full] == list(range(1, niter + 1))
+    for start in (1, 6, 7, 8, 20, 21, 39):
+        assert list(step_plan(n_proj, seed, niter, start=start)) == full[start:]
+
+    sch = Schedule([64, 64], n_projections=n_proj, epochs=6, base_lr=2e-3, downsampling_start=8,
+                   downsampling_update_interval=9, points_start=40, points_end=96, points_update_interval=4,
+                   warmup_steps=10)
+    full = list(step_plan(n_proj, seed, sch.total_projections, sch))
+    for start in (5, 14, 30):   # between the binning (9) and points-per-ray (4) updates
+        tail = list(step_plan(n_proj, seed, sch.total_projections, sch, start=start))
+        assert [(s, k) for s, k, _ in tail] == [(s, k) for s, k, _ in full[start:]]
+        for (_, _, a), (_, _, b) in zip(tail, full[start:]):
+            assert (a.detector_binning, a.points_per_ray) == (b.detector_binning, b.points_per_ray)
+            assert abs(a.lr - b.lr) <= 1e-12 * abs(b.lr)
+    # Resumed on an update boundary the reference applies that update twice:
+    # its resume derives binning and points per ray from projection // interval
+    # (base_trainer.py:198-205), then set_projection updates again at the same
+    # projection (base_trainer.py:244-262).  Schedule.steps(start) keeps that.
+    (_, _, a), (_, _, b) = next(iter(step_plan(n_proj, seed, sch.total_projections, sch, start=18))), full[18]
+    assert (a.detector_binning, a.points_per_ray) == (b.detector_binning // 2, b.points_per_ray)   # 18 % 9 == 0
+    (_, _, a), (_, _, b) = next(iter(step_plan(n_proj, seed, sch.total_projections, sch, start=36))), full[36]
+    assert (a.detector_binning, a.points_per_ray) == (b.detector_binning, b.points_per_ray + 1)    # 36 % 4 == 0
