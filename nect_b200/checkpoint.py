@@ -64,8 +64,10 @@ def _geometry_dict(geometry) -> dict:
 
 
 def save(run_dir: str | Path, model: _HashGridModel, trainer: Trainer | None = None, geometry=None,
-         epoch: int = 0, angle: int = 0) -> Path:
+         epoch: int = 0, angle: int = 0, keep_two: bool = False) -> Path:
     """Write ``run_dir/model/{config.yaml, geometry.yaml, checkpoints/last.ckpt}``.
+    With ``keep_two`` an existing last.ckpt first becomes 2nd_last.ckpt
+    (base_trainer.py:469-475).
 
     With a trainer whose optimizer is sharded over data-parallel ranks every
     rank calls this (the Adam moments are gathered); rank 0 writes."""
@@ -86,6 +88,8 @@ def save(run_dir: str | Path, model: _HashGridModel, trainer: Trainer | None = N
                           "param_groups": adam["param_groups"]}
         state["lr_scheduler"] = {"lr": trainer.lr}
     path = base / "checkpoints" / "last.ckpt"
+    if keep_two and path.exists():
+        path.replace(base / "checkpoints" / "2nd_last.ckpt")
     torch.save(state, path)
     return path
 

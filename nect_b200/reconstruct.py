@@ -231,8 +231,9 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     half, torch loss, backward half.
 
     ``checkpoint_dir`` gets the run's checkpoint (checkpoint.save: model,
-    Adam state, epoch and angle) at the start, every ``checkpoint_interval``
-    seconds and at the end (base_trainer.py:297-299, 452-478).
+    Adam state, epoch and angle; the previous one kept as 2nd_last.ckpt) at
+    the start, every ``checkpoint_interval`` seconds and at the end
+    (base_trainer.py:297-299, 452-478).
     ``resume_from`` (a last.ckpt) restores the model, the Adam state and the
     position, and training continues from the next projection with the
     schedule's settings at that point (base_trainer.py:189-212).  Random
@@ -273,7 +274,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         from . import checkpoint
 
         checkpoint.save(checkpoint_dir, model, trainer, geometry if with_geometry else None,
-                        epoch=step // n_proj, angle=step % n_proj)
+                        epoch=step // n_proj, angle=step % n_proj, keep_two=True)
 
     if schedule is not None:
         niter = min(niter, schedule.total_projections)

@@ -43,6 +43,9 @@ def test_resumed_fit_continues_the_uninterrupted_run(tmp_path, monkeypatch):
     ckpt = tmp_path / "a" / "model" / "checkpoints" / "last.ckpt"
     data = torch.load(ckpt, map_location="cpu", weights_only=False)
     assert (data["epoch"], data["angle"]) == (1, 5)          # 12 steps of 7 projections
+    prev = torch.load(tmp_path / "a" / "model" / "checkpoints" / "2nd_last.ckpt", map_location="cpu",
+                      weights_only=False)
+    assert (prev["epoch"], prev["angle"]) == (0, 0)           # the one saved at the start
     assert (tmp_path / "a" / "model" / "geometry.yaml").exists()
     assert seen_part == seen_full[:12]
 
