@@ -22,7 +22,9 @@ void clear_error() { g_last_error[0] = 0; }
 extern "C" const char* nectb_version(void) { return "nectb 0.1 sm_100a"; }
 extern "C" const char* nectb_last_error(void) { return nectb::g_last_error; }
 
-// ---- per-kernel event profiler --------------------------------------------
+// ---- per-kernel event profiler and NVTX ranges ----------------------------
+#include <nvtx3/nvToolsExt.h>
+
 #include <mutex>
 #include <vector>
 
@@ -38,6 +40,10 @@ std::vector<ProfRec> g_prof_pending;
 std::vector<cudaEvent_t> g_prof_free;
 int g_prof_launches[NECTB_PROFILE_SLOTS];
 double g_prof_ms[NECTB_PROFILE_SLOTS];
+// NVTX range names of the slots (ncu --nvtx --nvtx-include "nectb backward/")
+const char* const kProfNames[NECTB_PROFILE_SLOTS] = {
+    "nectb ray preparation", "nectb forward", "nectb backward", "nectb adam", "nectb sampling",
+    "nectb model and queries", "nectb staged scatter", "nectb ray ordering", "nectb time slice"};
 
 cudaEvent_t prof_event() {
   if (!g_prof_free.empty()) {
@@ -51,7 +57,11 @@ cudaEvent_t prof_event() {
 }
 }  // namespace
 
+// The NVTX range brackets the launches of the scope on the host thread
+// (a no-op unless a tool is attached); the events time them on the stream
+// while profiling is enabled.
 ProfScope::ProfScope(int slot, cudaStream_t s) : slot_(slot), s_(s), a_(nullptr) {
+  nvtxRangePushA(kProfNames[slot]);
   std::lock_guard<std::mutex> lk(g_prof_mu);
   if (!g_prof_on) return;
   a_ = prof_event();
@@ -59,11 +69,13 @@ ProfScope::ProfScope(int slot, cudaStream_t s) : slot_(slot), s_(s), a_(nullptr)
 }
 
 ProfScope::~ProfScope() {
-  if (!a_) return;
-  std::lock_guard<std::mutex> lk(g_prof_mu);
-  cudaEvent_t b = prof_event();
-  cudaEventRecord(b, s_);
-  g_prof_pending.push_back({slot_, (cudaEvent_t)a_, b});
+  if (a_) {
+    std::lock_guard<std::mutex> lk(g_prof_mu);
+    cudaEvent_t b = prof_event();
+    cudaEventRecord(b, s_);
+    g_prof_pending.push_back({slot_, (cudaEvent_t)a_, b});
+  }
+  nvtxRangePop();
 }
 
 }  // namespace nectb
