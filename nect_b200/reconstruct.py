@@ -213,7 +213,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
         add_poisson: bool = False, tv: float = 0.0, resume_from=None, checkpoint_dir=None,
-        checkpoint_interval: float | None = None) -> Reconstruction:
+        checkpoint_interval: float | None = None, log_fn=None) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -237,7 +237,14 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     ``resume_from`` (a last.ckpt) restores the model, the Adam state and the
     position, and training continues from the next projection with the
     schedule's settings at that point (base_trainer.py:189-212).  Random
-    draws (ray permutations, jitter, TV sub-grids) are not replayed."""
+    draws (ray permutations, jitter, TV sub-grids) are not replayed.
+
+    ``log_fn(step, metrics)`` is called after every step with the keys the
+    reference logs (base_trainer.py:596-609: loss, max_mem, current_mem,
+    epoch, downsample_detector_factor, points_per_ray,
+    distance_between_points, lr, num_proj_processed) and the batch's rays;
+    the loss is the device tensor, so logging adds no synchronisation unless
+    ``log_fn`` reads it."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -306,10 +313,18 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
             warm = schedule.warmup[0] if schedule is not None else 0
             patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
             tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
-            trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
-                               tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
+            loss = trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
+                                      tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
         else:
-            trainer.step(batch)
+            loss = trainer.step(batch)
+        if log_fn is not None:
+            on_gpu = dev.type == "cuda"
+            free, total = torch.cuda.mem_get_info(dev) if on_gpu else (0, 0)
+            log_fn(step, {"loss": loss, "max_mem": torch.cuda.max_memory_allocated(dev) if on_gpu else 0,
+                          "current_mem": total - free, "epoch": (step - 1) // n_proj,
+                          "downsample_detector_factor": binning, "points_per_ray": trainer.points_per_ray,
+                          "distance_between_points": batch.max_ray_distance_per_point, "lr": trainer.lr,
+                          "num_proj_processed": step - 1, "rays": batch.num_rays})
         if eval_every and (step % eval_every == 0 or step == niter):
             torch.cuda.synchronize(dev)
             train_s += time.perf_counter() - t0

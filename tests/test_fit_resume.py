@@ -58,3 +58,15 @@ def test_resumed_fit_continues_the_uninterrupted_run(tmp_path, monkeypatch):
     assert (data["epoch"], data["angle"]) == (2, 6)
     assert checkpoint.resume(tmp_path / "b" / "model" / "checkpoints" / "last.ckpt", resumed.model) == \
         {"epoch": 2, "angle": 6}
+
+
+def test_fit_logs_the_reference_keys(tmp_path, monkeypatch):
+    logged = []
+    run(tmp_path, monkeypatch, 9, log_fn=lambda step, m: logged.append((step, m)))
+    assert [s for s, _ in logged] == list(range(1, 10))
+    keys = {"loss", "max_mem", "current_mem", "epoch", "downsample_detector_factor", "points_per_ray",
+            "distance_between_points", "lr", "num_proj_processed", "rays"}
+    assert all(set(m) == keys for _, m in logged)
+    step, m = logged[-1]
+    assert (m["epoch"], m["num_proj_processed"], m["points_per_ray"], m["downsample_detector_factor"]) == (1, 8, 8, 1)
+
