@@ -15,6 +15,7 @@ terms; ``reconstruct`` resolves the reference's quality presets into them.
 """
 from __future__ import annotations
 
+import datetime
 import math
 import time
 from dataclasses import dataclass, field
@@ -40,6 +41,7 @@ class Reconstruction:
     maximum: float
     trainer: Trainer
     history: list = field(default_factory=list)   # (step, seconds of training, metrics dict)
+    stopped: str | None = None                    # "cancelled" (cancel_at) or "interrupted" (KeyboardInterrupt)
 
     def volume(self, t: float = 0.0, shape: tuple | None = None) -> torch.Tensor:
         """Attenuation on the voxel-centre grid [z, y, x] (create_volume)."""
@@ -213,7 +215,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
         add_poisson: bool = False, tv: float = 0.0, resume_from=None, checkpoint_dir=None,
-        checkpoint_interval: float | None = None, log_fn=None) -> Reconstruction:
+        checkpoint_interval: float | None = None, log_fn=None, cancel_at=None) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -244,7 +246,13 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     epoch, downsample_detector_factor, points_per_ray,
     distance_between_points, lr, num_proj_processed) and the batch's rays;
     the loss is the device tensor, so logging adds no synchronisation unless
-    ``log_fn`` reads it."""
+    ``log_fn`` reads it.
+
+    ``cancel_at`` (an ISO date-time string or datetime; UTC when it names no
+    zone) ends training after the first step that finishes later, saving the
+    checkpoint; a KeyboardInterrupt ends it too, saving only after more than
+    3000 steps (base_trainer.py:281-284, 659-666).  Where the reference then
+    exits the process, this returns the Reconstruction with ``stopped`` set."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -264,6 +272,13 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
                       loss=loss, lr=lr, device=dev)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
+    if isinstance(cancel_at, str):
+        try:
+            cancel_at = datetime.datetime.fromisoformat(cancel_at)
+        except ValueError:
+            raise ValueError(f"cancel_at {cancel_at!r} is not an ISO date-time") from None
+    if cancel_at is not None and cancel_at.tzinfo is None:
+        cancel_at = cancel_at.replace(tzinfo=datetime.timezone.utc)
     start = 0
     if resume_from is not None:
         from . import checkpoint
@@ -294,53 +309,62 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         save(start, with_geometry=True)   # config and geometry before any detector binning
     last_save = time.perf_counter()
     record(start)
-    for step, k, st in step_plan(n_proj, seed, niter, schedule, start):
-        t0 = time.perf_counter()
-        target = proj[k]
-        if st is not None:
-            if st.detector_binning != binning:
-                binning = st.detector_binning
-                geometry.set_detector_binning(binning)
-                trainer.c_geometry = geometry.get_c_geometry()
-            target = bin_projection(raw[k], binning).reshape(-1).contiguous()
-            trainer.points_per_ray = st.points_per_ray
-            trainer.points_per_batch = ppb
-            trainer.random_offset_detector = st.random_offset_detector
-            trainer.lr = st.lr
-        perm = torch.randperm(target.numel(), dtype=torch.int64, device=dev)
-        batch = trainer.make_batch(perm, 0, angles[k], target, ts[k])
-        if s3im or add_poisson or tv > 0:
-            warm = schedule.warmup[0] if schedule is not None else 0
-            patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
-            tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
-            loss = trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
-                                      tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
-        else:
-            loss = trainer.step(batch)
-        if log_fn is not None:
-            on_gpu = dev.type == "cuda"
-            free, total = torch.cuda.mem_get_info(dev) if on_gpu else (0, 0)
-            log_fn(step, {"loss": loss, "max_mem": torch.cuda.max_memory_allocated(dev) if on_gpu else 0,
-                          "current_mem": total - free, "epoch": (step - 1) // n_proj,
-                          "downsample_detector_factor": binning, "points_per_ray": trainer.points_per_ray,
-                          "distance_between_points": batch.max_ray_distance_per_point, "lr": trainer.lr,
-                          "num_proj_processed": step - 1, "rays": batch.num_rays})
-        if eval_every and (step % eval_every == 0 or step == niter):
-            torch.cuda.synchronize(dev)
-            train_s += time.perf_counter() - t0
-            record(step)
-        else:
-            train_s += time.perf_counter() - t0
-        if checkpoint_interval is not None and checkpoint_dir is not None and \
-                time.perf_counter() - last_save >= checkpoint_interval:
-            save(step)
-            last_save = time.perf_counter()
+    done = start
+    try:
+        for step, k, st in step_plan(n_proj, seed, niter, schedule, start):
+            t0 = time.perf_counter()
+            target = proj[k]
+            if st is not None:
+                if st.detector_binning != binning:
+                    binning = st.detector_binning
+                    geometry.set_detector_binning(binning)
+                    trainer.c_geometry = geometry.get_c_geometry()
+                target = bin_projection(raw[k], binning).reshape(-1).contiguous()
+                trainer.points_per_ray = st.points_per_ray
+                trainer.points_per_batch = ppb
+                trainer.random_offset_detector = st.random_offset_detector
+                trainer.lr = st.lr
+            perm = torch.randperm(target.numel(), dtype=torch.int64, device=dev)
+            batch = trainer.make_batch(perm, 0, angles[k], target, ts[k])
+            if s3im or add_poisson or tv > 0:
+                warm = schedule.warmup[0] if schedule is not None else 0
+                patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
+                tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
+                loss = trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
+                                          tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
+            else:
+                loss = trainer.step(batch)
+            done = step
+            if log_fn is not None:
+                on_gpu = dev.type == "cuda"
+                free, total = torch.cuda.mem_get_info(dev) if on_gpu else (0, 0)
+                log_fn(step, {"loss": loss, "max_mem": torch.cuda.max_memory_allocated(dev) if on_gpu else 0,
+                              "current_mem": total - free, "epoch": (step - 1) // n_proj,
+                              "downsample_detector_factor": binning, "points_per_ray": trainer.points_per_ray,
+                              "distance_between_points": batch.max_ray_distance_per_point, "lr": trainer.lr,
+                              "num_proj_processed": step - 1, "rays": batch.num_rays})
+            if eval_every and (step % eval_every == 0 or step == niter):
+                torch.cuda.synchronize(dev)
+                train_s += time.perf_counter() - t0
+                record(step)
+            else:
+                train_s += time.perf_counter() - t0
+            if checkpoint_interval is not None and checkpoint_dir is not None and \
+                    time.perf_counter() - last_save >= checkpoint_interval:
+                save(step)
+                last_save = time.perf_counter()
+            if cancel_at is not None and datetime.datetime.now(datetime.timezone.utc) > cancel_at:
+                rec.stopped = "cancelled"
+                break
+    except KeyboardInterrupt:
+        rec.stopped = "interrupted"
     torch.cuda.synchronize(dev)
     if binning != 1:
         geometry.set_detector_binning(1)
         trainer.c_geometry = geometry.get_c_geometry()
-    if checkpoint_dir is not None and niter > start:
-        save(niter)
+    # after an interrupt the reference saves only runs of more than 3000 steps
+    if checkpoint_dir is not None and done > start and (rec.stopped != "interrupted" or done > 3000):
+        save(done)
     rec.train_seconds = train_s
     return rec
 

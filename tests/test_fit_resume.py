@@ -70,3 +70,46 @@ def test_fit_logs_the_reference_keys(tmp_path, monkeypatch):
     step, m = logged[-1]
     assert (m["epoch"], m["num_proj_processed"], m["points_per_ray"], m["downsample_detector_factor"]) == (1, 8, 8, 1)
 
+
+
+def test_cancel_at_stops_and_saves(tmp_path, monkeypatch):
+    import datetime
+
+    import pytest
+
+    rec, seen = run(tmp_path, monkeypatch, 20, checkpoint_dir=tmp_path / "c", cancel_at="2000-01-01T00:00:00")
+    assert rec.stopped == "cancelled" and len(seen) == 1 and rec.trainer.step_count == 1
+    data = torch.load(tmp_path / "c" / "model" / "checkpoints" / "last.ckpt", map_location="cpu", weights_only=False)
+    assert (data["epoch"], data["angle"]) == (0, 1)
+    later = datetime.datetime.now(datetime.timezone.utc) + datetime.timedelta(days=1)
+    rec, seen = run(tmp_path, monkeypatch, 5, cancel_at=later)
+    assert rec.stopped is None and len(seen) == 5
+    with pytest.raises(ValueError, match="ISO"):
+        run(tmp_path, monkeypatch, 5, cancel_at="tomorrow")
+
+
+def test_keyboard_interrupt_ends_training_without_a_save_before_3000_steps(tmp_path, monkeypatch):
+    from nect_b200.trainer import Trainer
+
+    rec, seen = run(tmp_path, monkeypatch, 3)          # installs the stub
+    stub = Trainer.step
+
+    def interrupting(self, batch):
+        if self.step_count == 4:
+            raise KeyboardInterrupt
+        return stub(self, batch)
+
+    monkeypatch.setattr(Trainer, "step", interrupting)
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig
+    from nect_b200.reconstruct import fit
+    from nect_b200.sampling import Geometry
+
+    geo = Geometry(nDetector=[16, 16], dDetector=[1 / 16] * 2, mode="parallel", nVoxel=[16] * 3, dVoxel=[1 / 16] * 3)
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=10, base_resolution=4,
+                            finest_resolution=32)
+    cfg = ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), "plain_fp32")
+    rec = fit(geo, torch.rand(7, 16, 16), np.linspace(0, np.pi, 7, endpoint=False), model_cfg=cfg, niter=20,
+              points_per_ray=8, rays_per_batch=32, device="cpu", checkpoint_dir=tmp_path / "k")
+    assert rec.stopped == "interrupted" and rec.trainer.step_count == 4
+    data = torch.load(tmp_path / "k" / "model" / "checkpoints" / "last.ckpt", map_location="cpu", weights_only=False)
+    assert (data["epoch"], data["angle"]) == (0, 0)     # only the checkpoint written at the start
