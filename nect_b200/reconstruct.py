@@ -76,7 +76,8 @@ def default_model_config(geometry: Geometry, mode: str, precision: str, log2_has
 _COMMON_CONFIG = {"loss": "l1", "epochs": "auto", "lrf": "auto", "lr_otype": "cosine", "warmup_otype": "exponential",
                   "points_start": 100, "points_end": "auto", "points_update_interval": "auto", "points_linear": True,
                   "downsampling_start": 2, "downsampling_end": 1, "downsampling_update_interval": 1000,
-                  "points_per_batch": "auto", "s3im": False, "add_poisson": False}
+                  "points_per_batch": "auto", "s3im": False, "add_poisson": False, "batch_per_proj": 1,
+                  "clip_grad_value": None}
 _BASE_CONFIG = {
     "static": dict(_COMMON_CONFIG, base_lr=1e-3, warmup_steps=500, warmup_lr0=1e-3, log2_hashmap_size=21),
     "dynamic": dict(_COMMON_CONFIG, base_lr=2e-4, warmup_steps=2000, warmup_lr0=1e-4, log2_hashmap_size=23),
@@ -86,7 +87,8 @@ _BASE_CONFIG = {
 # -> the fields above; nested sections map key by key.
 _OVERRIDE_KEYS = {
     "epochs": "epochs", "base_lr": "base_lr", "loss": "loss", "points_per_batch": "points_per_batch",
-    "s3im": "s3im", "add_poisson": "add_poisson",
+    "s3im": "s3im", "add_poisson": "add_poisson", "batch_per_proj": "batch_per_proj",
+    "clip_grad_value": "clip_grad_value",
     ("warmup", "steps"): "warmup_steps", ("warmup", "lr0"): "warmup_lr0", ("warmup", "otype"): "warmup_otype",
     ("lr_scheduler", "otype"): "lr_otype", ("lr_scheduler", "lrf"): "lrf",
     ("points_per_ray", "start"): "points_start", ("points_per_ray", "end"): "points_end",
@@ -215,7 +217,8 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         device="cuda",
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
         add_poisson: bool = False, tv: float = 0.0, resume_from=None, checkpoint_dir=None,
-        checkpoint_interval: float | None = None, log_fn=None, cancel_at=None) -> Reconstruction:
+        checkpoint_interval: float | None = None, log_fn=None, cancel_at=None, batch_per_proj: int | str = 1,
+        clip_grad_value: float | None = None) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -252,7 +255,14 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     zone) ends training after the first step that finishes later, saving the
     checkpoint; a KeyboardInterrupt ends it too, saving only after more than
     3000 steps (base_trainer.py:281-284, 659-666).  Where the reference then
-    exits the process, this returns the Reconstruction with ``stopped`` set."""
+    exits the process, this returns the Reconstruction with ``stopped`` set.
+
+    ``batch_per_proj`` (an int or "all") batches of rays are taken from each
+    projection visit, each an optimizer step with the projection's settings,
+    up to the batches the detector holds (base_trainer.py:517-520);
+    ``clip_grad_value`` clamps the gradients before each Adam step
+    (base_trainer.py:651-652).  ``niter``, checkpoints and resume count
+    projection visits."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
     n_proj = proj.shape[0]
@@ -270,7 +280,8 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     model = get_model(cfg, device=dev)
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
     trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
-                      loss=loss, lr=lr, device=dev)
+                      loss=loss, lr=lr, device=dev, clip_grad_value=clip_grad_value)
+    n_batches = 10 ** 9 if batch_per_proj == "all" else int(batch_per_proj)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
     if isinstance(cancel_at, str):
         try:
@@ -309,7 +320,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         save(start, with_geometry=True)   # config and geometry before any detector binning
     last_save = time.perf_counter()
     record(start)
-    done = start
+    done, taken = start, 0   # projection visits completed, optimizer steps taken in this call
     try:
         for step, k, st in step_plan(n_proj, seed, niter, schedule, start):
             t0 = time.perf_counter()
@@ -325,24 +336,29 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
                 trainer.random_offset_detector = st.random_offset_detector
                 trainer.lr = st.lr
             perm = torch.randperm(target.numel(), dtype=torch.int64, device=dev)
-            batch = trainer.make_batch(perm, 0, angles[k], target, ts[k])
-            if s3im or add_poisson or tv > 0:
-                warm = schedule.warmup[0] if schedule is not None else 0
-                patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
-                tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
-                loss = trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
-                                          tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
-            else:
-                loss = trainer.step(batch)
+            for batch_num in range(n_batches):
+                batch = trainer.make_batch(perm, batch_num, angles[k], target, ts[k])
+                if batch is None:   # past the detector's batches (Projector.batch_per_epoch)
+                    break
+                if s3im or add_poisson or tv > 0:
+                    warm = schedule.warmup[0] if schedule is not None else 0
+                    patch = s3im_patch_size(target.numel(), trainer.batch_size) if s3im and step > warm else 0
+                    tv_w = tv if (tv > 0 and mode == "static" and step > warm) else 0.0
+                    loss = trainer.split_step(batch, add_poisson=add_poisson, s3im_patch=patch, tv_weight=tv_w,
+                                              tv_origin=tv_rng.random(3) * 0.8 if tv_w else None)
+                else:
+                    loss = trainer.step(batch)
+                taken += 1
+                if log_fn is not None:
+                    on_gpu = dev.type == "cuda"
+                    free, total = torch.cuda.mem_get_info(dev) if on_gpu else (0, 0)
+                    log_fn(trainer.step_count, {
+                        "loss": loss, "max_mem": torch.cuda.max_memory_allocated(dev) if on_gpu else 0,
+                        "current_mem": total - free, "epoch": (step - 1) // n_proj,
+                        "downsample_detector_factor": binning, "points_per_ray": trainer.points_per_ray,
+                        "distance_between_points": batch.max_ray_distance_per_point, "lr": trainer.lr,
+                        "num_proj_processed": step - 1, "rays": batch.num_rays})
             done = step
-            if log_fn is not None:
-                on_gpu = dev.type == "cuda"
-                free, total = torch.cuda.mem_get_info(dev) if on_gpu else (0, 0)
-                log_fn(step, {"loss": loss, "max_mem": torch.cuda.max_memory_allocated(dev) if on_gpu else 0,
-                              "current_mem": total - free, "epoch": (step - 1) // n_proj,
-                              "downsample_detector_factor": binning, "points_per_ray": trainer.points_per_ray,
-                              "distance_between_points": batch.max_ray_distance_per_point, "lr": trainer.lr,
-                              "num_proj_processed": step - 1, "rays": batch.num_rays})
             if eval_every and (step % eval_every == 0 or step == niter):
                 torch.cuda.synchronize(dev)
                 train_s += time.perf_counter() - t0
@@ -363,7 +379,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         geometry.set_detector_binning(1)
         trainer.c_geometry = geometry.get_c_geometry()
     # after an interrupt the reference saves only runs of more than 3000 steps
-    if checkpoint_dir is not None and done > start and (rec.stopped != "interrupted" or done > 3000):
+    if checkpoint_dir is not None and done > start and (rec.stopped != "interrupted" or taken > 3000):
         save(done)
     rec.train_seconds = train_s
     return rec
@@ -409,6 +425,8 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
                                config_override=config_override)
     kw.setdefault("s3im", bool(plan.config["s3im"]))
     kw.setdefault("add_poisson", bool(plan.config["add_poisson"]))
+    kw.setdefault("batch_per_proj", plan.config["batch_per_proj"])
+    kw.setdefault("clip_grad_value", plan.config["clip_grad_value"])
     if verbose:
         sch = plan.schedule
         print(f"nect_b200.reconstruct: {mode}, quality {quality}: {sch.total_projections} steps "

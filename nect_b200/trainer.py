@@ -336,10 +336,11 @@ class ShardedAdam:
 
     @torch.no_grad()
     def step(self, step: int, lr: float, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0,
-             halves=None) -> None:
+             halves=None, clip: float | None = None) -> None:
         """One update from the gradients accumulated in ``self.grads`` (zeroed
         afterwards).  ``halves[i]``, when given, is an fp16 copy of params[i]
-        that is rewritten from the updated parameters."""
+        that is rewritten from the updated parameters; ``clip`` clamps the
+        averaged gradients to [-clip, clip]."""
         import torch.distributed as dist
 
         halves = halves or [None] * len(self.params)
@@ -347,6 +348,8 @@ class ShardedAdam:
             n, chunk, lo, valid = self.shards[i]
             dist.reduce_scatter_tensor(self.shard_grad[i], self.grad_pad[i], op=dist.ReduceOp.SUM, group=self.group)
             self.shard_grad[i].div_(self.world)
+            if clip is not None:
+                self.shard_grad[i].clamp_(-clip, clip)
             self.grad_pad[i].zero_()
             flat = p.view(-1)
             if valid > 0:
@@ -397,7 +400,7 @@ class Trainer:
                  loss: str = "l2", lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8,
                  weight_decay: float = 0.0, batch_per_proj: int = 1, random_offset_detector: float = 0.0,
                  uniform_ray_spacing: bool = True, device="cuda", data_parallel: bool = False, process_group=None,
-                 shard_optimizer: bool = False):
+                 shard_optimizer: bool = False, clip_grad_value: float | None = None):
         self.model = model
         self.geometry = geometry
         self.c_geometry = geometry.get_c_geometry()
@@ -414,6 +417,8 @@ class Trainer:
         self.uniform_ray_spacing = uniform_ray_spacing
         self.step_count = 0
         self.workspace = Workspace()
+        # gradients clamped to [-c, c] after the averaging over ranks (base_trainer.py:651-652)
+        self.clip_grad_value = clip_grad_value
         # data parallel: every rank trains on its own rays, gradients are averaged before Adam
         self.data_parallel = data_parallel
         self.process_group = process_group
@@ -469,10 +474,13 @@ class Trainer:
                 self.table_grad.add_(g_table)
                 self.mlp_grad.add_(g_mlp)
             self.sharded.step(self.step_count, self.lr, self.betas, self.eps, self.weight_decay,
-                              halves=[self.model.table_half, None])
+                              halves=[self.model.table_half, None], clip=self.clip_grad_value)
             return
         if self.data_parallel:
             reduce_gradients([g_table, g_mlp], self.process_group)
+        if self.clip_grad_value is not None:
+            g_table.clamp_(-self.clip_grad_value, self.clip_grad_value)
+            g_mlp.clamp_(-self.clip_grad_value, self.clip_grad_value)
         adam_step(self.model.table, g_table, self.m_table, self.v_table, self.step_count, self.lr, self.betas,
                   self.eps, self.weight_decay, half=self.model.table_half)
         adam_step(self.model.mlp, g_mlp, self.m_mlp, self.v_mlp, self.step_count, self.lr, self.betas, self.eps,

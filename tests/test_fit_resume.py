@@ -113,3 +113,12 @@ def test_keyboard_interrupt_ends_training_without_a_save_before_3000_steps(tmp_p
     assert rec.stopped == "interrupted" and rec.trainer.step_count == 4
     data = torch.load(tmp_path / "k" / "model" / "checkpoints" / "last.ckpt", map_location="cpu", weights_only=False)
     assert (data["epoch"], data["angle"]) == (0, 0)     # only the checkpoint written at the start
+
+
+def test_batches_per_projection(tmp_path, monkeypatch):
+    rec, seen = run(tmp_path, monkeypatch, 5, batch_per_proj=3)
+    assert len(seen) == 15 and rec.trainer.step_count == 15
+    angles = [a for _, a in seen]
+    assert all(angles[3 * i] == angles[3 * i + 1] == angles[3 * i + 2] for i in range(5))
+    rec, seen = run(tmp_path, monkeypatch, 2, batch_per_proj="all")   # 256 pixels / 32 rays
+    assert len(seen) == 16

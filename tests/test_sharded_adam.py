@@ -30,7 +30,8 @@ def cpu_adam(param, grad, m, v, step, lr, betas=(0.9, 0.999), eps=1e-8, weight_d
 
 
 def rel(a, b):
-    return float((a.double() - b.double()).abs().max() / b.double().abs().max().clamp(min=1e-30))
+    a, b = a.detach().double(), b.detach().double()
+    return float((a - b).abs().max() / b.abs().max().clamp(min=1e-30))
 
 
 def make_trainer():
@@ -160,3 +161,49 @@ class _DummyGeometry:
 class _DummyModel:
     table = torch.zeros(4)
     mlp = torch.zeros(4)
+
+
+def test_gradient_value_clipping_both_optimizer_paths(monkeypatch):
+    """clip_grad_value clamps the averaged gradients before Adam
+    (base_trainer.py:651-652), in the plain update and in the sharded one."""
+    import torch.distributed as dist
+
+    from nect_b200 import trainer as tmod
+    from nect_b200.trainer import ShardedAdam
+
+    g = torch.Generator().manual_seed(4)
+    # plain path: Trainer._update with the module's Adam replaced by the torch rule
+    monkeypatch.setattr(tmod, "adam_step", torch.no_grad()(cpu_adam))   # the kernel writes through pointers
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig, get_model
+    from nect_b200.sampling import Geometry
+
+    geo = Geometry(nDetector=[32, 32], dDetector=[1.0, 1.0], mode="cone", DSD=300.0, DSO=200.0, nVoxel=[16] * 3,
+                   dVoxel=[1.0] * 3)
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=10, base_resolution=4,
+                            finest_resolution=64)
+    model = get_model(ModelConfig("hash_grid", enc, MLPNetConfig(n_hidden_layers=2), "plain_fp32"), device="cpu")
+    tr = tmod.Trainer(model, geo, points_per_batch=64 * 32, points_per_ray=32, lr=LR, device="cpu",
+                      clip_grad_value=0.05)
+    t0, m0 = model.table.detach().clone(), model.mlp.detach().clone()
+    gt, gm = torch.randn(t0.shape, generator=g), torch.randn(m0.shape, generator=g)
+    ref_t, ref_m = t0.clone(), m0.clone()
+    cpu_adam(ref_t, gt.clamp(-0.05, 0.05), torch.zeros_like(t0), torch.zeros_like(t0), 1, LR)
+    cpu_adam(ref_m, gm.clamp(-0.05, 0.05), torch.zeros_like(m0), torch.zeros_like(m0), 1, LR)
+    tr._update(gt.clone(), gm.clone())
+    assert rel(model.table, ref_t) < 1e-6 and rel(model.mlp, ref_m) < 1e-6
+
+    # sharded path on a one-rank group
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(28000 + os.getpid() % 1000)
+    dist.init_process_group("gloo", rank=0, world_size=1)
+    try:
+        p = torch.rand(100, generator=g)
+        ref = p.clone()
+        grad = torch.randn(100, generator=g)
+        sa = ShardedAdam([p], adam=cpu_adam)
+        sa.grads[0].add_(grad)
+        sa.step(1, LR, clip=0.1)
+        cpu_adam(ref, grad.clamp(-0.1, 0.1), torch.zeros(100), torch.zeros(100), 1, LR)
+        assert rel(p, ref) < 1e-6
+    finally:
+        dist.destroy_process_group()
