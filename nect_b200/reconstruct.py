@@ -143,6 +143,8 @@ def preset_config(mode: str, quality: str = "high", niter=None, lr: float | None
     override (nect/reconstruct.py:205-216)."""
     if quality not in QUALITY_PRESETS:
         raise ValueError(f"quality must be one of {list(QUALITY_PRESETS)} (got {quality!r})")
+    if mode not in _BASE_CONFIG:
+        raise ValueError(f"mode must be 'static' or 'dynamic' (got {mode!r})")
     cfg = dict(_BASE_CONFIG[mode])
     preset = QUALITY_PRESETS[quality]
     cfg.update(preset["set"])

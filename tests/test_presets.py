@@ -46,6 +46,8 @@ def test_dynamic_defaults_and_overrides():
     assert cfg["epochs"] == 7 and cfg["base_lr"] == 3e-3
     with pytest.raises(ValueError, match="quality"):
         preset_config("static", "best")
+    with pytest.raises(ValueError, match="mode"):
+        preset_config("4d", "high")
 
 
 def test_learning_rate_rule():
