@@ -2,8 +2,11 @@
 that counts steps and moves the table): a run stopped after 12 steps and
 resumed from its checkpoint takes the projections an uninterrupted 20-step
 run takes at steps 13-20, with the model, Adam step count and position
-restored (base_trainer.py:189-212, 297-299)."""
+restored (base_trainer.py:189-212, 297-299); the metrics log, cancel_at and
+KeyboardInterrupt handling, several batches per projection, and the batches
+Trainer.make_batch cuts from a projection."""
 import numpy as np
+import pytest
 import torch
 
 
@@ -122,3 +125,35 @@ def test_batches_per_projection(tmp_path, monkeypatch):
     assert all(angles[3 * i] == angles[3 * i + 1] == angles[3 * i + 2] for i in range(5))
     rec, seen = run(tmp_path, monkeypatch, 2, batch_per_proj="all")   # 256 pixels / 32 rays
     assert len(seen) == 16
+
+
+@pytest.mark.parametrize("P,bs,expect", [
+    (1024, 64, [(0, 64), (64, 64), (960, 64), None]),   # batches 0, 1, 15, 16
+    (40, 64, [(0, 40), None, None, None]),               # partial first batch (projector.py:108-112)
+    (128, 64, [(0, 64), (64, 64), None, None]),
+])
+def test_make_batch_follows_the_projector(P, bs, expect):
+    """Batches of a projection: full batches of batch_size rays from the
+    permutation, the partial first batch when the detector holds fewer, and
+    None past the end; jitter in [-0.5, 0.5) and detector offsets scaled by
+    random_offset_detector (ct_sampling.cu:619-622)."""
+    from nect_b200.trainer import Trainer
+
+    tr = Trainer.__new__(Trainer)
+    tr.points_per_batch, tr.points_per_ray, tr.random_offset_detector = bs * 8, 8, 0.5
+    tr.device, tr.uniform_ray_spacing = torch.device("cpu"), True
+
+    class Geo:
+        max_distance_traveled = 4.0
+
+    tr.geometry = Geo()
+    perm = torch.randperm(P)
+    got = []
+    for batch_num in (0, 1, 15, 16):
+        b = tr.make_batch(perm, batch_num, 0.3, torch.zeros(P), t=0.2)
+        got.append(None if b is None else (b.start, b.num_rays))
+        if b is not None:
+            assert b.jitter.shape == (b.num_rays,) and bool((b.jitter.abs() <= 0.5).all())
+            assert b.detector_offset.shape == (b.num_rays, 2) and bool((b.detector_offset.abs() <= 0.25).all())
+            assert b.max_ray_distance_per_point == 0.5 and (b.angle, b.t) == (0.3, 0.2)
+    assert got == expect
