@@ -28,6 +28,19 @@ from .sampling.geometry import Geometry
 LOSS = {"l1": 1, "l2": 2}
 
 
+def loss_kind(loss: str) -> str:
+    """The reference's loss selection (nect/config.py:481-497): "l1" when the
+    name contains l1 (so "L1+L2" is L1, its alternating branch being
+    unreachable there), else "l2" when it contains l2; other names raise
+    NotImplementedError."""
+    name = loss.casefold()
+    if "l1" in name:
+        return "l1"
+    if "l2" in name:
+        return "l2"
+    raise NotImplementedError(f"Loss {loss} is not supported")
+
+
 @dataclass
 class RayBatch:
     """One batch of rays of one projection (Projector.__call__ arguments)."""
@@ -100,7 +113,7 @@ def c_batch(batch: RayBatch, max_distance_traveled: float, loss: str, loss_scale
     b.jitter = batch.jitter.data_ptr()
     b.detector_offset = batch.detector_offset.data_ptr()
     b.projection = batch.projection.data_ptr()
-    b.loss_type = LOSS[loss.lower()]
+    b.loss_type = LOSS[loss_kind(loss)]
     b.loss_scale = float(loss_scale)
     return b
 
@@ -228,8 +241,8 @@ def tv_points(origin, n: int = 100, extent: float = 0.2, device="cuda") -> torch
 
 
 def projection_loss(y_pred: torch.Tensor, y: torch.Tensor, loss: str) -> torch.Tensor:
-    """L1 or L2 (mean over rays), nect/config.py:481-497."""
-    if loss.lower() == "l1":
+    """L1 or L2 (mean over rays), nect/config.py:481-497 (loss_kind)."""
+    if loss_kind(loss) == "l1":
         return torch.nn.functional.l1_loss(y_pred, y)
     return torch.nn.functional.mse_loss(y_pred, y)
 

@@ -2,7 +2,8 @@
 HashEncoderConfig.per_level_scale (nect/config.py:99-112) for both resolution
 types and sample_outside, its error when the size is missing, and the tcnn
 schema dicts of get_encoder_config / get_network_config
-(nect/config.py:86-94, 125-132)."""
+(nect/config.py:86-94, 125-132), and the loss selection by name
+(nect/config.py:481-497)."""
 import pytest
 
 
@@ -32,3 +33,16 @@ def test_tcnn_schema_dicts():
     cfg = net.get_network_config()
     assert set(cfg) == {"otype", "n_hidden_layers", "n_neurons", "activation", "output_activation"}
     assert (cfg["n_hidden_layers"], cfg["n_neurons"], cfg["activation"]) == (3, 64, "ReLU")
+
+
+def test_loss_selection_follows_the_reference():
+    import torch
+
+    from nect_b200.trainer import loss_kind, projection_loss
+
+    assert [loss_kind(n) for n in ("L1", "l2", "L1+L2", "myl2")] == ["l1", "l2", "l1", "l2"]
+    with pytest.raises(NotImplementedError):
+        loss_kind("huber")
+    a, b = torch.tensor([0.0, 1.0, 3.0]), torch.tensor([1.0, 1.0, 1.0])
+    assert float(projection_loss(a, b, "L1")) == pytest.approx(1.0)
+    assert float(projection_loss(a, b, "l2")) == pytest.approx(5.0 / 3)
