@@ -77,7 +77,7 @@ _COMMON_CONFIG = {"loss": "l1", "epochs": "auto", "lrf": "auto", "lr_otype": "co
                   "points_start": 100, "points_end": "auto", "points_update_interval": "auto", "points_linear": True,
                   "downsampling_start": 2, "downsampling_end": 1, "downsampling_update_interval": 1000,
                   "points_per_batch": "auto", "s3im": False, "add_poisson": False, "batch_per_proj": 1,
-                  "clip_grad_value": None}
+                  "clip_grad_value": None, "optimizer": "Adam", "beta1": 0.9, "beta2": 0.999, "weight_decay": 0.0}
 _BASE_CONFIG = {
     "static": dict(_COMMON_CONFIG, base_lr=1e-3, warmup_steps=500, warmup_lr0=1e-3, log2_hashmap_size=21),
     "dynamic": dict(_COMMON_CONFIG, base_lr=2e-4, warmup_steps=2000, warmup_lr0=1e-4, log2_hashmap_size=23),
@@ -96,6 +96,8 @@ _OVERRIDE_KEYS = {
     ("downsampling_detector", "start"): "downsampling_start", ("downsampling_detector", "end"): "downsampling_end",
     ("downsampling_detector", "update_interval"): "downsampling_update_interval",
     ("encoder", "log2_hashmap_size"): "log2_hashmap_size",
+    ("optimizer", "otype"): "optimizer", ("optimizer", "beta1"): "beta1", ("optimizer", "beta2"): "beta2",
+    ("optimizer", "weight_decay"): "weight_decay",
 }
 
 # nect/reconstruct.py:173-204: per quality, the fields set and the factor the
@@ -132,6 +134,9 @@ def apply_override(cfg: dict, override: dict) -> dict:
             raise ValueError(f"config_override: {key} is not supported here")
     if isinstance(out["loss"], str):
         out["loss"] = out["loss"].lower()
+    if str(out["optimizer"]).casefold() != "adam":
+        raise ValueError(f"config_override: optimizer {out['optimizer']} is not supported here (the fused "
+                         "update is Adam)")
     return out
 
 
@@ -220,7 +225,7 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
         evaluate=None, eval_every: int = 0, schedule=None, s3im: bool = False,
         add_poisson: bool = False, tv: float = 0.0, resume_from=None, checkpoint_dir=None,
         checkpoint_interval: float | None = None, log_fn=None, cancel_at=None, batch_per_proj: int | str = 1,
-        clip_grad_value: float | None = None) -> Reconstruction:
+        clip_grad_value: float | None = None, betas=(0.9, 0.999), weight_decay: float = 0.0) -> Reconstruction:
     """Train a model on ``projections`` [N, rows, cols] (raw line integrals) at
     ``angles`` (radians) and optional ``timesteps``.  Projections are min-max
     scaled over the data set (nect/data.py:177-183).  ``evaluate(rec)`` is
@@ -263,7 +268,8 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     projection visit, each an optimizer step with the projection's settings,
     up to the batches the detector holds (base_trainer.py:517-520);
     ``clip_grad_value`` clamps the gradients before each Adam step
-    (base_trainer.py:651-652).  ``niter``, checkpoints and resume count
+    (base_trainer.py:651-652); ``betas`` and ``weight_decay`` are Adam's
+    (nect/config.py:409-413).  ``niter``, checkpoints and resume count
     projection visits."""
     dev = torch.device(device)
     proj = torch.as_tensor(projections, dtype=torch.float32, device=dev)
@@ -282,7 +288,8 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     model = get_model(cfg, device=dev)
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
     trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
-                      loss=loss, lr=lr, device=dev, clip_grad_value=clip_grad_value)
+                      loss=loss, lr=lr, betas=tuple(betas), weight_decay=weight_decay, device=dev,
+                      clip_grad_value=clip_grad_value)
     n_batches = 10 ** 9 if batch_per_proj == "all" else int(batch_per_proj)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
     if isinstance(cancel_at, str):
@@ -429,6 +436,8 @@ def reconstruct(geometry: Geometry, projections, mode: str = "static", angles=No
     kw.setdefault("add_poisson", bool(plan.config["add_poisson"]))
     kw.setdefault("batch_per_proj", plan.config["batch_per_proj"])
     kw.setdefault("clip_grad_value", plan.config["clip_grad_value"])
+    kw.setdefault("betas", (plan.config["beta1"], plan.config["beta2"]))
+    kw.setdefault("weight_decay", plan.config["weight_decay"])
     if verbose:
         sch = plan.schedule
         print(f"nect_b200.reconstruct: {mode}, quality {quality}: {sch.total_projections} steps "

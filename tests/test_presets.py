@@ -122,6 +122,11 @@ def test_reconstruct_resolves_the_preset_and_turns_the_static_volume(monkeypatch
                                                    "warmup": {"steps": 7}})
     assert seen["niter"] == 20 and seen["s3im"] is True and seen["points_per_batch"] == 200_000
     assert seen["schedule"].warmup[0] == 7
+    assert seen["betas"] == (0.9, 0.999) and seen["weight_decay"] == 0.0
+    seen.clear()
+    rc.reconstruct(geo, np.zeros((10, 32, 32), np.float32), angles=np.arange(10) * 0.3, verbose=False,
+                   config_override={"optimizer": {"otype": "Adam", "beta1": 0.8, "weight_decay": 0.01}})
+    assert seen["betas"] == (0.8, 0.999) and seen["weight_decay"] == 0.01
     with pytest.raises(ValueError, match="array"):
         rc.reconstruct(geo, "projections.npy", angles=np.arange(10) * 0.3, verbose=False)
 
