@@ -5,18 +5,34 @@ device randperm of the detector pixels, per-ray jitter draw, fused
 sample -> encode -> MLP -> line integral -> loss -> backward (nectb_train_step),
 and the Adam update of the table and the MLP (fused Adam kernel).
 
-Default workload (N=1): static cone beam, 512x512 detector (one batch = all
-262,144 pixels of a projection), 256^3 porous-medium phantom, 512 jittered
-samples per ray, 16 levels x 2 features, 2^20 entries per level, 2x64 MLP.
-Inputs are seeded synthetic projections (exact line integrals) made before
-the timed region.  Timing: W warm-up steps, then K steps bracketed by a
-barrier and cuda synchronize, CUDA events on the launching stream, max over
-ranks.  Per-step state (tables, gradients, Adam moments) exceeds the 126 MB L2,
-so consecutive steps do not hit a warm L2.
+Default workload (N=1): the 4D dynamic cone beam, 512x512 detector (one batch
+= all 262,144 pixels of a projection, each projection at its own t), 256^3
+porous medium with a rising brine front and shrinking grains, 512 jittered
+samples per ray, 4D hash grid of 16 levels x 2 features, 2^21 entries per
+level, temporal base resolution 4, 2x64 MLP, mixed precision.  The plain fp32
+path is timed on the same workload in the same process (``plain_fp32`` and
+``mixed_over_plain`` in the line).  Inputs are seeded synthetic projections
+made before the timed region.  Timing: W warm-up steps, then K steps
+bracketed by a barrier and cuda synchronize, CUDA events on the launching
+stream, max over ranks.  Per-step state (tables, gradients, Adam moments)
+exceeds the 126 MB L2, so consecutive steps do not hit a warm L2.
 
---impl reference times the reference path's CPU restatement (the oracle:
-C sampler + PyTorch-CPU hash grid, MLP, loss, autograd backward and
-torch.optim.Adam) on the host cores, on a bounded sample of rays per step.
+Rooflines: the encoding's corner gathers and the gradient scatter's
+reductions are served by the L2 (the table and one scatter pass's gradient
+slice are L2-sized), so their roofs are measured here, before the timed
+region, by the library's probes: random gathers of the table's entry size
+from a buffer of the fp16 table's size, and random fp32 reductions of the
+gradient's entry size into a buffer of one scatter pass's slice.  Achieved =
+algorithmic bytes per launch (per valid sample: L * 2^d * F * 2 bytes for the
+forward, L * 2^d * F * 4 bytes for the scatter) / the kernel's mean CUDA-event
+launch time.  The tensor-core backward is reported against the measured bf16
+peak (MLP flops per sample: the forward recompute and the two backward
+products).
+
+--impl reference times the reference path's CPU restatement (oracle/
+workloads.py: the C sampler, PyTorch-CPU fp32 hash grid, MLP, autograd and
+torch.optim.Adam) on the host cores, on a bounded sample of each step's rays;
+it imports nothing of the product package.
 """
 from __future__ import annotations
 
@@ -37,6 +53,25 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "train rays/s fwd+bwd"
+
+# what each workload is, in words, and its batch: the `config` both arms print
+WORKLOAD_TEXT = {
+    "c1_static_parallel": "static parallel beam 128x128 detector, 128^3 volume, S=256, hash 16x2 fp32 2^19, MLP 2x64",
+    "c2_static_cone": "static cone beam 512x512 detector (DSO 500, DSD 1000), 256^3 volume, S=512, hash 16x2 2^20, "
+                      "MLP 2x64",
+    "c3_dynamic_cone": "4D cone beam 512x512 detector (DSO 500, DSD 1000), 256^3 volume, 3,600 views over 10 turns "
+                       "each at its own t, S=512, 4D hash 16x2 2^21 temporal base 4, MLP 2x64",
+    "c5_large_cone": "large 4D cylindrical cone beam 2048x2048 detector (DSO 2000, DSD 4000), 1024^3 volume, 7,200 "
+                     "views over 20 turns, S<=1024, 4D hash 16x4 2^22 finest 4096, MLP 3x64",
+}
+WORKLOAD_RAYS = {"c1_static_parallel": 65536, "c2_static_cone": 1 << 18, "c3_dynamic_cone": 1 << 18,
+                 "c5_large_cone": 1 << 20}
+WORKLOAD_S = {"c1_static_parallel": 256, "c2_static_cone": 512, "c3_dynamic_cone": 512, "c5_large_cone": 1024}
+
+
+def bench_config(name: str, rays: int) -> dict:
+    return {"workload": f"{name}: {WORKLOAD_TEXT[name]}", "rays_per_step": rays, "samples_per_ray": WORKLOAD_S[name],
+            "l2": "per-step state (tables, gradients, Adam moments) exceeds the 126 MB L2"}
 
 
 # ----------------------------------------------------------------- workloads
@@ -155,72 +190,64 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ CPU baseline
-def cpu_port_step(spec, geometry, model_cfg, table, mlp_flat, proj_flat_cpu, angle, t, rays: int, opt, rng):
-    """One step of the reference path's CPU restatement on a bounded sample."""
-    from oracle import hashgrid as ohg
-    from oracle import sampling as osamp
-
-    S = spec["S"]
-    P = proj_flat_cpu.numel()
-    perm = torch.randperm(P).numpy()
-    jitter = (rng.random(rays, dtype=np.float32) - 0.5).astype(np.float32)
-    det_off = np.zeros((rays, 2), np.float32)
-    cg = osamp.to_struct(geometry.get_c_geometry())
-    maxd = geometry.max_distance_traveled / S
-    pts, dist, counts = osamp.oracle_sample(cg, perm, 0, rays, S, angle, maxd, True, jitter, det_off)
-    enc = model_cfg.encoder
-    levels, _ = ohg.layout(spec["n_dims"], enc.n_levels, enc.log2_hashmap_size, float(enc.base_resolution),
-                           float(enc.per_level_scale), float(enc.base_resolution_t or enc.base_resolution))
-    keep = ~torch.all(torch.from_numpy(pts).clamp(0, 1).view(-1, 3) == 0, dim=-1)
-    x = torch.from_numpy(pts).clamp(0, 1).view(-1, 3)[keep]
-    if spec["n_dims"] == 4:
-        x = torch.cat([x, torch.full((x.shape[0], 1), t)], 1)
-    opt.zero_grad()
-    Ws = ohg.split_mlp_params(mlp_flat, enc.n_levels * enc.n_features_per_level, 64, 2)
-    sig = ohg.mlp(ohg.encode(x, table, levels, enc.log2_hashmap_size), Ws, "relu", "softplus").squeeze(-1)
-    full = torch.zeros(rays * S).masked_scatter(keep, sig)
-    y_pred = full.view(rays, S).sum(1) * (torch.from_numpy(dist) / geometry.max_distance_traveled)
-    y = proj_flat_cpu[torch.from_numpy(perm[:rays])]
-    loss = torch.nn.functional.mse_loss(y_pred, y)
-    loss.backward()
-    opt.step()
-    return float(loss.detach())
 
 
-def run_cpu(spec, geometry, model, projs, angles, ts, steps: int, warmup: int, rays: int):
+# ------------------------------------------------------------ CPU baseline
+def run_cpu_port(name: str, steps: int, warmup: int, rays: int, seed: int = 0):
+    """The reference path's CPU restatement (oracle/workloads.CpuTrainer) on a
+    bounded sample of ``rays`` rays per step; all host threads.  Returns
+    (rays/s, threads, seconds per step).  Projections are seeded uniform
+    values in [0, 1) (the min-max scaled range): the CPU time does not depend
+    on them."""
+    from oracle import workloads as owl
+
     threads = os.cpu_count() or 1
     torch.set_num_threads(threads)
-    table = model.table.detach().cpu().clone().requires_grad_(True)
-    mlp = model.mlp.detach().cpu().clone().requires_grad_(True)
-    opt = torch.optim.Adam([table, mlp], lr=1e-3)
-    rng = np.random.default_rng(0)
-    pc = projs.cpu()
+    w = owl.WORKLOADS[name]
+    tr = owl.CpuTrainer(w)
+    g = torch.Generator().manual_seed(seed)
+    projs = torch.rand(2, w.pixels, generator=g)
+    angles, ts = owl.view_angles(w, 2)
     for k in range(warmup):
-        cpu_port_step(spec, geometry, model_cfg_of(model), table, mlp, pc[k % len(pc)], angles[k % len(pc)],
-                      ts[k % len(pc)], rays, opt, rng)
+        tr.step(projs[k % 2], angles[k % 2], ts[k % 2], rays)
     t0 = time.perf_counter()
     for k in range(steps):
-        cpu_port_step(spec, geometry, model_cfg_of(model), table, mlp, pc[k % len(pc)], angles[k % len(pc)],
-                      ts[k % len(pc)], rays, opt, rng)
+        tr.step(projs[k % 2], angles[k % 2], ts[k % 2], rays)
     dt = time.perf_counter() - t0
     return rays * steps / dt, threads, dt / steps
 
 
-def model_cfg_of(model):
-    return model._bench_cfg
+def run_reference(args):
+    """--impl reference: the CPU arm alone (rank 0), product package untouched."""
+    name = args.workload
+    rays = args.cpu_rays
+    val, threads, per = run_cpu_port(name, args.steps, args.warmup, rays)
+    R = args.rays or WORKLOAD_RAYS[name]
+    sample = (f"{rays} of the {R} rays x {WORKLOAD_S[name]} samples of each step's batch, {args.steps} steps "
+              f"after {args.warmup} warm-up (C sampler + PyTorch-CPU fp32 hash grid/MLP/autograd/torch.optim.Adam)")
+    print(json.dumps({
+        "metric": METRIC, "value": val, "unit": "rays/s", "impl": "reference", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded projection values)",
+        "config": bench_config(name, R), "precision": "plain_fp32 on the host cores",
+        "cpu_baseline": {"value": val, "unit": "rays/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
 
 
 # ----------------------------------------------------------------- GPU arm
+PROFILE_SLOTS = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "scatter", "ray_order",
+                 "time_slice"]
+
+
 def collect_profile():
     from nect_b200 import _lib
     import ctypes
 
-    names = ["ray_prep", "forward", "backward", "adam", "sample", "model_forward", "scatter", "ray_order",
-             "time_slice"]
-    n = (ctypes.c_int32 * len(names))()
-    ms = (ctypes.c_double * len(names))()
+    n = (ctypes.c_int32 * len(PROFILE_SLOTS))()
+    ms = (ctypes.c_double * len(PROFILE_SLOTS))()
     _lib.lib.nectb_profile_collect(ctypes.addressof(n), ctypes.addressof(ms))
-    return {names[i]: (int(n[i]), float(ms[i])) for i in range(len(names)) if n[i]}
+    return {PROFILE_SLOTS[i]: (int(n[i]), float(ms[i])) for i in range(len(PROFILE_SLOTS)) if n[i]}
 
 
 def valid_samples(trainer, batches) -> int:
@@ -238,20 +265,97 @@ def valid_samples(trainer, batches) -> int:
     return total
 
 
+def probe_roofs(entries: int, gather_bytes: int, slice_entries: int, red_bytes: int, device) -> dict:
+    """Measured roofs (GB/s of useful bytes) of random gathers of gather_bytes
+    from a buffer of `entries` entries and of random fp32 reductions of
+    red_bytes into a buffer of `slice_entries` entries (library probes,
+    CUDA events on the launching stream, best of 3 after a warm-up)."""
+    from nect_b200 import _lib
+
+    out = {}
+    stream = torch.cuda.current_stream(device)
+    sink = torch.zeros(1, dtype=torch.int32, device=device)
+    for kind, n_ent, eb in (("gather", entries, gather_bytes), ("reduce", slice_entries, red_bytes)):
+        buf = torch.rand(n_ent * eb // 4, device=device)
+        n_ops = 1 << 28
+        ops = _lib.lib.nectb_probe_ops(n_ops)
+        best = None
+        for rep in range(4):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            if kind == "gather":
+                rc = _lib.lib.nectb_probe_gather(buf.data_ptr(), n_ent, eb, n_ops, sink.data_ptr(),
+                                                 _lib.stream_ptr(device))
+            else:
+                rc = _lib.lib.nectb_probe_reduce(buf.data_ptr(), n_ent, eb, n_ops, _lib.stream_ptr(device))
+            e1.record(stream)
+            _lib.check(rc, f"nectb_probe_{kind}")
+            e1.synchronize()
+            ms = e0.elapsed_time(e1)
+            if rep and (best is None or ms < best):
+                best = ms
+        out[kind] = {"gbs": ops * eb / (best / 1e3) / 1e9, "entry_bytes": eb, "buffer_mb": n_ent * eb / 1e6,
+                     "ops": int(ops), "ms": best}
+        del buf
+    return out
+
+
+def time_steps(trainer, make_step_batch, steps: int, first: int, world: int, clocks=None, nvtx: str | None = None):
+    """K training steps between a barrier + synchronize on both sides, timed
+    with CUDA events on the launching stream (max over ranks)."""
+    batches = []
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if nvtx:
+        torch.cuda.nvtx.range_push(nvtx)   # ncu --nvtx --nvtx-include "timed/" lists only these launches
+    ev0.record(stream)
+    for k in range(steps):
+        b = make_step_batch(first + k)
+        batches.append(b)
+        trainer.step(b)
+    ev1.record(stream)
+    if nvtx:
+        torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    if world > 1:
+        import torch.distributed as dist
+
+        t_ = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+        ms = float(t_.item())
+    return ms, batches
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2_static_cone",
-                    choices=["c2_static_cone", "c1_static_parallel", "c3_dynamic_cone", "c5_large_cone"])
+    ap.add_argument("--workload", default="c3_dynamic_cone",
+                    choices=["c3_dynamic_cone", "c2_static_cone", "c1_static_parallel", "c5_large_cone"])
     ap.add_argument("--precision", default=os.environ.get("NECTB_PRECISION", "mixed"),
                     choices=["mixed", "plain_fp32"])
     ap.add_argument("--cpu-rays", type=int, default=2048)
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain fp32 arm")
+    ap.add_argument("--plain-steps", type=int, default=0,
+                    help="timed steps of the plain fp32 arm (0: --steps, 2 on the large 4D workload)")
+    ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling of smaller cases)")
+    ap.add_argument("--recompute", action="store_true",
+                    help="recompute the encodings in the backward instead of storing them (encoding_store 0)")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (launch shapes and scheduling tuned on this workload before the "
                          "warm-up, outside the timed region); the library defaults are used")
@@ -260,19 +364,21 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    if args.impl == "reference" and rank != 0:
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
         return
-    if world > 1 and args.impl == "b200":
+    if world > 1:
         import datetime
 
         import torch.distributed as dist
 
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    dev = torch.device("cuda", local) if torch.cuda.is_available() else torch.device("cpu")
-    if dev.type == "cuda":
-        torch.cuda.set_device(dev)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
 
+    from nect_b200 import _lib, autotune
     from nect_b200.config import get_model
     from nect_b200.sampling import Geometry
     from nect_b200.trainer import Trainer
@@ -281,62 +387,31 @@ def main():
     geometry = Geometry(**spec["geo"])
     S, R = spec["S"], (args.rays or spec["rays"])
     model_cfg = spec["model"]
-    wl_name = (f"{args.workload}: {geometry.mode} {geometry.nDetector[0]}x{geometry.nDetector[1]} detector, "
-               f"{geometry.nVoxel[0]}^3 volume, S={S}, hash {model_cfg.encoder.n_levels}x"
-               f"{model_cfg.encoder.n_features_per_level} 2^{model_cfg.encoder.log2_hashmap_size}"
-               f"{' 4D' if spec['n_dims'] == 4 else ''}, MLP {model_cfg.net.n_hidden_layers}x64")
-
-    if args.impl == "reference":
-        torch.manual_seed(0)
-        projs, angles, ts = make_projections(spec, geometry, 2, "cpu")
-
-        class _M:  # CPU parameters with the same shapes and init as the model
-            pass
-
-        m = _M()
-        enc = model_cfg.encoder
-        from oracle import hashgrid as ohg
-
-        _, total = ohg.layout(spec["n_dims"], enc.n_levels, enc.log2_hashmap_size, float(enc.base_resolution),
-                              float(enc.per_level_scale), float(enc.base_resolution_t or enc.base_resolution))
-        g = torch.Generator().manual_seed(1337)
-        m.table = (torch.rand(total, enc.n_features_per_level, generator=g) * 2 - 1) * 1e-4
-        n_in = enc.n_levels * enc.n_features_per_level
-        m.mlp = torch.cat([(torch.rand(o * i, generator=g) * 2 - 1) * math.sqrt(6 / (o + i))
-                           for o, i in [(64, n_in), (64, 64), (1, 64)]])
-        m._bench_cfg = model_cfg
-        rays = args.cpu_rays
-        val, threads, per = run_cpu(spec, geometry, m, projs, angles, ts, args.steps, args.warmup, rays)
-        sample = f"{rays} rays x {S} samples per step of the {args.workload} workload"
-        print(json.dumps({
-            "metric": METRIC, "value": val, "unit": "rays/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wl_name, "precision": "plain_fp32 (CPU)", "rays_per_step": rays},
-            "cpu_baseline": {"value": val, "unit": "rays/s", "cores": threads, "kind": "port", "sample": sample},
-            "e2e": {"value": val, "unit": "rays/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        }))
-        return
+    recompute = args.recompute or (args.workload == "c5_large_cone" and args.precision == "mixed")
+    if recompute:
+        autotune.set_tuning({"encoding_store": 0})
 
     torch.manual_seed(1234 + rank)
     n_proj = 8
     projs, angles, ts = make_projections(spec, geometry, n_proj, dev, seed=rank)
-    model = get_model(model_cfg, device=dev)
-    model._bench_cfg = model_cfg
-    # N > 1: data parallel as the reference's DDP: each rank trains on its own projections (weak scaling) and
-    # the table and MLP gradients are averaged over NCCL before every Adam step
-    trainer = Trainer(model, geometry, points_per_batch=R * S, points_per_ray=S, loss="l2", lr=1e-3, device=dev,
-                      data_parallel=world > 1)
     P = projs.shape[1]
 
-    def make_step_batch(k):
-        perm = torch.randperm(P, dtype=torch.int64, device=dev)
-        return trainer.make_batch(perm, 0, angles[k % n_proj], projs[k % n_proj], ts[k % n_proj])
+    def make_trainer(cfg):
+        model = get_model(cfg, device=dev)
+        # N > 1: data parallel as the reference's DDP: each rank trains on its own projections (weak scaling) and
+        # the table and MLP gradients are averaged over NCCL before every Adam step
+        tr = Trainer(model, geometry, points_per_batch=R * S, points_per_ray=S, loss="l2", lr=1e-3, device=dev,
+                     data_parallel=world > 1)
 
+        def make_step_batch(k):
+            perm = torch.randperm(P, dtype=torch.int64, device=dev)
+            return tr.make_batch(perm, 0, angles[k % n_proj], projs[k % n_proj], ts[k % n_proj])
+
+        return model, tr, make_step_batch
+
+    model, trainer, make_step_batch = make_trainer(model_cfg)
     tuning = None
     if not args.no_autotune and args.precision == "mixed":   # the tunables belong to the mixed path
-        from nect_b200 import autotune
-
         # every rank tunes on its own GPU without the gradient all-reduce (the
         # search may take different numbers of steps on different ranks, and a
         # collective needs all of them), then all ranks take rank 0's choice
@@ -354,132 +429,149 @@ def main():
         trainer.step(make_step_batch(k))
     torch.cuda.synchronize()
 
-    from nect_b200 import _lib
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
+    # ---- roofs of the gathers and reductions, measured on this GPU (outside the timed region)
+    enc = model_cfg.encoder
+    F = enc.n_features_per_level
+    feat_bytes = 2 if args.precision == "mixed" else 4
+    cur = autotune.get_tuning()
+    slice_entries = max(1, min(model.table.shape[0], int(cur["scatter_group_bytes"]) // (F * 4)))
+    roofs = probe_roofs(model.table.shape[0], F * feat_bytes, slice_entries, F * 4, dev)
 
     clocks = ClockSampler(dev.index or 0)
     clocks.start()
     time.sleep(0.3)
     _lib.lib.nectb_profile_enable(1)
-    batches = []
-    barrier()
-    torch.cuda.synchronize()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.nvtx.range_push("timed")   # ncu --nvtx --nvtx-include "timed/" lists only these launches
-    ev0.record()
-    for k in range(args.steps):
-        b = make_step_batch(args.warmup + k)
-        batches.append(b)
-        trainer.step(b)
-    ev1.record()
-    torch.cuda.nvtx.range_pop()
-    torch.cuda.synchronize()
-    barrier()
+    ms, batches = time_steps(trainer, make_step_batch, args.steps, args.warmup, world, nvtx="timed")
     _lib.lib.nectb_profile_enable(0)
     clock_info = clocks.stop()
-    ms = ev0.elapsed_time(ev1)
     prof = collect_profile()
-    if world > 1:
-        import torch.distributed as dist
-
-        t_ = torch.tensor([ms], device=dev)
-        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
-        ms = float(t_.item())
     rays_per_step = batches[0].num_rays
     value = world * rays_per_step * args.steps / (ms / 1e3)
 
-    # ---- roofline of the dominant kernel (algorithmic bytes / event time)
+    # ---- rooflines (algorithmic bytes or flops per launch / mean launch time)
     n_valid = valid_samples(trainer, batches)
-    enc = model_cfg.encoder
+    per_step_samples = n_valid / args.steps
     corners = 1 << spec["n_dims"]
-    feat_bytes = 2 if args.precision == "mixed" else 4
-    gather = enc.n_levels * corners * enc.n_features_per_level * feat_bytes
-    scatter = enc.n_levels * corners * enc.n_features_per_level * 4
-    n_params = model.table.numel() + model.mlp.numel()
-    staged = "scatter" in prof   # the mixed backward ran as tensor-core pass + staged scatter passes
-    stage_io = enc.n_levels * enc.n_features_per_level * 4   # staged dL/d(encoding) per sample, each way
-    row = enc.n_levels * enc.n_features_per_level * 2        # stored bf16 encoding row per sample
-    stored = 0.0   # share of samples whose rows the forward stores (recommended workspace: min(R*S, 80 GiB) rows)
-    if staged:
-        stored = min(1.0, min(rays_per_step * S, (80 << 30) // row) / max(n_valid / args.steps, 1.0))
-    step_bytes = {   # algorithmic bytes per step of each kernel kind
-        "backward": n_valid / args.steps * (stored * row + (1 - stored) * gather + (stage_io if staged else scatter)),
-        "scatter": n_valid / args.steps * (scatter + stage_io),
-        "forward": n_valid / args.steps * (gather + stored * row),
-        "adam": n_params * (34 if args.precision == "mixed" else 32),
-        "ray_prep": rays_per_step * 64.0,
-    }
+    L = enc.n_levels
+    gather = L * corners * F * feat_bytes       # corner gathers of one sample
+    scatter = L * corners * F * 4               # fp32 gradient reductions of one sample
+    H = model_cfg.net.n_hidden_layers
+    n_in = L * F
+    mlp_fwd = 2 * (n_in * 64 + (H - 1) * 64 * 64 + 64)
     kernel_ms = {k: v[1] / max(v[0], 1) for k, v in prof.items()}
     launches_per_step = {k: v[0] / args.steps for k, v in prof.items()}
-    per_launch_bytes = {k: step_bytes[k] / launches_per_step[k] for k in prof if k in step_bytes}
-    dominant = max(prof, key=lambda k: prof[k][1]) if prof else "backward"
-    peaks = {}
-    pk = ROOT / "MEASURED_PEAKS.json"
-    if pk.exists():
-        peaks = json.loads(pk.read_text())
-    peak = float(peaks.get("hbm_gbs", 6650.0))
-    peak_src = "of measured" if "hbm_gbs" in peaks else "of fallback"
-    achieved = per_launch_bytes.get(dominant, 0.0) / (kernel_ms[dominant] / 1e3) / 1e9 if dominant in kernel_ms else None
-    traffic = None   # DRAM bytes per launch of the dominant kernel: the committed ncu capture's bytes per step
-    tfile = ROOT / "profiles" / "dram_bytes_per_step.txt"   # divided by this run's launches per step
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    tensor_peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
+    peak_src = "of measured" if peaks else "of fallback"
+    traffic_step = {}
+    tfile = ROOT / "profiles" / "dram_bytes_per_step.txt"
     if tfile.exists():
         for line in tfile.read_text().splitlines():
             f = line.split()
-            if len(f) == 4 and not line.startswith("#") and f[:3] == [args.workload, args.precision, dominant]:
-                traffic = float(f[3]) / max(launches_per_step.get(dominant, 1.0), 1.0)
+            if len(f) == 4 and not line.startswith("#") and f[:2] == [args.workload, args.precision]:
+                traffic_step[f[2]] = float(f[3])
+
+    def roof(kind, per_sample, unit_peak, peak, bound, unit, scale):
+        if kind not in kernel_ms:
+            return None
+        per_launch = per_step_samples * per_sample / launches_per_step[kind]
+        achieved = per_launch / (kernel_ms[kind] / 1e3) / scale
+        tr = traffic_step.get(kind)
+        out = {"bound": bound, "kernel": kind, "achieved": achieved, "peak": peak, "unit": unit,
+               "frac": achieved / peak, "peak_source": unit_peak,
+               "traffic": tr / launches_per_step[kind] if tr is not None else None,
+               "algorithmic_per_launch": per_launch, "launch_ms": kernel_ms[kind],
+               "launches_per_step": launches_per_step[kind]}
+        if tr is not None:
+            out["dram_frac_of_hbm"] = tr / launches_per_step[kind] / (kernel_ms[kind] / 1e3) / 1e9 / hbm
+        return out
+
+    rooflines = {
+        "forward": roof("forward", gather, f"measured in this run: random {F * feat_bytes}-byte gathers from a "
+                        f"{roofs['gather']['buffer_mb']:.0f} MB buffer (the table's size)", roofs["gather"]["gbs"],
+                        "l2", "GB/s", 1e9),
+        "scatter": roof("scatter", scatter, f"measured in this run: random {F * 4}-byte fp32 reductions into a "
+                        f"{roofs['reduce']['buffer_mb']:.0f} MB buffer (one scatter pass's gradient slice)",
+                        roofs["reduce"]["gbs"], "l2", "GB/s", 1e9),
+        "backward": roof("backward", 3 * mlp_fwd, f"{peak_src} bf16 dense, sustained", tensor_peak, "tensor",
+                         "TFLOP/s", 1e12),
+    }
+    if args.precision == "plain_fp32":
+        rooflines["backward"] = None   # the plain backward is SIMT, no tensor-core roof
+    rooflines = {k: v for k, v in rooflines.items() if v}
+    # the dominant kernel of the step (most time); the scatter kind if it has none of its own
+    dominant = max((k for k in rooflines), key=lambda k: prof[k][1])
+    roofline = dict(rooflines[dominant])
 
     # ---- end to end through the public API, host buffers (pinned projection in, loss out)
-    host = projs.cpu().pin_memory()
-    dproj = torch.empty_like(projs[0])
-    loss_host = torch.empty(1, pin_memory=True)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for k in range(args.steps):
-        dproj.copy_(host[k % n_proj], non_blocking=True)
-        loss = trainer.train_projection(dproj, angles[k % n_proj], ts[k % n_proj])
-        loss_host.copy_(loss, non_blocking=True)
-    e1.record()
-    torch.cuda.synchronize()
-    ems = e0.elapsed_time(e1)
-    if world > 1:
-        import torch.distributed as dist
+    e2e = None
+    if not args.no_e2e:
+        host = projs.cpu().pin_memory()
+        dproj = torch.empty_like(projs[0])
+        loss_host = torch.empty(1, pin_memory=True)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for k in range(args.steps):
+            dproj.copy_(host[k % n_proj], non_blocking=True)
+            loss = trainer.train_projection(dproj, angles[k % n_proj], ts[k % n_proj])
+            loss_host.copy_(loss, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        ems = e0.elapsed_time(e1)
+        if world > 1:
+            import torch.distributed as dist
 
-        t_ = torch.tensor([ems], device=dev)
-        dist.all_reduce(t_, op=dist.ReduceOp.MAX)
-        ems = float(t_.item())
-    e2e = {"value": world * rays_per_step * args.steps / (ems / 1e3), "unit": "rays/s",
-           "h2d_bytes_per_step": int(P * 4), "d2h_bytes_per_step": 4}
+            t_ = torch.tensor([ems], device=dev)
+            dist.all_reduce(t_, op=dist.ReduceOp.MAX)
+            ems = float(t_.item())
+        e2e = {"value": world * rays_per_step * args.steps / (ems / 1e3), "unit": "rays/s",
+               "h2d_bytes_per_step": int(P * 4), "d2h_bytes_per_step": 4}
+
+    # ---- the plain fp32 path on the same workload, same process
+    plain = None
+    if args.precision == "mixed" and not args.no_plain:
+        del trainer, model
+        torch.cuda.empty_cache()
+        pcfg = workload_spec(args.workload, "plain_fp32")["model"]
+        _, ptr, pbatch = make_trainer(pcfg)
+        psteps = args.plain_steps or (2 if args.workload == "c5_large_cone" else args.steps)
+        pwarm = min(args.warmup, 3 if args.workload != "c5_large_cone" else 1)
+        for k in range(pwarm):
+            ptr.step(pbatch(k))
+        pms, _ = time_steps(ptr, pbatch, psteps, pwarm, world)
+        pval = world * rays_per_step * psteps / (pms / 1e3)
+        plain = {"value": pval, "unit": "rays/s", "ms_per_step": pms / psteps, "steps": psteps, "warmup": pwarm}
+        del ptr
+        torch.cuda.empty_cache()
 
     cpu_baseline = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        val, threads, per = run_cpu(spec, geometry, model, projs, angles, ts, args.cpu_steps, 1, args.cpu_rays)
+        val, threads, per = run_cpu_port(args.workload, args.cpu_steps, 1, args.cpu_rays)
         cpu_baseline = {"value": val, "unit": "rays/s", "cores": threads, "kind": "port",
-                        "sample": f"{args.cpu_rays} rays x {S} samples per step, {args.cpu_steps} steps, of the "
-                                  f"same workload (C sampler + PyTorch-CPU fp32 hash grid/MLP/autograd/Adam)"}
+                        "sample": f"{args.cpu_rays} of the {rays_per_step} rays x {S} samples of each step's batch, "
+                                  f"{args.cpu_steps} steps (C sampler + PyTorch-CPU fp32 hash grid/MLP/autograd/"
+                                  f"torch.optim.Adam)"}
 
     # the ray-order slot times its three launches (count, scan, compaction) as one
     gpu_launches = sum(v[0] * (3 if k == "ray_order" else 1) for k, v in prof.items())
     out = {
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f16/bf16" if args.precision == "mixed" else "f32", "data": "synthetic",
-        "config": {"workload": wl_name, "precision": args.precision, "rays_per_step": rays_per_step,
-                   "samples_per_ray": S, "valid_samples_per_step": n_valid / args.steps,
-                   "samples_per_s": world * n_valid / (ms / 1e3),
-                   "l2": "per-step state (tables, gradients, Adam moments) exceeds the 126 MB L2",
-                   "parallelism": f"dp{world} (gradient all-reduce per step)" if world > 1 else "single",
-                   "tuning": tuning if tuning is not None else "defaults"},
-        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_src,
-                     "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes.get(dominant),
-                     "kernel_ms": kernel_ms, "launches_per_step": launches_per_step,
-                     "encoding_store_share": stored},
+        "vs_baseline": None, "dtype": "f16/bf16" if args.precision == "mixed" else "f32",
+        "data": "synthetic (seeded phantom, exact or ray-marched projections)",
+        "config": bench_config(args.workload, rays_per_step),
+        "precision": args.precision,
+        "samples_per_step": per_step_samples, "samples_per_s": world * n_valid / (ms / 1e3),
+        "parallelism": f"dp{world} (gradient all-reduce per step)" if world > 1 else "single",
+        "backward": "recompute (encodings gathered again)" if recompute else "encoding store",
+        "tuning": tuning if tuning is not None else autotune.get_tuning(),
+        "roofline": roofline,
+        "rooflines": rooflines,
+        "probes": roofs,
+        "plain_fp32": plain,
+        "mixed_over_plain": (value / plain["value"]) if plain else None,
         "cpu_baseline": cpu_baseline,
         "e2e": e2e,
         "gpu_launches": gpu_launches,

@@ -170,6 +170,18 @@ int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp,
                          const float* x, int64_t n, float t, const float* dsigma,
                          float* grid_grad, float* mlp_grad, void* stream);
 
+/* nectb_model_forward / nectb_model_backward with the timestep of a 4D grid
+ * read from device memory (t: one fp32, broadcast to every point), so a
+ * timestep held in a device tensor needs no host synchronisation: the
+ * reference broadcasts a 0-d tensor t on the device (nect/network/
+ * networks.py:85, 440-444).  Ignored for 3D grids (t must still be valid). */
+int nectb_model_forward_t(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                          const float* mlp_params, const float* x, int64_t n, const float* t, float* sigma,
+                          void* stream);
+int nectb_model_backward_t(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                           const float* mlp_params, const float* x, int64_t n, const float* t,
+                           const float* dsigma, float* grid_grad, float* mlp_grad, void* stream);
+
 /* ---- queries -------------------------------------------------------------- */
 /* One work item of a query: an nu x nv grid of points
  * x(i, j) = origin + i*du + j*dv (normalised (z,y,x) coordinates, i fast),
@@ -281,7 +293,9 @@ size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashG
 /* Device address of the error word inside a training (or re-projection)
  * workspace of num_rays rays (num_rays = detector pixels for a
  * re-projection); workspace NULL gives the word of the static scratch of
- * nectb_train_step_static on the current device.  Every step clears the word
+ * nectb_train_step_static on the current device (NULL, with
+ * NECTB_ERR_TOO_LARGE as the last error, for a batch that scratch cannot
+ * hold).  Every step clears the word
  * and sets it to non-zero when a tensor-core wait of that step timed out
  * (results of the step are then incomplete and the call's stream stays
  * usable).  Read it stream-ordered after the step, e.g. with cudaMemcpyAsync.
@@ -289,6 +303,21 @@ size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashG
  * reports only CUDA errors, ct_sampling.cu:639-644). */
 const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_t num_rays,
                                            const void* workspace);
+
+/* Diagnostic of the fused path's sampling: the rays a training step (or its
+ * forward half) prepared in a workspace of num_rays rays, read back after
+ * it.  counts[num_rays] int32: the samples the fused kernels evaluate per
+ * ray, the reference sampler's written samples (ct_sampling.cu:475-576);
+ * scale[num_rays] fp32: distances[r] / max_distance_traveled, the factor of
+ * the line integral (base_trainer.py:552-554); points[num_rays *
+ * num_points_per_ray * 3] fp32 (z,y,x): the positions the fused kernels
+ * regenerate for samples 0..S-1, after the Projector clamp
+ * (projector.py:127), 0 beyond the count, i.e. the reference's sample()
+ * output after clamp_(0, 1).  Any output may be NULL.  Stream-ordered.  No
+ * reference counterpart: the reference's fused equivalent does not exist,
+ * its sampler writes these to HBM. */
+int nectb_train_rays(const NectbGeometry* geometry, int32_t num_rays, int32_t num_points_per_ray,
+                     const void* workspace, int32_t* counts, float* scale, float* points, void* stream);
 
 /* Fused forward+backward.  grid_params is the table in grid->feature_dtype
  * (fp32 or fp16); mlp_params fp32; grid_params and grid_grad 16-byte
@@ -333,8 +362,9 @@ int nectb_train_backward(const NectbGeometry* geometry, const NectbHashGrid* gri
  * reference.  Scratch is a library-owned __device__ array of
  * nectb_train_static_scratch_bytes() (20 MiB + 4 KiB) that every GPU loading
  * the library reserves until exit; batches needing more (above 262,144 rays
- * on a 1024x1024 detector) fail with NECTB_ERR_TOO_LARGE.  The first call on
- * a device (that device current) looks up the array's address; make it before
+ * on a 1024x1024 detector) fail with NECTB_ERR_TOO_LARGE.  Every call (its
+ * device current) looks up the array's address, which allocates nothing; the
+ * first call on a device loads the library's module there, so make it before
  * any stream capture.  Calls share the array: calls that overlap on the GPU
  * race and must be serialised by the caller.  Allocates nothing. */
 int nectb_train_step_static(const NectbGeometry* geometry, const NectbHashGrid* grid,
@@ -388,9 +418,15 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * spread back to the two time vertices afterwards; the slice's fp16 rounding
  * lies below the bf16 rounding of the MLP input.  The other settings change
  * results by fp32 reassociation only; the Python autotuner
- * (nect_b200.autotune) picks them per workload.  nectb_set_tuning validates
- * and applies to steps issued after it returns; defaults: 4, 3, 0, 4,
- * 48 MiB, 1.0, 3.0, 1.  No reference counterpart. */
+ * (nect_b200.autotune) picks them per workload.  encoding_store: 1 lets the
+ * mixed forward keep each sample's bf16 MLP input row in the staging region
+ * for the backward to read back; 0 recomputes the encodings in the backward
+ * from the tables (positions are always regenerated), so the staging holds
+ * only the ray order and the staged gradients (identical results: the
+ * stored rows are the bits the gather produces).  nectb_train_staging_bytes
+ * follows it.  nectb_set_tuning validates and applies to steps issued after
+ * it returns; defaults: 4, 3, 0, 4, 48 MiB, 1.0, 3.0, 1, 1.  No reference
+ * counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;
   int32_t backward_blocks_per_sm;
@@ -400,9 +436,24 @@ typedef struct NectbTuning {
   float run_threshold_3d;
   float run_threshold_4d;
   int32_t time_slice;
+  int32_t encoding_store;
 } NectbTuning;
 int nectb_get_tuning(NectbTuning* tuning);
 int nectb_set_tuning(const NectbTuning* tuning);
+
+/* Roofline probes (no reference counterpart): the measured roofs that the
+ * encoding's corner gathers and the gradient scatter's reductions are
+ * reported against.  nectb_probe_gather loads entry_bytes (4, 8 or 16) from
+ * random entries of buf[n_entries * entry_bytes]; nectb_probe_reduce adds
+ * fp32 values with one entry_bytes-wide reduction into random entries of
+ * buf.  Both run about n_ops operations, exactly nectb_probe_ops(n_ops), in
+ * one launch of 64 warps per SM on the stream; the caller times them.  A
+ * buffer below the L2 size gives the L2 roof, a larger one the HBM
+ * random-access roof.  sink: one device uint32 the gather probe may write. */
+int nectb_probe_gather(const void* buf, int64_t n_entries, int32_t entry_bytes, int64_t n_ops,
+                       unsigned int* sink, void* stream);
+int nectb_probe_reduce(float* buf, int64_t n_entries, int32_t entry_bytes, int64_t n_ops, void* stream);
+int64_t nectb_probe_ops(int64_t n_ops);
 
 /* Version string and last error message of the calling thread. */
 const char* nectb_version(void);

@@ -103,6 +103,7 @@ class NectbTuning(ctypes.Structure):
         ("run_threshold_3d", c_f32),
         ("run_threshold_4d", c_f32),
         ("time_slice", c_int),
+        ("encoding_store", c_int),
     ]
 
 
@@ -123,6 +124,15 @@ _SIGNATURES = {
     "nectb_model_forward": (
         c_int,
         [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_ptr, c_ptr],
+    ),
+    "nectb_model_forward_t": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr, c_ptr],
+    ),
+    "nectb_model_backward_t": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_ptr, c_ptr, c_ptr,
+         c_ptr, c_ptr],
     ),
     "nectb_model_backward": (
         c_int,
@@ -163,6 +173,7 @@ _SIGNATURES = {
          c_f32, c_int, c_f32, c_f32, c_ptr, c_ptr, c_size, c_int, c_ptr],
     ),
     "nectb_train_error_word": (c_ptr, [ctypes.POINTER(NectbGeometry), c_int, c_ptr]),
+    "nectb_train_rays": (c_int, [ctypes.POINTER(NectbGeometry), c_int, c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr]),
     "nectb_train_staging_bytes": (
         c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int, c_int]),
     "nectb_selftest_bounded_wait": (c_int, [c_ptr, ctypes.c_uint32, c_ptr]),
@@ -170,6 +181,9 @@ _SIGNATURES = {
     "nectb_set_tuning": (c_int, [ctypes.POINTER(NectbTuning)]),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
+    "nectb_probe_gather": (c_int, [c_ptr, c_i64, c_int, c_i64, c_ptr, c_ptr]),
+    "nectb_probe_reduce": (c_int, [c_ptr, c_i64, c_int, c_i64, c_ptr]),
+    "nectb_probe_ops": (c_i64, [c_i64]),
     "nectb_adam_step": (
         c_int,
         [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_f32, c_f32, c_f32, c_f32, c_int, c_ptr, c_int, c_ptr],

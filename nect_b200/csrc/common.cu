@@ -113,7 +113,7 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
 namespace nectb {
 namespace {
 std::mutex g_tuning_mu;
-NectbTuning g_tuning = {4, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1};
+NectbTuning g_tuning = {4, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1, 1};
 }  // namespace
 
 NectbTuning current_tuning() {
@@ -143,6 +143,7 @@ extern "C" int nectb_set_tuning(const NectbTuning* t) {
                     t->run_threshold_4d <= 64.f,
                 "run thresholds must be in [0, 64]");
   NECTB_REQUIRE(t->time_slice == 0 || t->time_slice == 1, "time_slice must be 0 or 1");
+  NECTB_REQUIRE(t->encoding_store == 0 || t->encoding_store == 1, "encoding_store must be 0 or 1");
   std::lock_guard<std::mutex> lk(g_tuning_mu);
   g_tuning = *t;
   return NECTB_OK;

@@ -74,7 +74,8 @@ template <int D, int F, typename T, int IN, int H>
 __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g, const T* __restrict__ table,
                                                                       const float* __restrict__ W,
                                                                       const float* __restrict__ x, int64_t n,
-                                                                      float t, int act, int out_act,
+                                                                      float t, const float* __restrict__ t_dev,
+                                                                      int act, int out_act,
                                                                       float* __restrict__ sigma) {
   constexpr int LD = kModelThreads + 4;
   extern __shared__ float4 smem4[];
@@ -82,6 +83,7 @@ __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g,
   const SimtWeights sw = stage_weights<IN, H, false>(W, smem);
   float* xe = smem + simt_weight_floats<IN, H, false>() + threadIdx.x;
   float* hid = xe + IN * LD;
+  if (D == 4 && t_dev) t = *t_dev;   // the broadcast timestep, read on the device
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     float p[4];
@@ -110,8 +112,8 @@ int launch_encode(const GridDev& g, const void* params, const float* x, int64_t 
 }
 
 template <int D, int F, typename T, int H>
-int launch_model(const GridDev& g, const void* params, const float* W, const float* x, int64_t n, float t, int act,
-                 int out_act, float* sigma, cudaStream_t s) {
+int launch_model(const GridDev& g, const void* params, const float* W, const float* x, int64_t n, float t,
+                 const float* t_dev, int act, int out_act, float* sigma, cudaStream_t s) {
   constexpr int IN = 16 * F;
   auto k = model_forward_kernel<D, F, T, IN, H>;
   const size_t smem =
@@ -123,7 +125,7 @@ int launch_model(const GridDev& g, const void* params, const float* W, const flo
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kModelThreads, smem);
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(ceil_div(n, kModelThreads), (int64_t)sms * std::max(per_sm, 1)));
   ProfScope ps(kProfModel, s);
-  k<<<blocks, kModelThreads, smem, s>>>(g, (const T*)params, W, x, n, t, act, out_act, sigma);
+  k<<<blocks, kModelThreads, smem, s>>>(g, (const T*)params, W, x, n, t, t_dev, act, out_act, sigma);
   return launch_status("model_forward_kernel");
 }
 
@@ -146,13 +148,13 @@ int dispatch_encode(const GridDev& g, int dtype, const void* params, const float
 // Instantiated for 16 levels of 2 or 4 features over 3 or 4 inputs with 2 or 3
 // hidden layers of 64 (dispatch_shape), fp32 or fp16 tables.
 int dispatch_model(const GridDev& g, int dtype, int H, const void* p, const float* W, const float* x, int64_t n,
-                   float t, int act, int oact, float* sigma, cudaStream_t s) {
+                   float t, const float* t_dev, int act, int oact, float* sigma, cudaStream_t s) {
   const bool h = dtype == NECTB_F16;
   if (g.n_levels != 16) return set_error(NECTB_ERR_INVALID, "fused model paths need n_levels == 16");
   const int D = g.n_dims, F = g.n_features;
   const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
-    return h ? launch_model<d(), f(), __half, hl()>(g, p, W, x, n, t, act, oact, sigma, s)
-             : launch_model<d(), f(), float, hl()>(g, p, W, x, n, t, act, oact, sigma, s);
+    return h ? launch_model<d(), f(), __half, hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s)
+             : launch_model<d(), f(), float, hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s);
   });
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model forward: unsupported configuration (n_dims %d, n_features %d, "
@@ -205,17 +207,32 @@ extern "C" int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* para
   return dispatch_encode(g, grid->feature_dtype, params, x, n, out, (cudaStream_t)stream);
 }
 
-extern "C" int nectb_model_forward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
-                                   const float* mlp_params, const float* x, int64_t n, float t, float* sigma,
-                                   void* stream) {
+namespace {
+int model_forward_entry(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                        const float* mlp_params, const float* x, int64_t n, float t, const float* t_dev,
+                        float* sigma, void* stream) {
   clear_error();
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
   if (int rc = validate_mlp(mlp, g)) return rc;
   if (n == 0) return NECTB_OK;
   NECTB_REQUIRE(grid_params && mlp_params && x && sigma && n > 0, "null pointer or negative size");
-  return dispatch_model(g, grid->feature_dtype, mlp->n_hidden_layers, grid_params, mlp_params, x, n, t,
+  return dispatch_model(g, grid->feature_dtype, mlp->n_hidden_layers, grid_params, mlp_params, x, n, t, t_dev,
                         mlp->activation, mlp->output_activation, sigma, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" int nectb_model_forward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                   const float* mlp_params, const float* x, int64_t n, float t, float* sigma,
+                                   void* stream) {
+  return model_forward_entry(grid, mlp, grid_params, mlp_params, x, n, t, nullptr, sigma, stream);
+}
+
+extern "C" int nectb_model_forward_t(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                     const float* mlp_params, const float* x, int64_t n, const float* t,
+                                     float* sigma, void* stream) {
+  if (!t) return set_error(NECTB_ERR_INVALID, "null timestep pointer");
+  return model_forward_entry(grid, mlp, grid_params, mlp_params, x, n, 0.f, t, sigma, stream);
 }
 
 namespace nectb {

@@ -55,6 +55,7 @@ int validate_geometry(const NectbGeometry* g) {
   NECTB_REQUIRE(g->kind >= NECTB_CONE_VOXEL && g->kind <= NECTB_PARALLEL_CYLINDRICAL, "unknown geometry kind %d",
                 g->kind);
   NECTB_REQUIRE(g->nDetector[0] > 0 && g->nDetector[1] > 0, "nDetector must be positive");
+  NECTB_REQUIRE((int64_t)g->nDetector[0] * g->nDetector[1] <= INT32_MAX, "nDetector has more than 2^31 - 1 pixels");
   return NECTB_OK;
 }
 

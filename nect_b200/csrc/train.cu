@@ -17,8 +17,8 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
                 float* y_pred, float* loss, cudaStream_t s);
 
 int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void* table, const float* W,
-                   const float* x, int64_t n, float tval, const float* dsigma, float* table_grad, float* W_grad,
-                   cudaStream_t s);
+                   const float* x, int64_t n, float tval, const float* t_dev, const float* dsigma, float* table_grad,
+                   float* W_grad, cudaStream_t s);
 
 namespace {
 
@@ -70,6 +70,29 @@ extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, con
 
 namespace nectb {
 namespace {
+
+// Warp per prepared ray: its count and scale, and (points non-null) the
+// positions sample_point regenerates for samples 0..S-1, zeros past the count.
+__global__ void train_rays_kernel(const RayRec* __restrict__ recs, int R, int S, int32_t* __restrict__ counts,
+                                  float* __restrict__ scale, float* __restrict__ points) {
+  const int lane = threadIdx.x & 31;
+  const int r = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (r >= R) return;
+  const RayRec rec = recs[r];
+  if (lane == 0) {
+    if (counts) counts[r] = rec.count;
+    if (scale) scale[r] = rec.scale;
+  }
+  if (!points) return;
+  float* out = points + (int64_t)r * S * 3;
+  for (int i = lane; i < S; i += 32) {
+    float p[3] = {0.f, 0.f, 0.f};
+    if (i < rec.count) sample_point(rec, i, p);
+    out[3 * i + 0] = p[0];
+    out[3 * i + 1] = p[1];
+    out[3 * i + 2] = p[2];
+  }
+}
 
 // dL/dsigma of every sample of ray r is dL/dy_pred[r] * scale[r] (y_pred is the
 // scaled sum of the ray's sigmas, base_trainer.py:552-554).
@@ -184,6 +207,22 @@ extern "C" int nectb_train_backward(const NectbGeometry* geometry, const NectbHa
                      nullptr, workspace, workspace_size, stream, kPhaseBackward);
 }
 
+extern "C" int nectb_train_rays(const NectbGeometry* geometry, int32_t num_rays, int32_t num_points_per_ray,
+                                const void* workspace, int32_t* counts, float* scale, float* points, void* stream) {
+  using namespace nectb;
+  clear_error();
+  if (int rc = validate_geometry(geometry)) return rc;
+  NECTB_REQUIRE(num_rays >= 0 && num_points_per_ray >= 1, "bad sizes");
+  if (num_rays == 0) return NECTB_OK;
+  NECTB_REQUIRE(workspace != nullptr, "null workspace");
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  const Workspace ws = carve_workspace(const_cast<void*>(workspace), num_rays, P);
+  train_rays_kernel<<<(unsigned)ceil_div(num_rays, 8), 256, 0, (cudaStream_t)stream>>>(ws.rays, num_rays,
+                                                                                        num_points_per_ray, counts,
+                                                                                        scale, points);
+  return launch_status("train_rays_kernel");
+}
+
 extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                             const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray) {
   using namespace nectb;
@@ -193,10 +232,11 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   const size_t per_ray = (size_t)num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
   // order and offsets, the staged rounds, and an encoding store for every
   // sample slot of the batch (bf16 rows of n_levels x n_features), capped
-  const size_t row_bytes = (size_t)grid->n_levels * grid->n_features * 2;
-  const size_t rows = std::min<size_t>({(size_t)num_rays * num_points_per_ray, kEncodingStoreCap / row_bytes,
-                                        (size_t)0xffffffffu});
   const NectbTuning tune = current_tuning();
+  const size_t row_bytes = (size_t)grid->n_levels * grid->n_features * 2;
+  const size_t rows = tune.encoding_store ? std::min<size_t>({(size_t)num_rays * num_points_per_ray,
+                                                             kEncodingStoreCap / row_bytes, (size_t)0xffffffffu})
+                                          : 0;
   size_t bytes = order_bytes(num_rays, P) + staged_round_bytes(num_rays, tune.staged_rounds, per_ray) + 256 +
                  align256(rows * row_bytes);
   GridDev g;
@@ -205,9 +245,10 @@ extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const
   return bytes;
 }
 
-extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
-                                    const float* mlp_params, const float* x, int64_t n, float t, const float* dsigma,
-                                    float* grid_grad, float* mlp_grad, void* stream) {
+namespace {
+int model_backward_entry(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                         const float* mlp_params, const float* x, int64_t n, float t, const float* t_dev,
+                         const float* dsigma, float* grid_grad, float* mlp_grad, void* stream) {
   clear_error();
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
@@ -217,8 +258,24 @@ extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* m
   if (n == 0) return NECTB_OK;
   NECTB_REQUIRE(grid_params && mlp_params && x && dsigma && grid_grad && mlp_grad, "null pointer argument");
   NECTB_REQUIRE(((uintptr_t)grid_grad & 15u) == 0, "grid_grad must be 16-byte aligned");
-  return model_backward(g, *mlp, grid->feature_dtype, grid_params, mlp_params, x, n, t, dsigma, grid_grad, mlp_grad,
-                        (cudaStream_t)stream);
+  return model_backward(g, *mlp, grid->feature_dtype, grid_params, mlp_params, x, n, t, t_dev, dsigma, grid_grad,
+                        mlp_grad, (cudaStream_t)stream);
+}
+}  // namespace
+
+extern "C" int nectb_model_backward(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                    const float* mlp_params, const float* x, int64_t n, float t, const float* dsigma,
+                                    float* grid_grad, float* mlp_grad, void* stream) {
+  return model_backward_entry(grid, mlp, grid_params, mlp_params, x, n, t, nullptr, dsigma, grid_grad, mlp_grad,
+                              stream);
+}
+
+extern "C" int nectb_model_backward_t(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                      const float* mlp_params, const float* x, int64_t n, const float* t,
+                                      const float* dsigma, float* grid_grad, float* mlp_grad, void* stream) {
+  if (!t) return set_error(NECTB_ERR_INVALID, "null timestep pointer");
+  return model_backward_entry(grid, mlp, grid_params, mlp_params, x, n, 0.f, t, dsigma, grid_grad, mlp_grad,
+                              stream);
 }
 
 extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr,

@@ -128,8 +128,10 @@ inline size_t staged_round_bytes(int R, int rounds, size_t per_ray) {
   return std::min((size_t)per_round * per_ray, kStagingCap / per_ray * per_ray);
 }
 
+// store == false: no encoding store whatever the buffer size (the backward
+// recomputes every sample's encoding from the tables).
 inline StageLayout stage_layout(const Workspace& ws, int R, int P, int S, size_t row_bytes, size_t per_ray,
-                                int rounds) {
+                                int rounds, bool store = true) {
   StageLayout L;
   const size_t ob = order_bytes(R, P);
   if (!ws.stage || ws.stage_bytes <= ob || R <= 0) return L;
@@ -143,7 +145,7 @@ inline StageLayout stage_layout(const Workspace& ws, int R, int P, int S, size_t
   const size_t avail = ws.stage_bytes - ob;
   const size_t want = staged_round_bytes(R, rounds, per_ray);
   size_t xbytes = 0;
-  if (avail >= want + (size_t)S * row_bytes + 256) {
+  if (store && avail >= want + (size_t)S * row_bytes + 256) {
     const size_t rows = std::min<size_t>({(avail - want - 256) / row_bytes, (size_t)R * S, 0xffffffffu});
     if (rows >= (size_t)S) {
       L.xcap = (uint32_t)rows;

@@ -1038,7 +1038,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // staging region: ray order and sample offsets, the encoding store, then
   // dL/d(encoding) of one round of per_round rays
   const StageLayout L = stage_layout(ws, R, a.n_pixels, a.S, IN * sizeof(__nv_bfloat16),
-                                     (size_t)a.S * IN * sizeof(float), tune.staged_rounds);
+                                     (size_t)a.S * IN * sizeof(float), tune.staged_rounds, tune.encoding_store != 0);
   auto run_order = [&]() -> int {
     ProfScope ps(kProfOrder, s);
     const int n_blocks = order_blocks(R, a.n_pixels);

@@ -420,8 +420,8 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
 template <int D, int F, int IN, int H, int NT, typename T>
 __global__ void __launch_bounds__(NT, 1)
 model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restrict__ W, const float* __restrict__ x,
-                 int64_t n, float tval, const float* __restrict__ dsigma, int act, int out_act,
-                 float* __restrict__ table_grad, float* __restrict__ W_grad) {
+                 int64_t n, float tval, const float* __restrict__ t_dev, const float* __restrict__ dsigma, int act,
+                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad) {
   constexpr int LD = NT + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
@@ -439,6 +439,7 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
 #pragma unroll
   for (int k = 0; k < H - 1; ++k) gh[k].zero();
   float dwout[2] = {0.f, 0.f};
+  if (D == 4 && t_dev) tval = *t_dev;   // the broadcast timestep, read on the device
   __syncthreads();
   for (int64_t c0 = (int64_t)blockIdx.x * NT; c0 < n; c0 += (int64_t)gridDim.x * NT) {  // block-uniform
     const int64_t i = c0 + t;
@@ -509,7 +510,8 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
 
 template <int D, int F, int H, typename T>
 int launch_model_bwd(const GridDev& grid, const void* table, const float* W, const float* x, int64_t n, float tval,
-                     const float* dsigma, int act, int out_act, float* table_grad, float* W_grad, cudaStream_t s) {
+                     const float* t_dev, const float* dsigma, int act, int out_act, float* table_grad, float* W_grad,
+                     cudaStream_t s) {
   constexpr int IN = 16 * F;
   // 64-thread tiles when 128 would not fit shared memory (3 hidden layers over 64 inputs)
   constexpr int NT = (IN + (H + 2) * kWidth) * (128 + 4) * 4 + simt_weight_floats<IN, H, true>() * 4 > 227 * 1024
@@ -523,7 +525,7 @@ int launch_model_bwd(const GridDev& grid, const void* table, const float* W, con
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(sms, ceil_div(n, NT)));
   ProfScope ps(kProfModel, s);
-  k<<<blocks, NT, smem, s>>>(grid, (const T*)table, W, x, n, tval, dsigma, act, out_act, table_grad, W_grad);
+  k<<<blocks, NT, smem, s>>>(grid, (const T*)table, W, x, n, tval, t_dev, dsigma, act, out_act, table_grad, W_grad);
   return launch_status("model_bwd_kernel");
 }
 
@@ -573,16 +575,16 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
 }  // namespace
 
 int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void* table, const float* W,
-                   const float* x, int64_t n, float tval, const float* dsigma, float* table_grad, float* W_grad,
-                   cudaStream_t s) {
+                   const float* x, int64_t n, float tval, const float* t_dev, const float* dsigma, float* table_grad,
+                   float* W_grad, cudaStream_t s) {
   const bool h = dtype == NECTB_F16;
   const int D = g.n_dims, F = g.n_features, H = mlp.n_hidden_layers;
   const int act = mlp.activation, oact = mlp.output_activation;
   const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
-    return h ? launch_model_bwd<d(), f(), hl(), __half>(g, table, W, x, n, tval, dsigma, act, oact, table_grad,
-                                                        W_grad, s)
-             : launch_model_bwd<d(), f(), hl(), float>(g, table, W, x, n, tval, dsigma, act, oact, table_grad,
-                                                       W_grad, s);
+    return h ? launch_model_bwd<d(), f(), hl(), __half>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
+                                                        table_grad, W_grad, s)
+             : launch_model_bwd<d(), f(), hl(), float>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
+                                                       table_grad, W_grad, s);
   });
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model backward: unsupported configuration (n_dims %d, n_features %d, "

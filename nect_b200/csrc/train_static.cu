@@ -10,16 +10,14 @@
 //
 // The scratch is one file-scope __device__ array of kStaticScratchBytes
 // (20 MiB + 4 KiB); every GPU that loads the library reserves it until the
-// process exits.  The first call on a device (with that device current)
-// looks up the array's device address with cudaGetSymbolAddress; make that
-// first call before any stream capture.  All calls share the one array and it
+// process exits.  Every call (with its device current) looks up the array's
+// device address with cudaGetSymbolAddress; the first call on a device loads
+// the module there, so make it before any stream capture.  All calls share the one array and it
 // keeps the last call's contents: nectb_train_step clears what has to start
 // at zero (scheduling cursors, error word, pixel slots) and overwrites the
 // per-ray records, so results never depend on a previous call, but calls
 // whose work overlaps on the GPU (different streams, or threads without
 // ordering) race on the array and must be serialised by the caller.
-#include <mutex>
-
 #include "common.cuh"
 #include "train_common.cuh"
 
@@ -27,29 +25,22 @@ extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, con
                                               const NectbMLP* mlp, int32_t num_rays);
 
 namespace nectb {
+int validate_geometry(const NectbGeometry* g);
 namespace {
 
 constexpr size_t kStaticScratchBytes = (size_t(20) << 20) + 4096;
 static __device__ __align__(256) unsigned char g_train_scratch[kStaticScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_scratch_mu;
-void* g_scratch_ptr[kMaxDevices] = {nullptr};
-
-// Device address of g_train_scratch on the current device (looked up once per
-// device; the host-side symbol itself is not a device address).
+// Device address of g_train_scratch on the current device (the host-side
+// symbol itself is not a device address).  Looked up on every call: the
+// lookup allocates nothing, and a module reloaded after a context reset gets
+// its new address.  It loads the module on the call's first use of the
+// device, so that first call must come before any stream capture.
 int scratch_address(void** out) {
-  int dev = 0;
-  if (int rc = cuda_status(cudaGetDevice(&dev), "cudaGetDevice")) return rc;
-  if (dev < 0 || dev >= kMaxDevices) return set_error(NECTB_ERR_INVALID, "device index %d out of range", dev);
-  std::lock_guard<std::mutex> lk(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    if (int rc = cuda_status(cudaGetSymbolAddress(&p, g_train_scratch), "cudaGetSymbolAddress(g_train_scratch)"))
-      return rc;
-    g_scratch_ptr[dev] = p;
-  }
-  *out = g_scratch_ptr[dev];
+  void* p = nullptr;
+  if (int rc = cuda_status(cudaGetSymbolAddress(&p, g_train_scratch), "cudaGetSymbolAddress(g_train_scratch)"))
+    return rc;
+  *out = p;
   return NECTB_OK;
 }
 
@@ -65,6 +56,7 @@ extern "C" int nectb_train_step_static(const NectbGeometry* geometry, const Nect
   using namespace nectb;
   clear_error();
   NECTB_REQUIRE(geometry && grid && mlp && batch, "null description");
+  if (int rc = validate_geometry(geometry)) return rc;
   const size_t need = nectb_train_workspace_bytes(geometry, grid, mlp, batch->num_rays);
   if (need > kStaticScratchBytes)
     return set_error(NECTB_ERR_TOO_LARGE,
@@ -85,8 +77,16 @@ extern "C" const unsigned int* nectb_train_error_word(const NectbGeometry* geome
     set_error(NECTB_ERR_INVALID, "nectb_train_error_word: null geometry or num_rays <= 0");
     return nullptr;
   }
+  if (validate_geometry(geometry) != NECTB_OK) return nullptr;
   void* ws = const_cast<void*>(workspace);
-  if (!ws && scratch_address(&ws) != NECTB_OK) return nullptr;
+  if (!ws) {
+    // the static scratch: only batches that nectb_train_step_static accepts have a word there
+    if (nectb_train_workspace_bytes(geometry, nullptr, nullptr, num_rays) > kStaticScratchBytes) {
+      set_error(NECTB_ERR_TOO_LARGE, "nectb_train_error_word: %d rays do not fit the static scratch", num_rays);
+      return nullptr;
+    }
+    if (scratch_address(&ws) != NECTB_OK) return nullptr;
+  }
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
   return carve_workspace(ws, num_rays, P).counters + 2;
 }

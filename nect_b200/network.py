@@ -10,8 +10,11 @@ PyTorch Linear layout; with ``precision="mixed"`` an fp16 copy of the table is
 kept for the gathers and refreshed by the fused Adam step.
 
 Initialisation: table entries U(-1e-4, 1e-4) (Mueller et al. 2022, section 4);
-weights Glorot-uniform per layer.  ``forward`` runs the CUDA model kernel
-(inference; training goes through ``nect_b200.trainer``).
+weights Glorot-uniform per layer.  ``forward`` runs the CUDA model kernel;
+when autograd records it is a differentiable node (``ModelPoints``, the
+hand-written backward), so ``loss.backward()`` through ``model(points)``
+trains the table and the MLP as in the reference's loop.  The fused
+training step of ``nect_b200.trainer`` is the fast path for ray batches.
 """
 from __future__ import annotations
 
@@ -108,18 +111,15 @@ class _HashGridModel(nn.Module):
         super()._load_from_state_dict(*args, **kwargs)
         self.refresh_half()
 
-    @torch.no_grad()
-    def _forward(self, x: torch.Tensor, t: float) -> torch.Tensor:
-        _lib.require_cuda(x, "x")
-        if x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] != 3:
-            raise ValueError("x must be fp32 [N, 3] (z, y, x) in [0, 1]")
-        n = x.shape[0]
-        out = torch.empty(n, 1, device=x.device, dtype=torch.float32)
-        rc = _lib.lib.nectb_model_forward(ctypes.byref(self.grid_desc), ctypes.byref(self.mlp_desc),
-                                          self.grid_table.data_ptr(), self.mlp.data_ptr(), x.data_ptr(), n,
-                                          float(t), out.data_ptr(), _lib.stream_ptr(x.device))
-        _lib.check(rc, "nectb_model_forward")
-        return out
+    def _forward(self, x: torch.Tensor, t) -> torch.Tensor:
+        """sigma [N, 1] at x [N, 3]; differentiable in (table, mlp) whenever
+        autograd records (the hand-written backward, ModelPoints), plain
+        inference otherwise."""
+        if torch.is_grad_enabled() and (self.table.requires_grad or self.mlp.requires_grad):
+            sigma = ModelPoints.apply(self.table, self.mlp, self, x, t)
+        else:
+            sigma = _model_forward(self, x, t)
+        return sigma.unsqueeze(1)
 
     def corners(self, x: torch.Tensor):
         """Per-level corner indices/weights [N, L, 2^d] (diagnostic)."""
@@ -148,14 +148,87 @@ class HashGrid(_HashGridModel):
     n_dims = 3
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
-        return self._forward(x.contiguous(), 0.0)
+        return self._forward(x, 0.0)
 
 
 class HashGrid4D(_HashGridModel):
-    """Dynamic model with one 4D grid: forward(x [N,3], t in [0,1]) -> sigma [N,1]."""
+    """Dynamic model with one 4D grid: forward(x [N,3], t in [0,1]) -> sigma [N,1].
+
+    t is a float or a one-element tensor; a CUDA tensor stays on the device
+    (the kernels read it there, as the reference broadcasts it on the device,
+    networks.py:85), so a dynamic query never waits for the host."""
     n_dims = 4
 
     def forward(self, x: torch.Tensor, t) -> torch.Tensor:
-        if isinstance(t, torch.Tensor):
-            t = float(t.item())
-        return self._forward(x.contiguous(), float(t))
+        return self._forward(x, t)
+
+
+def _timestep(t):
+    """(host value, device tensor or None) of a timestep argument."""
+    if isinstance(t, torch.Tensor):
+        if t.numel() != 1:
+            raise ValueError(f"t must hold one value, got shape {tuple(t.shape)}")
+        if t.is_cuda:
+            return 0.0, t.detach().reshape(1).to(torch.float32).contiguous()
+        return float(t.reshape(())), None
+    return float(t), None
+
+
+def _check_points(x: torch.Tensor) -> torch.Tensor:
+    _lib.require_cuda(x, "x")
+    if x.dtype != torch.float32 or x.dim() != 2 or x.shape[1] != 3:
+        raise ValueError("x must be fp32 [N, 3] (z, y, x) in [0, 1]")
+    return x.detach().contiguous()
+
+
+def _model_forward(model: _HashGridModel, x: torch.Tensor, t) -> torch.Tensor:
+    """sigma [N] = MLP(encode(x, t)) by nectb_model_forward(_t), no autograd."""
+    x = _check_points(x)
+    tv, td = _timestep(t)
+    sigma = torch.empty(x.shape[0], device=x.device, dtype=torch.float32)
+    args = (ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+            model.mlp.data_ptr(), x.data_ptr(), x.shape[0])
+    if td is None:
+        rc = _lib.lib.nectb_model_forward(*args, tv, sigma.data_ptr(), _lib.stream_ptr(x.device))
+    else:
+        rc = _lib.lib.nectb_model_forward_t(*args, td.data_ptr(), sigma.data_ptr(), _lib.stream_ptr(x.device))
+    _lib.check(rc, "nectb_model_forward")
+    return sigma
+
+
+class ModelPoints(torch.autograd.Function):
+    """sigma(x) [N] at points x [N, 3], differentiable in (table, mlp):
+    forward nectb_model_forward, backward nectb_model_backward (fp32 SIMT for
+    both table precisions; the gradient of the fp16 copy is the fp32
+    table's).  This is the autograd node behind HashGrid.forward, for the
+    reference's loss.backward() through model(points) (base_trainer.py:
+    535-542, 650) and for losses on model outputs such as the total-variation
+    term (base_trainer.py:615-649).  No gradient flows to x."""
+
+    @staticmethod
+    def forward(ctx, table, mlp, model, x, t):
+        sigma = _model_forward(model, x, t)
+        ctx.model, ctx.x, ctx.t = model, _check_points(x), _timestep(t)
+        return sigma
+
+    @staticmethod
+    def backward(ctx, dsigma):
+        model, x = ctx.model, ctx.x
+        tv, td = ctx.t
+        g = dsigma.detach().to(torch.float32).contiguous()
+        tg, mg = torch.zeros_like(model.table), torch.zeros_like(model.mlp)
+        args = (ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                model.mlp.data_ptr(), x.data_ptr(), x.shape[0])
+        if td is None:
+            rc = _lib.lib.nectb_model_backward(*args, tv, g.data_ptr(), tg.data_ptr(), mg.data_ptr(),
+                                               _lib.stream_ptr(x.device))
+        else:
+            rc = _lib.lib.nectb_model_backward_t(*args, td.data_ptr(), g.data_ptr(), tg.data_ptr(), mg.data_ptr(),
+                                                 _lib.stream_ptr(x.device))
+        _lib.check(rc, "nectb_model_backward")
+        return tg, mg, None, None, None
+
+
+def model_points(model: _HashGridModel, x: torch.Tensor, t=0.0) -> torch.Tensor:
+    """Differentiable sigma [n] of the model at points x [n, 3] ((z, y, x) in [0, 1])."""
+    return ModelPoints.apply(model.table, model.mlp, model, x, t)

@@ -21,7 +21,8 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib
-from .network import _HashGridModel
+from .network import ModelPoints, _HashGridModel, model_points  # noqa: F401
+from .sampling import batching
 from .sampling.ct_sampling import draw_ray_randoms
 from .sampling.geometry import Geometry
 
@@ -186,41 +187,6 @@ def ray_integral(model: _HashGridModel, c_geometry, batch: RayBatch, max_distanc
                  workspace: Workspace) -> torch.Tensor:
     """Differentiable y_pred [R] of one batch (see RayIntegral)."""
     return RayIntegral.apply(model.table, model.mlp, model, c_geometry, batch, max_distance_traveled, workspace)
-
-
-class ModelPoints(torch.autograd.Function):
-    """sigma(x) at n points, differentiable in (table, mlp): forward
-    nectb_model_forward, backward nectb_model_backward.  For losses on model
-    outputs, such as the total-variation term (base_trainer.py:615-649)."""
-
-    @staticmethod
-    def forward(ctx, table, mlp, model, x, t):
-        x = x.detach().to(torch.float32).contiguous()
-        _lib.require_cuda(x, "x")
-        sigma = torch.empty(x.shape[0], device=x.device, dtype=torch.float32)
-        rc = _lib.lib.nectb_model_forward(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
-                                          model.grid_table.data_ptr(), model.mlp.data_ptr(), x.data_ptr(),
-                                          x.shape[0], float(t), sigma.data_ptr(), _lib.stream_ptr(x.device))
-        _lib.check(rc, "nectb_model_forward")
-        ctx.model, ctx.x, ctx.t = model, x, float(t)
-        return sigma
-
-    @staticmethod
-    def backward(ctx, dsigma):
-        model, x = ctx.model, ctx.x
-        g = dsigma.detach().to(torch.float32).contiguous()
-        tg, mg = torch.zeros_like(model.table), torch.zeros_like(model.mlp)
-        rc = _lib.lib.nectb_model_backward(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
-                                           model.grid_table.data_ptr(), model.mlp.data_ptr(), x.data_ptr(),
-                                           x.shape[0], ctx.t, g.data_ptr(), tg.data_ptr(), mg.data_ptr(),
-                                           _lib.stream_ptr(x.device))
-        _lib.check(rc, "nectb_model_backward")
-        return tg, mg, None, None, None
-
-
-def model_points(model: _HashGridModel, x: torch.Tensor, t: float = 0.0) -> torch.Tensor:
-    """Differentiable sigma [n] of the model at points x [n, 3] ((z, y, x) in [0, 1])."""
-    return ModelPoints.apply(model.table, model.mlp, model, x, t)
 
 
 def total_variation_3d(volume: torch.Tensor, weight: float = 1.0) -> torch.Tensor:
@@ -454,18 +420,14 @@ class Trainer:
 
     @property
     def batch_size(self) -> int:
-        return self.points_per_batch // self.points_per_ray
+        return batching.rays_per_batch(self.points_per_batch, self.points_per_ray)
 
     def make_batch(self, perm: torch.Tensor, batch_num: int, angle: float, projection: torch.Tensor,
                    t: float = 0.0) -> RayBatch | None:
-        P = perm.numel()
-        bs = self.batch_size
-        start, size = batch_num * bs, bs
-        if (batch_num + 1) * bs > P:  # projector.py:108-112
-            if batch_num == 0:
-                size = P % bs
-            else:
-                return None
+        window = batching.batch_window(perm.numel(), self.batch_size, batch_num)
+        if window is None:
+            return None
+        start, size = window
         jitter, det_off = draw_ray_randoms(size, self.random_offset_detector, self.device)
         return RayBatch(perm=perm, start=start, num_rays=size, points_per_ray=self.points_per_ray, angle=angle,
                         max_ray_distance_per_point=self.geometry.max_distance_traveled / self.points_per_ray,
@@ -583,7 +545,7 @@ class Trainer:
         """All batches of one projection (flattened, min-max scaled, on device)."""
         P = projection.numel()
         perm = torch.randperm(P, dtype=torch.int64, device=self.device)
-        n_batches = P // self.batch_size + (1 if P % self.batch_size else 0)
+        n_batches = batching.batches_per_projection(P, self.batch_size)
         loss = None
         for b in range(min(self.batch_per_proj, n_batches)):
             batch = self.make_batch(perm, b, angle, projection, t)

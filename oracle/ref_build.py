@@ -1,8 +1,9 @@
 """Compile the reference's own CUDA sampling extension into ``oracle/_ref``.
 
 Test infrastructure only.  This recipe builds ``nect/sampling/ct_sampling.cu``
-from the reference checkout (default ``/root/reference``; override with
-``NECT_REFERENCE``) exactly as its ``setup.py:12-26`` would (same nvcc flags:
+from the reference checkout named by the ``NECT_REFERENCE`` environment
+variable (the ``ref`` target of ``oracle/Makefile`` sets it; with it unset
+nothing is built) exactly as its ``setup.py:12-26`` would (same nvcc flags:
 ``-g -D__USE_GPU -DCUDA_VERSION=12030 -O3``), but for sm_100a only and without
 running the reference's build system.  The result, ``oracle/_ref/ct_sampling.so``,
 is the GPU-side authority for the sampling kernel: GPU parity tests and the
@@ -19,12 +20,17 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE / "_ref"
 
 
-def reference_root() -> Path:
-    return Path(os.environ.get("NECT_REFERENCE", "/root/reference"))
+def reference_root() -> Path | None:
+    root = os.environ.get("NECT_REFERENCE")
+    return Path(root) if root else None
 
 
 def build(verbose: bool = False) -> Path | None:
-    src = reference_root() / "nect" / "sampling" / "ct_sampling.cu"
+    root = reference_root()
+    if root is None:
+        print("[oracle/_ref] NECT_REFERENCE is not set; skipping the reference build", file=sys.stderr)
+        return None
+    src = root / "nect" / "sampling" / "ct_sampling.cu"
     if not src.exists():
         print(f"[oracle/_ref] reference source {src} not present; skipping", file=sys.stderr)
         return None
@@ -57,7 +63,7 @@ def load():
 
     so = OUT / "ct_sampling.so"
     if not so.exists():
-        raise FileNotFoundError(f"{so} is missing: run `python oracle/ref_build.py` where the reference is mounted")
+        raise FileNotFoundError(f"{so} is missing: run `make -C oracle ref` where the reference is checked out")
     loader = importlib.machinery.ExtensionFileLoader("ct_sampling", str(so))
     spec = importlib.util.spec_from_loader("ct_sampling", loader)
     mod = importlib.util.module_from_spec(spec)

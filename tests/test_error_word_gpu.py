@@ -48,3 +48,11 @@ def test_error_word_address_checks_arguments(cuda_device):
     assert not _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), 0, None)
     addr = _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), 256, None)   # static scratch
     assert addr
+    # more rays than the static scratch holds: no address (NECTB_ERR_TOO_LARGE), not one past its end
+    assert not _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), 1 << 20, None)
+    assert b"static scratch" in _lib.lib.nectb_last_error()
+    # a geometry the library rejects gives no address either
+    bad = Geometry(nDetector=[16, 16], dDetector=[1.0, 1.0], mode="parallel", nVoxel=[8] * 3,
+                   dVoxel=[2.0] * 3).get_c_geometry()
+    bad.c_struct.nDetector[0] = -16
+    assert not _lib.lib.nectb_train_error_word(ctypes.byref(bad.c_struct), 256, None)
