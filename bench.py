@@ -265,36 +265,52 @@ def valid_samples(trainer, batches) -> int:
     return total
 
 
-def probe_roofs(entries: int, gather_bytes: int, slice_entries: int, red_bytes: int, device) -> dict:
-    """Measured roofs (GB/s of useful bytes) of random gathers of gather_bytes
-    from a buffer of `entries` entries and of random fp32 reductions of
-    red_bytes into a buffer of `slice_entries` entries (library probes,
-    CUDA events on the launching stream, best of 3 after a warm-up)."""
+def probe_roofs(table_entries: int, entry_bytes: int, slice_entries: int, grad_entry_bytes: int, device) -> dict:
+    """Measured roofs (GB/s of the bytes each access moves) of the memory
+    system under the kernels' access kinds, on buffers the size of the fp16
+    table (gathers) and of one scatter pass's fp32 gradient slice
+    (reductions): random entries of the table's entry size, random whole
+    32-byte sectors, random whole lines (a warp's 32 consecutive entries), and
+    for reductions random entries, random 16-byte pairs and random lines of
+    16-byte reductions.  Library probes (nectb_probe_gather/_reduce), CUDA
+    events on the launching stream, best of 3 after a warm-up."""
     from nect_b200 import _lib
 
-    out = {}
     stream = torch.cuda.current_stream(device)
     sink = torch.zeros(1, dtype=torch.int32, device=device)
-    for kind, n_ent, eb in (("gather", entries, gather_bytes), ("reduce", slice_entries, red_bytes)):
-        buf = torch.rand(n_ent * eb // 4, device=device)
-        n_ops = 1 << 28
-        ops = _lib.lib.nectb_probe_ops(n_ops)
+    table_bytes = table_entries * entry_bytes
+    slice_bytes = slice_entries * grad_entry_bytes
+    runs = {   # name: (kind, buffer bytes, access bytes, mode)
+        "gather_entry": ("gather", table_bytes, entry_bytes, 0),
+        "gather_sector": ("gather", table_bytes, 32, 0),
+        "gather_line": ("gather", table_bytes, entry_bytes, 1),
+        "reduce_entry": ("reduce", slice_bytes, grad_entry_bytes, 0),
+        "reduce_pair": ("reduce", slice_bytes, 16, 0),
+        "reduce_line": ("reduce", slice_bytes, 16, 1),
+    }
+    out = {}
+    n_ops = 1 << 28
+    ops = _lib.lib.nectb_probe_ops(n_ops)
+    for name, (kind, nbytes, eb, mode) in runs.items():
+        n_ent = nbytes // eb
+        buf = torch.zeros(n_ent * eb // 4, device=device)
         best = None
         for rep in range(4):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             if kind == "gather":
-                rc = _lib.lib.nectb_probe_gather(buf.data_ptr(), n_ent, eb, n_ops, sink.data_ptr(),
+                rc = _lib.lib.nectb_probe_gather(buf.data_ptr(), n_ent, eb, mode, n_ops, sink.data_ptr(),
                                                  _lib.stream_ptr(device))
             else:
-                rc = _lib.lib.nectb_probe_reduce(buf.data_ptr(), n_ent, eb, n_ops, _lib.stream_ptr(device))
+                rc = _lib.lib.nectb_probe_reduce(buf.data_ptr(), n_ent, eb, mode, n_ops, _lib.stream_ptr(device))
             e1.record(stream)
             _lib.check(rc, f"nectb_probe_{kind}")
             e1.synchronize()
             ms = e0.elapsed_time(e1)
             if rep and (best is None or ms < best):
                 best = ms
-        out[kind] = {"gbs": ops * eb / (best / 1e3) / 1e9, "entry_bytes": eb, "buffer_mb": n_ent * eb / 1e6,
+        out[name] = {"gbs": ops * eb / (best / 1e3) / 1e9, "access_bytes": eb, "buffer_mb": n_ent * eb / 1e6,
+                     "pattern": "random lines of 32 consecutive entries per warp" if mode else "random entry per lane",
                      "ops": int(ops), "ms": best}
         del buf
     return out
@@ -434,7 +450,7 @@ def main():
     F = enc.n_features_per_level
     feat_bytes = 2 if args.precision == "mixed" else 4
     cur = autotune.get_tuning()
-    slice_entries = max(1, min(model.table.shape[0], int(cur["scatter_group_bytes"]) // (F * 4)))
+    slice_entries = max(64, min(model.table.shape[0], int(cur["scatter_group_bytes"]) // (F * 4)))
     roofs = probe_roofs(model.table.shape[0], F * feat_bytes, slice_entries, F * 4, dev)
 
     clocks = ClockSampler(dev.index or 0)
@@ -472,35 +488,46 @@ def main():
             if len(f) == 4 and not line.startswith("#") and f[:2] == [args.workload, args.precision]:
                 traffic_step[f[2]] = float(f[3])
 
-    def roof(kind, per_sample, unit_peak, peak, bound, unit, scale):
+    l2_step = {}   # L2 bytes per step and kernel kind (lts__t_bytes.sum of an ncu capture, scaled per sample)
+    lfile = ROOT / "profiles" / "l2_bytes_per_sample.txt"
+    if lfile.exists():
+        for line in lfile.read_text().splitlines():
+            f = line.split()
+            if len(f) == 4 and not line.startswith("#") and f[:2] == [args.workload, args.precision]:
+                l2_step[f[2]] = float(f[3]) * per_step_samples
+
+    def roof(kind, per_sample, peak_name, bound, unit, scale, peak=None, peak_src=None):
         if kind not in kernel_ms:
             return None
         per_launch = per_step_samples * per_sample / launches_per_step[kind]
-        achieved = per_launch / (kernel_ms[kind] / 1e3) / scale
+        secs = kernel_ms[kind] / 1e3
+        achieved = per_launch / secs / scale
+        if peak is None:
+            peak, peak_src = roofs[peak_name]["gbs"], f"measured in this run: {peak_name} probe ({roofs[peak_name]['pattern']}, {roofs[peak_name]['access_bytes']} B, {roofs[peak_name]['buffer_mb']:.0f} MB buffer)"
         tr = traffic_step.get(kind)
         out = {"bound": bound, "kernel": kind, "achieved": achieved, "peak": peak, "unit": unit,
-               "frac": achieved / peak, "peak_source": unit_peak,
+               "frac": achieved / peak, "peak_source": peak_src,
                "traffic": tr / launches_per_step[kind] if tr is not None else None,
                "algorithmic_per_launch": per_launch, "launch_ms": kernel_ms[kind],
                "launches_per_step": launches_per_step[kind]}
         if tr is not None:
-            out["dram_frac_of_hbm"] = tr / launches_per_step[kind] / (kernel_ms[kind] / 1e3) / 1e9 / hbm
+            out["dram_gbs"] = tr / launches_per_step[kind] / secs / 1e9
+            out["dram_frac_of_hbm"] = out["dram_gbs"] / hbm
+        if kind in l2_step and bound == "l2":
+            out["l2_gbs"] = l2_step[kind] / launches_per_step[kind] / secs / 1e9
+            out["l2_frac"] = out["l2_gbs"] / peak
         return out
 
     rooflines = {
-        "forward": roof("forward", gather, f"measured in this run: random {F * feat_bytes}-byte gathers from a "
-                        f"{roofs['gather']['buffer_mb']:.0f} MB buffer (the table's size)", roofs["gather"]["gbs"],
-                        "l2", "GB/s", 1e9),
-        "scatter": roof("scatter", scatter, f"measured in this run: random {F * 4}-byte fp32 reductions into a "
-                        f"{roofs['reduce']['buffer_mb']:.0f} MB buffer (one scatter pass's gradient slice)",
-                        roofs["reduce"]["gbs"], "l2", "GB/s", 1e9),
-        "backward": roof("backward", 3 * mlp_fwd, f"{peak_src} bf16 dense, sustained", tensor_peak, "tensor",
-                         "TFLOP/s", 1e12),
+        "forward": roof("forward", gather, "gather_line", "l2", "GB/s", 1e9),
+        "scatter": roof("scatter", scatter, "reduce_line", "l2", "GB/s", 1e9),
+        "backward": roof("backward", 3 * mlp_fwd, None, "tensor", "TFLOP/s", 1e12, tensor_peak,
+                         f"{peak_src} bf16 dense, sustained"),
     }
     if args.precision == "plain_fp32":
         rooflines["backward"] = None   # the plain backward is SIMT, no tensor-core roof
     rooflines = {k: v for k, v in rooflines.items() if v}
-    # the dominant kernel of the step (most time); the scatter kind if it has none of its own
+    # the dominant kernel of the step (most time)
     dominant = max((k for k in rooflines), key=lambda k: prof[k][1])
     roofline = dict(rooflines[dominant])
 

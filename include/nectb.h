@@ -355,6 +355,43 @@ int nectb_train_backward(const NectbGeometry* geometry, const NectbHashGrid* gri
                          const float* dloss_dy, float* grid_grad, float* mlp_grad,
                          void* workspace, size_t workspace_bytes, void* stream);
 
+/* Continuous-scan training step (nect/trainers/continous_scanning_trainer.py:
+ * 85-140): the detector integrates while the object turns, so each pixel's
+ * prediction is the mean over sub_angles (1..32) sub-angles of its line
+ * integral, y_pred[r] = sum_j (sum_s sigma_jrs * distances_jr /
+ * max_distance_traveled) / sub_angles, with every sub-angle ray of the pixel
+ * at the batch's t.  All sub-angle rays of the batch (sub_angles *
+ * num_rays) run through ONE launch of each fused kernel instead of one
+ * forward per sub-angle.  sub_angles_rad: host array of the sub angles
+ * (batch->angle_rad is ignored); batch->jitter holds sub_angles * num_rays
+ * and batch->detector_offset sub_angles * num_rays * 2 draws, sub-angle-major
+ * (the reference draws them per sub-angle call of sample(), in that order).
+ * y_pred[num_rays]; loss = mean over the num_rays pixels; gradients are
+ * ADDED.  The forward/backward halves take dL/dy_pred per pixel.  Workspace:
+ * nectb_train_scan_workspace_bytes() plus, for the mixed path's two-pass
+ * backward, nectb_train_scan_staging_bytes(); its error word is
+ * nectb_train_scan_error_word().  No other reference counterpart. */
+size_t nectb_train_scan_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                        const NectbMLP* mlp, int32_t num_rays, int32_t sub_angles);
+size_t nectb_train_scan_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                      const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray,
+                                      int32_t sub_angles);
+int nectb_train_scan_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                          const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                          const float* sub_angles_rad, int32_t sub_angles, float* grid_grad, float* mlp_grad,
+                          float* y_pred, float* loss, void* workspace, size_t workspace_bytes, void* stream);
+int nectb_train_scan_forward(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                             const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                             const float* sub_angles_rad, int32_t sub_angles, float* y_pred, void* workspace,
+                             size_t workspace_bytes, void* stream);
+int nectb_train_scan_backward(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                              const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                              const float* sub_angles_rad, int32_t sub_angles, const float* dloss_dy,
+                              float* grid_grad, float* mlp_grad, void* workspace, size_t workspace_bytes,
+                              void* stream);
+const unsigned int* nectb_train_scan_error_word(const NectbGeometry* geometry, int32_t num_rays,
+                                                int32_t sub_angles, const void* workspace);
+
 /* nectb_train_step without a caller workspace, for callers that cannot
  * allocate device memory (a runtime that binds this library through its C ABI
  * and has no CUDA allocator, or a loop that must never call cudaMalloc, which
@@ -376,12 +413,15 @@ size_t nectb_train_static_scratch_bytes(void);
 
 /* Adam (torch.optim.Adam semantics, as configured in nect/config.py:400-414)
  * over n fp32 parameters with fp32 moments; step is the 1-based step count.
- * When param_half is non-NULL the updated parameter is also written there as
+ * The hyper-parameters are doubles, as torch holds them: 1 - beta1,
+ * 1 - beta2, lr / (1 - beta1^step) and sqrt(1 - beta2^step) are formed in
+ * double before the fp32 update, in torch's order of operations.  When
+ * param_half is non-NULL the updated parameter is also written there as
  * fp16 (the mixed path's table copy).  grad is zeroed after use when
  * zero_grad != 0 (optim.zero_grad, base_trainer.py:518). */
 int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq,
-                    int64_t n, float lr, float beta1, float beta2, float eps,
-                    float weight_decay, int32_t step, void* param_half,
+                    int64_t n, double lr, double beta1, double beta2, double eps,
+                    double weight_decay, int32_t step, void* param_half,
                     int32_t zero_grad, void* stream);
 
 /* Per-kernel timing of the library's own launches with CUDA events recorded
@@ -443,16 +483,21 @@ int nectb_set_tuning(const NectbTuning* tuning);
 
 /* Roofline probes (no reference counterpart): the measured roofs that the
  * encoding's corner gathers and the gradient scatter's reductions are
- * reported against.  nectb_probe_gather loads entry_bytes (4, 8 or 16) from
- * random entries of buf[n_entries * entry_bytes]; nectb_probe_reduce adds
- * fp32 values with one entry_bytes-wide reduction into random entries of
- * buf.  Both run about n_ops operations, exactly nectb_probe_ops(n_ops), in
- * one launch of 64 warps per SM on the stream; the caller times them.  A
- * buffer below the L2 size gives the L2 roof, a larger one the HBM
- * random-access roof.  sink: one device uint32 the gather probe may write. */
-int nectb_probe_gather(const void* buf, int64_t n_entries, int32_t entry_bytes, int64_t n_ops,
+ * reported against.  nectb_probe_gather loads entry_bytes (4, 8, 16, or 32 =
+ * one whole L2 sector) from entries of buf[n_entries * entry_bytes];
+ * nectb_probe_reduce (4, 8 or 16 bytes) adds fp32 values with one
+ * entry_bytes-wide reduction into entries of buf.  mode 0: every lane takes
+ * its own random entry (hashed corners); mode 1: the 32 lanes of a warp take
+ * 32 consecutive entries at a random 32-entry boundary (whole lines: the
+ * memory system's byte bandwidth).  Both run about n_ops accesses, exactly
+ * nectb_probe_ops(n_ops), in one launch of 64 warps per SM on the stream; the
+ * caller times them.  A buffer below the L2 size gives the L2 roof, a larger
+ * one the HBM random-access roof.  sink: one device uint32 the gather probe
+ * may write. */
+int nectb_probe_gather(const void* buf, int64_t n_entries, int32_t entry_bytes, int32_t mode, int64_t n_ops,
                        unsigned int* sink, void* stream);
-int nectb_probe_reduce(float* buf, int64_t n_entries, int32_t entry_bytes, int64_t n_ops, void* stream);
+int nectb_probe_reduce(float* buf, int64_t n_entries, int32_t entry_bytes, int32_t mode, int64_t n_ops,
+                       void* stream);
 int64_t nectb_probe_ops(int64_t n_ops);
 
 /* Version string and last error message of the calling thread. */

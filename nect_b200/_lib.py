@@ -20,6 +20,7 @@ LIB_PATH = Path(os.environ.get("NECTB_LIB", _PKG / "_lib" / "libnectb.so"))
 c_int = ctypes.c_int32
 c_i64 = ctypes.c_int64
 c_f32 = ctypes.c_float
+c_f64 = ctypes.c_double
 c_ptr = ctypes.c_void_p
 c_size = ctypes.c_size_t
 
@@ -156,6 +157,28 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
          ctypes.POINTER(NectbTrainBatch), c_ptr, c_ptr, c_ptr, c_ptr, c_size, c_ptr],
     ),
+    "nectb_train_scan_workspace_bytes": (
+        c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int,
+                 c_int]),
+    "nectb_train_scan_staging_bytes": (
+        c_size, [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int, c_int,
+                 c_int]),
+    "nectb_train_scan_step": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
+         ctypes.POINTER(NectbTrainBatch), c_ptr, c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr, c_size, c_ptr],
+    ),
+    "nectb_train_scan_forward": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
+         ctypes.POINTER(NectbTrainBatch), c_ptr, c_int, c_ptr, c_ptr, c_size, c_ptr],
+    ),
+    "nectb_train_scan_backward": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
+         ctypes.POINTER(NectbTrainBatch), c_ptr, c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_size, c_ptr],
+    ),
+    "nectb_train_scan_error_word": (c_ptr, [ctypes.POINTER(NectbGeometry), c_int, c_int, c_ptr]),
     "nectb_train_step_static": (
         c_int,
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr,
@@ -181,12 +204,12 @@ _SIGNATURES = {
     "nectb_set_tuning": (c_int, [ctypes.POINTER(NectbTuning)]),
     "nectb_profile_enable": (c_int, [c_int]),
     "nectb_profile_collect": (c_int, [c_ptr, c_ptr]),
-    "nectb_probe_gather": (c_int, [c_ptr, c_i64, c_int, c_i64, c_ptr, c_ptr]),
-    "nectb_probe_reduce": (c_int, [c_ptr, c_i64, c_int, c_i64, c_ptr]),
+    "nectb_probe_gather": (c_int, [c_ptr, c_i64, c_int, c_int, c_i64, c_ptr, c_ptr]),
+    "nectb_probe_reduce": (c_int, [c_ptr, c_i64, c_int, c_int, c_i64, c_ptr]),
     "nectb_probe_ops": (c_i64, [c_i64]),
     "nectb_adam_step": (
         c_int,
-        [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_f32, c_f32, c_f32, c_f32, c_int, c_ptr, c_int, c_ptr],
+        [c_ptr, c_ptr, c_ptr, c_ptr, c_i64, c_f64, c_f64, c_f64, c_f64, c_f64, c_int, c_ptr, c_int, c_ptr],
     ),
 }
 

@@ -25,21 +25,41 @@ inline int launch_status(const char* what) { return cuda_status(cudaGetLastError
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
-// The model shapes the fused kernels are instantiated for: 16 levels of F = 2
-// or 4 features over D = 3 or 4 inputs, H = 2 or 3 hidden layers of 64.
-// Calls fn(integral_constant D, F, H) for a supported shape and returns its
-// result, else kUnsupportedShape.
+// The model shapes the fused kernels are instantiated for, as (inputs D,
+// features per level F, levels L, hidden layers H of width 64): 16 levels of
+// 2 or 4 features over 3 or 4 inputs with 2 or 3 hidden layers (the
+// benchmark workloads and their neighbours), and the reference's default
+// static model, 19 levels of 4 features with 6 hidden layers
+// (nect/cfg/static/hash_grid.yaml:1-13).  Calls fn(integral_constant D, F, L,
+// H) for a supported shape and returns its result, else kUnsupportedShape.
 constexpr int kUnsupportedShape = -1000;
 template <typename Fn>
-inline int dispatch_shape(int D, int F, int H, Fn&& fn) {
+inline int dispatch_shape(int D, int F, int L, int H, Fn&& fn) {
   using std::integral_constant;
-#define NECTB_SHAPE(d, f, h) \
-  if (D == d && F == f && H == h) return fn(integral_constant<int, d>{}, integral_constant<int, f>{}, integral_constant<int, h>{});
-  NECTB_SHAPE(3, 2, 2) NECTB_SHAPE(3, 2, 3) NECTB_SHAPE(3, 4, 2) NECTB_SHAPE(3, 4, 3)
-  NECTB_SHAPE(4, 2, 2) NECTB_SHAPE(4, 2, 3) NECTB_SHAPE(4, 4, 2) NECTB_SHAPE(4, 4, 3)
+#define NECTB_SHAPE(d, f, l, h)                                                                                 \
+  if (D == d && F == f && L == l && H == h)                                                                   \
+    return fn(integral_constant<int, d>{}, integral_constant<int, f>{}, integral_constant<int, l>{},          \
+              integral_constant<int, h>{});
+  NECTB_SHAPE(3, 2, 16, 2) NECTB_SHAPE(3, 2, 16, 3) NECTB_SHAPE(3, 4, 16, 2) NECTB_SHAPE(3, 4, 16, 3)
+  NECTB_SHAPE(4, 2, 16, 2) NECTB_SHAPE(4, 2, 16, 3) NECTB_SHAPE(4, 4, 16, 2) NECTB_SHAPE(4, 4, 16, 3)
+  NECTB_SHAPE(3, 4, 19, 6)
 #undef NECTB_SHAPE
   return kUnsupportedShape;
 }
+
+// Input row of the MLP for L levels of F features: IN values, padded with
+// zeros to INP (a multiple of the MMA's K step of 16), held in KT tiles of 64
+// columns (NCH 16-byte chunks of 8 bf16).
+template <int L, int F>
+struct InShape {
+  static constexpr int IN = L * F;
+  static constexpr int INP = (IN + 15) / 16 * 16;
+  static constexpr int KT = (INP + 63) / 64;
+  static constexpr int NCH = INP / 8;
+  static_assert(KT <= 2, "at most 128 MLP inputs");
+};
+
+inline int input_padded(int n_input) { return (n_input + 15) / 16 * 16; }
 
 // The current launch shapes and scheduling (nectb_set_tuning), copied under a lock.
 NectbTuning current_tuning();

@@ -82,7 +82,7 @@ __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g,
   float* smem = reinterpret_cast<float*>(smem4);
   const SimtWeights sw = stage_weights<IN, H, false>(W, smem);
   float* xe = smem + simt_weight_floats<IN, H, false>() + threadIdx.x;
-  float* hid = xe + IN * LD;
+  float* hid = xe + IN * LD;  // two [64][LD] buffers, alternating between layers
   if (D == 4 && t_dev) t = *t_dev;   // the broadcast timestep, read on the device
   __syncthreads();
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -98,8 +98,9 @@ __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g,
       gemv_cols<IN, kWidth, LD>(sw.WT[0], xe, hid, act);
 #pragma unroll
       for (int k = 1; k < H - 1; ++k)
-        gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + (k - 1) * kWidth * LD, hid + k * kWidth * LD, act);
-      z = gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + (H - 2) * kWidth * LD, sw.wout, act);
+        gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + ((k - 1) & 1) * kWidth * LD, hid + (k & 1) * kWidth * LD,
+                                      act);
+      z = gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + ((H - 2) & 1) * kWidth * LD, sw.wout, act);
     }
     sigma[i] = act_fwd(z, out_act);
   }
@@ -111,13 +112,13 @@ int launch_encode(const GridDev& g, const void* params, const float* x, int64_t 
   return launch_status("encode_kernel");
 }
 
-template <int D, int F, typename T, int H>
+template <int D, int F, typename T, int L, int H>
 int launch_model(const GridDev& g, const void* params, const float* W, const float* x, int64_t n, float t,
                  const float* t_dev, int act, int out_act, float* sigma, cudaStream_t s) {
-  constexpr int IN = 16 * F;
+  constexpr int IN = L * F;
   auto k = model_forward_kernel<D, F, T, IN, H>;
-  const size_t smem =
-      (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (kModelThreads + 4)) * sizeof(float);
+  const size_t smem = (size_t)(simt_weight_floats<IN, H, false>() +
+                               (IN + simt_hidden_buffers<H>() * kWidth) * (kModelThreads + 4)) * sizeof(float);
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 148, per_sm = 1;
   cudaGetDevice(&dev);
@@ -145,20 +146,18 @@ int dispatch_encode(const GridDev& g, int dtype, const void* params, const float
   return set_error(NECTB_ERR_INVALID, "unsupported grid (n_dims %d, n_features %d)", g.n_dims, g.n_features);
 }
 
-// Instantiated for 16 levels of 2 or 4 features over 3 or 4 inputs with 2 or 3
-// hidden layers of 64 (dispatch_shape), fp32 or fp16 tables.
+// Instantiated for the shapes of dispatch_shape, fp32 or fp16 tables.
 int dispatch_model(const GridDev& g, int dtype, int H, const void* p, const float* W, const float* x, int64_t n,
                    float t, const float* t_dev, int act, int oact, float* sigma, cudaStream_t s) {
   const bool h = dtype == NECTB_F16;
-  if (g.n_levels != 16) return set_error(NECTB_ERR_INVALID, "fused model paths need n_levels == 16");
-  const int D = g.n_dims, F = g.n_features;
-  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
-    return h ? launch_model<d(), f(), __half, hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s)
-             : launch_model<d(), f(), float, hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s);
+  const int D = g.n_dims, F = g.n_features, L = g.n_levels;
+  const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto hl) {
+    return h ? launch_model<d(), f(), __half, l(), hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s)
+             : launch_model<d(), f(), float, l(), hl()>(g, p, W, x, n, t, t_dev, act, oact, sigma, s);
   });
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model forward: unsupported configuration (n_dims %d, n_features %d, "
-                   "hidden %d, %s table)", D, F, H, h ? "fp16" : "fp32");
+                   "n_levels %d, hidden %d, %s table)", D, F, L, H, h ? "fp16" : "fp32");
 }
 
 int64_t mlp_param_count(const NectbMLP* m) {
@@ -168,7 +167,8 @@ int64_t mlp_param_count(const NectbMLP* m) {
 int validate_mlp(const NectbMLP* m, const GridDev& g) {
   NECTB_REQUIRE(m != nullptr, "mlp is null");
   NECTB_REQUIRE(m->width == kWidth, "only width 64 is supported (got %d)", m->width);
-  NECTB_REQUIRE(m->n_hidden_layers >= 1 && m->n_hidden_layers <= 3, "n_hidden_layers must be 1..3");
+  NECTB_REQUIRE(m->n_hidden_layers >= 1 && m->n_hidden_layers <= kMaxHidden, "n_hidden_layers must be 1..%d",
+                kMaxHidden);
   NECTB_REQUIRE(m->n_input == g.n_levels * g.n_features, "n_input %d != n_levels*n_features %d", m->n_input,
                 g.n_levels * g.n_features);
   NECTB_REQUIRE(m->activation == NECTB_ACT_RELU || m->activation == NECTB_ACT_LEAKY_RELU ||

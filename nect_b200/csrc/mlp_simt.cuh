@@ -63,11 +63,15 @@ __device__ __forceinline__ float act_grad_a(float a, int kind) {
 }
 
 // out[o*LD] = act(sum_k M[k][o] * in[k*LD]) for o < N.  M is [K][N] row-major
-// in shared memory; in/out point at this thread's column of [.][LD] arrays.
+// (shared or global memory, rows 16-byte aligned); in/out point at this
+// thread's column of [.][LD] arrays.  When N is not a multiple of 32 the last
+// group of 32 outputs reads past the end of each row of M into the next row
+// (or the next array: M must be followed by at least 32 - N % 32 floats) and
+// stores only the outputs below N.
 template <int K, int N, int LD>
 __device__ __forceinline__ void gemv_cols(const float* __restrict__ M, const float* __restrict__ in,
                                           float* __restrict__ out, int act) {
-  static_assert(N % 32 == 0, "N must be a multiple of 32");
+  static_assert(N % 4 == 0, "rows of M must be 16-byte aligned");
   const int t = 0;
 #pragma unroll 1
   for (int og = 0; og < N; og += 32) {
@@ -88,7 +92,8 @@ __device__ __forceinline__ void gemv_cols(const float* __restrict__ M, const flo
       }
     }
 #pragma unroll
-    for (int o = 0; o < 32; ++o) out[(og + o) * LD + t] = act_fwd(acc[o], act);
+    for (int o = 0; o < 32; ++o)
+      if (N % 32 == 0 || og + o < N) out[(og + o) * LD + t] = act_fwd(acc[o], act);
   }
 }
 
@@ -164,12 +169,14 @@ __device__ __forceinline__ void warp_reduce_scatter64(const float* v, int lane, 
   j0 = ((lane >> 4) & 1) * 32 + ((lane >> 3) & 1) * 16 + ((lane >> 2) & 1) * 8 + ((lane >> 1) & 1) * 4 + (lane & 1) * 2;
 }
 
-// Weights in shared memory for the SIMT paths: for every layer k both the
-// transposed copy WT_k [in][64] (forward products) and the PyTorch layout
-// W_k [64][in] (backward products), then w_out [64].
+// Weights of the SIMT paths: for every layer k the transposed copy WT_k
+// [in][64] in shared memory (forward products) and the PyTorch layout W_k
+// [64][in] (backward products; in shared memory too when there is room,
+// else read from the global weight buffer through L1), then w_out [64].
+constexpr int kMaxHidden = 6;
 struct SimtWeights {
-  const float* WT[4];
-  const float* W[4];
+  const float* WT[kMaxHidden];
+  const float* W[kMaxHidden];
   const float* wout;
 };
 
@@ -179,9 +186,11 @@ __host__ __device__ constexpr int simt_weight_floats() {
 }
 
 // Copies the fp32 weight buffer (PyTorch layout, nect's W0, W1.., w_out) into
-// shared memory as SimtWeights; all threads of the block must call.
+// shared memory as SimtWeights; all threads of the block must call.  Without
+// kBoth the PyTorch-layout pointers address the global buffer.
 template <int IN, int H, bool kBoth>
 __device__ __forceinline__ SimtWeights stage_weights(const float* __restrict__ W, float* smem) {
+  static_assert(H >= 1 && H <= kMaxHidden, "hidden layers");
   SimtWeights sw;
   int off_g = 0, off_s = 0;
 #pragma unroll
@@ -195,15 +204,22 @@ __device__ __forceinline__ SimtWeights stage_weights(const float* __restrict__ W
       WT[(e % K) * kWidth + e / K] = v;
     }
     sw.WT[k] = WT;
-    sw.W[k] = Wd;
+    sw.W[k] = kBoth ? Wd : W + off_g;
     off_g += K * kWidth;
     off_s += (kBoth ? 2 : 1) * K * kWidth;
   }
   float* wo = smem + off_s;
   for (int e = threadIdx.x; e < kWidth; e += blockDim.x) wo[e] = W[off_g + e];
   sw.wout = wo;
-  for (int k = H; k < 4; ++k) sw.WT[k] = sw.W[k] = nullptr;
+  for (int k = H; k < kMaxHidden; ++k) sw.WT[k] = sw.W[k] = nullptr;
   return sw;
+}
+
+// Hidden activations of the SIMT forward kernels: two [64][LD] buffers that
+// consecutive layers alternate between.
+template <int H>
+__host__ __device__ constexpr int simt_hidden_buffers() {
+  return H - 1 < 2 ? H - 1 : 2;
 }
 
 }  // namespace nectb

@@ -12,8 +12,7 @@
 // detector pixels of a view.
 #include <algorithm>
 
-#include "mlp_simt.cuh"
-#include "tcgen05.cuh"
+#include "mixed_common.cuh"
 #include "train_common.cuh"
 
 namespace nectb {
@@ -75,17 +74,18 @@ __device__ __forceinline__ uint8_t* qalign1024(uint8_t* p) {
 // At most 128 registers so that three blocks share an SM under the 164 KB
 // shared split (a background block beside two slice blocks, or three blocks of
 // one query).
-template <int D, int F, int H>
+template <int D, int F, int L, int H>
 __global__ void __launch_bounds__(kQThreads, 4)
 query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W,
                    const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
-                   unsigned int* __restrict__ counter, int out_act) {
-  constexpr int IN = 16 * F;
+                   unsigned int* __restrict__ counter, int act, int out_act) {
+  using S = InShape<L, F>;
+  constexpr int KT = S::KT;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = qalign1024(smem_raw);
-  uint8_t* sW = base;                // H weight tiles
-  uint8_t* sX = sW + H * kQWTile;
-  uint8_t* sA = sX + kQTile;         // every hidden layer's activations in turn
+  uint8_t* sW = base;                   // KT + H - 1 weight tiles
+  uint8_t* sX = sW + (KT + H - 1) * kQWTile;
+  uint8_t* sA = sX + KT * kQTile;       // every hidden layer's activations in turn
   float* sWout = reinterpret_cast<float*>(sA + kQTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
@@ -94,25 +94,7 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
 
   const int t = threadIdx.x, warp = t >> 5;
   // fp32 weights -> bf16 swizzled tiles (same layout as the training kernels)
-  for (int e = t; e < 64 * (IN / 8); e += kQThreads) {
-    const int o = e / (IN / 8), j = e % (IN / 8);
-    float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
-    tc::st_chunk_bf16(sW, o, j, v);
-  }
-#pragma unroll 1
-  for (int k = 1; k < H; ++k) {
-    const float* Wk = W + 64 * IN + (k - 1) * 64 * 64;
-    for (int e = t; e < 64 * 8; e += kQThreads) {
-      const int o = e / 8, j = e % 8;
-      float v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = Wk[o * 64 + 8 * j + q];
-      tc::st_chunk_bf16(sW + k * kQWTile, o, j, v);
-    }
-  }
-  for (int e = t; e < 64; e += kQThreads) sWout[e] = W[64 * IN + (H - 1) * 64 * 64 + e];
+  stage_mixed_weights<L, F, H>(W, sW, sWout);
   if (warp == 0) {
     tc::tmem_alloc(tslot, 128);
     tc::tmem_relinquish();
@@ -138,36 +120,7 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
     const long long chunk = *s_chunk;
     if (chunk >= total_chunks) break;
     const QPoint q = query_point(items[*s_item], chunk, t);
-    // the encoder's row writer (fp16 gathers, bf16 row)
-    {
-      constexpr int LPC = 8 / F;
-#pragma unroll 1
-      for (int j = 0; j < 16 / LPC; ++j) {
-        float v[8];
-        if (q.valid) {
-#pragma unroll
-          for (int qq = 0; qq < LPC; ++qq) {
-            const int l = j * LPC + qq;
-            LevelCorners<D> lc;
-            level_corners<D>(grid, l, q.p, lc);
-            float vals[1 << D][F];
-#pragma unroll
-            for (int c = 0; c < (1 << D); ++c) Feat<F, __half>::load(table, grid.offset[l] + lc.idx[c], vals[c]);
-#pragma unroll
-            for (int f = 0; f < F; ++f) {
-              float acc = 0.f;
-#pragma unroll
-              for (int c = 0; c < (1 << D); ++c) acc = fmaf(lc.w[c], vals[c][f], acc);
-              v[qq * F + f] = acc;
-            }
-          }
-        } else {
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq) v[qq] = 0.f;
-        }
-        tc::st_chunk_bf16(sX, t, j, v);
-      }
-    }
+    encode_row<D, F, L>(grid, table, q.p, q.valid, sX, t);   // the encoder's row writer (fp16 gathers, bf16 row)
     // layer k writes TMEM columns 64 * (k & 1); its input is X for k = 0, else
     // the previous layer's activations in sA (written once the MMA that read
     // sA before has completed)
@@ -175,13 +128,8 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
 #pragma unroll
     for (int k = 0; k < H; ++k) {
       if (k > 0) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          float v[8];
-#pragma unroll
-          for (int qq = 0; qq < 8; ++qq) v[qq] = fmaxf(h[8 * j + qq], 0.f);
-          tc::st_chunk_bf16(sA, t, j, v);
-        }
+        uint32_t mlo, mhi;
+        act_row(h, sA, t, act, mlo, mhi);
       }
       tc::fence_async_smem();
       tc::fence_before();
@@ -190,11 +138,14 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
         tc::fence_after();
         if (k == 0) {
 #pragma unroll
-          for (int c = 0; c < IN / 16; ++c) tc::mma(tm, tc::desc_k(sX_a, c), tc::desc_k(sW_a, c), idesc, c > 0);
+          for (int c = 0; c < S::INP / 16; ++c)
+            tc::mma(tm, tc::desc_k(sX_a + (c / 4) * kQTile, c % 4), tc::desc_k(sW_a + (c / 4) * kQWTile, c % 4),
+                    idesc, c > 0);
         } else {
 #pragma unroll
           for (int c = 0; c < 4; ++c)
-            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, c), tc::desc_k(sW_a + k * kQWTile, c), idesc, c > 0);
+            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, c), tc::desc_k(sW_a + (KT + k - 1) * kQWTile, c), idesc,
+                    c > 0);
         }
         tc::commit(bar);
       }
@@ -212,7 +163,7 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
     if (timed_out) break;
     float z = 0.f;
 #pragma unroll
-    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], hidden_act(h[j], act), z);
     if (q.valid) *q.dst = fmaf(act_fwd(z, out_act), q.scale, q.offset);
     tc::fence_before();
     __syncthreads();
@@ -229,18 +180,18 @@ query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* 
   }
 }
 
-template <int D, int F, typename T, int H>
+template <int D, int F, typename T, int L, int H>
 __global__ void __launch_bounds__(kQThreads)
 query_plain_kernel(GridDev grid, const T* __restrict__ table, const float* __restrict__ W,
                    const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
                    unsigned int* __restrict__ counter, int act, int out_act) {
-  constexpr int IN = 16 * F;
+  constexpr int IN = L * F;
   constexpr int LD = kQThreads + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
   const SimtWeights sw = stage_weights<IN, H, false>(W, smem);
   float* xe = smem + simt_weight_floats<IN, H, false>() + threadIdx.x;
-  float* hid = xe + IN * LD;
+  float* hid = xe + IN * LD;  // two [64][LD] buffers, alternating between layers
   __shared__ long long s_chunk;
   __shared__ int s_item;
   const int t = threadIdx.x;
@@ -264,8 +215,9 @@ query_plain_kernel(GridDev grid, const T* __restrict__ table, const float* __res
         gemv_cols<IN, kWidth, LD>(sw.WT[0], xe, hid, act);
 #pragma unroll
         for (int k = 1; k < H - 1; ++k)
-          gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + (k - 1) * kWidth * LD, hid + k * kWidth * LD, act);
-        z = gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + (H - 2) * kWidth * LD, sw.wout, act);
+          gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + ((k - 1) & 1) * kWidth * LD, hid + (k & 1) * kWidth * LD,
+                                        act);
+        z = gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + ((H - 2) & 1) * kWidth * LD, sw.wout, act);
       }
       *q.dst = fmaf(act_fwd(z, out_act), q.scale, q.offset);
     }
@@ -280,25 +232,27 @@ int sm_count() {
   return sms;
 }
 
-template <int D, int F, int H>
+template <int D, int F, int L, int H>
 int launch_query_mixed(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
-                       int64_t chunks, unsigned int* counter, int oact, int max_blocks, cudaStream_t s) {
-  auto k = query_mixed_kernel<D, F, H>;
-  const size_t smem = 1024 + H * kQWTile + 2 * kQTile + 64 * 4 + 64;
+                       int64_t chunks, unsigned int* counter, int act, int oact, int max_blocks, cudaStream_t s) {
+  using S = InShape<L, F>;
+  auto k = query_mixed_kernel<D, F, L, H>;
+  const size_t smem = 1024 + (S::KT + H - 1) * kQWTile + (S::KT + 1) * kQTile + 64 * 4 + 64;
   set_smem(k, smem, true);
   int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 3 * sm_count()));
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   ProfScope ps(kProfModel, s);
-  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);
+  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, act, oact);
   return launch_status("query_mixed_kernel");
 }
 
-template <int D, int F, typename T, int H>
+template <int D, int F, typename T, int L, int H>
 int launch_query_plain(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
                        int64_t chunks, unsigned int* counter, int act, int oact, int max_blocks, cudaStream_t s) {
-  constexpr int IN = 16 * F;
-  auto k = query_plain_kernel<D, F, T, H>;
-  const size_t smem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (kQThreads + 4)) * 4;
+  constexpr int IN = L * F;
+  auto k = query_plain_kernel<D, F, T, L, H>;
+  const size_t smem =
+      (size_t)(simt_weight_floats<IN, H, false>() + (IN + simt_hidden_buffers<H>() * kWidth) * (kQThreads + 4)) * 4;
   set_smem(k, smem, true);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kQThreads, smem);
@@ -321,36 +275,35 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
   if (int rc = validate_mlp(mlp, g)) return rc;
-  NECTB_REQUIRE(g.n_levels == 16, "queries need n_levels == 16");
   if (n_items == 0 || total_chunks == 0) return NECTB_OK;
   NECTB_REQUIRE(grid_params && mlp_params && items && counter && n_items > 0 && total_chunks > 0,
                 "null pointer or empty query");
   NECTB_REQUIRE(total_chunks < (int64_t(1) << 31), "too many chunks in one launch");
   cudaStream_t s = (cudaStream_t)stream;
   if (int rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s), "memset query counter")) return rc;
-  const int D = g.n_dims, F = g.n_features, H = mlp->n_hidden_layers;
+  const int D = g.n_dims, F = g.n_features, L = g.n_levels, H = mlp->n_hidden_layers;
+  const int act = mlp->activation, oact = mlp->output_activation;
   const bool mixed = mlp->compute_dtype != NECTB_F32;
   if (mixed) {
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
-    NECTB_REQUIRE(mlp->activation == NECTB_ACT_RELU, "mixed queries need ReLU hidden layers");
-    const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
-      return launch_query_mixed<d(), f(), h()>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                               mlp->output_activation, max_blocks, s);
+    NECTB_REQUIRE(H >= 2, "mixed queries need at least 2 hidden layers");
+    const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
+      return launch_query_mixed<d(), f(), l(), h()>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
+                                                    act, oact, max_blocks, s);
     });
     if (rc != kUnsupportedShape) return rc;
   } else {
-    const int act = mlp->activation, oact = mlp->output_activation;
     const bool h = grid->feature_dtype == NECTB_F16;
-    const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
-      return h ? launch_query_plain<d(), f(), __half, hl()>(g, grid_params, mlp_params, items, n_items,
-                                                            total_chunks, counter, act, oact, max_blocks, s)
-               : launch_query_plain<d(), f(), float, hl()>(g, grid_params, mlp_params, items, n_items, total_chunks,
-                                                           counter, act, oact, max_blocks, s);
+    const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto hl) {
+      return h ? launch_query_plain<d(), f(), __half, l(), hl()>(g, grid_params, mlp_params, items, n_items,
+                                                                 total_chunks, counter, act, oact, max_blocks, s)
+               : launch_query_plain<d(), f(), float, l(), hl()>(g, grid_params, mlp_params, items, n_items,
+                                                                total_chunks, counter, act, oact, max_blocks, s);
     });
     if (rc != kUnsupportedShape) return rc;
   }
-  return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, hidden %d)", D,
-                   F, H);
+  return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, n_levels %d, "
+                   "hidden %d)", D, F, L, H);
 }
 
 extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,

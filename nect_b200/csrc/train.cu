@@ -22,21 +22,26 @@ int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void*
 
 namespace {
 
-// torch.optim.Adam (no amsgrad, not maximize), one element per thread.
+// torch.optim.Adam (no amsgrad, not maximize), one element per thread, in
+// torch's order of operations: g += wd * p; m = lerp(m, g, 1 - b1);
+// v = v * b2 + (1 - b2) * g * g; p += -(lr / bc1) * m / (sqrt(v) / sqrt(bc2) + eps).
+// The host computes 1 - b1, 1 - b2, lr / bc1 and sqrt(bc2) in double, as torch
+// does before casting its scalars to fp32.
 __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float* __restrict__ m,
-                            float* __restrict__ v, int64_t n, float lr, float b1, float b2, float eps, float wd,
-                            float bc1, float bc2_sqrt, __half* __restrict__ p_half, int zero_grad) {
+                            float* __restrict__ v, int64_t n, float w1, float b2, float w2, float eps, float wd,
+                            float neg_step, float bc2_sqrt, __half* __restrict__ p_half, int zero_grad) {
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += stride) {
     float grad = g[i];
     float param = p[i];
-    if (wd != 0.f) grad = fmaf(wd, param, grad);
-    const float mi = fmaf(b1, m[i] - grad, grad);           // m = b1*m + (1-b1)*g  (lerp form)
-    const float vi = fmaf(b2, v[i], (1.f - b2) * grad * grad);
+    if (wd != 0.f) grad = grad + wd * param;
+    const float m0 = m[i];
+    const float mi = m0 + w1 * (grad - m0);
+    const float vi = v[i] * b2 + w2 * grad * grad;
     m[i] = mi;
     v[i] = vi;
     const float denom = sqrtf(vi) / bc2_sqrt + eps;
-    param = param - (lr / bc1) * (mi / denom);
+    param = param + neg_step * (mi / denom);
     p[i] = param;
     if (p_half) p_half[i] = __float2half_rn(param);
     if (zero_grad) g[i] = 0.f;
@@ -94,33 +99,77 @@ __global__ void train_rays_kernel(const RayRec* __restrict__ recs, int R, int S,
   }
 }
 
-// dL/dsigma of every sample of ray r is dL/dy_pred[r] * scale[r] (y_pred is the
-// scaled sum of the ray's sigmas, base_trainer.py:552-554).
-__global__ void set_ray_grad_kernel(RayRec* __restrict__ recs, const float* __restrict__ dloss_dy, int R) {
+// dL/dsigma of every sample of ray v is dL/dy_pred[r] * scale[v] / sub (y_pred
+// is the scaled sum of the ray's sigmas, base_trainer.py:552-554; a
+// continuous-scan step averages it over the sub angles of pixel r = v mod
+// n_batch, continous_scanning_trainer.py:126-137).
+__global__ void set_ray_grad_kernel(RayRec* __restrict__ recs, const float* __restrict__ dloss_dy, int R, int n_batch,
+                                    int sub) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v < R) recs[v].gsig = dloss_dy[v % n_batch] * recs[v].scale / (float)sub;
+}
+
+// Continuous scan, after the forward kernels wrote each virtual ray's
+// integral: y_pred[r] = sum_j part[j * n + r] / sub in the reference's
+// order (continous_scanning_trainer.py:126-137), the loss (mean over the n
+// pixels) and, with grads, dL/dsigma of every virtual ray.
+__global__ void scan_finalize_kernel(RayRec* __restrict__ recs, const float* __restrict__ part, int n, int sub,
+                                     float* __restrict__ y_pred, float* __restrict__ loss, int loss_type,
+                                     float loss_scale, int grads) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r < R) recs[r].gsig = dloss_dy[r] * recs[r].scale;
+  float term = 0.f;
+  if (r < n) {
+    float y = 0.f;
+    for (int j = 0; j < sub; ++j) y += part[(int64_t)j * n + r] / (float)sub;
+    y_pred[r] = y;
+    const float meas = recs[r].y;
+    term = loss_term(y, meas, loss_type) / (float)n;
+    if (grads) {
+      const float g = loss_grad(y, meas, loss_type, n, 1.f) * loss_scale;
+      for (int j = 0; j < sub; ++j) {
+        RayRec& rec = recs[(int64_t)j * n + r];
+        rec.gsig = g * rec.scale / (float)sub;
+      }
+    }
+  }
+  if (loss) {
+    term = warp_sum(term);
+    if ((threadIdx.x & 31) == 0) atomicAdd(loss, term);
+  }
+}
+
+// Bytes of a continuous-scan workspace: the prepared virtual rays and pixel
+// slots, then the per-virtual-ray integrals; staging follows.
+size_t scan_workspace_bytes(int R, int P, int sub) {
+  return align256(workspace_bytes(R * sub, P * sub)) + align256((size_t)R * sub * 4);
 }
 
 // The whole step (phase forward | backward, built-in loss), its forward half
 // (y_pred only; the workspace keeps the prepared rays) or its backward half
 // (dL/dy_pred given by the caller, the workspace of the matching forward).
+// sub > 1: a continuous-scan step over sub_angles (host array of sub angles);
+// the batch's jitter and detector offsets hold sub * num_rays entries,
+// sub-angle-major.
 int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
                 const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
                 const float* dloss_dy, float* grid_grad, float* mlp_grad, float* y_pred, float* loss,
-                void* workspace, size_t workspace_size, void* stream, int phase) {
+                void* workspace, size_t workspace_size, void* stream, int phase, const float* sub_angles = nullptr,
+                int sub = 1) {
   clear_error();
   if (int rc = validate_geometry(geometry)) return rc;
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
   if (int rc = validate_mlp(mlp, g)) return rc;
   NECTB_REQUIRE(batch != nullptr, "batch is null");
-  NECTB_REQUIRE(g.n_levels == 16, "fused training needs n_levels == 16 (got %d)", g.n_levels);
   NECTB_REQUIRE(batch->num_rays >= 0 && batch->num_points_per_ray >= 1, "bad batch sizes");
   NECTB_REQUIRE(batch->loss_type == 1 || batch->loss_type == 2, "loss_type must be 1 (L1) or 2 (L2)");
   NECTB_REQUIRE(batch->max_distance_traveled > 0.f, "max_distance_traveled must be positive");
   NECTB_REQUIRE(grid_params && mlp_params, "null parameters");
   NECTB_REQUIRE(!(phase & kPhaseBackward) || (grid_grad && mlp_grad), "null gradient buffers");
   NECTB_REQUIRE(phase != (kPhaseForward | kPhaseBackward) || loss, "null loss");
+  NECTB_REQUIRE(sub >= 1 && sub <= kMaxSubAngles, "sub_angles must be 1..%d (got %d)", kMaxSubAngles, sub);
+  NECTB_REQUIRE(sub == 1 || sub_angles, "null sub-angle array");
+  NECTB_REQUIRE((int64_t)batch->num_rays * sub <= INT32_MAX, "num_rays * sub_angles exceeds 2^31 - 1");
   cudaStream_t s = (cudaStream_t)stream;
   if (loss)
     if (int rc = cuda_status(cudaMemsetAsync(loss, 0, sizeof(float), s), "memset loss")) return rc;
@@ -132,15 +181,17 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
   NECTB_REQUIRE(batch->random_ray_index && batch->jitter && batch->detector_offset && batch->projection,
                 "null batch input");
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
-  if (!workspace || workspace_size < workspace_bytes(batch->num_rays, P))
-    return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
-                     workspace_bytes(batch->num_rays, P));
+  NECTB_REQUIRE((int64_t)P * sub <= INT32_MAX, "detector pixels * sub_angles exceeds 2^31 - 1");
+  const int n_batch = batch->num_rays;
+  const size_t need = sub > 1 ? scan_workspace_bytes(n_batch, P, sub) : workspace_bytes(n_batch, P);
+  if (!workspace || workspace_size < need)
+    return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size, need);
   TrainArgs a;
-  a.n_pixels = P;
+  a.n_pixels = P * sub;
   a.perm = batch->random_ray_index;
   a.perm_len = batch->random_ray_index_len;
   a.start = batch->starting_ray_index;
-  a.num_rays = batch->num_rays;
+  a.num_rays = n_batch * sub;
   a.S = batch->num_points_per_ray;
   a.angle = batch->angle_rad;
   a.t = batch->t;
@@ -154,35 +205,116 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
   a.loss_scale = batch->loss_scale;
   a.max_blocks = 0;
   a.phase = phase;
-  Workspace ws = carve_workspace(workspace, a.num_rays, P, workspace_size);
+  a.sub = sub;
+  for (int j = 0; j < sub; ++j) a.sub_angle[j] = sub_angles ? sub_angles[j] : batch->angle_rad;
+  Workspace ws = carve_workspace(workspace, a.num_rays, a.n_pixels, workspace_size);
+  float* part = nullptr;  // continuous scan: each virtual ray's integral
+  if (sub > 1) {
+    part = reinterpret_cast<float*>(static_cast<char*>(workspace) + align256(workspace_bytes(a.num_rays, a.n_pixels)));
+    const size_t pb = align256((size_t)a.num_rays * 4);
+    if (ws.stage && ws.stage_bytes > pb) {
+      ws.stage = reinterpret_cast<float*>(reinterpret_cast<char*>(ws.stage) + pb);
+      ws.stage_bytes -= pb;
+    } else {
+      ws.stage = nullptr;
+      ws.stage_bytes = 0;
+    }
+  }
   // the forward half has no loss output of its own: its loss sum lands in the workspace
-  if (!loss) loss = reinterpret_cast<float*>(ws.counters + 8);
+  float* scratch_loss = reinterpret_cast<float*>(ws.counters + 8);
+  float* fwd_loss = (sub > 1 || !loss) ? scratch_loss : loss;
+  float* fwd_y = sub > 1 ? part : y_pred;
   if (phase & kPhaseForward) {
     if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
-    if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
+    if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)a.n_pixels * 4, s), "memset slots")) return rc;
     ProfScope ps(kProfRayPrep, s);
     ray_prep_kernel<<<(unsigned)ceil_div(a.num_rays, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters,
-                                                                       y_pred, loss);
+                                                                       fwd_y, fwd_loss);
   } else {
     // backward half: fresh backward cursor, the caller's loss gradient per ray
     if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor"))
       return rc;
-    set_ray_grad_kernel<<<(unsigned)ceil_div(a.num_rays, 256), 256, 0, s>>>(ws.rays, dloss_dy, a.num_rays);
+    set_ray_grad_kernel<<<(unsigned)ceil_div(a.num_rays, 256), 256, 0, s>>>(ws.rays, dloss_dy, a.num_rays, n_batch,
+                                                                            sub);
   }
   if (int rc = launch_status(phase & kPhaseForward ? "ray_prep_kernel" : "set_ray_grad_kernel")) return rc;
   const int nW = (int)mlp_param_count(mlp);
-  float* tg = (phase & kPhaseBackward) ? grid_grad : nullptr;
-  float* mg = (phase & kPhaseBackward) ? mlp_grad : nullptr;
-  if (mlp->compute_dtype == NECTB_F32) {
-    NECTB_REQUIRE(grid->feature_dtype == NECTB_F32, "plain path needs an fp32 table");
-    return train_plain(*geometry, g, *mlp, (const float*)grid_params, mlp_params, nW, a, ws, tg, mg, y_pred, loss,
-                       s);
+  const bool plain = mlp->compute_dtype == NECTB_F32;
+  NECTB_REQUIRE(!plain || grid->feature_dtype == NECTB_F32, "plain path needs an fp32 table");
+  auto run = [&](int ph, float* yp, float* ls) -> int {
+    TrainArgs b = a;
+    b.phase = ph;
+    float* tg = (ph & kPhaseBackward) ? grid_grad : nullptr;
+    float* mg = (ph & kPhaseBackward) ? mlp_grad : nullptr;
+    if (plain) return train_plain(*geometry, g, *mlp, (const float*)grid_params, mlp_params, nW, b, ws, tg, mg, yp, ls, s);
+    return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, b, ws, tg, mg, yp, ls, s);
+  };
+  if (sub == 1) return run(phase, y_pred, fwd_loss);
+  // continuous scan: the forward kernels integrate every virtual ray, the
+  // sub-angle average and the loss follow, then the backward
+  if (phase & kPhaseForward) {
+    if (int rc = run(kPhaseForward, part, scratch_loss)) return rc;
+    scan_finalize_kernel<<<(unsigned)ceil_div(n_batch, 256), 256, 0, s>>>(
+        ws.rays, part, n_batch, sub, y_pred, phase & kPhaseBackward ? loss : nullptr, a.loss_type, a.loss_scale,
+        (phase & kPhaseBackward) ? 1 : 0);
+    if (int rc = launch_status("scan_finalize_kernel")) return rc;
   }
-  return train_mixed(*geometry, g, *mlp, grid_params, mlp_params, nW, a, ws, tg, mg, y_pred, loss, s);
+  if (phase & kPhaseBackward) return run(kPhaseBackward, nullptr, nullptr);
+  return NECTB_OK;
 }
 
 }  // namespace
 }  // namespace nectb
+
+extern "C" size_t nectb_train_scan_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                                   const NectbMLP* mlp, int32_t num_rays, int32_t sub_angles) {
+  (void)grid;
+  (void)mlp;
+  const int P = geometry ? geometry->nDetector[0] * geometry->nDetector[1] : 0;
+  return nectb::scan_workspace_bytes(std::max(num_rays, 1), std::max(P, 0), std::max(sub_angles, 1));
+}
+
+extern "C" int nectb_train_scan_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                     const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                                     const float* sub_angles_rad, int32_t sub_angles, float* grid_grad,
+                                     float* mlp_grad, float* y_pred, float* loss, void* workspace,
+                                     size_t workspace_size, void* stream) {
+  return nectb::train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, nullptr, grid_grad, mlp_grad, y_pred,
+                            loss, workspace, workspace_size, stream, nectb::kPhaseForward | nectb::kPhaseBackward,
+                            sub_angles_rad, sub_angles);
+}
+
+extern "C" int nectb_train_scan_forward(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                        const void* grid_params, const float* mlp_params,
+                                        const NectbTrainBatch* batch, const float* sub_angles_rad, int32_t sub_angles,
+                                        float* y_pred, void* workspace, size_t workspace_size, void* stream) {
+  return nectb::train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, nullptr, nullptr, nullptr, y_pred,
+                            nullptr, workspace, workspace_size, stream, nectb::kPhaseForward, sub_angles_rad,
+                            sub_angles);
+}
+
+extern "C" int nectb_train_scan_backward(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                         const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
+                                         const NectbTrainBatch* batch, const float* sub_angles_rad,
+                                         int32_t sub_angles, const float* dloss_dy, float* grid_grad, float* mlp_grad,
+                                         void* workspace, size_t workspace_size, void* stream) {
+  return nectb::train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, dloss_dy, grid_grad, mlp_grad,
+                            nullptr, nullptr, workspace, workspace_size, stream, nectb::kPhaseBackward,
+                            sub_angles_rad, sub_angles);
+}
+
+extern "C" const unsigned int* nectb_train_scan_error_word(const NectbGeometry* geometry, int32_t num_rays,
+                                                           int32_t sub_angles, const void* workspace) {
+  using namespace nectb;
+  clear_error();
+  if (!geometry || !workspace || num_rays <= 0 || sub_angles < 1 || sub_angles > kMaxSubAngles ||
+      validate_geometry(geometry) != NECTB_OK) {
+    set_error(NECTB_ERR_INVALID, "nectb_train_scan_error_word: invalid arguments");
+    return nullptr;
+  }
+  const int P = geometry->nDetector[0] * geometry->nDetector[1];
+  return carve_workspace(const_cast<void*>(workspace), num_rays * sub_angles, P * sub_angles).counters + 2;
+}
 
 extern "C" int nectb_train_step(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
                                 const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
@@ -223,26 +355,44 @@ extern "C" int nectb_train_rays(const NectbGeometry* geometry, int32_t num_rays,
   return launch_status("train_rays_kernel");
 }
 
-extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
-                                            const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray) {
-  using namespace nectb;
-  if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0) return 0;
-  if (mlp->compute_dtype == NECTB_F32) return 0;  // the plain path scatters in its backward
-  const int P = geometry->nDetector[0] * geometry->nDetector[1];
-  const size_t per_ray = (size_t)num_points_per_ray * grid->n_levels * grid->n_features * sizeof(float);
-  // order and offsets, the staged rounds, and an encoding store for every
-  // sample slot of the batch (bf16 rows of n_levels x n_features), capped
+namespace nectb {
+namespace {
+// Recommended staging of the mixed path's two-pass backward for R (virtual)
+// rays over P (virtual) pixels: ray order and offsets, the staged rounds, the
+// encoding store (when enabled) and a 4D grid's time slice.
+size_t staging_bytes(const NectbHashGrid* grid, int R, int P, int S) {
+  const size_t per_ray = (size_t)S * grid->n_levels * grid->n_features * sizeof(float);
   const NectbTuning tune = current_tuning();
-  const size_t row_bytes = (size_t)grid->n_levels * grid->n_features * 2;
-  const size_t rows = tune.encoding_store ? std::min<size_t>({(size_t)num_rays * num_points_per_ray,
-                                                             kEncodingStoreCap / row_bytes, (size_t)0xffffffffu})
+  const size_t row_bytes = (size_t)input_padded(grid->n_levels * grid->n_features) * 2;  // bf16 MLP input row
+  const size_t rows = tune.encoding_store ? std::min<size_t>({(size_t)R * S, kEncodingStoreCap / row_bytes,
+                                                             (size_t)0xffffffffu})
                                           : 0;
-  size_t bytes = order_bytes(num_rays, P) + staged_round_bytes(num_rays, tune.staged_rounds, per_ray) + 256 +
+  size_t bytes = order_bytes(R, P) + staged_round_bytes(R, tune.staged_rounds, per_ray) + 256 +
                  align256(rows * row_bytes);
   GridDev g;
   if (tune.time_slice && grid->n_dims == 4 && make_grid_dev(grid, &g))
     bytes += slice_bytes(g) + 256;  // the time slice and its gradient
   return bytes;
+}
+}  // namespace
+}  // namespace nectb
+
+extern "C" size_t nectb_train_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                            const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray) {
+  using namespace nectb;
+  if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0) return 0;
+  if (mlp->compute_dtype == NECTB_F32) return 0;  // the plain path scatters in its backward
+  return staging_bytes(grid, num_rays, geometry->nDetector[0] * geometry->nDetector[1], num_points_per_ray);
+}
+
+extern "C" size_t nectb_train_scan_staging_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                                 const NectbMLP* mlp, int32_t num_rays, int32_t num_points_per_ray,
+                                                 int32_t sub_angles) {
+  using namespace nectb;
+  if (!geometry || !grid || !mlp || num_rays <= 0 || num_points_per_ray <= 0 || sub_angles < 1) return 0;
+  if (mlp->compute_dtype == NECTB_F32) return 0;
+  return staging_bytes(grid, num_rays * sub_angles, geometry->nDetector[0] * geometry->nDetector[1] * sub_angles,
+                       num_points_per_ray);
 }
 
 namespace {
@@ -253,7 +403,6 @@ int model_backward_entry(const NectbHashGrid* grid, const NectbMLP* mlp, const v
   GridDev g;
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
   if (int rc = validate_mlp(mlp, g)) return rc;
-  NECTB_REQUIRE(g.n_levels == 16, "model backward needs n_levels == 16 (got %d)", g.n_levels);
   NECTB_REQUIRE(n >= 0, "n must be >= 0");
   if (n == 0) return NECTB_OK;
   NECTB_REQUIRE(grid_params && mlp_params && x && dsigma && grid_grad && mlp_grad, "null pointer argument");
@@ -278,21 +427,21 @@ extern "C" int nectb_model_backward_t(const NectbHashGrid* grid, const NectbMLP*
                               stream);
 }
 
-extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, float lr,
-                               float beta1, float beta2, float eps, float weight_decay, int32_t step,
+extern "C" int nectb_adam_step(float* param, float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, double lr,
+                               double beta1, double beta2, double eps, double weight_decay, int32_t step,
                                void* param_half, int32_t zero_grad, void* stream) {
   clear_error();
   if (n == 0) return NECTB_OK;
   NECTB_REQUIRE(param && grad && exp_avg && exp_avg_sq && n > 0 && step >= 1, "bad Adam arguments");
-  const double bc1 = 1.0 - std::pow((double)beta1, step);
-  const double bc2 = 1.0 - std::pow((double)beta2, step);
+  const double bc1 = 1.0 - std::pow(beta1, step);
+  const double bc2 = 1.0 - std::pow(beta2, step);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int blocks = (int)std::min<int64_t>(ceil_div(n, 256), (int64_t)sms * 8);
   ProfScope ps(kProfAdam, (cudaStream_t)stream);
-  adam_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, lr, beta1, beta2, eps,
-                                                        weight_decay, (float)bc1, (float)std::sqrt(bc2),
-                                                        (__half*)param_half, zero_grad);
+  adam_kernel<<<blocks, 256, 0, (cudaStream_t)stream>>>(
+      param, grad, exp_avg, exp_avg_sq, n, (float)(1.0 - beta1), (float)beta2, (float)(1.0 - beta2), (float)eps,
+      (float)weight_decay, (float)(-lr / bc1), (float)std::sqrt(bc2), (__half*)param_half, zero_grad);
   return launch_status("adam_kernel");
 }

@@ -26,6 +26,9 @@ static_assert(sizeof(RayRec) == 64, "RayRec must be 64 bytes");
 
 enum { kPhaseForward = 1, kPhaseBackward = 2 };
 
+// Continuous-scan steps: at most this many sub-angles per batch.
+constexpr int kMaxSubAngles = 32;
+
 struct TrainArgs {
   const int64_t* perm;
   int64_t perm_len;
@@ -46,6 +49,12 @@ struct TrainArgs {
   int max_blocks;  // > 0: cap on the persistent grids (queries); 0: default
   int phase = kPhaseForward | kPhaseBackward;  // which half of the step to run
   float run_threshold = 0.75f;                 // run merging of the scatter (set from the tuning)
+  // Continuous scan (sub > 1): num_rays = sub * (pixels of the batch) virtual
+  // rays, sub-angle-major (ray v = j * pixels + r is pixel r at sub_angle[j],
+  // with jitter[v] and det_off[2v..2v+1]); n_pixels = sub * detector pixels,
+  // slot index = pixel * sub + j.
+  int sub = 1;
+  float sub_angle[kMaxSubAngles];
 };
 
 enum : unsigned int { kFlagDuplicatePixels = 1u };

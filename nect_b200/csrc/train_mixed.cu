@@ -5,24 +5,27 @@
 // Block = 4 warps = one warpgroup; a tile is 128 samples (each warp 32
 // consecutive samples of its current ray), i.e. the M = 128 rows of every
 // MMA and the 128 TMEM lanes (warp w reads lanes 32w..32w+31 with
-// tcgen05.ld.32x32b, so each thread owns its sample's row).  Per tile:
-//   forward:  X[128xIN] -> A1 = relu(X W0^T) -> A2 = relu(A1 W1^T) -> sigma
-//   backward: G2 = dsigma * w_out * 1[A2>0]
-//             dA1 = G2 W1            dW1 += G2^T A1   (TMEM accumulator)
-//             G1 = dA1 * 1[A1>0]
-//             dX = G1 W0             dW0 += G1^T X    (TMEM accumulator)
-//             table_grad[corner] += w_corner * dX   (fp32 vector atomics)
+// tcgen05.ld.32x32b, so each thread owns its sample's row).  Per tile, with
+// H hidden layers and hidden activation a():
+//   forward:  X[128xIN] -> A1 = a(X W0^T) -> ... -> A_H = a(A_{H-1} W_{H-1}^T) -> sigma
+//   backward: G_H = dsigma * w_out * a'(A_H)
+//             dA_k = G_{k+1} W_k      dW_k += G_{k+1}^T A_k  (TMEM accumulator), k = H-1..1
+//             G_k = dA_k * a'(A_k)
+//             dX = G_1 W0             dW0 += G_1^T X          (TMEM accumulator)
+//             table_grad[corner] += w_corner * dX   (fp32 vector reductions)
 // Operands are 128-byte-swizzled bf16 tiles in shared memory; the same tile
 // is the K-major A operand of the next layer and the MN-major operand of the
 // weight-gradient product, so no transposed copies are made.  The weight
 // gradients use M = 128 with the 64 real rows first (rows 64..127 read a
-// second, unused tile and are never stored).  One thread issues the MMAs and
-// commits them to an mbarrier; every wait is bounded and reports through an
-// error word instead of hanging.
+// second, unused tile and are never stored).  Inputs wider than 64 (the
+// reference's default 19 x 4 levels) take two X tiles: layer 0 runs K over
+// both, dX is an N = 128 product and the layer-0 weight gradient is taken
+// transposed, dW0^T += X^T G_1, with the two X tiles as the M = 128 operand.
+// One thread issues the MMAs and commits them to an mbarrier; every wait is
+// bounded and reports through an error word instead of hanging.
 #include <algorithm>
 
-#include "mlp_simt.cuh"
-#include "tcgen05.cuh"
+#include "mixed_common.cuh"
 #include "train_common.cuh"
 
 namespace nectb {
@@ -31,102 +34,6 @@ namespace {
 
 constexpr int kMixThreads = 128;
 constexpr int kScatterThreads = 256;
-constexpr uint32_t kTile = 128 * 128;  // bytes of a [128][64 bf16] tile
-constexpr uint32_t kWTile = 64 * 128;  // bytes of a [64][64 bf16] tile
-
-__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
-  return reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(p) + 1023) & ~uintptr_t(1023));
-}
-
-// fp32 weights (PyTorch layout) -> bf16 swizzled tiles: W0 rows o (IN used
-// columns), W1..W_{H-1} rows o (64 columns) in consecutive 8 KB tiles after
-// W0; w_out stays fp32.
-template <int IN, int H>
-__device__ __forceinline__ void stage_mixed_weights(const float* __restrict__ W, uint8_t* sW, float* sWout) {
-  for (int e = threadIdx.x; e < 64 * (IN / 8); e += blockDim.x) {
-    const int o = e / (IN / 8), j = e % (IN / 8);
-    float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = W[o * IN + 8 * j + q];
-    tc::st_chunk_bf16(sW, o, j, v);
-  }
-#pragma unroll 1
-  for (int k = 1; k < H; ++k) {
-    const float* Wk = W + 64 * IN + (k - 1) * 64 * 64;
-    for (int e = threadIdx.x; e < 64 * 8; e += blockDim.x) {
-      const int o = e / 8, j = e % 8;
-      float v[8];
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = Wk[o * 64 + 8 * j + q];
-      tc::st_chunk_bf16(sW + k * kWTile, o, j, v);
-    }
-  }
-  for (int e = threadIdx.x; e < 64; e += blockDim.x) sWout[e] = W[64 * IN + (H - 1) * 64 * 64 + e];
-}
-
-// ReLU of 64 accumulator values into row r of a bf16 tile; bit j of m = (x_j > 0).
-__device__ __forceinline__ void relu_row(const float* h, uint8_t* tile, int r, uint32_t& mlo, uint32_t& mhi) {
-  mlo = 0;
-  mhi = 0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    float v[8];
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-      const float x = h[8 * j + q];
-      v[q] = fmaxf(x, 0.f);
-      const uint32_t bit = x > 0.f ? 1u : 0u;
-      if (8 * j + q < 32) mlo |= bit << (8 * j + q); else mhi |= bit << (8 * j + q - 32);
-    }
-    tc::st_chunk_bf16(tile, r, j, v);
-  }
-}
-
-// Encodes one sample into row r of the swizzled X tile (bf16), 8 features
-// (one 16-byte chunk) at a time; invalid samples write zeros.  With xdst the
-// row is also written there (evict-first: the store streams past the L2 that
-// holds the tables).
-template <int D, int F>
-__device__ __forceinline__ void encode_row(const GridDev& g, const __half* __restrict__ table, const float* p,
-                                           bool valid, uint8_t* sX, int r, uint4* __restrict__ xdst = nullptr) {
-  constexpr int LPC = 8 / F;  // levels per 16-byte chunk
-#pragma unroll 1
-  for (int j = 0; j < 16 / LPC; ++j) {
-    float v[8];
-    if (valid) {
-#pragma unroll
-      for (int q = 0; q < LPC; ++q) {
-        const int l = j * LPC + q;
-        LevelCorners<D> lc;
-        level_corners<D>(g, l, p, lc);
-        float vals[1 << D][F];
-#pragma unroll
-        for (int c = 0; c < (1 << D); ++c) Feat<F, __half>::load(table, g.offset[l] + lc.idx[c], vals[c]);
-#pragma unroll
-        for (int f = 0; f < F; ++f) {
-          float acc = 0.f;
-#pragma unroll
-          for (int c = 0; c < (1 << D); ++c) acc = fmaf(lc.w[c], vals[c][f], acc);
-          v[q * F + f] = acc;
-        }
-      }
-    } else {
-#pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = 0.f;
-    }
-    const uint4 packed = tc::pack_bf16x8(v);
-    tc::st_chunk_raw(sX, r, j, packed);
-    if (xdst) __stcs(xdst + j, packed);
-  }
-}
-
-// Loads 64 fp32 TMEM columns [col, col+64) of this thread's lane.
-__device__ __forceinline__ void ld64(uint32_t taddr, float* v) {
-#pragma unroll
-  for (int c = 0; c < 4; ++c) tc::tmem_ld16(taddr + 16 * c, v + 16 * c);
-  tc::tmem_wait_ld();
-}
-
 // Per-warp ray cursor shared by the mixed kernels.
 struct RayCursor {
   int ray = -1;
@@ -197,35 +104,37 @@ __device__ __forceinline__ bool wg_or(int wg, bool p) {
   return r != 0;
 }
 
-template <int D, int F, int H>
+template <int D, int F, int L, int H>
 __global__ void __launch_bounds__(kFwdBlocksPerSM * kMixThreads, 1)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int out_act, float* __restrict__ y_pred, float* __restrict__ loss, const int32_t* __restrict__ order,
-                 const uint64_t* __restrict__ offs, uint4* __restrict__ xstore, uint32_t xcap) {
-  constexpr int IN = 16 * F;
+                 int act, int out_act, float* __restrict__ y_pred, float* __restrict__ loss,
+                 const int32_t* __restrict__ order, const uint64_t* __restrict__ offs, uint4* __restrict__ xstore,
+                 uint32_t xcap) {
+  using S = InShape<L, F>;
+  constexpr int KT = S::KT;
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
   unsigned int* err = ctrl + 2;
   const int n_wg = blockDim.x / kMixThreads;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
-  uint8_t* sW = base;  // H weight tiles, shared by the warpgroups
-  float* sWout = reinterpret_cast<float*>(sW + H * kWTile + n_wg * kTile);
+  uint8_t* sW = base;  // KT + H - 1 weight tiles, shared by the warpgroups
+  float* sWout = reinterpret_cast<float*>(sW + (KT + H - 1) * kWTile + n_wg * KT * kTile);
   uint64_t* bars = reinterpret_cast<uint64_t*>(sWout + 64);       // [n_wg]
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kFwdBlocksPerSM);
   float* red = reinterpret_cast<float*>(tslot + 4);                 // [warps]
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int wg = t / kMixThreads, r = t % kMixThreads;  // warpgroup, and this thread's row of its tile
-  // Each hidden layer's activations overwrite X: the MMA that read the tile has
-  // finished (its commit has arrived) before the next activations are written,
-  // and the next X is written only after the last MMA has completed.
-  uint8_t* sX = sW + H * kWTile + wg * kTile;
+  // Each hidden layer's activations overwrite X (tile 0): the MMA that read the
+  // tile has finished (its commit has arrived) before the next activations are
+  // written, and the next X is written only after the last MMA has completed.
+  uint8_t* sX = sW + (KT + H - 1) * kWTile + wg * KT * kTile;
   uint8_t* sA = sX;
   uint64_t* bar = bars + wg;
   if (xstore && blockIdx.x == 0 && t == 0) ctrl[7] = xcap;  // rows this forward fills, for the backward
-  stage_mixed_weights<IN, H>(W, sW, sWout);
+  stage_mixed_weights<L, F, H>(W, sW, sWout);
   const uint32_t ncols = n_wg == 1 ? 128u : (n_wg == 2 ? 256u : 512u);
   if (warp == 0) {
     tc::tmem_alloc(tslot, ncols);
@@ -255,8 +164,8 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     bool valid = false;
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
-    encode_row<D, F>(grid, table, p, valid, sX, r,
-                     valid && cur.xrow >= 0 ? xstore + (size_t)(cur.xrow + i) * (IN / 8) : nullptr);
+    encode_row<D, F, L>(grid, table, p, valid, sX, r,
+                        valid && cur.xrow >= 0 ? xstore + (size_t)(cur.xrow + i) * S::NCH : nullptr);
     float h[64];
     // layer k (0-based) writes TMEM columns 64 * (k & 1) of the warpgroup's
     // quarter; its input is X for k = 0, else the previous layer's
@@ -265,7 +174,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     for (int k = 0; k < H; ++k) {
       if (k > 0) {
         uint32_t mlo, mhi;
-        relu_row(h, sA, r, mlo, mhi);
+        act_row(h, sA, r, act, mlo, mhi);
       }
       tc::fence_async_smem();
       tc::fence_before();
@@ -274,11 +183,14 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         tc::fence_after();
         if (k == 0) {
 #pragma unroll
-          for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sX_a, q), tc::desc_k(sW_a, q), idesc, q > 0);
+          for (int q = 0; q < S::INP / 16; ++q)
+            tc::mma(tm, tc::desc_k(sX_a + (q / 4) * kTile, q % 4), tc::desc_k(sW_a + (q / 4) * kWTile, q % 4),
+                    idesc, q > 0);
         } else {
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, q), tc::desc_k(sW_a + k * kWTile, q), idesc, q > 0);
+            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, q), tc::desc_k(sW_a + (KT + k - 1) * kWTile, q), idesc,
+                    q > 0);
         }
         tc::commit(bar);
       }
@@ -294,7 +206,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (timed_out) break;
     float z = 0.f;
 #pragma unroll
-    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], hidden_act(h[j], act), z);
     if (valid) {  // Kahan-compensated accumulation along the ray
       const float y = act_fwd(z, out_act) - kcomp;
       const float s = ksum + y;
@@ -336,15 +248,32 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 // is written to the staging buffer, level-major: stage[(l * slots + s) * F + f]
 // with s = (scheduling index - lo) * S + sample, for the rays whose
 // scheduling index lies in [lo, hi); scatter_stage_kernel applies it.
-template <int D, int F, int H, bool kStaged>
+//
+// TMEM (BW columns): [0, T) the transient result of every layer and gradient
+// product (T = 64, or 128 for the N = 128 dX of two X tiles), dW_k at
+// T + 64 (k - 1) for k = 1..H-1, dW0 at T + 64 (H - 1): IN columns, or for
+// two X tiles the transposed dW0^T, 64 columns in lanes 0..IN-1.
+template <int L, int F, int H>
+struct BwdPlan {
+  using S = InShape<L, F>;
+  static constexpr int T = S::KT == 2 ? 128 : 64;
+  static constexpr int kUsed = T + 64 * H;
+  static constexpr uint32_t kCols = kUsed <= 256 ? 256u : 512u;
+  static_assert(kUsed <= 512, "TMEM plan exceeds 512 columns");
+  static constexpr size_t smem = 1024 + (S::KT + H - 1) * kWTile + (H + S::KT) * kTile + 64 * 4 + 64 + 4 * 64 * 4;
+};
+
+template <int D, int F, int L, int H, bool kStaged>
 __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
+                 int act, int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
                  float* __restrict__ stage, int64_t slots, const int32_t* __restrict__ order,
                  const uint64_t* __restrict__ offs, const uint4* __restrict__ xstore, uint32_t xcap) {
-  constexpr int IN = 16 * F;
-  static_assert(IN <= 64 && H >= 2 && H <= 3, "TMEM plan: 64 transient + (H - 1) x 64 + IN columns <= 256");
+  using S = InShape<L, F>;
+  using Plan = BwdPlan<L, F, H>;
+  constexpr int IN = S::IN, KT = S::KT;
+  static_assert(H >= 2, "at least two hidden layers");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
   // rows below both this launch's store size and the forward's are valid
@@ -353,22 +282,22 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
   // Tiles: sG (G_H), then A_{H-1} ... A_1 (each later replaced by G_k), then
-  // X.  Order matters: the padded (M = 128) weight-gradient products read a
-  // second 16 KB block right after their G tile, which is always the next
-  // tile of this list, inside this block's allocation.
-  uint8_t* sW = base;  // H weight tiles
-  uint8_t* sG = sW + H * kWTile;
+  // the KT X tiles.  Order matters: the padded (M = 128) weight-gradient
+  // products read a second 16 KB block right after their G tile, which is
+  // always the next tile of this list, inside this block's allocation.
+  uint8_t* sW = base;  // KT + H - 1 weight tiles
+  uint8_t* sG = sW + (KT + H - 1) * kWTile;
   uint8_t* sX = sG + H * kTile;
-  float* sWout = reinterpret_cast<float*>(sX + kTile);
+  float* sWout = reinterpret_cast<float*>(sX + KT * kTile);
   uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
   float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
   auto sAk = [&](int k) { return sG + (H - k) * kTile; };   // A_k (k = 1..H-1), later G_k
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  stage_mixed_weights<IN, H>(W, sW, sWout);
+  stage_mixed_weights<L, F, H>(W, sW, sWout);
   if (warp == 0) {
-    tc::tmem_alloc(tslot, 256);
+    tc::tmem_alloc(tslot, Plan::kCols);
     tc::tmem_relinquish();
   }
   if (t == 0) tc::mbar_init(bar, 1);
@@ -378,16 +307,15 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   tc::fence_after();
   const uint32_t tm = *tslot;
   const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
-  // TMEM columns: [0,64) every layer's and every gradient product's transient
-  // result, [192 - 64k, 256 - 64k) dW_k for k = 1..H-1, [192, 192 + IN) dW0.
   const uint32_t sX_a = tc::smem_u32(sX), sG_a = tc::smem_u32(sG), sW_a = tc::smem_u32(sW);
+  const uint32_t dw0 = tm + Plan::T + 64 * (H - 1);
   // M = 128 weight-gradient products: rows 64..127 of A come from the tile kTile further on.
   const uint32_t pad_lbo = kTile;
   constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
   constexpr uint32_t id_dA = tc::idesc_bf16(128, 64, false, true);
   constexpr uint32_t id_dW = tc::idesc_bf16(128, 64, true, true);
-  constexpr uint32_t id_dX = tc::idesc_bf16(128, IN, false, true);
-  constexpr uint32_t id_dW0 = tc::idesc_bf16(128, IN, true, true);
+  constexpr uint32_t id_dX = tc::idesc_bf16(128, KT == 2 ? 128 : S::INP, false, true);
+  constexpr uint32_t id_dW0 = tc::idesc_bf16(128, S::INP, true, true);
 
   uint32_t phase = 0;
   uint32_t wacc = 0;  // weight-gradient accumulators start at the first tile
@@ -395,7 +323,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   int j0_out = 0;
   RayCursor cur;
   bool timed_out = false;
-  uint4 xrow[IN / 8];    // stored rows of the current chunk (this thread's sample)
+  uint4 xrow[S::NCH];    // stored rows of the current chunk (this thread's sample)
   bool pre_ok = false;   // xrow already holds them (prefetched during the previous tile)
   // Issues the MMAs of one phase (thread 0), waits for them; false on time-out.
   auto run_phase = [&](auto issue) -> bool {
@@ -423,41 +351,44 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (active && i < cur.rec.count) valid = sample_point(cur.rec, i, p);
     if (D == 4) p[3] = a.t;
     if (cur.xrow >= 0) {  // the forward stored this ray's rows: stream them back (warp-uniform branch)
-      const uint4* src = xstore + (size_t)(cur.xrow + i) * (IN / 8);
+      const uint4* src = xstore + (size_t)(cur.xrow + i) * S::NCH;
       if (!pre_ok && valid) {  // not prefetched: the first chunk of a ray
 #pragma unroll
-        for (int j = 0; j < IN / 8; ++j) xrow[j] = __ldcs(src + j);
+        for (int j = 0; j < S::NCH; ++j) xrow[j] = __ldcs(src + j);
       }
 #pragma unroll
-      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sX, t, j, valid ? xrow[j] : make_uint4(0u, 0u, 0u, 0u));
+      for (int j = 0; j < S::NCH; ++j)
+        tc::st_chunk_raw(sX + (j / 8) * kTile, t, j % 8, valid ? xrow[j] : make_uint4(0u, 0u, 0u, 0u));
       // prefetch the rows of the warp's next chunk of this ray; they arrive
       // while this tile's MMAs run (rows below the ray's count lie in its
       // stored range)
       pre_ok = cur.base + 32 < cur.rec.count;
       if (pre_ok && i + 32 < cur.rec.count) {
 #pragma unroll
-        for (int j = 0; j < IN / 8; ++j) xrow[j] = __ldcs(src + 32 * (IN / 8) + j);
+        for (int j = 0; j < S::NCH; ++j) xrow[j] = __ldcs(src + 32 * S::NCH + j);
       }
     } else {
       pre_ok = false;
-      encode_row<D, F>(grid, table, p, valid, sX, t);
+      encode_row<D, F, L>(grid, table, p, valid, sX, t);
     }
-    // forward recompute: layer 0 from X, layer k from A_k (stored with its ReLU mask)
+    // forward recompute: layer 0 from X, layer k from A_k (stored with its sign mask)
     float h[64];
     uint32_t mlo[H], mhi[H];
     bool ok = run_phase([&] {
 #pragma unroll
-      for (int q = 0; q < IN / 16; ++q) tc::mma(tm, tc::desc_k(sX_a, q), tc::desc_k(sW_a, q), id_fwd, q > 0);
+      for (int q = 0; q < S::INP / 16; ++q)
+        tc::mma(tm, tc::desc_k(sX_a + (q / 4) * kTile, q % 4), tc::desc_k(sW_a + (q / 4) * kWTile, q % 4), id_fwd,
+                q > 0);
     });
     if (ok) ld64(my_lanes, h);
 #pragma unroll
     for (int k = 1; k < H && ok; ++k) {
-      relu_row(h, sAk(k), t, mlo[k], mhi[k]);
+      act_row(h, sAk(k), t, act, mlo[k], mhi[k]);
       const uint32_t a_k = tc::smem_u32(sAk(k));
       ok = run_phase([&] {
 #pragma unroll
         for (int q = 0; q < 4; ++q)
-          tc::mma(tm, tc::desc_k(a_k, q), tc::desc_k(sW_a + k * kWTile, q), id_fwd, q > 0);
+          tc::mma(tm, tc::desc_k(a_k, q), tc::desc_k(sW_a + (KT + k - 1) * kWTile, q), id_fwd, q > 0);
       });
       if (ok) ld64(my_lanes, h);
     }
@@ -467,13 +398,13 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     }
     float z = 0.f;
 #pragma unroll
-    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], fmaxf(h[j], 0.f), z);
+    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], hidden_act(h[j], act), z);
     const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
-    // w_out gradient over the warp's samples; G_H = dz * w_out * 1[a_H > 0]
+    // w_out gradient over the warp's samples; G_H = dz * w_out * a'(h_H)
     {
       float v[64];
 #pragma unroll
-      for (int j = 0; j < 64; ++j) v[j] = dz * fmaxf(h[j], 0.f);
+      for (int j = 0; j < 64; ++j) v[j] = dz * hidden_act(h[j], act);
       float s0, s1;
       warp_reduce_scatter64(v, lane, s0, s1, j0_out);
       dwout0 += s0;
@@ -483,19 +414,19 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     for (int j = 0; j < 8; ++j) {
       float v[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = h[8 * j + q] > 0.f ? dz * sWout[8 * j + q] : 0.f;
+      for (int q = 0; q < 8; ++q) v[q] = dz * sWout[8 * j + q] * hidden_slope(h[8 * j + q] > 0.f, act);
       tc::st_chunk_bf16(sG, t, j, v);
     }
     // backward through the hidden layers: G_{k+1} (tile gt) gives
     //   dA_k = G_{k+1} W_k        (A = G K-major, B = W_k MN-major) -> transient columns
     //   dW_k += G_{k+1}^T A_k     (A = G MN-major, M = 128 padded; B = A_k MN-major; K = 128 samples)
-    // and G_k = dA_k * 1[a_k > 0] replaces A_k once the dW_k product has completed.
+    // and G_k = dA_k * a'(a_k) replaces A_k once the dW_k product has completed.
     uint32_t gt = sG_a;
 #pragma unroll
     for (int k = H - 1; k >= 1 && ok; --k) {
       const uint32_t a_k = tc::smem_u32(sAk(k));
-      const uint32_t wk = sW_a + k * kWTile;
-      const uint32_t dwk = tm + 192 - 64 * k;
+      const uint32_t wk = sW_a + (KT + k - 1) * kWTile;
+      const uint32_t dwk = tm + Plan::T + 64 * (k - 1);
       ok = run_phase([&] {
 #pragma unroll
         for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(gt, q), tc::desc_mn(wk, q, kWTile), id_dA, q > 0);
@@ -512,35 +443,44 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         for (int q = 0; q < 8; ++q) {
           const int c = 8 * j + q;
           const uint32_t bit = c < 32 ? (mlo[k] >> c) & 1u : (mhi[k] >> (c - 32)) & 1u;
-          v[q] = bit ? h[c] : 0.f;
+          v[q] = h[c] * hidden_slope(bit != 0, act);
         }
         tc::st_chunk_bf16(sAk(k), t, j, v);
       }
       gt = a_k;
     }
-    // dX = G_1 W0 (A = G_1 K-major, B = W0 MN-major, N = IN); dW0 += G_1^T X
+    // dX = G_1 W0 (A = G_1 K-major, B = W0 MN-major over the KT tiles); the
+    // layer-0 weight gradient: dW0 += G_1^T X (one X tile), or
+    // dW0^T += X^T G_1 (two X tiles as the M = 128 operand, B = G_1 MN-major)
     if (ok)
       ok = run_phase([&] {
 #pragma unroll
         for (int q = 0; q < 4; ++q) tc::mma(tm, tc::desc_k(gt, q), tc::desc_mn(sW_a, q, kWTile), id_dX, q > 0);
+        if constexpr (KT == 1) {
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-          tc::mma(tm + 192, tc::desc_mn(gt, q, pad_lbo), tc::desc_mn(sX_a, q, kTile), id_dW0, (q > 0) | wacc);
+          for (int q = 0; q < 8; ++q)
+            tc::mma(dw0, tc::desc_mn(gt, q, pad_lbo), tc::desc_mn(sX_a, q, kTile), id_dW0, (q > 0) | wacc);
+        } else {
+#pragma unroll
+          for (int q = 0; q < 8; ++q)
+            tc::mma(dw0, tc::desc_mn(sX_a, q, kTile), tc::desc_mn(gt, q, kTile), id_dW, (q > 0) | wacc);
+        }
       });
     if (!ok) {
       timed_out = true;
       break;
     }
     wacc = 1;
-    float dx[IN];
+    constexpr int NX = (IN + 15) / 16;  // 16-column chunks holding the IN values of dX
+    float dx[NX * 16];
 #pragma unroll
-    for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 16 * c, dx + 16 * c);
+    for (int c = 0; c < NX; ++c) tc::tmem_ld16(my_lanes + 16 * c, dx + 16 * c);
     tc::tmem_wait_ld();
     if constexpr (kStaged) {
       if (valid) {
         float* dst = stage + ((int64_t)(cur.sched - lo) * a.S + i) * F;
 #pragma unroll
-        for (int l = 0; l < 16; ++l) {
+        for (int l = 0; l < L; ++l) {
           // evict-first: each staged value is read once, by the scatter pass
           if constexpr (F == 2)
             __stcs(reinterpret_cast<float2*>(dst + l * slots * F), make_float2(dx[2 * l], dx[2 * l + 1]));
@@ -571,17 +511,29 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 #pragma unroll 1
       for (int k = 1; k < H; ++k) {
         float v[64];
-        ld64(my_lanes + 192 - 64 * k, v);
+        ld64(my_lanes + Plan::T + 64 * (k - 1), v);
         float* dst = W_grad + 64 * IN + (k - 1) * 64 * 64 + o * 64;
 #pragma unroll
         for (int i2 = 0; i2 < 64; ++i2) atomicAdd(dst + i2, v[i2]);
       }
-      float w0[IN];
+    }
+    if constexpr (KT == 1) {
+      if (warp < 2) {
+        const int o = t;
+        float w0[S::INP];
 #pragma unroll
-      for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 192 + 16 * c, w0 + 16 * c);
-      tc::tmem_wait_ld();
+        for (int c = 0; c < S::INP / 16; ++c) tc::tmem_ld16(dw0 + ((uint32_t)(32 * warp) << 16) + 16 * c, w0 + 16 * c);
+        tc::tmem_wait_ld();
 #pragma unroll
-      for (int i2 = 0; i2 < IN; ++i2) atomicAdd(W_grad + o * IN + i2, w0[i2]);
+        for (int i2 = 0; i2 < IN; ++i2) atomicAdd(W_grad + o * IN + i2, w0[i2]);
+      }
+    } else if (32 * warp < IN) {  // dW0^T: lane i holds input i's 64 output columns
+      float v[64];
+      ld64(dw0 + ((uint32_t)(32 * warp) << 16), v);
+      if (t < IN) {
+#pragma unroll 8
+        for (int o = 0; o < 64; ++o) atomicAdd(W_grad + o * IN + t, v[o]);
+      }
     }
   }
   {
@@ -599,7 +551,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     atomicAdd(W_grad + 64 * IN + (H - 1) * 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
   if (warp == 0) {
     tc::fence_after();
-    tc::tmem_dealloc(tm, 256);
+    tc::tmem_dealloc(tm, Plan::kCols);
   }
 }
 
@@ -620,9 +572,9 @@ template <int D, int F>
 __global__ void __launch_bounds__(kMixThreads, 3)
 bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                 const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage, int64_t slots,
-                const int32_t* __restrict__ order, const uint64_t* __restrict__ offs, const uint4* __restrict__ xstore,
-                uint32_t xcap) {
+                int act, int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage,
+                int64_t slots, const int32_t* __restrict__ order, const uint64_t* __restrict__ offs,
+                const uint4* __restrict__ xstore, uint32_t xcap) {
   constexpr int IN = 16 * F;
   constexpr int H = 2;
   static_assert(IN <= 64, "dW0 shares the 64 weight-gradient columns");
@@ -644,7 +596,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
 
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  stage_mixed_weights<IN, H>(W, sW, sWout);
+  stage_mixed_weights<16, F, H>(W, sW, sWout);
   {
     uint4* z = reinterpret_cast<uint4*>(sZ);
     for (int e = t; e < (int)(kZero / 16); e += kMixThreads) z[e] = make_uint4(0u, 0u, 0u, 0u);
@@ -713,7 +665,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       }
     } else {
       pre_ok = false;
-      encode_row<D, F>(grid, table, p, valid, sX, t);
+      encode_row<D, F, 16>(grid, table, p, valid, sX, t);
     }
     // layer 0: h1 = X W0^T
     bool ok = run_phase([&] {
@@ -733,8 +685,8 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       float v[8], u[8];
 #pragma unroll
       for (int q = 0; q < 8; ++q) {
-        v[q] = fmaxf(h[q], 0.f);
-        u[q] = fmaxf(h[8 + q], 0.f);
+        v[q] = hidden_act(h[q], act);
+        u[q] = hidden_act(h[8 + q], act);
       }
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
@@ -761,7 +713,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       tc::tmem_ld16(my_lanes + 16 * c, h);
       tc::tmem_wait_ld();
 #pragma unroll
-      for (int q = 0; q < 16; ++q) z = fmaf(sWout[16 * c + q], fmaxf(h[q], 0.f), z);
+      for (int q = 0; q < 16; ++q) z = fmaf(sWout[16 * c + q], hidden_act(h[q], act), z);
     }
     const float dz = valid ? cur.rec.gsig * act_grad_z(z, out_act) : 0.f;
     // second pass over h2: the w_out gradient and G2 = dz * w_out * 1[h2 > 0]
@@ -773,8 +725,8 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       float v[16], g[16];
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
-        v[q] = dz * fmaxf(h[q], 0.f);
-        g[q] = h[q] > 0.f ? dz * sWout[16 * c + q] : 0.f;
+        v[q] = dz * hidden_act(h[q], act);
+        g[q] = dz * sWout[16 * c + q] * hidden_slope(h[q] > 0.f, act);
       }
       tc::st_chunk_bf16(sG, t, 2 * c, g);
       tc::st_chunk_bf16(sG, t, 2 * c + 1, g + 8);
@@ -809,7 +761,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       for (int q = 0; q < 16; ++q) {
         const int col = 16 * c + q;
         const uint32_t bit = col < 32 ? (m1lo >> col) & 1u : (m1hi >> (col - 32)) & 1u;
-        h[q] = bit ? h[q] : 0.f;
+        h[q] = h[q] * hidden_slope(bit != 0, act);
       }
       tc::st_chunk_bf16(sA, t, 2 * c, h);
       tc::st_chunk_bf16(sA, t, 2 * c + 1, h + 8);
@@ -969,10 +921,10 @@ __global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, fl
 
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
 // slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
-template <int D, int F, int H>
+template <int D, int F, int L, int H>
 int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W,
-              const TrainArgs& args, Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred,
-              float* loss, cudaStream_t s) {
+              const TrainArgs& args, Workspace ws, int act, int out_act, float* table_grad, float* W_grad,
+              float* y_pred, float* loss, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -1004,8 +956,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
       if (bwd)
         if (int rc = cuda_status(cudaMemsetAsync(g3, 0, (size_t)n3 * F * sizeof(float), s), "memset slice gradient"))
           return rc;
-      if (int rc = run_mixed<3, F, H>(geo, ts.g3, t3, W, args, ws3, out_act, bwd ? g3 : nullptr, W_grad, y_pred,
-                                      loss, s))
+      if (int rc = run_mixed<3, F, L, H>(geo, ts.g3, t3, W, args, ws3, act, out_act, bwd ? g3 : nullptr, W_grad,
+                                         y_pred, loss, s))
         return rc;
       if (bwd) {
         {
@@ -1028,61 +980,66 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
                     ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
                                                 (int)ceil_div(a.num_rays, 4)))
                     : std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * wgs)));
-  int blocks = std::max(1, std::min<int>(std::min(tune.backward_blocks_per_sm, 2) * sms, (int)ceil_div(a.num_rays, 4)));
+  // the general backward: two blocks per SM of 256 TMEM columns, one of 512
+  const int bwd_per_sm = BwdPlan<L, F, H>::kCols == 512u ? 1 : std::min(tune.backward_blocks_per_sm, 2);
+  int blocks = std::max(1, std::min<int>(bwd_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if (a.max_blocks > 0) {
     fblocks = std::min(fblocks, a.max_blocks);
     blocks = std::min(blocks, a.max_blocks);
   }
-  constexpr int IN = 16 * F;
+  using Shape = InShape<L, F>;
+  constexpr int IN = Shape::IN, KT = Shape::KT;
   const int R = a.num_rays;
-  // staging region: ray order and sample offsets, the encoding store, then
-  // dL/d(encoding) of one round of per_round rays
-  const StageLayout L = stage_layout(ws, R, a.n_pixels, a.S, IN * sizeof(__nv_bfloat16),
-                                     (size_t)a.S * IN * sizeof(float), tune.staged_rounds, tune.encoding_store != 0);
+  // staging region: ray order and sample offsets, the encoding store (bf16
+  // input rows with their zero padding), then dL/d(encoding) of one round of
+  // per_round rays
+  const StageLayout SL = stage_layout(ws, R, a.n_pixels, a.S, Shape::INP * sizeof(__nv_bfloat16),
+                                      (size_t)a.S * IN * sizeof(float), tune.staged_rounds, tune.encoding_store != 0);
   auto run_order = [&]() -> int {
     ProfScope ps(kProfOrder, s);
     const int n_blocks = order_blocks(R, a.n_pixels);
-    order_count_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, L.block_sums,
-                                                        L.block_samples);
-    order_scan_kernel<<<1, kOrderBlock, 0, s>>>(L.block_sums, L.block_samples, n_blocks, ws.counters);
-    order_compact_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, L.block_sums,
-                                                          L.block_samples, L.order, L.offs);
+    order_count_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, SL.block_sums,
+                                                        SL.block_samples);
+    order_scan_kernel<<<1, kOrderBlock, 0, s>>>(SL.block_sums, SL.block_samples, n_blocks, ws.counters);
+    order_compact_kernel<<<n_blocks, kOrderBlock, 0, s>>>(ws.slot, ws.rays, ws.counters, R, a.n_pixels, SL.block_sums,
+                                                          SL.block_samples, SL.order, SL.offs);
     return launch_status("order kernels");
   };
   if (a.phase & kPhaseForward) {
     // with an encoding store the forward runs the rays in rank order and keeps their rows
-    if (L.xstore)
+    if (SL.xstore)
       if (int rc = run_order()) return rc;
-    auto k = fwd_mixed_kernel<D, F, H>;
-    const size_t smem = 1024 + H * kWTile + wgs * kTile + 64 * 4 + kFwdBlocksPerSM * 8 + 16 + 4 * kFwdBlocksPerSM * 4;
+    auto k = fwd_mixed_kernel<D, F, L, H>;
+    const size_t smem = 1024 + (KT + H - 1) * kWTile + wgs * KT * kTile + 64 * 4 + kFwdBlocksPerSM * 8 + 16 +
+                        4 * kFwdBlocksPerSM * 4;
     set_smem(k, smem, a.max_blocks > 0);
     {
       ProfScope ps(kProfForward, s);
-      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
-                                           L.xstore ? L.order : nullptr, L.offs, L.xstore, L.xcap);
+      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred,
+                                           loss, SL.xstore ? SL.order : nullptr, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   }
   if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
-  // at least 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM
-  const size_t bsmem =
-      std::max<size_t>(1024 + H * kWTile + (H + 1) * kTile + 64 * 4 + 64 + 4 * 64 * 4, 80 * 1024);
-  if (L.per_round <= 0) {
+  // at least 80 KB keeps at most two blocks (2 x 256 TMEM columns) per SM;
+  // the 512-column plans take more than half of the shared memory
+  const size_t bsmem = std::max<size_t>(BwdPlan<L, F, H>::smem, 80 * 1024);
+  if (SL.per_round <= 0) {
     // fused single pass: the backward scatters its own gradients
-    auto k = bwd_mixed_kernel<D, F, H, false>;
+    auto k = bwd_mixed_kernel<D, F, L, H, false>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
-    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, table_grad,
                                          W_grad, 0, 0x7fffffff, nullptr, 0, nullptr, nullptr, nullptr, 0u);
     return launch_status("bwd_mixed_kernel");
   }
   // the order is a function of the prepared rays alone: computed again unless
   // this call's forward just did
-  if (!((a.phase & kPhaseForward) && L.xstore))
+  if (!((a.phase & kPhaseForward) && SL.xstore))
     if (int rc = run_order()) return rc;
-  const int64_t per_round = L.per_round;
-  float* stage = L.stage;
-  const int32_t* order = L.order;
+  const int64_t per_round = SL.per_round;
+  float* stage = SL.stage;
+  const int32_t* order = SL.order;
   // two passes per round of Q ordered rays: the tensor-core backward stages
   // dL/d(encoding), then one scatter pass per level group
   int group_start[NECTB_MAX_LEVELS + 1], n_groups = 0;
@@ -1099,15 +1056,15 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     }
     group_start[n_groups] = grid.n_levels;
   }
-  // tensor-core pass of a round: the lean kernel for two hidden layers (up to
-  // three blocks per SM), else the general one (two)
-  constexpr bool kLean = H == 2;
+  // tensor-core pass of a round: the lean kernel for two hidden layers over at
+  // most 64 inputs (up to three blocks per SM), else the general one (two)
+  constexpr bool kLean = H == 2 && L == 16 && IN <= 64;
   const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 2048 + 64 * 4 + 64 + 4 * 64 * 4;
   const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if constexpr (kLean)
     set_smem(bwd_lean_kernel<D, F>, lsmem, false);
   else
-    cudaFuncSetAttribute(bwd_mixed_kernel<D, F, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+    cudaFuncSetAttribute(bwd_mixed_kernel<D, F, L, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
@@ -1121,12 +1078,12 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
       ProfScope ps(kProfBackward, s);
       if constexpr (kLean)
         bwd_lean_kernel<D, F><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters,
-                                                                  out_act, W_grad, (int)lo, hi, stage, slots, order,
-                                                                  L.offs, L.xstore, L.xcap);
+                                                                  act, out_act, W_grad, (int)lo, hi, stage, slots,
+                                                                  order, SL.offs, SL.xstore, SL.xcap);
       else
-        bwd_mixed_kernel<D, F, H, true><<<blocks, kMixThreads, bsmem, s>>>(
-            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
-            order, L.offs, L.xstore, L.xcap);
+        bwd_mixed_kernel<D, F, L, H, true><<<blocks, kMixThreads, bsmem, s>>>(
+            grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, table_grad, W_grad, (int)lo, hi, stage,
+            slots, order, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
@@ -1149,20 +1106,18 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
                 const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
                 float* y_pred, float* loss, cudaStream_t s) {
   (void)nW;
-  const int D = grid.n_dims, F = grid.n_features;
+  const int D = grid.n_dims, F = grid.n_features, L = grid.n_levels;
   const int H = mlp.n_hidden_layers;
-  if ((H != 2 && H != 3) || mlp.activation != NECTB_ACT_RELU)
-    return set_error(NECTB_ERR_INVALID, "mixed path: needs 2 or 3 hidden ReLU layers (got %d, act %d)", H,
-                     mlp.activation);
-  if (grid.n_levels != 16 || mlp.n_input != 16 * F || mlp.width != 64)
-    return set_error(NECTB_ERR_INVALID, "mixed path: needs 16 levels, n_input 16 x n_features and width 64");
+  if (H < 2)
+    return set_error(NECTB_ERR_INVALID, "mixed path: needs at least 2 hidden layers (got %d)", H);
   const __half* tab = (const __half*)table;
-  const int oact = mlp.output_activation;
-  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
-    return run_mixed<d(), f(), h()>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad, y_pred, loss, s);
+  const int act = mlp.activation, oact = mlp.output_activation;
+  const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
+    return run_mixed<d(), f(), l(), h()>(geo, grid, tab, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
   });
   if (rc != kUnsupportedShape) return rc;
-  return set_error(NECTB_ERR_INVALID, "mixed path: unsupported grid (n_dims %d, n_features %d, hidden %d)", D, F, H);
+  return set_error(NECTB_ERR_INVALID, "mixed path: unsupported model shape (n_dims %d, n_features %d, n_levels %d, "
+                   "hidden %d)", D, F, L, H);
 }
 
 }  // namespace nectb

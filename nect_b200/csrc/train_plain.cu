@@ -28,18 +28,22 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
   RaySetup r;
   r.valid = 0;
   r.distance = 0.f;
+  // continuous scan: virtual ray tid is pixel rb of the batch at sub-angle j
+  const int n_batch = a.num_rays / a.sub;
+  const int j = tid / n_batch, rb = tid - j * n_batch;
+  const float angle = a.sub > 1 ? a.sub_angle[j] : a.angle;
   // perm == nullptr: every detector pixel in order (re-projection queries);
   // jitter / detector offsets default to 0 when absent.
   bool ok;
   if (a.perm) {
-    ok = ray_lookup(a.perm, a.perm_len, a.start, tid, a.num_rays, g, ray_index);
+    ok = ray_lookup(a.perm, a.perm_len, a.start, rb, n_batch, g, ray_index);
   } else {
     ray_index = tid;
     ok = tid < a.n_pixels;
   }
   if (ok)
     ray_setup(g, ray_index, a.det_off ? a.det_off[2 * (int64_t)tid] : 0.f,
-              a.det_off ? a.det_off[2 * (int64_t)tid + 1] : 0.f, a.jitter ? a.jitter[tid] : 0.f, a.angle, a.S,
+              a.det_off ? a.det_off[2 * (int64_t)tid + 1] : 0.f, a.jitter ? a.jitter[tid] : 0.f, angle, a.S,
               a.maxd, a.uniform != 0, r);
   int count = 0;
   if (r.valid) count = warp_sample_count(g, r, a.S, lane);
@@ -59,7 +63,7 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
     rec.y = (in_range && a.projection) ? a.projection[ray_index] : 0.f;
     rec.gsig = 0.f;
     if (count > 0) {
-      if (atomicCAS(slot + ray_index, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
+      if (atomicCAS(slot + (int64_t)ray_index * a.sub + j, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
     } else {
       // no samples: y_pred = 0 (the reference's zero attenuation sum)
       y_pred[tid] = 0.f;
@@ -191,7 +195,7 @@ fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   float* cols = smem + simt_weight_floats<IN, H, false>();
   const int t = threadIdx.x;
   float* x = cols + t;                 // [IN][LD]
-  float* hid = cols + IN * LD + t;     // [(H-1)*64][LD]
+  float* hid = cols + IN * LD + t;     // two [64][LD] buffers, alternating between layers
   __syncthreads();
   const int lane = t & 31;
   float loss_acc = 0.f;
@@ -215,8 +219,10 @@ fwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
           gemv_cols<IN, kWidth, LD>(sw.WT[0], in, hid, act);
 #pragma unroll
           for (int k = 1; k < H - 1; ++k)
-            gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + (k - 1) * kWidth * LD, hid + k * kWidth * LD, act);
-          sum += act_fwd(gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + (H - 2) * kWidth * LD, sw.wout, act), out_act);
+            gemv_cols<kWidth, kWidth, LD>(sw.WT[k], hid + ((k - 1) & 1) * kWidth * LD, hid + (k & 1) * kWidth * LD,
+                                          act);
+          sum += act_fwd(gemv_dot<kWidth, LD>(sw.WT[H - 1], hid + ((H - 2) & 1) * kWidth * LD, sw.wout, act),
+                         out_act);
         }
       }
     }
@@ -294,7 +300,33 @@ __host__ __device__ constexpr bool carry_layer0() {
   return 4 * (IN + (H - 1) * kWidth) / (NT / 16) <= 160;
 }
 
-template <int D, int F, int IN, int H, int NT>
+// Whether the hidden layers' weight-gradient tiles stay in registers across
+// the loop (at most 160 accumulators); otherwise each is computed and added
+// to W_grad per sample tile, one layer at a time (the deep models).
+template <int H, int NT>
+__host__ __device__ constexpr bool carry_hidden() {
+  return 4 * (H - 1) * kWidth / (NT / 16) <= 160;
+}
+
+// Shared-memory plan of the SIMT backward kernels for IN inputs and H hidden
+// layers: tiles of 128, 64 or 32 samples with both weight copies in shared
+// memory, or, when even 32 do not fit (the deep models), tiles of 32 with the
+// PyTorch-layout weights read from the global buffer through L1.
+template <int IN, int H>
+struct SimtBwdPlan {
+  static constexpr size_t kBudget = 227 * 1024;
+  static constexpr size_t cols(int nt) { return (size_t)(IN + (H + 2) * kWidth) * (nt + 4) * 4; }
+  static constexpr size_t wbytes(bool both) {
+    return (size_t)(both ? simt_weight_floats<IN, H, true>() : simt_weight_floats<IN, H, false>()) * 4;
+  }
+  static constexpr bool kBoth = wbytes(true) + cols(32) <= kBudget;
+  static constexpr int NT =
+      wbytes(kBoth) + cols(128) <= kBudget ? 128 : (wbytes(kBoth) + cols(64) <= kBudget ? 64 : 32);
+  static constexpr size_t smem = wbytes(kBoth) + cols(NT);
+  static_assert(smem <= kBudget, "SIMT backward does not fit shared memory");
+};
+
+template <int D, int F, int IN, int H, int NT, bool kBoth>
 __global__ void __launch_bounds__(NT, 1)
 bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
@@ -304,8 +336,8 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   constexpr int LD = NT + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
-  const SimtWeights sw = stage_weights<IN, H, true>(W, smem);
-  float* cols = smem + simt_weight_floats<IN, H, true>();
+  const SimtWeights sw = stage_weights<IN, H, kBoth>(W, smem);
+  float* cols = smem + simt_weight_floats<IN, H, kBoth>();
   float* sX = cols;                      // [IN][LD]
   float* sA = sX + IN * LD;              // [H][64][LD]  a_1..a_H
   float* sG = sA + H * kWidth * LD;      // [64][LD]
@@ -313,11 +345,13 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   const int t = threadIdx.x;
   const int lane = t & 31;
   (void)NW;
+  constexpr bool kCarry0 = carry_layer0<IN, H, NT>();
+  constexpr bool kCarryH = carry_hidden<H, NT>();
   WGrad<IN, NT, LD> g0;
   g0.zero();
-  WGrad<kWidth, NT, LD> gh[H > 1 ? H - 1 : 1];
+  WGrad<kWidth, NT, LD> gh[kCarryH && H > 1 ? H - 1 : 1];
 #pragma unroll
-  for (int k = 0; k < H - 1; ++k) gh[k].zero();
+  for (int k = 0; k < (kCarryH ? H - 1 : 1); ++k) gh[k].zero();
   float dwout[2] = {0.f, 0.f};  // lane owns w_out[lane] and w_out[lane + 32]
 
   int ray = -1, base = 0;
@@ -371,7 +405,13 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
 #pragma unroll
     for (int k = H - 1; k >= 1; --k) {
       __syncthreads();
-      gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      if constexpr (kCarryH) {
+        gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      } else {  // this layer's tile, added to W_grad now
+        gh[0].zero();
+        gh[0].add(G, sA + (k - 1) * kWidth * LD);
+        gh[0].flush(W_grad + kWidth * IN + (k - 1) * kWidth * kWidth);
+      }
       // G_k = (W_k^T G_{k+1}) * act'(a_k); W_k is [64 out][64 in] = M[j][i]
       gemv_cols<kWidth, kWidth, LD>(sw.W[k], G + t, G2 + t, NECTB_ACT_NONE);
       const float* ak = sA + (k - 1) * kWidth * LD + t;
@@ -381,11 +421,9 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
       G2 = tmp;
     }
     __syncthreads();
+    if constexpr (!kCarry0) g0.zero();
     g0.add(G, sX);
-    if constexpr (!carry_layer0<IN, H, NT>()) {
-      g0.flush(W_grad);
-      g0.zero();
-    }
+    if constexpr (!kCarry0) g0.flush(W_grad);
     // dX = W_0^T G_1 (W_0 is [64][IN] = M[j][i]) into G2, then scatter
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
     // per-sample atomics: the SIMT path is issue-bound and the run reduction's
@@ -394,9 +432,11 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
     __syncthreads();
     base += 32;
   }
-  if constexpr (carry_layer0<IN, H, NT>()) g0.flush(W_grad);
+  if constexpr (kCarry0) g0.flush(W_grad);
+  if constexpr (kCarryH) {
 #pragma unroll
-  for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+    for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+  }
   const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
   // combine the warps' w_out partials through shared memory (reuse sG)
   __syncthreads();
@@ -417,7 +457,7 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
 // weight gradients, per-sample table reductions) with points read from x
 // (n x 3, (z, y, x); t broadcast in 4D) instead of regenerated along rays
 // and a per-point dL/dsigma.  Tables of either precision are gathered.
-template <int D, int F, int IN, int H, int NT, typename T>
+template <int D, int F, int IN, int H, int NT, bool kBoth, typename T>
 __global__ void __launch_bounds__(NT, 1)
 model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restrict__ W, const float* __restrict__ x,
                  int64_t n, float tval, const float* __restrict__ t_dev, const float* __restrict__ dsigma, int act,
@@ -425,19 +465,21 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
   constexpr int LD = NT + 4;
   extern __shared__ float4 smem4[];
   float* smem = reinterpret_cast<float*>(smem4);
-  const SimtWeights sw = stage_weights<IN, H, true>(W, smem);
-  float* cols = smem + simt_weight_floats<IN, H, true>();
+  const SimtWeights sw = stage_weights<IN, H, kBoth>(W, smem);
+  float* cols = smem + simt_weight_floats<IN, H, kBoth>();
   float* sX = cols;                      // [IN][LD]
   float* sA = sX + IN * LD;              // [H][64][LD]
   float* sG = sA + H * kWidth * LD;      // [64][LD]
   float* sG2 = sG + kWidth * LD;         // [64][LD]
   const int t = threadIdx.x;
   const int lane = t & 31;
+  constexpr bool kCarry0 = carry_layer0<IN, H, NT>();
+  constexpr bool kCarryH = carry_hidden<H, NT>();
   WGrad<IN, NT, LD> g0;
   g0.zero();
-  WGrad<kWidth, NT, LD> gh[H > 1 ? H - 1 : 1];
+  WGrad<kWidth, NT, LD> gh[kCarryH && H > 1 ? H - 1 : 1];
 #pragma unroll
-  for (int k = 0; k < H - 1; ++k) gh[k].zero();
+  for (int k = 0; k < (kCarryH ? H - 1 : 1); ++k) gh[k].zero();
   float dwout[2] = {0.f, 0.f};
   if (D == 4 && t_dev) tval = *t_dev;   // the broadcast timestep, read on the device
   __syncthreads();
@@ -474,7 +516,13 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
 #pragma unroll
     for (int k = H - 1; k >= 1; --k) {
       __syncthreads();
-      gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      if constexpr (kCarryH) {
+        gh[k - 1].add(G, sA + (k - 1) * kWidth * LD);
+      } else {  // this layer's tile, added to W_grad now
+        gh[0].zero();
+        gh[0].add(G, sA + (k - 1) * kWidth * LD);
+        gh[0].flush(W_grad + kWidth * IN + (k - 1) * kWidth * kWidth);
+      }
       gemv_cols<kWidth, kWidth, LD>(sw.W[k], G + t, G2 + t, NECTB_ACT_NONE);
       const float* ak = sA + (k - 1) * kWidth * LD + t;
       for (int j = 0; j < kWidth; ++j) G2[j * LD + t] *= act_grad_a(ak[j * LD], act);
@@ -483,18 +531,18 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
       G2 = tmp;
     }
     __syncthreads();
+    if constexpr (!kCarry0) g0.zero();
     g0.add(G, sX);
-    if constexpr (!carry_layer0<IN, H, NT>()) {
-      g0.flush(W_grad);
-      g0.zero();
-    }
+    if constexpr (!kCarry0) g0.flush(W_grad);
     gemv_cols<kWidth, IN, LD>(sw.W[0], G + t, G2 + t, NECTB_ACT_NONE);
     scatter_warp<D, F>(grid, table_grad, p, valid, G2 + t, (int64_t)F * LD, LD, 0u, 0, grid.n_levels);
     __syncthreads();
   }
-  if constexpr (carry_layer0<IN, H, NT>()) g0.flush(W_grad);
+  if constexpr (kCarry0) g0.flush(W_grad);
+  if constexpr (kCarryH) {
 #pragma unroll
-  for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+    for (int k = 0; k < H - 1; ++k) gh[k].flush(W_grad + kWidth * IN + k * kWidth * kWidth);
+  }
   const int nHidden = kWidth * IN + (H - 1) * kWidth * kWidth;
   __syncthreads();
   float* red = sG;  // [NT/32][64]
@@ -508,17 +556,15 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
   }
 }
 
-template <int D, int F, int H, typename T>
+template <int D, int F, int L, int H, typename T>
 int launch_model_bwd(const GridDev& grid, const void* table, const float* W, const float* x, int64_t n, float tval,
                      const float* t_dev, const float* dsigma, int act, int out_act, float* table_grad, float* W_grad,
                      cudaStream_t s) {
-  constexpr int IN = 16 * F;
-  // 64-thread tiles when 128 would not fit shared memory (3 hidden layers over 64 inputs)
-  constexpr int NT = (IN + (H + 2) * kWidth) * (128 + 4) * 4 + simt_weight_floats<IN, H, true>() * 4 > 227 * 1024
-                         ? 64 : 128;
-  auto k = model_bwd_kernel<D, F, IN, H, NT, T>;
-  const size_t smem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
-  if (smem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "model backward needs %zu B of shared memory", smem);
+  constexpr int IN = L * F;
+  using Plan = SimtBwdPlan<IN, H>;
+  constexpr int NT = Plan::NT;
+  auto k = model_bwd_kernel<D, F, IN, H, NT, Plan::kBoth, T>;
+  const size_t smem = Plan::smem;
   cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
@@ -529,11 +575,11 @@ int launch_model_bwd(const GridDev& grid, const void* table, const float* W, con
   return launch_status("model_bwd_kernel");
 }
 
-template <int D, int F, int H>
+template <int D, int F, int L, int H>
 int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table, const float* W, const TrainArgs& a,
               Workspace ws, int act, int out_act, float* table_grad, float* W_grad, float* y_pred, float* loss,
               cudaStream_t s) {
-  constexpr int IN = 16 * F;
+  constexpr int IN = L * F;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -541,7 +587,8 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
 
   constexpr int FNT = kPlainFwdThreads;
   auto fk = fwd_plain_kernel<D, F, IN, H>;
-  const size_t fsmem = (size_t)(simt_weight_floats<IN, H, false>() + (IN + (H - 1) * kWidth) * (FNT + 4)) * 4;
+  const size_t fsmem =
+      (size_t)(simt_weight_floats<IN, H, false>() + (IN + simt_hidden_buffers<H>() * kWidth) * (FNT + 4)) * 4;
   set_smem(fk, fsmem, a.max_blocks > 0);
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fk, FNT, fsmem);
@@ -556,12 +603,10 @@ int run_plain(const NectbGeometry& geo, const GridDev& grid, const float* table,
   }
   if (!table_grad || !(a.phase & kPhaseBackward)) return NECTB_OK;  // forward only (queries, split step)
 
-  // 64-thread tiles when 128 would not fit shared memory (3 hidden layers over 64 inputs)
-  constexpr int NT = (IN + (H + 2) * kWidth) * (128 + 4) * 4 + simt_weight_floats<IN, H, true>() * 4 > 227 * 1024
-                         ? 64 : 128;
-  auto bk = bwd_plain_kernel<D, F, IN, H, NT>;
-  const size_t bsmem = (size_t)(simt_weight_floats<IN, H, true>() + (IN + (H + 2) * kWidth) * (NT + 4)) * 4;
-  if (bsmem > 227 * 1024) return set_error(NECTB_ERR_INVALID, "plain backward needs %zu B of shared memory", bsmem);
+  using Plan = SimtBwdPlan<IN, H>;
+  constexpr int NT = Plan::NT;
+  auto bk = bwd_plain_kernel<D, F, IN, H, NT, Plan::kBoth>;
+  const size_t bsmem = Plan::smem;
   cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
   const int bblocks = std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, NT / 32)));
   {
@@ -578,31 +623,32 @@ int model_backward(const GridDev& g, const NectbMLP& mlp, int dtype, const void*
                    const float* x, int64_t n, float tval, const float* t_dev, const float* dsigma, float* table_grad,
                    float* W_grad, cudaStream_t s) {
   const bool h = dtype == NECTB_F16;
-  const int D = g.n_dims, F = g.n_features, H = mlp.n_hidden_layers;
+  const int D = g.n_dims, F = g.n_features, L = g.n_levels, H = mlp.n_hidden_layers;
   const int act = mlp.activation, oact = mlp.output_activation;
-  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto hl) {
-    return h ? launch_model_bwd<d(), f(), hl(), __half>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
-                                                        table_grad, W_grad, s)
-             : launch_model_bwd<d(), f(), hl(), float>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
-                                                       table_grad, W_grad, s);
+  const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto hl) {
+    return h ? launch_model_bwd<d(), f(), l(), hl(), __half>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
+                                                             table_grad, W_grad, s)
+             : launch_model_bwd<d(), f(), l(), hl(), float>(g, table, W, x, n, tval, t_dev, dsigma, act, oact,
+                                                            table_grad, W_grad, s);
   });
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "model backward: unsupported configuration (n_dims %d, n_features %d, "
-                   "hidden %d)", D, F, H);
+                   "n_levels %d, hidden %d)", D, F, L, H);
 }
 
 int train_plain(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const float* table,
                 const float* W, int nW, const TrainArgs& a, Workspace ws, float* table_grad, float* W_grad,
                 float* y_pred, float* loss, cudaStream_t s) {
   (void)nW;
-  const int D = grid.n_dims, F = grid.n_features, H = mlp.n_hidden_layers;
+  const int D = grid.n_dims, F = grid.n_features, L = grid.n_levels, H = mlp.n_hidden_layers;
   const int act = mlp.activation, oact = mlp.output_activation;
-  const int rc = dispatch_shape(D, F, H, [&](auto d, auto f, auto h) {
-    return run_plain<d(), f(), h()>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+  const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
+    return run_plain<d(), f(), l(), h()>(geo, grid, table, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss,
+                                         s);
   });
   if (rc != kUnsupportedShape) return rc;
-  return set_error(NECTB_ERR_INVALID, "plain path supports 16 levels of 2 or 4 features with 2 or 3 hidden layers "
-                   "(got n_dims %d, n_features %d, hidden %d)", D, F, H);
+  return set_error(NECTB_ERR_INVALID, "plain path: unsupported model shape (n_dims %d, n_features %d, n_levels %d, "
+                   "hidden %d)", D, F, L, H);
 }
 
 }  // namespace nectb

@@ -52,18 +52,25 @@ class Reconstruction:
         return out
 
 
-def default_model_config(geometry: Geometry, mode: str, precision: str, log2_hashmap_size: int = 19) -> ModelConfig:
-    """The model of the static parallel-beam workload: 16 levels x 2 features,
-    2^19 entries (unless given), base 16, finest 2 x the largest detector
-    extent, 2 x 64 ReLU MLP with softplus output (temporal base 4 for dynamic
-    scans).  The reference's own preset (nect/cfg/static/hash_grid.yaml: 19
-    levels x 4 features, 6 x 64 LeakyReLU) is outside the kernel
-    instantiations."""
-    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_hashmap_size,
-                            base_resolution=16, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
-                            nVoxel=list(geometry.nVoxel), base_resolution_t=4 if mode == "dynamic" else None)
-    return ModelConfig("hash_grid_4d" if mode == "dynamic" else "hash_grid", enc, MLPNetConfig(n_hidden_layers=2),
-                       precision)
+def default_model_config(geometry: Geometry, mode: str, precision: str, log2_hashmap_size: int = 21) -> ModelConfig:
+    """The reference's default model of the mode.  Static: its hash_grid
+    preset (nect/cfg/static/hash_grid.yaml:1-13): 19 levels x 4 features,
+    2^21 entries (unless the quality preset sets another size), base
+    resolution 8, finest 2 x the largest detector extent, 6 x 64 LeakyReLU
+    MLP with a ReLU output.  Dynamic: the reference's default (QuadCubes,
+    nect/cfg/dynamic/quadcubes.yaml) is four 3D grids that this path does not
+    build; its single-4D-grid model takes 16 levels x 2 features, temporal
+    base resolution 4 and a 2 x 64 ReLU MLP with a softplus output."""
+    if mode == "dynamic":
+        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_hashmap_size,
+                                base_resolution=16, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
+                                nVoxel=list(geometry.nVoxel), base_resolution_t=4)
+        return ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision)
+    enc = HashEncoderConfig(n_levels=19, n_features_per_level=4, log2_hashmap_size=log2_hashmap_size,
+                            base_resolution=8, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
+                            nVoxel=list(geometry.nVoxel))
+    net = MLPNetConfig(n_hidden_layers=6, n_neurons=64, activation="LeakyReLU", output_activation="ReLU")
+    return ModelConfig("hash_grid", enc, net, precision)
 
 
 # ---------------------------------------------------------- quality presets ----

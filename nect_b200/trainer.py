@@ -75,16 +75,22 @@ class Workspace:
         self.staging_fraction = staging_fraction
 
     def get(self, model: _HashGridModel, c_geometry, num_rays: int, device,
-            points_per_ray: int = 0) -> tuple[int, int]:
-        need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
-                                                    ctypes.byref(model.mlp_desc), num_rays)
+            points_per_ray: int = 0, sub_angles: int = 1) -> tuple[int, int]:
+        """(pointer, bytes) of a workspace for a batch of num_rays rays (a
+        continuous-scan batch of sub_angles sub-angles when sub_angles > 1)."""
+        args = (ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc))
+        if sub_angles > 1:
+            need = _lib.lib.nectb_train_scan_workspace_bytes(*args, num_rays, sub_angles)
+        else:
+            need = _lib.lib.nectb_train_workspace_bytes(*args, num_rays)
         if self.staging and points_per_ray > 0:
-            need = ((need + 255) // 256) * 256 + int(self.staging_fraction * _lib.lib.nectb_train_staging_bytes(
-                ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
-                num_rays, points_per_ray))
+            staging = (_lib.lib.nectb_train_scan_staging_bytes(*args, num_rays, points_per_ray, sub_angles)
+                       if sub_angles > 1 else _lib.lib.nectb_train_staging_bytes(*args, num_rays, points_per_ray))
+            need = ((need + 255) // 256) * 256 + int(self.staging_fraction * staging)
         if self.buf is None or self.buf.numel() < need or self.buf.device != torch.device(device):
             self.buf = torch.empty(need, dtype=torch.uint8, device=device)
         self.num_rays = num_rays
+        self.sub_angles = sub_angles
         self.c_geometry = c_geometry
         return self.buf.data_ptr(), self.buf.numel()
 
@@ -92,7 +98,11 @@ class Workspace:
         """The device error word of the last step run in this workspace (0 = every
         tensor-core wait completed).  Synchronises the current stream."""
         cg = c_geometry if c_geometry is not None else self.c_geometry
-        addr = _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), int(self.num_rays), self.buf.data_ptr())
+        if getattr(self, "sub_angles", 1) > 1:
+            addr = _lib.lib.nectb_train_scan_error_word(ctypes.byref(cg.c_struct), int(self.num_rays),
+                                                        int(self.sub_angles), self.buf.data_ptr())
+        else:
+            addr = _lib.lib.nectb_train_error_word(ctypes.byref(cg.c_struct), int(self.num_rays), self.buf.data_ptr())
         if not addr:
             raise RuntimeError("nectb_train_error_word: " + _lib.lib.nectb_last_error().decode())
         off = addr - self.buf.data_ptr()
@@ -187,6 +197,79 @@ def ray_integral(model: _HashGridModel, c_geometry, batch: RayBatch, max_distanc
                  workspace: Workspace) -> torch.Tensor:
     """Differentiable y_pred [R] of one batch (see RayIntegral)."""
     return RayIntegral.apply(model.table, model.mlp, model, c_geometry, batch, max_distance_traveled, workspace)
+
+
+class ScanIntegral(torch.autograd.Function):
+    """The continuous-scan prediction y_pred[r] = mean over the sub angles of
+    pixel r's line integral (continous_scanning_trainer.py:85-137) as a
+    function of (table, mlp), all sub-angle rays in one launch of each fused
+    kernel: forward nectb_train_scan_forward, backward
+    nectb_train_scan_backward.  ``batch`` carries sub_angles * R jitter and
+    detector-offset draws (sub-angle-major); its angle is ignored."""
+
+    @staticmethod
+    def forward(ctx, table, mlp, model, c_geometry, batch, sub_angles, max_distance_traveled, workspace):
+        dev = batch.perm.device
+        k = len(sub_angles)
+        for name, t in (("perm", batch.perm), ("jitter", batch.jitter), ("detector_offset", batch.detector_offset),
+                        ("projection", batch.projection)):
+            _lib.require_cuda(t, name)
+        if batch.jitter.numel() != k * batch.num_rays or batch.detector_offset.numel() != 2 * k * batch.num_rays:
+            raise ValueError("a continuous-scan batch needs sub_angles * num_rays jitter and offset draws")
+        angles = (ctypes.c_float * k)(*[float(a) for a in sub_angles])
+        y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
+        ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev, batch.points_per_ray, k)
+        cb = c_batch(batch, max_distance_traveled, "l2")
+        rc = _lib.lib.nectb_train_scan_forward(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                               ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                               model.mlp.data_ptr(), ctypes.byref(cb), angles, k, y_pred.data_ptr(),
+                                               ws_ptr, ws_size, _lib.stream_ptr(dev))
+        _lib.check(rc, "nectb_train_scan_forward")
+        ctx.model, ctx.c_geometry, ctx.batch, ctx.cb, ctx.angles, ctx.k = model, c_geometry, batch, cb, angles, k
+        ctx.ws_buf, ctx.ws = workspace.buf, (ws_ptr, ws_size)
+        return y_pred
+
+    @staticmethod
+    def backward(ctx, grad_y):
+        model, dev = ctx.model, ctx.batch.perm.device
+        g = grad_y.detach().to(torch.float32).contiguous()
+        tg = torch.zeros_like(model.table)
+        mg = torch.zeros_like(model.mlp)
+        rc = _lib.lib.nectb_train_scan_backward(ctypes.byref(ctx.c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                                ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                                model.mlp.data_ptr(), ctypes.byref(ctx.cb), ctx.angles, ctx.k,
+                                                g.data_ptr(), tg.data_ptr(), mg.data_ptr(), ctx.ws[0], ctx.ws[1],
+                                                _lib.stream_ptr(dev))
+        _lib.check(rc, "nectb_train_scan_backward")
+        return tg, mg, None, None, None, None, None, None
+
+
+def scan_integral(model: _HashGridModel, c_geometry, batch: RayBatch, sub_angles, max_distance_traveled: float,
+                  workspace: Workspace) -> torch.Tensor:
+    """Differentiable continuous-scan y_pred [R] of one batch (see ScanIntegral)."""
+    return ScanIntegral.apply(model.table, model.mlp, model, c_geometry, batch, list(sub_angles),
+                              max_distance_traveled, workspace)
+
+
+def scan_step(model: _HashGridModel, c_geometry, batch: RayBatch, sub_angles, max_distance_traveled: float,
+              table_grad: torch.Tensor, mlp_grad: torch.Tensor, workspace: Workspace, loss: str = "l2",
+              loss_scale: float = 1.0):
+    """The fused continuous-scan step with the built-in L1/L2 loss
+    (nectb_train_scan_step); gradients are ADDED.  Returns (loss [1], y_pred [R])."""
+    dev = batch.perm.device
+    k = len(sub_angles)
+    angles = (ctypes.c_float * k)(*[float(a) for a in sub_angles])
+    y_pred = torch.empty(batch.num_rays, device=dev, dtype=torch.float32)
+    loss_out = torch.empty(1, device=dev, dtype=torch.float32)
+    ws_ptr, ws_size = workspace.get(model, c_geometry, batch.num_rays, dev, batch.points_per_ray, k)
+    cb = c_batch(batch, max_distance_traveled, loss, loss_scale)
+    rc = _lib.lib.nectb_train_scan_step(ctypes.byref(c_geometry.c_struct), ctypes.byref(model.grid_desc),
+                                        ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                        model.mlp.data_ptr(), ctypes.byref(cb), angles, k, table_grad.data_ptr(),
+                                        mlp_grad.data_ptr(), y_pred.data_ptr(), loss_out.data_ptr(), ws_ptr, ws_size,
+                                        _lib.stream_ptr(dev))
+    _lib.check(rc, "nectb_train_scan_step")
+    return loss_out, y_pred
 
 
 def total_variation_3d(volume: torch.Tensor, weight: float = 1.0) -> torch.Tensor:
@@ -481,24 +564,43 @@ class Trainer:
 
     def continuous_step(self, perm: torch.Tensor, batch_num: int, angle_start: float, angle_stop: float,
                         projection: torch.Tensor, t: float = 0.0, accumulation_steps: int = 4,
-                        add_poisson: bool = False) -> torch.Tensor | None:
+                        add_poisson: bool = False, fused: bool = True) -> torch.Tensor | None:
         """One continuous-rotation step (continous_scanning_trainer.py:85-140):
         the detector integrates while the object turns from angle_start to
         angle_stop, so y_pred is the mean of ``accumulation_steps`` forwards at
         the mid-angles of equal sub-intervals (same pixels and t, a fresh
-        jitter draw per sub-angle), optionally with the reference's Poisson
-        noise term; then the loss, the hand-written backward of every
-        sub-angle forward and the Adam update."""
+        jitter draw per sub-angle, drawn in the reference's order), optionally
+        with the reference's Poisson noise term; then the loss, the
+        hand-written backward and the Adam update.  ``fused``: every
+        sub-angle's rays in one launch of each kernel (ScanIntegral); else
+        one forward per sub-angle, each on its own workspace."""
         import numpy as np
 
         edges = np.linspace(angle_start, angle_stop, accumulation_steps + 1)
+        mids = [float((edges[j] + edges[j + 1]) / 2) for j in range(accumulation_steps)]
+        if fused:
+            window = batching.batch_window(perm.numel(), self.batch_size, batch_num)
+            if window is None:
+                return None
+            start, size = window
+            draws = [draw_ray_randoms(size, self.random_offset_detector, self.device)
+                     for _ in range(accumulation_steps)]
+            batch = RayBatch(perm=perm, start=start, num_rays=size, points_per_ray=self.points_per_ray,
+                             angle=mids[0], max_ray_distance_per_point=self.geometry.max_distance_traveled /
+                             self.points_per_ray, jitter=torch.cat([d[0] for d in draws]),
+                             detector_offset=torch.cat([d[1] for d in draws]), projection=projection, t=t,
+                             uniform_ray_spacing=self.uniform_ray_spacing)
+            y_pred = scan_integral(self.model, self.c_geometry, batch, mids, self.geometry.max_distance_traveled,
+                                   self.workspace)
+            y = projection[perm[start:start + size]]
+            return self._loss_and_update(y_pred, y, add_poisson)
         if not hasattr(self, "_scan_ws") or len(self._scan_ws) != accumulation_steps:
             # every sub-angle forward keeps its workspace until the backward:
             # together they take one step's recommended staging
             self._scan_ws = [Workspace(staging_fraction=1.0 / accumulation_steps) for _ in range(accumulation_steps)]
         y_pred, batch = None, None
         for j in range(accumulation_steps):
-            batch = self.make_batch(perm, batch_num, float((edges[j] + edges[j + 1]) / 2), projection, t)
+            batch = self.make_batch(perm, batch_num, mids[j], projection, t)
             if batch is None:
                 return None
             yj = ray_integral(self.model, self.c_geometry, batch, self.geometry.max_distance_traveled,

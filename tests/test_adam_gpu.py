@@ -7,10 +7,10 @@ gradients exercise the bias corrections; the fp16 shadow the mixed path
 gathers from must equal the updated fp32 parameters rounded to fp16, and the
 gradient must read zero afterwards when zero_grad is set.
 
-Tolerances: parameters within 1e-6 relative + 1e-8 absolute (the two updates
-differ only in fp32 rounding of the moment blends: torch lerps, the kernel
-uses an fma of the same terms), moments within 1e-5 relative; the fp16
-shadow bit for bit.
+Tolerances: parameters within 1e-6 relative + 1e-8 absolute, moments within
+1e-6 of their largest entry (the kernel follows torch's order of operations;
+what remains is fp32 contraction inside either kernel); the fp16 shadow bit
+for bit.
 """
 import ctypes
 
@@ -53,8 +53,8 @@ def test_adam_matches_torch_optim_adam(cuda_device, betas, wd, lr):
         assert not gk.any(), "zero_grad left gradient entries"
         st = opt.state[ref]
         torch.testing.assert_close(p, ref.detach(), rtol=1e-6, atol=1e-8)
-        torch.testing.assert_close(m, st["exp_avg"], rtol=1e-5, atol=1e-12)
-        torch.testing.assert_close(v, st["exp_avg_sq"], rtol=1e-5, atol=1e-16)
+        for mine, theirs in ((m, st["exp_avg"]), (v, st["exp_avg_sq"])):
+            assert float((mine - theirs).abs().max()) <= 1e-6 * float(theirs.abs().max())
         assert torch.equal(half.view(torch.int16), p.half().view(torch.int16)), "fp16 shadow != table.half()"
 
 

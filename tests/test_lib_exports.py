@@ -9,7 +9,7 @@ ROOT = Path(__file__).resolve().parents[1]
 
 def declared_symbols():
     text = (ROOT / "include" / "nectb.h").read_text()
-    return sorted(set(re.findall(r"^\s*(?:int|int64_t|size_t|const char\*)\s+(nectb_\w+)\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|int64_t|size_t|const char\*|const unsigned int\*)\s+(nectb_\w+)\(", text, re.M)))
 
 
 def test_header_declares_entry_points():

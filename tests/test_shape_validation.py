@@ -1,4 +1,7 @@
-"""Model shapes outside the instantiated set are rejected through the C ABI
+"""Model shapes outside the instantiated set (dispatch_shape: 16 levels of 2 or
+4 features with 2 or 3 hidden layers in 3D and 4D, and the reference's
+default static model of 19 levels of 4 features with 6 hidden layers) are
+rejected through the C ABI
 with NECTB_ERR_INVALID and a message, before any device work (they are not
 run on another path).  Host-side checks only: the calls fail validation, so
 no pointer is dereferenced and no kernel is launched; they are skipped where
@@ -45,8 +48,10 @@ def last_error():
     (3, 16, 8, 2, 64, "relu", "unsupported configuration"),   # 8 features per level
     (4, 16, 1, 2, 64, "relu", "unsupported configuration"),   # 1 feature per level
     (3, 16, 2, 1, 64, "relu", "unsupported configuration"),   # one hidden layer
-    (3, 16, 4, 6, 64, "relu", "n_hidden_layers"),            # six hidden layers
-    (3, 19, 4, 2, 64, "relu", "n_levels"),                   # 19 levels
+    (3, 16, 4, 6, 64, "relu", "unsupported configuration"),  # six hidden layers over 16 levels
+    (3, 19, 4, 2, 64, "relu", "unsupported configuration"),  # 19 levels with two hidden layers
+    (3, 19, 4, 7, 64, "leakyrelu", "n_hidden_layers"),       # seven hidden layers
+    (4, 19, 4, 6, 64, "leakyrelu", "unsupported configuration"),  # the reference's static shape, in 4D
     (3, 16, 2, 2, 128, "relu", "width"),                     # width 128
     (3, 16, 2, 2, 64, "sigmoid", "hidden activation"),       # sigmoid hidden layers
 ])
