@@ -123,14 +123,14 @@ def make_projections(spec, geometry, n_proj: int, device, seed: int = 0):
     elif spec["phantom"] == "dynamic":
         # each projection at its own t; Poisson noise at 1e4 incident photons on the attenuation
         # expressed per object width (p / n), so that exp(-p) stays in the detector's range
-        ph = phantoms.dynamic_porous(geometry.nVoxel[0], seed=seed, attempts=60000)
+        ph = phantoms.dynamic_porous(geometry.nVoxel[0], seed=seed, attempts=8000)
         projs = torch.stack([phantoms.dynamic_porous_projection(ph, geometry, float(a), float(t), device)
                              for a, t in zip(angles, ts)])
         gen = torch.Generator(device=projs.device).manual_seed(seed)
         counts = torch.poisson(1e4 * torch.exp(-projs.double() / geometry.nVoxel[0]), generator=gen)
         projs = (-torch.log(torch.clamp(counts, min=1.0) / 1e4) * geometry.nVoxel[0]).float()
     else:
-        ph = phantoms.porous_phantom(geometry.nVoxel[0], seed=seed, attempts=60000)
+        ph = phantoms.porous_phantom(geometry.nVoxel[0], seed=seed, attempts=8000)
         projs = torch.stack([phantoms.porous_projection(ph, geometry, float(a), device) for a in angles])
     projs, _, _ = phantoms.minmax_scale(projs)
     return projs.reshape(n_proj, -1).contiguous(), [float(a) for a in angles], [float(t) for t in ts]
@@ -772,8 +772,66 @@ def run_serving(args):
     }))
 
 
+def run_scan(args):
+    """Continuous-scan training steps (nect/trainers/continous_scanning_trainer.py:
+    85-140) on the 4D cone workload: each step's prediction averages k
+    sub-angles of the same 262,144 pixels.  The fused step (every sub-angle's
+    rays in one launch of each kernel) is timed beside the per-sub-angle
+    version (one forward and backward per sub-angle), same draws, CUDA events
+    on the training stream after warm-up."""
+    from nect_b200.config import get_model
+    from nect_b200.sampling import Geometry
+    from nect_b200.trainer import Trainer
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    spec = workload_spec("c3_dynamic_cone", "mixed")
+    geometry = Geometry(**spec["geo"])
+    S, R, k = spec["S"], spec["rays"], args.sub_angles
+    torch.manual_seed(0)
+    projs, angles, ts = make_projections(spec, geometry, 4, dev)
+    step_angle = 2 * math.pi * spec["turns"] / spec["n_angles"]
+    out = {"metric": "continuous-scan train rays/s fwd+bwd (pixels per step x steps / time)", "unit": "rays/s",
+           "higher_is_better": True, "n_gpus": 1, "sub_angles": k, "steps": args.steps,
+           "config": bench_config("c3_dynamic_cone", R), "data": "synthetic"}
+    for fused in (True, False):
+        model = get_model(spec["model"], device=dev)
+        tr = Trainer(model, geometry, points_per_batch=R * S, points_per_ray=S, loss="l2", lr=1e-3, device=dev)
+        P = projs.shape[1]
+
+        def step(i):
+            perm = torch.randperm(P, dtype=torch.int64, device=dev)
+            a0 = angles[i % 4]
+            return tr.continuous_step(perm, 0, a0, a0 + step_angle, projs[i % 4], ts[i % 4], accumulation_steps=k,
+                                      fused=fused)
+
+        for i in range(args.warmup):
+            step(i)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for i in range(args.steps):
+            step(args.warmup + i)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+        out["fused" if fused else "per_sub_angle"] = {"ms_per_step": ms, "value": R / (ms / 1e3)}
+        del tr, model
+        torch.cuda.empty_cache()
+    out["value"] = out["fused"]["value"]
+    out["fused_over_per_sub_angle"] = out["per_sub_angle"]["ms_per_step"] / out["fused"]["ms_per_step"]
+    print(json.dumps(out))
+
+
 if __name__ == "__main__":
-    if "--psnr" in sys.argv:
+    if "--scan" in sys.argv:
+        ap = argparse.ArgumentParser()
+        ap.add_argument("--scan", action="store_true")
+        ap.add_argument("--sub-angles", type=int, default=4)
+        ap.add_argument("--steps", type=int, default=10)
+        ap.add_argument("--warmup", type=int, default=3)
+        run_scan(ap.parse_args())
+    elif "--psnr" in sys.argv:
         ap = argparse.ArgumentParser()
         ap.add_argument("--psnr", action="store_true")
         ap.add_argument("--psnr-steps", type=int, default=2000)

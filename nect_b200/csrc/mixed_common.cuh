@@ -58,8 +58,9 @@ __device__ __forceinline__ void stage_mixed_weights(const float* __restrict__ W,
 __device__ __forceinline__ float hidden_act(float x, int act) {
   return act == NECTB_ACT_RELU ? fmaxf(x, 0.f) : (act == NECTB_ACT_LEAKY_RELU ? (x > 0.f ? x : 0.01f * x) : x);
 }
-__device__ __forceinline__ float hidden_slope(bool positive, int act) {
-  return act == NECTB_ACT_RELU ? (positive ? 1.f : 0.f) : (act == NECTB_ACT_LEAKY_RELU ? (positive ? 1.f : 0.01f) : 1.f);
+// g times the activation's slope at a pre-activation of the given sign.
+__device__ __forceinline__ float hidden_grad(float g, bool positive, int act) {
+  return act == NECTB_ACT_RELU ? (positive ? g : 0.f) : (act == NECTB_ACT_LEAKY_RELU ? (positive ? g : 0.01f * g) : g);
 }
 
 // Activation of 64 accumulator values into row r of a bf16 tile; bit j of m = (x_j > 0).
@@ -98,7 +99,7 @@ __device__ __forceinline__ void encode_row(const GridDev& g, const __half* __res
 #pragma unroll
       for (int q = 0; q < LPC; ++q) {
         const int l = j * LPC + q;
-        if (l >= L) break;
+        if (L % LPC != 0 && l >= L) break;   // the padding chunk after an odd last level
         LevelCorners<D> lc;
         level_corners<D>(g, l, p, lc);
         float vals[1 << D][F];

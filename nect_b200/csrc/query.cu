@@ -74,13 +74,14 @@ __device__ __forceinline__ uint8_t* qalign1024(uint8_t* p) {
 // At most 128 registers so that three blocks share an SM under the 164 KB
 // shared split (a background block beside two slice blocks, or three blocks of
 // one query).
-template <int D, int F, int L, int H>
+template <int D, int F, int L, int H, int ACT>
 __global__ void __launch_bounds__(kQThreads, 4)
 query_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W,
                    const NectbQueryItem* __restrict__ items, int n_items, int64_t total_chunks,
-                   unsigned int* __restrict__ counter, int act, int out_act) {
+                   unsigned int* __restrict__ counter, int out_act) {
   using S = InShape<L, F>;
   constexpr int KT = S::KT;
+  constexpr int act = ACT;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = qalign1024(smem_raw);
   uint8_t* sW = base;                   // KT + H - 1 weight tiles
@@ -232,17 +233,17 @@ int sm_count() {
   return sms;
 }
 
-template <int D, int F, int L, int H>
+template <int D, int F, int L, int H, int ACT>
 int launch_query_mixed(const GridDev& g, const void* table, const float* W, const NectbQueryItem* items, int n,
-                       int64_t chunks, unsigned int* counter, int act, int oact, int max_blocks, cudaStream_t s) {
+                       int64_t chunks, unsigned int* counter, int oact, int max_blocks, cudaStream_t s) {
   using S = InShape<L, F>;
-  auto k = query_mixed_kernel<D, F, L, H>;
+  auto k = query_mixed_kernel<D, F, L, H, ACT>;
   const size_t smem = 1024 + (S::KT + H - 1) * kQWTile + (S::KT + 1) * kQTile + 64 * 4 + 64;
   set_smem(k, smem, true);
   int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 3 * sm_count()));
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
   ProfScope ps(kProfModel, s);
-  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, act, oact);
+  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);
   return launch_status("query_mixed_kernel");
 }
 
@@ -288,8 +289,16 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
     NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
     NECTB_REQUIRE(H >= 2, "mixed queries need at least 2 hidden layers");
     const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
-      return launch_query_mixed<d(), f(), l(), h()>(g, grid_params, mlp_params, items, n_items, total_chunks, counter,
-                                                    act, oact, max_blocks, s);
+      if (act == NECTB_ACT_RELU)
+        return launch_query_mixed<d(), f(), l(), h(), NECTB_ACT_RELU>(g, grid_params, mlp_params, items, n_items,
+                                                                       total_chunks, counter, oact, max_blocks, s);
+      if constexpr (l() != 16) {
+        if (act == NECTB_ACT_LEAKY_RELU)
+          return launch_query_mixed<d(), f(), l(), h(), NECTB_ACT_LEAKY_RELU>(
+              g, grid_params, mlp_params, items, n_items, total_chunks, counter, oact, max_blocks, s);
+      }
+      return set_error(NECTB_ERR_INVALID, "mixed queries: hidden activation %d is not instantiated for this shape",
+                       act);
     });
     if (rc != kUnsupportedShape) return rc;
   } else {

@@ -104,15 +104,16 @@ __device__ __forceinline__ bool wg_or(int wg, bool p) {
   return r != 0;
 }
 
-template <int D, int F, int L, int H>
+template <int D, int F, int L, int H, int ACT>
 __global__ void __launch_bounds__(kFwdBlocksPerSM * kMixThreads, 1)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int act, int out_act, float* __restrict__ y_pred, float* __restrict__ loss,
+                 int out_act, float* __restrict__ y_pred, float* __restrict__ loss,
                  const int32_t* __restrict__ order, const uint64_t* __restrict__ offs, uint4* __restrict__ xstore,
                  uint32_t xcap) {
   using S = InShape<L, F>;
   constexpr int KT = S::KT;
+  constexpr int act = ACT;  // hidden activation, a compile-time constant of the hot loops
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
   unsigned int* err = ctrl + 2;
@@ -263,16 +264,17 @@ struct BwdPlan {
   static constexpr size_t smem = 1024 + (S::KT + H - 1) * kWTile + (H + S::KT) * kTile + 64 * 4 + 64 + 4 * 64 * 4;
 };
 
-template <int D, int F, int L, int H, bool kStaged>
+template <int D, int F, int L, int H, bool kStaged, int ACT>
 __global__ void __launch_bounds__(kMixThreads, 2)
 bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                 int act, int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
+                 int out_act, float* __restrict__ table_grad, float* __restrict__ W_grad, int lo, int hi,
                  float* __restrict__ stage, int64_t slots, const int32_t* __restrict__ order,
                  const uint64_t* __restrict__ offs, const uint4* __restrict__ xstore, uint32_t xcap) {
   using S = InShape<L, F>;
   using Plan = BwdPlan<L, F, H>;
   constexpr int IN = S::IN, KT = S::KT;
+  constexpr int act = ACT;
   static_assert(H >= 2, "at least two hidden layers");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = order ? ctrl[6] : 0u;
@@ -414,7 +416,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     for (int j = 0; j < 8; ++j) {
       float v[8];
 #pragma unroll
-      for (int q = 0; q < 8; ++q) v[q] = dz * sWout[8 * j + q] * hidden_slope(h[8 * j + q] > 0.f, act);
+      for (int q = 0; q < 8; ++q) v[q] = hidden_grad(dz * sWout[8 * j + q], h[8 * j + q] > 0.f, act);
       tc::st_chunk_bf16(sG, t, j, v);
     }
     // backward through the hidden layers: G_{k+1} (tile gt) gives
@@ -443,7 +445,7 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         for (int q = 0; q < 8; ++q) {
           const int c = 8 * j + q;
           const uint32_t bit = c < 32 ? (mlo[k] >> c) & 1u : (mhi[k] >> (c - 32)) & 1u;
-          v[q] = h[c] * hidden_slope(bit != 0, act);
+          v[q] = hidden_grad(h[c], bit != 0, act);
         }
         tc::st_chunk_bf16(sAk(k), t, j, v);
       }
@@ -568,15 +570,16 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 //   Shared memory: W0, W1 | G2 | zero block | A1, then G1 | X.
 //   Accumulator rows are read 16 columns at a time; the w_out gradient is a
 //   16-column butterfly reduce-scatter per chunk.
-template <int D, int F>
+template <int D, int F, int ACT>
 __global__ void __launch_bounds__(kMixThreads, 3)
 bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                 const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
-                int act, int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage,
+                int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage,
                 int64_t slots, const int32_t* __restrict__ order, const uint64_t* __restrict__ offs,
                 const uint4* __restrict__ xstore, uint32_t xcap) {
   constexpr int IN = 16 * F;
   constexpr int H = 2;
+  constexpr int act = ACT;
   static_assert(IN <= 64, "dW0 shares the 64 weight-gradient columns");
   const bool by_pixel = !(ctrl[3] & kFlagDuplicatePixels);
   const unsigned int n_valid = ctrl[6];
@@ -726,7 +729,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
 #pragma unroll
       for (int q = 0; q < 16; ++q) {
         v[q] = dz * hidden_act(h[q], act);
-        g[q] = dz * sWout[16 * c + q] * hidden_slope(h[q] > 0.f, act);
+        g[q] = hidden_grad(dz * sWout[16 * c + q], h[q] > 0.f, act);
       }
       tc::st_chunk_bf16(sG, t, 2 * c, g);
       tc::st_chunk_bf16(sG, t, 2 * c + 1, g + 8);
@@ -761,7 +764,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       for (int q = 0; q < 16; ++q) {
         const int col = 16 * c + q;
         const uint32_t bit = col < 32 ? (m1lo >> col) & 1u : (m1hi >> (col - 32)) & 1u;
-        h[q] = h[q] * hidden_slope(bit != 0, act);
+        h[q] = hidden_grad(h[q], bit != 0, act);
       }
       tc::st_chunk_bf16(sA, t, 2 * c, h);
       tc::st_chunk_bf16(sA, t, 2 * c + 1, h + 8);
@@ -921,10 +924,10 @@ __global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, fl
 
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
 // slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
-template <int D, int F, int L, int H>
+template <int D, int F, int L, int H, int ACT>
 int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table, const float* W,
-              const TrainArgs& args, Workspace ws, int act, int out_act, float* table_grad, float* W_grad,
-              float* y_pred, float* loss, cudaStream_t s) {
+              const TrainArgs& args, Workspace ws, int out_act, float* table_grad, float* W_grad, float* y_pred,
+              float* loss, cudaStream_t s) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -956,8 +959,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
       if (bwd)
         if (int rc = cuda_status(cudaMemsetAsync(g3, 0, (size_t)n3 * F * sizeof(float), s), "memset slice gradient"))
           return rc;
-      if (int rc = run_mixed<3, F, L, H>(geo, ts.g3, t3, W, args, ws3, act, out_act, bwd ? g3 : nullptr, W_grad,
-                                         y_pred, loss, s))
+      if (int rc = run_mixed<3, F, L, H, ACT>(geo, ts.g3, t3, W, args, ws3, out_act, bwd ? g3 : nullptr, W_grad,
+                                              y_pred, loss, s))
         return rc;
       if (bwd) {
         {
@@ -1009,14 +1012,14 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     // with an encoding store the forward runs the rays in rank order and keeps their rows
     if (SL.xstore)
       if (int rc = run_order()) return rc;
-    auto k = fwd_mixed_kernel<D, F, L, H>;
+    auto k = fwd_mixed_kernel<D, F, L, H, ACT>;
     const size_t smem = 1024 + (KT + H - 1) * kWTile + wgs * KT * kTile + 64 * 4 + kFwdBlocksPerSM * 8 + 16 +
                         4 * kFwdBlocksPerSM * 4;
     set_smem(k, smem, a.max_blocks > 0);
     {
       ProfScope ps(kProfForward, s);
-      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, y_pred,
-                                           loss, SL.xstore ? SL.order : nullptr, SL.offs, SL.xstore, SL.xcap);
+      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
+                                           SL.xstore ? SL.order : nullptr, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
   }
@@ -1026,10 +1029,10 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   const size_t bsmem = std::max<size_t>(BwdPlan<L, F, H>::smem, 80 * 1024);
   if (SL.per_round <= 0) {
     // fused single pass: the backward scatters its own gradients
-    auto k = bwd_mixed_kernel<D, F, L, H, false>;
+    auto k = bwd_mixed_kernel<D, F, L, H, false, ACT>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
-    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, table_grad,
+    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
                                          W_grad, 0, 0x7fffffff, nullptr, 0, nullptr, nullptr, nullptr, 0u);
     return launch_status("bwd_mixed_kernel");
   }
@@ -1062,9 +1065,10 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 2048 + 64 * 4 + 64 + 4 * 64 * 4;
   const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if constexpr (kLean)
-    set_smem(bwd_lean_kernel<D, F>, lsmem, false);
+    set_smem(bwd_lean_kernel<D, F, ACT>, lsmem, false);
   else
-    cudaFuncSetAttribute(bwd_mixed_kernel<D, F, L, H, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
+    cudaFuncSetAttribute(bwd_mixed_kernel<D, F, L, H, true, ACT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)bsmem);
   auto ks = scatter_stage_kernel<D, F>;
   int per_sm = 1;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
@@ -1077,13 +1081,14 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     {
       ProfScope ps(kProfBackward, s);
       if constexpr (kLean)
-        bwd_lean_kernel<D, F><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters,
-                                                                  act, out_act, W_grad, (int)lo, hi, stage, slots,
-                                                                  order, SL.offs, SL.xstore, SL.xcap);
+        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot,
+                                                                       ws.counters, out_act, W_grad, (int)lo, hi,
+                                                                       stage, slots, order, SL.offs, SL.xstore,
+                                                                       SL.xcap);
       else
-        bwd_mixed_kernel<D, F, L, H, true><<<blocks, kMixThreads, bsmem, s>>>(
-            grid, table, W, a, ws.rays, ws.slot, ws.counters, act, out_act, table_grad, W_grad, (int)lo, hi, stage,
-            slots, order, SL.offs, SL.xstore, SL.xcap);
+        bwd_mixed_kernel<D, F, L, H, true, ACT><<<blocks, kMixThreads, bsmem, s>>>(
+            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
+            order, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
@@ -1112,8 +1117,19 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
     return set_error(NECTB_ERR_INVALID, "mixed path: needs at least 2 hidden layers (got %d)", H);
   const __half* tab = (const __half*)table;
   const int act = mlp.activation, oact = mlp.output_activation;
+  // the hidden activation is a template constant of the kernels: ReLU for
+  // every shape, LeakyReLU for the reference's default static model too
   const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
-    return run_mixed<d(), f(), l(), h()>(geo, grid, tab, W, a, ws, act, oact, table_grad, W_grad, y_pred, loss, s);
+    if (act == NECTB_ACT_RELU)
+      return run_mixed<d(), f(), l(), h(), NECTB_ACT_RELU>(geo, grid, tab, W, a, ws, oact, table_grad, W_grad,
+                                                            y_pred, loss, s);
+    if constexpr (l() != 16) {
+      if (act == NECTB_ACT_LEAKY_RELU)
+        return run_mixed<d(), f(), l(), h(), NECTB_ACT_LEAKY_RELU>(geo, grid, tab, W, a, ws, oact, table_grad,
+                                                                    W_grad, y_pred, loss, s);
+    }
+    return set_error(NECTB_ERR_INVALID, "mixed path: hidden activation %d is not instantiated for this shape (ReLU "
+                     "for every shape, LeakyReLU for 19 levels x 4 features)", act);
   });
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "mixed path: unsupported model shape (n_dims %d, n_features %d, n_levels %d, "

@@ -444,10 +444,10 @@ bwd_plain_kernel(GridDev grid, const float* __restrict__ table, const float* __r
   red[(t >> 5) * kWidth + lane] = dwout[0];
   red[(t >> 5) * kWidth + lane + 32] = dwout[1];
   __syncthreads();
-  if (t < kWidth) {
+  for (int j = t; j < kWidth; j += NT) {  // tiles of 32 samples: each thread adds two entries
     float s = 0.f;
-    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + t];
-    atomicAdd(W_grad + nHidden + t, s);
+    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + j];
+    atomicAdd(W_grad + nHidden + j, s);
   }
 }
 
@@ -549,10 +549,10 @@ model_bwd_kernel(GridDev grid, const T* __restrict__ table, const float* __restr
   red[(t >> 5) * kWidth + lane] = dwout[0];
   red[(t >> 5) * kWidth + lane + 32] = dwout[1];
   __syncthreads();
-  if (t < kWidth) {
+  for (int j = t; j < kWidth; j += NT) {  // tiles of 32 samples: each thread adds two entries
     float s = 0.f;
-    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + t];
-    atomicAdd(W_grad + nHidden + t, s);
+    for (int w = 0; w < NT / 32; ++w) s += red[w * kWidth + j];
+    atomicAdd(W_grad + nHidden + j, s);
   }
 }
 

@@ -27,9 +27,16 @@ less.  Here the fused path runs the benchmark shapes themselves:
    loss within fp32 summation error, and its gradients within fp32
    reassociation.
 
-Tolerances as the small parity tests: plain fp32 y_pred 1e-4 of the largest,
-gradients 1e-3 of the largest entry; mixed y_pred 2e-2, gradients cosine >
-0.99 and max deviation < 5e-2 of the largest entry.
+Tolerances.  Plain fp32 with a smooth network (no hidden activation,
+softplus output): y_pred 1e-4 and gradients 1e-4 of the largest entry,
+5e-5 in relative L2 norm (measured: about 2e-6 and 5e-7, as plain fp32
+arithmetic on the CPU).  Plain fp32 with ReLU hidden layers: y_pred 1e-4;
+gradients within 1e-2 of the largest entry and 3e-3 in relative L2 norm,
+because with a million samples some pre-activations sit within fp32
+rounding of the kink, where either order of fp32 arithmetic may take the
+other side (plain fp32 on the CPU deviates from fp64 by up to 1.7e-3 of
+the largest entry on the same batch).  Mixed: y_pred 2e-2, gradients cosine
+> 0.99 and max deviation < 5e-2 of the largest entry.
 """
 import contextlib
 import ctypes
@@ -71,7 +78,7 @@ def tuning(**values):
         autotune.set_tuning(before)
 
 
-def build(name, precision, table_scale=0.5, seed=0):
+def build(name, precision, table_scale=0.5, seed=0, act="ReLU"):
     from nect_b200.config import HashEncoderConfig, MLPNetConfig
     from nect_b200.network import HashGrid, HashGrid4D
     from nect_b200.sampling import Geometry
@@ -81,7 +88,7 @@ def build(name, precision, table_scale=0.5, seed=0):
     enc = HashEncoderConfig(n_levels=16, n_features_per_level=w["F"], log2_hashmap_size=w["log2_T"],
                             base_resolution=w["base"], max_resolution_factor=2.0, nDetector=w["geo"]["nDetector"],
                             finest_resolution=w["finest"], base_resolution_t=w["base_t"])
-    net = MLPNetConfig(n_hidden_layers=w["H"], n_neurons=64, activation="ReLU", output_activation="Softplus")
+    net = MLPNetConfig(n_hidden_layers=w["H"], n_neurons=64, activation=act, output_activation="Softplus")
     m = (HashGrid if w["n_dims"] == 3 else HashGrid4D)(enc, net, precision=precision, device="cuda", seed=seed)
     with torch.no_grad():
         g = torch.Generator(device="cuda").manual_seed(seed + 1)
@@ -103,6 +110,10 @@ def ref_geometry(ref, cg):
 
 def rel_max(a, b):
     return float((a - b).abs().max() / b.abs().max().clamp(min=1e-30))
+
+
+def rel_l2(a, b):
+    return float((a - b).norm() / b.norm().clamp(min=1e-30))
 
 
 def cosine(a, b):
@@ -217,19 +228,21 @@ def test_fused_path_sampling_is_the_reference_sampler(ref_sampler, name, angle, 
 
 
 # ---------------------------------------------------------- training step
-CASES = [("c2_cone", "mixed", 1, 2048), ("c2_cone", "mixed", 0, 2048), ("c2_cone", "plain_fp32", 1, 2048),
-         ("c3_cone_4d", "mixed", 1, 2048), ("c3_cone_4d", "plain_fp32", 1, 2048),
-         ("c5_large_4d", "mixed", 0, 1024), ("c5_large_4d", "plain_fp32", 0, 1024)]
+CASES = [("c2_cone", "mixed", 1, 2048, "ReLU"), ("c2_cone", "mixed", 0, 2048, "ReLU"),
+         ("c2_cone", "plain_fp32", 1, 2048, "None"), ("c2_cone", "plain_fp32", 1, 2048, "ReLU"),
+         ("c3_cone_4d", "mixed", 1, 2048, "ReLU"), ("c3_cone_4d", "plain_fp32", 1, 2048, "None"),
+         ("c3_cone_4d", "plain_fp32", 1, 2048, "ReLU"), ("c5_large_4d", "mixed", 0, 1024, "ReLU"),
+         ("c5_large_4d", "plain_fp32", 0, 1024, "None"), ("c5_large_4d", "plain_fp32", 0, 1024, "ReLU")]
 
 
-@pytest.mark.parametrize("name,precision,store,n_check", CASES,
-                         ids=[f"{c[0]}-{c[1]}-{'store' if c[2] else 'recompute'}" for c in CASES])
-def test_fullsize_step_matches_oracle(cuda_device, name, precision, store, n_check):
+@pytest.mark.parametrize("name,precision,store,n_check,act", CASES,
+                         ids=[f"{c[0]}-{c[1]}-{'store' if c[2] else 'recompute'}-{c[4]}" for c in CASES])
+def test_fullsize_step_matches_oracle(cuda_device, name, precision, store, n_check, act):
     from nect_b200.sampling import ct_sampling
     from nect_b200.trainer import RayBatch, Workspace, train_step
 
     torch.cuda.empty_cache()
-    w, geo, m, enc = build(name, precision)
+    w, geo, m, enc = build(name, precision, act=act)
     cg = geo.get_c_geometry()
     P = geo.nDetector[0] * geo.nDetector[1]
     S = w["S"]
@@ -281,7 +294,7 @@ def test_fullsize_step_matches_oracle(cuda_device, name, precision, store, n_che
     tab = m.grid_table.detach().cpu().double().requires_grad_(True)
     wf = m.mlp.detach().cpu().double().requires_grad_(True)
     yo = ohg.line_integrals(pts, dist, tab, wf, levels, enc.log2_hashmap_size, n_in, 64, w["H"],
-                            geo.max_distance_traveled, t=t if w["n_dims"] == 4 else None)
+                            geo.max_distance_traveled, act=act.lower(), t=t if w["n_dims"] == 4 else None)
     (yo * dy[sub].double()).sum().backward()
     ys = y[sub.cuda()].cpu().double()
     assert int((torch.from_numpy(counts) > 0).sum()) > n_check // 4
@@ -294,5 +307,6 @@ def test_fullsize_step_matches_oracle(cuda_device, name, precision, store, n_che
     else:
         assert rel_max(ys, yo.detach()) < 1e-4, rel_max(ys, yo.detach())
         gt, gm = tg.cpu().double(), mg.cpu().double()
-        assert rel_max(gt, tab.grad) < 1e-3, rel_max(gt, tab.grad)
-        assert rel_max(gm, wf.grad) < 1e-3, rel_max(gm, wf.grad)
+        tol_max, tol_l2 = (1e-4, 5e-5) if act == "None" else (1e-2, 3e-3)
+        for a, b in ((gt, tab.grad), (gm, wf.grad)):
+            assert rel_max(a, b) < tol_max and rel_l2(a, b) < tol_l2, (rel_max(a, b), rel_l2(a, b))
