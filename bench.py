@@ -370,8 +370,9 @@ def main():
                     help="timed steps of the plain fp32 arm (0: --steps, 2 on the large 4D workload)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling of smaller cases)")
-    ap.add_argument("--recompute", action="store_true",
-                    help="recompute the encodings in the backward instead of storing them (encoding_store 0)")
+    ap.add_argument("--encoding-store", default="auto", choices=["auto", "on", "off"],
+                    help="off: the mixed backward recomputes the encodings instead of reading the rows the forward "
+                         "stored (encoding_store 0); auto: off on the large 4D workload, on elsewhere")
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (launch shapes and scheduling tuned on this workload before the "
                          "warm-up, outside the timed region); the library defaults are used")
@@ -403,9 +404,8 @@ def main():
     geometry = Geometry(**spec["geo"])
     S, R = spec["S"], (args.rays or spec["rays"])
     model_cfg = spec["model"]
-    recompute = args.recompute or (args.workload == "c5_large_cone" and args.precision == "mixed")
-    if recompute:
-        autotune.set_tuning({"encoding_store": 0})
+    recompute = args.encoding_store == "off" or (args.encoding_store == "auto" and args.workload == "c5_large_cone")
+    autotune.set_tuning({"encoding_store": 0 if recompute else 1})
 
     torch.manual_seed(1234 + rank)
     n_proj = 8
