@@ -496,6 +496,11 @@ def main():
             if len(f) == 4 and not line.startswith("#") and f[:2] == [args.workload, args.precision]:
                 l2_step[f[2]] = float(f[3]) * per_step_samples
 
+    # the 4D mixed step gathers and reduces on the time slice: 8 spatial corners per level, half of the
+    # 16 the 4D interpolation counts (the time blend runs once per table entry and step instead)
+    sliced = spec["n_dims"] == 4 and args.precision == "mixed" and bool(autotune.get_tuning()["time_slice"])
+    executed = {"forward": gather // 2 if sliced else gather, "scatter": scatter // 2 if sliced else scatter}
+
     def roof(kind, per_sample, peak_name, bound, unit, scale, peak=None, peak_src=None):
         if kind not in kernel_ms:
             return None
@@ -510,6 +515,10 @@ def main():
                "traffic": tr / launches_per_step[kind] if tr is not None else None,
                "algorithmic_per_launch": per_launch, "launch_ms": kernel_ms[kind],
                "launches_per_step": launches_per_step[kind]}
+        if kind in executed:   # the bytes the kernel's own algorithm moves (time slice: 8 corners)
+            ex = per_step_samples * executed[kind] / launches_per_step[kind]
+            out["executed_per_launch"] = ex
+            out["executed_frac"] = ex / secs / scale / peak
         if tr is not None:
             out["dram_gbs"] = tr / launches_per_step[kind] / secs / 1e9
             out["dram_frac_of_hbm"] = out["dram_gbs"] / hbm

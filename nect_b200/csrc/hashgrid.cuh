@@ -210,7 +210,9 @@ __device__ __forceinline__ uint32_t run_levels(const GridDev& g, double dx, doub
 
 // Adds the contributions of corners c and c + 1 (which differ along axis 0,
 // the axis with hash prime 1 and dense stride 1): when their entries form an
-// aligned pair (i0 even, i1 = i0 + 1) one 16-byte reduction carries both,
+// aligned pair (i0 even and i1 = i0 + 1, or i1 even and i0 = i1 + 1: on a
+// hashed level with an even cell coordinate the two entries differ in the
+// lowest bit only, in either order) one 16-byte reduction carries both,
 // otherwise one 8-byte reduction each.  The gradient table must be 16-byte
 // aligned (level offsets are multiples of 8 entries).
 __device__ __forceinline__ void red_pair_f2(float* base, uint32_t i0, uint32_t i1, float a0, float a1, float b0,
@@ -218,6 +220,8 @@ __device__ __forceinline__ void red_pair_f2(float* base, uint32_t i0, uint32_t i
   float* dst = base + (int64_t)i0 * 2;
   if (!(i0 & 1u) && i1 == i0 + 1u) {
     atomicAdd(reinterpret_cast<float4*>(dst), make_float4(a0, a1, b0, b1));
+  } else if (!(i1 & 1u) && i0 == i1 + 1u) {
+    atomicAdd(reinterpret_cast<float4*>(base + (int64_t)i1 * 2), make_float4(b0, b1, a0, a1));
   } else {
     atomicAdd(reinterpret_cast<float2*>(dst), make_float2(a0, a1));
     atomicAdd(reinterpret_cast<float2*>(base + (int64_t)i1 * 2), make_float2(b0, b1));
