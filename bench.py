@@ -781,6 +781,64 @@ def run_serving(args):
     }))
 
 
+def run_psnr4d(args):
+    """Reconstruction quality of the 4D cone workload, mixed against plain fp32
+    at equal iterations: the dynamic porous phantom (brine front, shrinking
+    grains), ``--views`` projections spread over the 10 turns, each at its own
+    t, Poisson noise at 1e4 incident photons, one full 512^2 projection per
+    step (262,144 rays, S = 512), L2, Adam 1e-3.  PSNR (-10 log10 MSE) of the
+    exported 256^3 volume against the phantom, averaged over t = 0.2, 0.5,
+    0.8, with the training seconds at each evaluation."""
+    from nect_b200 import phantoms
+    from nect_b200.reconstruct import fit, psnr
+    from nect_b200.sampling import Geometry
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    spec = workload_spec("c3_dynamic_cone", "mixed")
+    geometry = Geometry(**spec["geo"])
+    n = geometry.nVoxel[0]
+    all_angles = np.linspace(0, 2 * math.pi * spec["turns"], spec["n_angles"], endpoint=False)
+    idx = np.linspace(0, spec["n_angles"] - 1, args.views).astype(int)
+    angles, ts = all_angles[idx], idx / (spec["n_angles"] - 1)
+    ph = phantoms.dynamic_porous(n, seed=0)
+    projs = torch.stack([phantoms.dynamic_porous_projection(ph, geometry, float(a), float(t), dev)
+                         for a, t in zip(angles, ts)])
+    gen = torch.Generator(device=dev).manual_seed(0)
+    counts = torch.poisson(1e4 * torch.exp(-projs.double() / n), generator=gen)
+    projs = (-torch.log(torch.clamp(counts, min=1.0) / 1e4) * n).float()
+    t_eval = (0.2, 0.5, 0.8)
+    truths = {t: phantoms.dynamic_porous_volume(ph, n, t, dev) for t in t_eval}
+
+    def evaluate(rec):
+        return {"psnr": float(np.mean([psnr(rec.volume(t), truths[t]) for t in t_eval]))}
+
+    out = {"metric": "4D reconstruction PSNR, mixed vs plain fp32 at equal iterations", "unit": "dB",
+           "higher_is_better": True, "n_gpus": 1, "steps": args.psnr_steps, "views": args.views,
+           "config": bench_config("c3_dynamic_cone", spec["rays"]),
+           "data": "synthetic (seeded dynamic porous phantom, ray-marched front, Poisson noise)"}
+    runs = {}
+    for precision in ("plain_fp32", "mixed"):
+        cfg = workload_spec("c3_dynamic_cone", precision)["model"]
+        rec = fit(geometry, projs, list(angles), timesteps=list(ts), model_cfg=cfg, niter=args.psnr_steps, lr=1e-3,
+                  rays_per_batch=spec["rays"], points_per_ray=spec["S"], loss="l2", seed=0, device=dev,
+                  evaluate=evaluate, eval_every=args.eval_every)
+        runs[precision] = {"history": [(st, round(sec, 3), m["psnr"]) for st, sec, m in rec.history],
+                           "final_psnr": rec.history[-1][2]["psnr"], "train_seconds": rec.train_seconds}
+        del rec
+        torch.cuda.empty_cache()
+    target = runs["plain_fp32"]["final_psnr"] - 0.1
+    for r in runs.values():
+        hit = next(((st, sec) for st, sec, p_ in r["history"] if p_ >= target), None)
+        r["time_to_target_s"] = hit[1] if hit else None
+    out["runs"] = runs
+    out["target_psnr"] = target
+    out["psnr_gap_db"] = runs["mixed"]["final_psnr"] - runs["plain_fp32"]["final_psnr"]
+    out["value"] = runs["mixed"]["final_psnr"]
+    out["train_seconds_ratio"] = runs["plain_fp32"]["train_seconds"] / runs["mixed"]["train_seconds"]
+    print(json.dumps(out))
+
+
 def run_scan(args):
     """Continuous-scan training steps (nect/trainers/continous_scanning_trainer.py:
     85-140) on the 4D cone workload: each step's prediction averages k
@@ -840,6 +898,13 @@ if __name__ == "__main__":
         ap.add_argument("--steps", type=int, default=10)
         ap.add_argument("--warmup", type=int, default=3)
         run_scan(ap.parse_args())
+    elif "--psnr4d" in sys.argv:
+        ap = argparse.ArgumentParser()
+        ap.add_argument("--psnr4d", action="store_true")
+        ap.add_argument("--psnr-steps", type=int, default=240)
+        ap.add_argument("--views", type=int, default=60)
+        ap.add_argument("--eval-every", type=int, default=60)
+        run_psnr4d(ap.parse_args())
     elif "--psnr" in sys.argv:
         ap = argparse.ArgumentParser()
         ap.add_argument("--psnr", action="store_true")
