@@ -480,13 +480,13 @@ def main():
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     tensor_peak = float(peaks.get("bf16_tflops_sustained", 1400.0))
     peak_src = "of measured" if peaks else "of fallback"
-    traffic_step = {}
-    tfile = ROOT / "profiles" / "dram_bytes_per_step.txt"
+    traffic_step = {}   # DRAM bytes per step and kernel kind (an ncu capture of a small case, scaled per sample)
+    tfile = ROOT / "profiles" / "dram_bytes_per_sample.txt"
     if tfile.exists():
         for line in tfile.read_text().splitlines():
             f = line.split()
             if len(f) == 4 and not line.startswith("#") and f[:2] == [args.workload, args.precision]:
-                traffic_step[f[2]] = float(f[3])
+                traffic_step[f[2]] = float(f[3]) * per_step_samples
 
     l2_step = {}   # L2 bytes per step and kernel kind (lts__t_bytes.sum of an ncu capture, scaled per sample)
     lfile = ROOT / "profiles" / "l2_bytes_per_sample.txt"
