@@ -685,7 +685,8 @@ def run_serving(args):
     (serving cost does not depend on the values)."""
     from nect_b200.config import get_model
     from nect_b200.sampling import Geometry
-    from nect_b200.serving import QueryServer, Request, reproject, query_points, slice_items, volume_items
+    from nect_b200.serving import (QueryServer, Request, reproject, reproject_workspace_bytes, query_points,
+                                   slice_items, volume_items)
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -721,7 +722,42 @@ def run_serving(args):
             reqs.append(dict(kind="reproject", t=t, angle=float(rng.random() * 2 * math.pi)))
         else:
             reqs.append(dict(kind="volume", size=256, t=t))
-    srv = QueryServer(model, geometry, memory_budget=40 << 30, points_per_ray=S)
+    # the mixed model alone, one request at a time (GPU time of each class as the server launches it):
+    # the load the request stream offers is sum over classes of rate x share x time
+    alone = {}
+    srv_slow_blocks = args.slow_blocks or torch.cuda.get_device_properties(dev).multi_processor_count
+    for kind, n in (("slice", 10), ("reproject", 4), ("volume", 2)):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ms = []
+        for k in range(n + 1):
+            torch.cuda.synchronize()
+            e0.record()
+            if kind == "slice":
+                out = torch.empty(512, 512, device=dev)
+                query_points(model, slice_items(out, out.shape, 0.5))
+            elif kind == "reproject":
+                out = torch.empty(geometry.nDetector[0] * geometry.nDetector[1], device=dev)
+                ws = torch.empty(reproject_workspace_bytes(model, geometry, args.piece_pixels), dtype=torch.uint8,
+                                 device=dev)
+                P = out.numel()
+                for b in range(0, P, args.piece_pixels):
+                    reproject(model, geometry, 0.3 * k, 0.5, S, out=out, workspace=ws,
+                              pixels=(b, min(args.piece_pixels, P - b)), warpgroups=args.slow_warpgroups)
+            else:
+                out = torch.empty(256, 256, 256, device=dev)
+                query_points(model, volume_items(out, out.shape, 0.5), max_blocks=srv_slow_blocks)
+            e1.record()
+            torch.cuda.synchronize()
+            if k:
+                ms.append(e0.elapsed_time(e1))
+        alone[kind] = {"n": n, "mean_ms": float(np.mean(ms))}
+    mean_slice_points = float(np.mean(np.array([256, 384, 512, 768, 1024]) ** 2))
+    share = {"slice": 0.6, "reproject": 0.3, "volume": 0.1}
+    per_req_ms = {"slice": alone["slice"]["mean_ms"] * mean_slice_points / 512 ** 2,
+                  "reproject": alone["reproject"]["mean_ms"], "volume": alone["volume"]["mean_ms"]}
+    offered = args.serve_rate * sum(share[k] * per_req_ms[k] for k in share) / 1e3
+    srv = QueryServer(model, geometry, memory_budget=40 << 30, points_per_ray=S, piece_pixels=args.piece_pixels,
+                      slow_warpgroups=args.slow_warpgroups, slow_blocks=args.slow_blocks)
     warm = [srv.submit(Request(**d)) for d in reqs[:6]]
     for r in warm:
         r.event.wait(120)
@@ -774,6 +810,12 @@ def run_serving(args):
                      "p99_ms": float(np.percentile(s512, 99)) if s512.size else None,
                      "wait_p99_ms": float(np.percentile(w512, 99)) if w512.size else None},
         "one_at_a_time_plain_fp32": base,
+        "one_at_a_time_mixed_gpu_ms": alone,
+        "offered_gpu_load": offered, "offered_gpu_load_is": "GPU-seconds per second the request stream asks for "
+                                                            "(rate x class share x the class's GPU time alone); "
+                                                            "above 1 no schedule keeps up",
+        "server": {"piece_pixels": args.piece_pixels, "slow_warpgroups": args.slow_warpgroups,
+                   "slow_blocks": args.slow_blocks},
         "config": {"workload": "4D cone 512x512, 2^21 x 16 x 2 fp16, MLP 2x64 (bf16 tensor cores); requests: "
                                "60% slices 256^2-1024^2 axis/oblique, 30% re-projections 512^2 (S=512), "
                                "10% volumes 256^3, random t; 40 GB admission budget",
@@ -917,6 +959,9 @@ if __name__ == "__main__":
         ap.add_argument("--serve-rate", type=float, default=200.0)
         ap.add_argument("--serve-seconds", type=float, default=5.0)
         ap.add_argument("--serve-mix", default="full", choices=["full", "no_reproject"])
+        ap.add_argument("--piece-pixels", type=int, default=32768)
+        ap.add_argument("--slow-warpgroups", type=int, default=2)
+        ap.add_argument("--slow-blocks", type=int, default=None)
         run_serving(ap.parse_args())
     else:
         main()

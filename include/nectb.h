@@ -117,8 +117,11 @@ typedef struct NectbHashGrid {
  * NECTB_BF16 runs the tensor-core path (bf16 operands, fp32 accumulation).
  * The fused model, training and query calls take width 64 and 2 or 3 hidden
  * layers over a grid of 16 levels of 2 or 4 features (n_input 32 or 64) in
- * 3D or 4D; hidden activation ReLU on the tensor-core path, ReLU, LeakyReLU
- * or none on the SIMT path.  Other shapes return NECTB_ERR_INVALID. */
+ * 3D or 4D, and the reference's default static model (nect/cfg/static/
+ * hash_grid.yaml): 6 hidden layers over 19 levels of 4 features (n_input 76)
+ * in 3D; hidden activation ReLU on the tensor-core path (LeakyReLU too for
+ * the 19-level shape), ReLU, LeakyReLU or none on the SIMT path.  Other
+ * shapes return NECTB_ERR_INVALID. */
 typedef struct NectbMLP {
   int32_t n_input;
   int32_t n_hidden_layers;
@@ -232,6 +235,35 @@ int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* gr
                           float max_ray_distance_per_point, float max_distance_traveled,
                           float* out, void* workspace, size_t workspace_bytes, int32_t max_blocks,
                           void* stream);
+
+/* The detector pixels [pixel_begin, pixel_begin + pixel_count) of the same
+ * re-projection (row-major pixel index), written to out[pixel_begin ...]:
+ * a server splits a view into pieces of a few milliseconds so that
+ * latency-critical launches on higher-priority streams get SMs between them.
+ * Values are identical to the whole view's.  workspace:
+ * nectb_train_workspace_bytes(geometry, grid, mlp, pixel_count) bytes; a 4D
+ * mixed model with nectb_query_reproject_slice_bytes(grid, pixel_count) more
+ * bytes gathers 8 corners per level on a time slice at t, built in the
+ * workspace by each call, instead of the 16 of the 4D interpolation (the
+ * result agrees within fp16 rounding of the blended features).
+ * warpgroups_per_sm 1..4: the mixed forward runs one block of that many
+ * 128-thread warpgroups per SM (tensor memory is allocated in powers of two:
+ * 1 and 2 take 128 and 256 of an SM's 512 columns and leave the rest to
+ * query blocks on other streams, 3 and 4 take all of it); 0 = max_blocks'
+ * rule.
+ * No reference counterpart. */
+int nectb_query_reproject_range(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
+                                float angle_rad, float t, int32_t num_points_per_ray,
+                                float max_ray_distance_per_point, float max_distance_traveled,
+                                float* out, int32_t pixel_begin, int32_t pixel_count, void* workspace,
+                                size_t workspace_bytes, int32_t max_blocks, int32_t warpgroups_per_sm,
+                                void* stream);
+
+/* Extra workspace bytes that let nectb_query_reproject_range run a 4D mixed
+ * model on a time slice (0 for other models). */
+size_t nectb_query_reproject_slice_bytes(const NectbHashGrid* grid, const NectbMLP* mlp,
+                                         int32_t pixel_count);
 
 /* ---- fused training step ------------------------------------------------ */
 /* One batch of rays from one projection.  Fuses Projector.__call__

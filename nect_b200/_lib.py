@@ -195,6 +195,12 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_f32,
          c_f32, c_int, c_f32, c_f32, c_ptr, c_ptr, c_size, c_int, c_ptr],
     ),
+    "nectb_query_reproject_range": (
+        c_int,
+        [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_f32,
+         c_f32, c_int, c_f32, c_f32, c_ptr, c_int, c_int, c_ptr, c_size, c_int, c_int, c_ptr],
+    ),
+    "nectb_query_reproject_slice_bytes": (c_size, [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_int]),
     "nectb_train_error_word": (c_ptr, [ctypes.POINTER(NectbGeometry), c_int, c_ptr]),
     "nectb_train_rays": (c_int, [ctypes.POINTER(NectbGeometry), c_int, c_int, c_ptr, c_ptr, c_ptr, c_ptr, c_ptr]),
     "nectb_train_staging_bytes": (

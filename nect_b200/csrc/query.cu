@@ -315,11 +315,16 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
                    "hidden %d)", D, F, L, H);
 }
 
-extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
-                                     const void* grid_params, const float* mlp_params, float angle_rad, float t,
-                                     int32_t num_points_per_ray, float max_ray_distance_per_point,
-                                     float max_distance_traveled, float* out, void* workspace,
-                                     size_t workspace_size, int32_t max_blocks, void* stream) {
+namespace {
+
+// Pixels [begin, begin + count) of a re-projection at (angle, t), written to
+// out[begin ...].  stage: use the workspace past the base size (a 4D mixed
+// model's time slice).
+int reproject_range(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                    const void* grid_params, const float* mlp_params, float angle_rad, float t,
+                    int32_t num_points_per_ray, float max_ray_distance_per_point, float max_distance_traveled,
+                    float* out, int32_t begin, int32_t count, void* workspace, size_t workspace_size,
+                    int32_t max_blocks, int32_t warpgroups, bool stage, cudaStream_t s) {
   clear_error();
   if (int rc = validate_geometry(geometry)) return rc;
   GridDev g;
@@ -328,15 +333,17 @@ extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbH
   NECTB_REQUIRE(grid_params && mlp_params && out, "null pointer");
   NECTB_REQUIRE(num_points_per_ray >= 1 && max_distance_traveled > 0.f, "bad sampling parameters");
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
-  if (!workspace || workspace_size < workspace_bytes(P, P))
+  NECTB_REQUIRE(begin >= 0 && count >= 1 && (int64_t)begin + count <= P, "pixel range outside the detector");
+  NECTB_REQUIRE(warpgroups >= 0 && warpgroups <= 4, "warpgroups_per_sm must be 0..4");
+  if (!workspace || workspace_size < workspace_bytes(count, count))
     return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
-                     workspace_bytes(P, P));
+                     workspace_bytes(count, count));
   TrainArgs a;
-  a.perm = nullptr;  // every pixel, in pixel order
-  a.perm_len = P;
-  a.start = 0;
-  a.num_rays = P;
-  a.n_pixels = P;
+  a.perm = nullptr;  // the pixels begin, begin + 1, ... in pixel order
+  a.perm_len = count;
+  a.start = begin;
+  a.num_rays = count;
+  a.n_pixels = count;
   a.S = num_points_per_ray;
   a.angle = angle_rad;
   a.t = t;
@@ -349,15 +356,50 @@ extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbH
   a.loss_type = 2;
   a.loss_scale = 0.f;
   a.max_blocks = max_blocks;
-  Workspace ws = carve_workspace(workspace, P, P);
-  cudaStream_t s = (cudaStream_t)stream;
+  a.fwd_warpgroups = max_blocks > 0 ? 0 : warpgroups;
+  Workspace ws = carve_workspace(workspace, count, count, stage ? workspace_size : 0);
+  float* y = out + begin;
   float* loss = reinterpret_cast<float*>(ws.counters + 8);
   if (int rc = cuda_status(cudaMemsetAsync(ws.counters, 0, 64, s), "memset counters")) return rc;
-  if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)P * 4, s), "memset slots")) return rc;
+  if (int rc = cuda_status(cudaMemsetAsync(ws.slot, 0xFF, (size_t)count * 4, s), "memset slots")) return rc;
   {
     ProfScope ps(kProfRayPrep, s);
-    ray_prep_kernel<<<(unsigned)ceil_div(P, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters, out, loss);
+    ray_prep_kernel<<<(unsigned)ceil_div(count, 8), 256, 0, s>>>(*geometry, a, ws.rays, ws.slot, ws.counters, y,
+                                                                  loss);
   }
   if (int rc = launch_status("ray_prep_kernel")) return rc;
-  return train_forward_only(*geometry, g, *mlp, grid_params, mlp_params, a, ws, out, loss, s);
+  return train_forward_only(*geometry, g, *mlp, grid_params, mlp_params, a, ws, y, loss, s);
+}
+
+}  // namespace
+
+extern "C" int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                                     const void* grid_params, const float* mlp_params, float angle_rad, float t,
+                                     int32_t num_points_per_ray, float max_ray_distance_per_point,
+                                     float max_distance_traveled, float* out, void* workspace,
+                                     size_t workspace_size, int32_t max_blocks, void* stream) {
+  const int P = geometry ? geometry->nDetector[0] * geometry->nDetector[1] : 0;
+  return reproject_range(geometry, grid, mlp, grid_params, mlp_params, angle_rad, t, num_points_per_ray,
+                         max_ray_distance_per_point, max_distance_traveled, out, 0, P, workspace, workspace_size,
+                         max_blocks, 0, false, (cudaStream_t)stream);
+}
+
+extern "C" int nectb_query_reproject_range(const NectbGeometry* geometry, const NectbHashGrid* grid,
+                                           const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
+                                           float angle_rad, float t, int32_t num_points_per_ray,
+                                           float max_ray_distance_per_point, float max_distance_traveled,
+                                           float* out, int32_t pixel_begin, int32_t pixel_count, void* workspace,
+                                           size_t workspace_size, int32_t max_blocks, int32_t warpgroups_per_sm,
+                                           void* stream) {
+  return reproject_range(geometry, grid, mlp, grid_params, mlp_params, angle_rad, t, num_points_per_ray,
+                         max_ray_distance_per_point, max_distance_traveled, out, pixel_begin, pixel_count, workspace,
+                         workspace_size, max_blocks, warpgroups_per_sm, true, (cudaStream_t)stream);
+}
+
+extern "C" size_t nectb_query_reproject_slice_bytes(const NectbHashGrid* grid, const NectbMLP* mlp,
+                                                    int32_t pixel_count) {
+  GridDev g;
+  if (!grid || !mlp || pixel_count < 1 || !make_grid_dev(grid, &g)) return 0;
+  if (g.n_dims != 4 || mlp->compute_dtype == NECTB_F32 || grid->feature_dtype != NECTB_F16) return 0;
+  return slice_half_bytes(g) + 256;
 }

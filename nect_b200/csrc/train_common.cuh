@@ -47,6 +47,9 @@ struct TrainArgs {
   int loss_type;
   float loss_scale;
   int max_blocks;  // > 0: cap on the persistent grids (queries); 0: default
+  // > 0: the forward runs one block of this many warpgroups per SM under the
+  // shared-SM carveout (re-projection pieces beside serving kernels); 0: the tuning's
+  int fwd_warpgroups = 0;
   int phase = kPhaseForward | kPhaseBackward;  // which half of the step to run
   float run_threshold = 0.75f;                 // run merging of the scatter (set from the tuning)
   // Continuous scan (sub > 1): num_rays = sub * (pixels of the batch) virtual
@@ -231,6 +234,11 @@ inline TimeSlice make_time_slice(const GridDev& g, float t) {
 inline size_t slice_bytes(const GridDev& g) {
   const int64_t n3 = make_time_slice(g, 0.f).g3.total_entries;
   return align256((size_t)n3 * g.n_features * 2) + align256((size_t)n3 * g.n_features * 4);
+}
+
+// Bytes of the fp16 time slice alone (forward-only queries).
+inline size_t slice_half_bytes(const GridDev& g) {
+  return align256((size_t)make_time_slice(g, 0.f).g3.total_entries * g.n_features * 2);
 }
 
 // Warp per ray: set-up, sample count (warp ballot), measured value, scale;

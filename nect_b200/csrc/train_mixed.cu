@@ -935,16 +935,27 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   if constexpr (D == 4) {
     // Training with staging: the 3D kernels on the time slice at the batch's t
     // (queries and steps without staging room keep the 4D kernels).  The slice
-    // and its gradient sit at the end of the staging region.
-    const size_t sb = slice_bytes(grid);
-    if (tune.time_slice && args.max_blocks == 0 && ws.stage &&
-        ws.stage_bytes >= sb + order_bytes(args.num_rays, args.n_pixels) + (size_t(1) << 20)) {
+    // and its gradient sit at the end of the staging region.  A re-projection
+    // piece (forward only, fwd_warpgroups > 0) builds only the fp16 slice, at
+    // the start of its staging region, and runs without staging.
+    const bool piece = args.fwd_warpgroups > 0 && !table_grad;
+    const size_t sb = piece ? slice_half_bytes(grid) : slice_bytes(grid);
+    const size_t need = piece ? sb : sb + order_bytes(args.num_rays, args.n_pixels) + (size_t(1) << 20);
+    if (tune.time_slice && args.max_blocks == 0 && ws.stage && ws.stage_bytes >= need) {
       const TimeSlice ts = make_time_slice(grid, args.t);
       const int64_t n3 = ts.g3.total_entries;
       Workspace ws3 = ws;
-      ws3.stage_bytes = (ws.stage_bytes - sb) & ~size_t(255);
-      __half* t3 = reinterpret_cast<__half*>(reinterpret_cast<char*>(ws.stage) + ws3.stage_bytes);
-      float* g3 = reinterpret_cast<float*>(reinterpret_cast<char*>(t3) + align256((size_t)n3 * F * 2));
+      __half* t3;
+      if (piece) {
+        t3 = reinterpret_cast<__half*>(ws.stage);
+        ws3.stage = nullptr;
+        ws3.stage_bytes = 0;
+      } else {
+        ws3.stage_bytes = (ws.stage_bytes - sb) & ~size_t(255);
+        t3 = reinterpret_cast<__half*>(reinterpret_cast<char*>(ws.stage) + ws3.stage_bytes);
+      }
+      float* g3 =
+          piece ? nullptr : reinterpret_cast<float*>(reinterpret_cast<char*>(t3) + align256((size_t)n3 * F * 2));
       int64_t max_level = 0;
       for (int l = 0; l < grid.n_levels; ++l) max_level = std::max(max_level, ts.n_real[l] + 8);
       const dim3 sgrid((unsigned)std::min<int64_t>(ceil_div(max_level, 256), 1024), (unsigned)grid.n_levels);
@@ -977,8 +988,12 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   a.run_threshold = D == 4 ? tune.run_threshold_4d : tune.run_threshold_3d;
   const size_t group_bytes = (size_t)tune.scatter_group_bytes;
   // forward: one block of `wgs` warpgroups per SM when training; queries
-  // (which share SMs with serving kernels) one warpgroup per block
-  const int wgs = a.max_blocks > 0 ? 1 : std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM);
+  // (which share SMs with serving kernels) one warpgroup per block, or the
+  // caller's warpgroups per SM
+  const bool shares_sms = a.max_blocks > 0 || a.fwd_warpgroups > 0;
+  const int wgs = a.max_blocks > 0       ? 1
+                  : a.fwd_warpgroups > 0 ? std::min(a.fwd_warpgroups, kFwdBlocksPerSM)
+                                         : std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM);
   int fblocks = a.max_blocks > 0
                     ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
                                                 (int)ceil_div(a.num_rays, 4)))
@@ -997,7 +1012,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // input rows with their zero padding), then dL/d(encoding) of one round of
   // per_round rays
   const StageLayout SL = stage_layout(ws, R, a.n_pixels, a.S, Shape::INP * sizeof(__nv_bfloat16),
-                                      (size_t)a.S * IN * sizeof(float), tune.staged_rounds, tune.encoding_store != 0);
+                                      (size_t)a.S * IN * sizeof(float), tune.staged_rounds,
+                                      tune.encoding_store != 0 && !shares_sms);
   auto run_order = [&]() -> int {
     ProfScope ps(kProfOrder, s);
     const int n_blocks = order_blocks(R, a.n_pixels);
@@ -1015,7 +1031,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     auto k = fwd_mixed_kernel<D, F, L, H, ACT>;
     const size_t smem = 1024 + (KT + H - 1) * kWTile + wgs * KT * kTile + 64 * 4 + kFwdBlocksPerSM * 8 + 16 +
                         4 * kFwdBlocksPerSM * 4;
-    set_smem(k, smem, a.max_blocks > 0);
+    set_smem(k, smem, shares_sms);
     {
       ProfScope ps(kProfForward, s);
       k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,

@@ -32,14 +32,19 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
   const int n_batch = a.num_rays / a.sub;
   const int j = tid / n_batch, rb = tid - j * n_batch;
   const float angle = a.sub > 1 ? a.sub_angle[j] : a.angle;
-  // perm == nullptr: every detector pixel in order (re-projection queries);
-  // jitter / detector offsets default to 0 when absent.
+  // perm == nullptr: the detector pixels start, start + 1, ... in order
+  // (re-projection queries, whole views or pieces of them; the slots are
+  // indexed from the first pixel); jitter / detector offsets default to 0
+  // when absent.
   bool ok;
+  int sidx;  // scheduling slot of the ray's pixel
   if (a.perm) {
     ok = ray_lookup(a.perm, a.perm_len, a.start, rb, n_batch, g, ray_index);
+    sidx = ray_index;
   } else {
-    ray_index = tid;
+    ray_index = (int)a.start + tid;
     ok = tid < a.n_pixels;
+    sidx = tid;
   }
   if (ok)
     ray_setup(g, ray_index, a.det_off ? a.det_off[2 * (int64_t)tid] : 0.f,
@@ -63,7 +68,7 @@ __global__ void ray_prep_kernel(NectbGeometry g, TrainArgs a, RayRec* __restrict
     rec.y = (in_range && a.projection) ? a.projection[ray_index] : 0.f;
     rec.gsig = 0.f;
     if (count > 0) {
-      if (atomicCAS(slot + (int64_t)ray_index * a.sub + j, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
+      if (atomicCAS(slot + (int64_t)sidx * a.sub + j, -1, tid) != -1) atomicOr(ctrl + 3, kFlagDuplicatePixels);
     } else {
       // no samples: y_pred = 0 (the reference's zero attenuation sum)
       y_pred[tid] = 0.f;

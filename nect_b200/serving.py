@@ -111,8 +111,10 @@ def _call_points(model: _HashGridModel, items_dev: int, n_items: int, total_chun
     _lib.check(rc, "nectb_query_points")
 
 
-def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.Stream | None = None):
-    """Evaluate the items (any requests) in one launch (outputs written in place)."""
+def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.Stream | None = None,
+                 max_blocks: int = 0):
+    """Evaluate the items (any requests) in one launch (outputs written in place);
+    max_blocks > 0 caps the persistent grid."""
     if items.size == 0:
         return
     stream = stream or torch.cuda.current_stream()
@@ -125,31 +127,60 @@ def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.St
         buf[items.nbytes:].zero_()   # work cursor and error word
         buf[:items.nbytes].copy_(torch.from_numpy(items.view(np.uint8)), non_blocking=False)
         _call_points(model, buf.data_ptr(), items.size, int(ch.sum()), buf.data_ptr() + items.nbytes,
-                     stream.cuda_stream)
+                     stream.cuda_stream, max_blocks)
+
+
+def reproject_workspace_bytes(model: _HashGridModel, geometry, pixels: int | None = None) -> int:
+    """Workspace of a re-projection of ``pixels`` detector pixels (default the
+    whole view) by pieces: the sampler's workspace plus, for a 4D mixed model,
+    room for the time slice."""
+    cg = geometry.get_c_geometry()
+    n = pixels or geometry.nDetector[0] * geometry.nDetector[1]
+    return int(_lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
+                                                    ctypes.byref(model.mlp_desc), n)
+               + _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(model.grid_desc),
+                                                            ctypes.byref(model.mlp_desc), n))
 
 
 def reproject(model: _HashGridModel, geometry, angle: float, t: float = 0.0, points_per_ray: int | None = None,
               out: torch.Tensor | None = None, workspace: torch.Tensor | None = None,
-              stream: torch.cuda.Stream | None = None, max_blocks: int = 0) -> torch.Tensor:
-    """Detector view [nDetector] at (angle, t): sum of sigma * distance / max_distance_traveled per ray."""
+              stream: torch.cuda.Stream | None = None, max_blocks: int = 0, pixels: tuple[int, int] | None = None,
+              warpgroups: int = 0) -> torch.Tensor:
+    """Detector view [nDetector] at (angle, t): sum of sigma * distance / max_distance_traveled per ray.
+
+    pixels=(begin, count) computes only those detector pixels (row-major) of
+    ``out``; warpgroups (1-4) sets the mixed forward's warpgroups per SM, and
+    such a call runs a 4D mixed model on a time slice at t when the
+    workspace has room for it (reproject_workspace_bytes)."""
     cg = geometry.get_c_geometry()
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
     P = geometry.nDetector[0] * geometry.nDetector[1]
     dev = model.table.device
     if out is None:
         out = torch.empty(P, device=dev)
-    need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
-                                                ctypes.byref(model.mlp_desc), P)
-    if workspace is None or workspace.numel() < need:
-        workspace = torch.empty(need, dtype=torch.uint8, device=dev)
     stream = stream or torch.cuda.current_stream()
-    rc = _lib.lib.nectb_query_reproject(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
-                                        ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
-                                        model.mlp.data_ptr(), float(angle), float(t), S,
-                                        geometry.max_distance_traveled / S, geometry.max_distance_traveled,
-                                        out.data_ptr(), workspace.data_ptr(), workspace.numel(), int(max_blocks),
-                                        stream.cuda_stream)
-    _lib.check(rc, "nectb_query_reproject")
+    if pixels is None and not warpgroups:
+        need = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
+                                                    ctypes.byref(model.mlp_desc), P)
+        if workspace is None or workspace.numel() < need:
+            workspace = torch.empty(need, dtype=torch.uint8, device=dev)
+        rc = _lib.lib.nectb_query_reproject(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
+                                            ctypes.byref(model.mlp_desc), model.grid_table.data_ptr(),
+                                            model.mlp.data_ptr(), float(angle), float(t), S,
+                                            geometry.max_distance_traveled / S, geometry.max_distance_traveled,
+                                            out.data_ptr(), workspace.data_ptr(), workspace.numel(), int(max_blocks),
+                                            stream.cuda_stream)
+        _lib.check(rc, "nectb_query_reproject")
+    else:
+        begin, count = pixels or (0, P)
+        if workspace is None:
+            workspace = torch.empty(reproject_workspace_bytes(model, geometry, count), dtype=torch.uint8, device=dev)
+        rc = _lib.lib.nectb_query_reproject_range(
+            ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc),
+            model.grid_table.data_ptr(), model.mlp.data_ptr(), float(angle), float(t), S,
+            geometry.max_distance_traveled / S, geometry.max_distance_traveled, out.data_ptr(), int(begin), int(count),
+            workspace.data_ptr(), workspace.numel(), int(max_blocks), int(warpgroups), stream.cuda_stream)
+        _lib.check(rc, "nectb_query_reproject_range")
     return out.view(geometry.nDetector[0], geometry.nDetector[1])
 
 
@@ -287,16 +318,21 @@ class QueryServer:
     free (admission by memory); nothing is allocated while serving.
 
     Slices run on ``n_fast`` high-priority lanes, packed several requests per
-    launch.  Volumes and re-projections share ``n_slow`` low-priority lanes
-    whose persistent grids are capped at ``slow_blocks`` (default one block
-    per SM): with one background lane an SM keeps room for a slice block while
-    background work runs, which is what keeps slice p99 near its unloaded
-    latency."""
+    launch.  Volumes and re-projections share ``n_slow`` low-priority lanes.
+    Volume launches are persistent grids capped at ``slow_blocks`` (default
+    one block per SM): an SM keeps room for slice blocks while background
+    work runs, which is what keeps slice p99 near its unloaded latency.  A
+    re-projection runs as pieces of ``piece_pixels`` detector pixels, each a
+    launch of a few milliseconds with ``slow_warpgroups`` warpgroups per SM
+    (2 take half of an SM's tensor memory and leave the other half to slice
+    blocks; a 4D mixed model runs on a time slice at the request's t), so a
+    slice waits at most one piece for SMs."""
 
     def __init__(self, model: _HashGridModel, geometry, memory_budget: int = 40 << 30, n_fast: int = 2,
                  n_slow: int = 1, minimum: float = 0.0, maximum: float = 1.0, points_per_ray: int | None = None,
                  slow_blocks: int | None = None, max_slice: int = 1024, max_volume: int = 256,
-                 slot_mix=(0.25, 0.25, 0.5), max_slots: int = 64):
+                 slot_mix=(0.25, 0.25, 0.5), max_slots: int = 64, piece_pixels: int = 32768,
+                 slow_warpgroups: int = 2):
         self.model = model
         self.geometry = geometry
         self.dev = model.table.device
@@ -304,15 +340,18 @@ class QueryServer:
         self.points_per_ray = points_per_ray
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
         self.slow_blocks = slow_blocks if slow_blocks is not None else sms
+        if not 1 <= slow_warpgroups <= 4 or piece_pixels < 1:
+            raise ValueError("slow_warpgroups must be 1..4 and piece_pixels positive")
+        self.slow_warpgroups = slow_warpgroups
         lo, hi = torch.cuda.Stream.priority_range()
         self.fast = [_Lane(self.dev, priority=hi) for _ in range(n_fast)]
         self.slow = [_Lane(self.dev, priority=lo, max_blocks=self.slow_blocks) for _ in range(n_slow)]
         for ln in self.fast + self.slow:
             ln.capture(model)
-        cg = geometry.get_c_geometry()
         P = geometry.nDetector[0] * geometry.nDetector[1]
-        ws = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), ctypes.byref(model.grid_desc),
-                                                  ctypes.byref(model.mlp_desc), P)
+        self.n_pixels = P
+        self.piece_pixels = min(piece_pixels, P)
+        ws = (reproject_workspace_bytes(model, geometry, self.piece_pixels) + 255) // 256 * 256
         per = {"slice": 8 * max_slice ** 2, "volume": 8 * max_volume ** 3, "reproject": 8 * P + ws}
         nslots = {k: max(1, min(max_slots, int(memory_budget * f // per[k])))
                   for k, f in zip(("slice", "reproject", "volume"), slot_mix)}
@@ -470,25 +509,20 @@ class QueryServer:
                         self._finish_on(st, ln)
                         slices.remove(st)
                         flying.append(st)
-            # background: one launch per idle slow lane, oldest request first
+            # background: one launch per idle slow lane, oldest request first;
+            # a re-projection's pieces run in order on the lane of its first piece
             while reprojs or volumes:
                 ln = self._lane("slow", want_idle=True)
                 if ln is None:
                     break
-                if reprojs and (not volumes or reprojs[0]["req"].arrival <= volumes[0]["req"].arrival):
-                    st = reprojs.pop(0)
-                    r, pool = st["req"], self.pools["reproject"]
-                    with torch.cuda.stream(ln.stream):
-                        reproject(self.model, self.geometry, r.angle, r.t, self.points_per_ray,
-                                  out=pool.dev_buf[st["slot"]], workspace=pool.ws[st["slot"]], stream=ln.stream,
-                                  max_blocks=self.slow_blocks)
-                        ev = torch.cuda.Event()
-                        ev.record(ln.stream)
-                    ln.last = ev
-                    r.launched = time.perf_counter()
-                    st["events"].append(ev)
-                    self._finish_on(st, ln)
-                    flying.append(st)
+                st = next((x for x in reprojs if x.get("lane") in (None, ln)), None)
+                if st is not None and (not volumes or st["req"].arrival <= volumes[0]["req"].arrival):
+                    if self._reproject_piece(st, ln):
+                        reprojs.remove(st)
+                        self._finish_on(st, ln)
+                        flying.append(st)
+                elif not volumes:
+                    break
                 else:
                     batch, touched = self._pack(volumes, 4096)
                     ev = ln.launch(batch)
@@ -507,6 +541,28 @@ class QueryServer:
                     self._done_q.put(st)
             if self.queue.empty() and not slices and (flying or reprojs or volumes or waiting):
                 time.sleep(0.0001)
+
+    def _reproject_piece(self, st: dict, ln: _Lane) -> bool:
+        """Launches the next piece of a re-projection on lane ln; True when it
+        was the last one."""
+        r, pool = st["req"], self.pools["reproject"]
+        begin = st.get("next", 0)
+        count = min(self.piece_pixels, self.n_pixels - begin)
+        with torch.cuda.stream(ln.stream):
+            reproject(self.model, self.geometry, r.angle, r.t, self.points_per_ray, out=pool.dev_buf[st["slot"]],
+                      workspace=pool.ws[st["slot"]], stream=ln.stream, pixels=(begin, count),
+                      warpgroups=self.slow_warpgroups)
+            ev = torch.cuda.Event()
+            ev.record(ln.stream)
+        ln.last = ev
+        if begin == 0:
+            r.launched = time.perf_counter()
+            st["lane"] = ln
+        st["next"] = begin + count
+        if st["next"] < self.n_pixels:
+            return False
+        st["events"].append(ev)
+        return True
 
     def device_errors(self) -> int:
         """OR of the error words of every lane (0 = no tensor-core wait timed out)."""

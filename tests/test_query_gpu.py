@@ -7,9 +7,13 @@ Tolerances vs the fp64 oracle: plain fp32 model 1e-5 relative to the largest
 value; mixed model (bf16 tensor-core MLP) 2e-2.
 """
 
+import ctypes
+
 import numpy as np
 import pytest
 import torch
+
+from nect_b200 import _lib
 
 from oracle import hashgrid as ohg
 from oracle import sampling as osamp
@@ -87,6 +91,11 @@ def test_reprojection_matches_oracle(cuda_device, precision):
     angle, t, S = 0.8, 0.6, 64
     view = serving.reproject(m, geo, angle, t, S)
     torch.cuda.synchronize()
+    assert rel(view.cpu(), oracle_view(m, geo, levels, angle, t, S)) < TOL[precision]
+
+
+def oracle_view(m, geo, levels, angle, t, S):
+    """The re-projection from the oracle's sampler and fp64 model."""
     cg = geo.get_c_geometry()
     P = geo.nDetector[0] * geo.nDetector[1]
     a = torch.tensor([angle, 0.0], dtype=torch.float32, device="cuda")
@@ -98,8 +107,45 @@ def test_reprojection_matches_oracle(cuda_device, precision):
     keep = ~np.all(np.clip(pts, 0, 1).reshape(-1, 3) == 0, axis=1)
     sig = np.zeros(P * S)
     sig[keep] = oracle_sigma(m, levels, np.clip(pts, 0, 1).reshape(-1, 3)[keep], t).numpy()
-    ref = sig.reshape(P, S).sum(1) * dist / geo.max_distance_traveled
-    assert rel(view.cpu(), ref) < TOL[precision]
+    return sig.reshape(P, S).sum(1) * dist / geo.max_distance_traveled
+
+
+@pytest.mark.parametrize("precision,n_dims", [("plain_fp32", 4), ("mixed", 3), ("mixed", 4)])
+def test_reprojection_pieces_match_the_whole_view(cuda_device, precision, n_dims):
+    """A view computed in pieces (nectb_query_reproject_range, 1, 3 and 4
+    warpgroups per SM) equals the whole view bit for bit where both gather the
+    same table.  With room for a time slice a 4D mixed model gathers 8 corners
+    on the slice at t: that view agrees with the 16-corner one within 1e-2 and
+    with the oracle within the mixed tolerance."""
+    from nect_b200 import serving
+
+    m, geo, levels = model_and_geometry(precision, n_dims)
+    angle, t, S = 0.8, 0.6, 64
+    whole = serving.reproject(m, geo, angle, t, S).flatten().clone()
+    P = whole.numel()
+    piece = 500
+    sliced = n_dims == 4 and precision == "mixed"
+    cg = geo.get_c_geometry()
+    base = _lib.lib.nectb_train_workspace_bytes(ctypes.byref(cg.c_struct), None, None, piece)
+    for wg in (1, 3, 4):
+        for room in ((False, True) if sliced else (False,)):
+            nbytes = serving.reproject_workspace_bytes(m, geo, piece) if room else base
+            ws = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+            out = torch.full((P,), float("nan"), device="cuda")
+            for b in range(0, P, piece):
+                serving.reproject(m, geo, angle, t, S, out=out, workspace=ws, pixels=(b, min(piece, P - b)),
+                                  warpgroups=wg)
+            torch.cuda.synchronize()
+            assert not torch.isnan(out).any()
+            if room:
+                assert rel(out.cpu(), whole.cpu()) < 1e-2
+            else:
+                assert torch.equal(out, whole), (wg, room)
+    if sliced:
+        one = serving.reproject(m, geo, angle, t, S, warpgroups=3).flatten()   # one piece, slice room included
+        torch.cuda.synchronize()
+        assert rel(one.cpu(), whole.cpu()) < 1e-2
+        assert rel(one.cpu(), oracle_view(m, geo, levels, angle, t, S)) < TOL[precision]
 
 
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
@@ -114,7 +160,7 @@ def test_server_results_same_alone_and_in_mix(cuda_device, precision):
         reqs.append(dict(kind=kind, t=float(rng.random()), size=int(rng.choice([40, 64, 96])) if kind != "volume"
                          else 24, angle=float(rng.random() * 6.28),
                          centre=tuple(rng.random(3) * 0.4 + 0.3), u=(0.0, 0.0, 1.0), v=(0.0, 1.0, 0.0)))
-    srv = QueryServer(m, geo, memory_budget=256 << 20, points_per_ray=64)
+    srv = QueryServer(m, geo, memory_budget=256 << 20, points_per_ray=64, piece_pixels=700)   # 3 pieces a view
     alone = []
     for d in reqs:  # one at a time
         r = srv.submit(Request(**d))
