@@ -121,14 +121,11 @@ def make_projections(spec, geometry, n_proj: int, device, seed: int = 0):
         ph = phantoms.ellipsoid_phantom(20, seed, size=geometry.sVoxel[0])   # the large 4D workload: 1024 voxels
         projs = torch.stack([phantoms.ellipsoid_projection(ph, geometry, float(a), device) for a in angles])
     elif spec["phantom"] == "dynamic":
-        # each projection at its own t; Poisson noise at 1e4 incident photons on the attenuation
-        # expressed per object width (p / n), so that exp(-p) stays in the detector's range
+        # each projection at its own t; Poisson noise at 1e4 incident photons
         ph = phantoms.dynamic_porous(geometry.nVoxel[0], seed=seed, attempts=8000)
         projs = torch.stack([phantoms.dynamic_porous_projection(ph, geometry, float(a), float(t), device)
                              for a, t in zip(angles, ts)])
-        gen = torch.Generator(device=projs.device).manual_seed(seed)
-        counts = torch.poisson(1e4 * torch.exp(-projs.double() / geometry.nVoxel[0]), generator=gen)
-        projs = (-torch.log(torch.clamp(counts, min=1.0) / 1e4) * geometry.nVoxel[0]).float()
+        projs = phantoms.poisson_projections(projs, geometry.nVoxel[0], seed=seed)
     else:
         ph = phantoms.porous_phantom(geometry.nVoxel[0], seed=seed, attempts=8000)
         projs = torch.stack([phantoms.porous_projection(ph, geometry, float(a), device) for a in angles])
@@ -685,8 +682,8 @@ def run_serving(args):
     (serving cost does not depend on the values)."""
     from nect_b200.config import get_model
     from nect_b200.sampling import Geometry
-    from nect_b200.serving import (QueryServer, Request, reproject, reproject_workspace_bytes, query_points,
-                                   slice_items, volume_items)
+    from nect_b200.serving import (QueryServer, Request, query_points, reproject, reproject_workspace_bytes,
+                                   slice_items, time_slice, time_slice_bytes, volume_items)
 
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
@@ -726,6 +723,12 @@ def run_serving(args):
     # the load the request stream offers is sum over classes of rate x share x time
     alone = {}
     srv_slow_blocks = args.slow_blocks or torch.cuda.get_device_properties(dev).multi_processor_count
+    P = geometry.nDetector[0] * geometry.nDetector[1]
+    out_s, out_r, out_v = (torch.empty(512, 512, device=dev), torch.empty(P, device=dev),
+                           torch.empty(256, 256, 256, device=dev))
+    items_s, items_v = slice_items(out_s, out_s.shape, 0.5), volume_items(out_v, out_v.shape, 0.5)
+    ws_r = torch.empty(reproject_workspace_bytes(model, geometry, args.piece_pixels), dtype=torch.uint8, device=dev)
+    slc = torch.empty(max(time_slice_bytes(model), 1), dtype=torch.uint8, device=dev)
     for kind, n in (("slice", 10), ("reproject", 4), ("volume", 2)):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ms = []
@@ -733,19 +736,16 @@ def run_serving(args):
             torch.cuda.synchronize()
             e0.record()
             if kind == "slice":
-                out = torch.empty(512, 512, device=dev)
-                query_points(model, slice_items(out, out.shape, 0.5))
+                query_points(model, items_s)
             elif kind == "reproject":
-                out = torch.empty(geometry.nDetector[0] * geometry.nDetector[1], device=dev)
-                ws = torch.empty(reproject_workspace_bytes(model, geometry, args.piece_pixels), dtype=torch.uint8,
-                                 device=dev)
-                P = out.numel()
                 for b in range(0, P, args.piece_pixels):
-                    reproject(model, geometry, 0.3 * k, 0.5, S, out=out, workspace=ws,
+                    reproject(model, geometry, 0.3 * k, 0.5, S, out=out_r, workspace=ws_r,
                               pixels=(b, min(args.piece_pixels, P - b)), warpgroups=args.slow_warpgroups)
+            elif time_slice_bytes(model):   # as the server: the time slice at t, then the items on it
+                time_slice(model, 0.5, out=slc)
+                query_points(model, items_v, max_blocks=srv_slow_blocks, slice=slc)
             else:
-                out = torch.empty(256, 256, 256, device=dev)
-                query_points(model, volume_items(out, out.shape, 0.5), max_blocks=srv_slow_blocks)
+                query_points(model, items_v, max_blocks=srv_slow_blocks)
             e1.record()
             torch.cuda.synchronize()
             if k:
@@ -846,9 +846,7 @@ def run_psnr4d(args):
     ph = phantoms.dynamic_porous(n, seed=0)
     projs = torch.stack([phantoms.dynamic_porous_projection(ph, geometry, float(a), float(t), dev)
                          for a, t in zip(angles, ts)])
-    gen = torch.Generator(device=dev).manual_seed(0)
-    counts = torch.poisson(1e4 * torch.exp(-projs.double() / n), generator=gen)
-    projs = (-torch.log(torch.clamp(counts, min=1.0) / 1e4) * n).float()
+    projs = phantoms.poisson_projections(projs, n, seed=0)
     t_eval = (0.2, 0.5, 0.8)
     truths = {t: phantoms.dynamic_porous_volume(ph, n, t, dev) for t in t_eval}
 
@@ -959,8 +957,8 @@ if __name__ == "__main__":
         ap.add_argument("--serve-rate", type=float, default=200.0)
         ap.add_argument("--serve-seconds", type=float, default=5.0)
         ap.add_argument("--serve-mix", default="full", choices=["full", "no_reproject"])
-        ap.add_argument("--piece-pixels", type=int, default=32768)
-        ap.add_argument("--slow-warpgroups", type=int, default=2)
+        ap.add_argument("--piece-pixels", type=int, default=16384)
+        ap.add_argument("--slow-warpgroups", type=int, default=4)
         ap.add_argument("--slow-blocks", type=int, default=None)
         run_serving(ap.parse_args())
     else:

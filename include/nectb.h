@@ -221,6 +221,27 @@ int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const voi
                        const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
                        int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream);
 
+/* Time slice of a 4D model with an fp16 table: per level, the blend of the
+ * two time vertices at t of every entry, w0 * table[e0] + w1 * table[e1]
+ * rounded to fp16, in a 3D layout (hashed levels keep the 4D level's hash
+ * without its t term; dense levels hold the (res+1)^3 vertices, rounded up
+ * to 8 entries).  Queries at that t then gather 8 corners per level instead
+ * of 16 (nectb_query_points_slice); the values differ from the 4D
+ * interpolation by the fp16 rounding of the blend.  slice_bytes >=
+ * nectb_time_slice_bytes(grid), which is 0 for grids without a slice.
+ * t in [0, 1].  No reference counterpart (tiny-cuda-nn interpolates the 16
+ * corners). */
+size_t nectb_time_slice_bytes(const NectbHashGrid* grid);
+int nectb_time_slice(const NectbHashGrid* grid, const void* grid_params, float t, void* slice,
+                     size_t slice_bytes, void* stream);
+
+/* nectb_query_points on the time slice of a 4D grid (grid describes the 4D
+ * model; the items' t is ignored: every point is evaluated at the slice's t). */
+int nectb_query_points_slice(const NectbHashGrid* grid, const NectbMLP* mlp, const void* slice,
+                             const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
+                             int64_t total_chunks, unsigned int* counter, int32_t max_blocks,
+                             void* stream);
+
 /* Re-projection of the model: line integrals for every detector pixel of a
  * view at (angle, t), y[p] = sum_s sigma * distances/max_distance_traveled
  * with the training sampler (no jitter, no detector offset), i.e. the

@@ -190,6 +190,13 @@ _SIGNATURES = {
         [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_int, c_i64, c_ptr, c_int,
          c_ptr],
     ),
+    "nectb_time_slice_bytes": (c_size, [ctypes.POINTER(NectbHashGrid)]),
+    "nectb_time_slice": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_f32, c_ptr, c_size, c_ptr]),
+    "nectb_query_points_slice": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_int, c_i64, c_ptr, c_int,
+         c_ptr],
+    ),
     "nectb_query_reproject": (
         c_int,
         [ctypes.POINTER(NectbGeometry), ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_f32,

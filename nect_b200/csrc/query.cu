@@ -22,6 +22,7 @@ int validate_mlp(const NectbMLP* m, const GridDev& g);
 int64_t mlp_param_count(const NectbMLP* m);
 int train_forward_only(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& mlp, const void* table,
                        const float* W, const TrainArgs& a, Workspace ws, float* y_pred, float* loss, cudaStream_t s);
+int launch_time_slice(const GridDev& grid, const __half* table, float t, __half* slice, cudaStream_t s);
 
 namespace {
 
@@ -269,24 +270,24 @@ int launch_query_plain(const GridDev& g, const void* table, const float* W, cons
 
 using namespace nectb;
 
-extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
-                                  const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
-                                  int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream) {
-  clear_error();
-  GridDev g;
-  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+namespace {
+
+// Items of one launch on grid g (a 3D or 4D table, or the 3D view of a 4D
+// table's time slice).
+int query_points_impl(const GridDev& g, bool f16_table, const NectbMLP* mlp, const void* grid_params,
+                      const float* mlp_params, const NectbQueryItem* items, int32_t n_items, int64_t total_chunks,
+                      unsigned int* counter, int32_t max_blocks, cudaStream_t s) {
   if (int rc = validate_mlp(mlp, g)) return rc;
   if (n_items == 0 || total_chunks == 0) return NECTB_OK;
   NECTB_REQUIRE(grid_params && mlp_params && items && counter && n_items > 0 && total_chunks > 0,
                 "null pointer or empty query");
   NECTB_REQUIRE(total_chunks < (int64_t(1) << 31), "too many chunks in one launch");
-  cudaStream_t s = (cudaStream_t)stream;
   if (int rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s), "memset query counter")) return rc;
   const int D = g.n_dims, F = g.n_features, L = g.n_levels, H = mlp->n_hidden_layers;
   const int act = mlp->activation, oact = mlp->output_activation;
   const bool mixed = mlp->compute_dtype != NECTB_F32;
   if (mixed) {
-    NECTB_REQUIRE(grid->feature_dtype == NECTB_F16, "mixed queries need an fp16 table");
+    NECTB_REQUIRE(f16_table, "mixed queries need an fp16 table");
     NECTB_REQUIRE(H >= 2, "mixed queries need at least 2 hidden layers");
     const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto h) {
       if (act == NECTB_ACT_RELU)
@@ -302,17 +303,69 @@ extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp
     });
     if (rc != kUnsupportedShape) return rc;
   } else {
-    const bool h = grid->feature_dtype == NECTB_F16;
     const int rc = dispatch_shape(D, F, L, H, [&](auto d, auto f, auto l, auto hl) {
-      return h ? launch_query_plain<d(), f(), __half, l(), hl()>(g, grid_params, mlp_params, items, n_items,
-                                                                 total_chunks, counter, act, oact, max_blocks, s)
-               : launch_query_plain<d(), f(), float, l(), hl()>(g, grid_params, mlp_params, items, n_items,
-                                                                total_chunks, counter, act, oact, max_blocks, s);
+      return f16_table ? launch_query_plain<d(), f(), __half, l(), hl()>(g, grid_params, mlp_params, items, n_items,
+                                                                         total_chunks, counter, act, oact,
+                                                                         max_blocks, s)
+                       : launch_query_plain<d(), f(), float, l(), hl()>(g, grid_params, mlp_params, items, n_items,
+                                                                        total_chunks, counter, act, oact,
+                                                                        max_blocks, s);
     });
     if (rc != kUnsupportedShape) return rc;
   }
   return set_error(NECTB_ERR_INVALID, "queries: unsupported configuration (n_dims %d, n_features %d, n_levels %d, "
                    "hidden %d)", D, F, L, H);
+}
+
+// A 4D fp16 grid's slice layout, or false.
+bool slice_grid(const NectbHashGrid* grid, GridDev* g3) {
+  GridDev g;
+  if (!grid || grid->n_dims != 4 || grid->feature_dtype != NECTB_F16 || !make_grid_dev(grid, &g)) return false;
+  *g3 = make_time_slice(g, 0.f).g3;
+  return true;
+}
+
+}  // namespace
+
+extern "C" int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
+                                  const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
+                                  int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream) {
+  clear_error();
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  return query_points_impl(g, grid->feature_dtype == NECTB_F16, mlp, grid_params, mlp_params, items, n_items,
+                           total_chunks, counter, max_blocks, (cudaStream_t)stream);
+}
+
+extern "C" size_t nectb_time_slice_bytes(const NectbHashGrid* grid) {
+  GridDev g3;
+  if (!slice_grid(grid, &g3)) return 0;
+  return (size_t)g3.total_entries * g3.n_features * 2;
+}
+
+extern "C" int nectb_time_slice(const NectbHashGrid* grid, const void* grid_params, float t, void* slice,
+                                size_t slice_bytes, void* stream) {
+  clear_error();
+  GridDev g, g3;
+  if (!slice_grid(grid, &g3) || !make_grid_dev(grid, &g))
+    return set_error(NECTB_ERR_INVALID, "time slice: needs a valid 4D grid with an fp16 table");
+  NECTB_REQUIRE(grid_params && slice, "null pointer");
+  NECTB_REQUIRE(t >= 0.f && t <= 1.f, "t must lie in [0, 1]");
+  const size_t need = (size_t)g3.total_entries * g3.n_features * 2;
+  if (slice_bytes < need) return set_error(NECTB_ERR_WORKSPACE, "slice of %zu bytes < required %zu", slice_bytes, need);
+  return launch_time_slice(g, (const __half*)grid_params, t, (__half*)slice, (cudaStream_t)stream);
+}
+
+extern "C" int nectb_query_points_slice(const NectbHashGrid* grid, const NectbMLP* mlp, const void* slice,
+                                        const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
+                                        int64_t total_chunks, unsigned int* counter, int32_t max_blocks,
+                                        void* stream) {
+  clear_error();
+  GridDev g3;
+  if (!slice_grid(grid, &g3))
+    return set_error(NECTB_ERR_INVALID, "slice queries: needs a valid 4D grid with an fp16 table");
+  return query_points_impl(g3, true, mlp, slice, mlp_params, items, n_items, total_chunks, counter, max_blocks,
+                           (cudaStream_t)stream);
 }
 
 namespace {

@@ -1152,4 +1152,20 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
                    "hidden %d)", D, F, L, H);
 }
 
+// The fp16 time slice of a 4D fp16 table at t (layout make_time_slice(grid, t).g3).
+int launch_time_slice(const GridDev& grid, const __half* table, float t, __half* slice, cudaStream_t s) {
+  const TimeSlice ts = make_time_slice(grid, t);
+  int64_t max_level = 0;
+  for (int l = 0; l < grid.n_levels; ++l) max_level = std::max(max_level, ts.n_real[l] + 8);
+  const dim3 sgrid((unsigned)std::min<int64_t>(ceil_div(max_level, 256), 1024), (unsigned)grid.n_levels);
+  ProfScope ps(kProfSlice, s);
+  if (grid.n_features == 2)
+    time_slice_kernel<2><<<sgrid, 256, 0, s>>>(ts, table, slice);
+  else if (grid.n_features == 4)
+    time_slice_kernel<4><<<sgrid, 256, 0, s>>>(ts, table, slice);
+  else
+    return set_error(NECTB_ERR_INVALID, "time slice: %d features per level (2 or 4)", grid.n_features);
+  return launch_status("time_slice_kernel");
+}
+
 }  // namespace nectb

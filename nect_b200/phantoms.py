@@ -392,6 +392,19 @@ def dynamic_porous_volume(ph: DynamicPorousPhantom, n: int, t: float, device) ->
     return vol.float()
 
 
+def poisson_projections(projs: torch.Tensor, width: float, photons: float = 1e4, seed: int = 0) -> torch.Tensor:
+    """Poisson noise on line integrals ``projs`` (voxel units): counts
+    I = Poisson(photons * exp(-p / width)) on the attenuation per object
+    width, so that exp(-p) stays in the detector's range, and
+    p' = -ln(I / photons) * width with I clamped to [1, photons].  The upper
+    clamp (a flat-field-corrected reading does not exceed the open beam)
+    keeps p' >= 0, so the data set's minimum is 0 as the reference's export
+    (sigma * (max - min) / max_distance_traveled + min) assumes."""
+    gen = torch.Generator(device=projs.device).manual_seed(seed)
+    counts = torch.poisson(photons * torch.exp(-projs.double() / width), generator=gen)
+    return (-torch.log(torch.clamp(counts, min=1.0, max=photons) / photons) * width).float()
+
+
 def minmax_scale(projs: torch.Tensor):
     """Dataset-wide min-max scaling to [0,1] (nect/data.py:177-183)."""
     mn = projs.min()

@@ -111,10 +111,41 @@ def _call_points(model: _HashGridModel, items_dev: int, n_items: int, total_chun
     _lib.check(rc, "nectb_query_points")
 
 
+def time_slice_bytes(model: _HashGridModel) -> int:
+    """Bytes of a time slice of the model (0: a model without one, i.e. not
+    4D with an fp16 table)."""
+    return int(_lib.lib.nectb_time_slice_bytes(ctypes.byref(model.grid_desc)))
+
+
+def time_slice(model: _HashGridModel, t: float, out: torch.Tensor | None = None,
+               stream: torch.cuda.Stream | None = None) -> torch.Tensor:
+    """The model's fp16 table blended at t into a 3D slice (nectb_time_slice):
+    queries at that t gather 8 corners per level on it instead of 16."""
+    n = time_slice_bytes(model)
+    if n == 0:
+        raise ValueError("the model has no time slice (4D with an fp16 table only)")
+    if out is None:
+        out = torch.empty(n, dtype=torch.uint8, device=model.table.device)
+    stream = stream or torch.cuda.current_stream()
+    rc = _lib.lib.nectb_time_slice(ctypes.byref(model.grid_desc), model.grid_table.data_ptr(), float(t),
+                                   out.data_ptr(), out.numel() * out.element_size(), stream.cuda_stream)
+    _lib.check(rc, "nectb_time_slice")
+    return out
+
+
+def _call_points_slice(model: _HashGridModel, slice_ptr: int, items_dev: int, n_items: int, total_chunks: int,
+                       counter_dev: int, stream: int, max_blocks: int = 0):
+    rc = _lib.lib.nectb_query_points_slice(ctypes.byref(model.grid_desc), ctypes.byref(model.mlp_desc), slice_ptr,
+                                           model.mlp.data_ptr(), items_dev, n_items, total_chunks, counter_dev,
+                                           max_blocks, stream)
+    _lib.check(rc, "nectb_query_points_slice")
+
+
 def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.Stream | None = None,
-                 max_blocks: int = 0):
+                 max_blocks: int = 0, slice: torch.Tensor | None = None):
     """Evaluate the items (any requests) in one launch (outputs written in place);
-    max_blocks > 0 caps the persistent grid."""
+    max_blocks > 0 caps the persistent grid.  With ``slice`` (time_slice at
+    some t) every item is evaluated on it, at its t."""
     if items.size == 0:
         return
     stream = stream or torch.cuda.current_stream()
@@ -126,8 +157,12 @@ def query_points(model: _HashGridModel, items: np.ndarray, stream: torch.cuda.St
     with torch.cuda.stream(stream):
         buf[items.nbytes:].zero_()   # work cursor and error word
         buf[:items.nbytes].copy_(torch.from_numpy(items.view(np.uint8)), non_blocking=False)
-        _call_points(model, buf.data_ptr(), items.size, int(ch.sum()), buf.data_ptr() + items.nbytes,
-                     stream.cuda_stream, max_blocks)
+        if slice is None:
+            _call_points(model, buf.data_ptr(), items.size, int(ch.sum()), buf.data_ptr() + items.nbytes,
+                         stream.cuda_stream, max_blocks)
+        else:
+            _call_points_slice(model, slice.data_ptr(), buf.data_ptr(), items.size, int(ch.sum()),
+                               buf.data_ptr() + items.nbytes, stream.cuda_stream, max_blocks)
 
 
 def reproject_workspace_bytes(model: _HashGridModel, geometry, pixels: int | None = None) -> int:
@@ -293,7 +328,10 @@ class _Lane:
         if bucket > used:
             tail["nu"][0], tail["nv"][0], tail["chunk_begin"][0] = CHUNK, bucket - used, used
 
-    def launch(self, items: np.ndarray) -> torch.cuda.Event:
+    def launch(self, items: np.ndarray, model: _HashGridModel | None = None,
+               slice_ptr: int = 0) -> torch.cuda.Event:
+        """Items in one launch: the bucket's captured graph, or with slice_ptr
+        (items of one request, on its time slice) a direct launch."""
         total = int(item_chunks(items).sum())
         bucket = next(b for b in BUCKETS if b >= total)
         if self.last is not None:
@@ -301,7 +339,11 @@ class _Lane:
         self._write(items, bucket)
         with torch.cuda.stream(self.stream):
             self.items_dev[:self.items_host.numel()].copy_(self.items_host, non_blocking=True)
-            self.graphs[bucket].replay()
+            if slice_ptr:
+                _call_points_slice(model, slice_ptr, self.items_dev.data_ptr(), MAX_ITEMS, bucket,
+                                   self.counter_ptr(), self.stream.cuda_stream, self.max_blocks)
+            else:
+                self.graphs[bucket].replay()
             ev = torch.cuda.Event()
             ev.record(self.stream)
         self.last = ev
@@ -323,16 +365,18 @@ class QueryServer:
     one block per SM): an SM keeps room for slice blocks while background
     work runs, which is what keeps slice p99 near its unloaded latency.  A
     re-projection runs as pieces of ``piece_pixels`` detector pixels, each a
-    launch of a few milliseconds with ``slow_warpgroups`` warpgroups per SM
-    (2 take half of an SM's tensor memory and leave the other half to slice
-    blocks; a 4D mixed model runs on a time slice at the request's t), so a
-    slice waits at most one piece for SMs."""
+    launch of about a millisecond with ``slow_warpgroups`` warpgroups per SM
+    (4 take all of an SM's tensor memory, 2 leave half of it to slice blocks
+    at half the throughput; a 4D mixed model runs on a time slice at the
+    request's t), so a slice waits at most one piece for SMs.  Volumes of a
+    4D mixed model are evaluated on a time slice at their t too, built once
+    per request."""
 
     def __init__(self, model: _HashGridModel, geometry, memory_budget: int = 40 << 30, n_fast: int = 2,
                  n_slow: int = 1, minimum: float = 0.0, maximum: float = 1.0, points_per_ray: int | None = None,
                  slow_blocks: int | None = None, max_slice: int = 1024, max_volume: int = 256,
-                 slot_mix=(0.25, 0.25, 0.5), max_slots: int = 64, piece_pixels: int = 32768,
-                 slow_warpgroups: int = 2):
+                 slot_mix=(0.25, 0.25, 0.5), max_slots: int = 64, piece_pixels: int = 16384,
+                 slow_warpgroups: int = 4):
         self.model = model
         self.geometry = geometry
         self.dev = model.table.device
@@ -352,11 +396,13 @@ class QueryServer:
         self.n_pixels = P
         self.piece_pixels = min(piece_pixels, P)
         ws = (reproject_workspace_bytes(model, geometry, self.piece_pixels) + 255) // 256 * 256
-        per = {"slice": 8 * max_slice ** 2, "volume": 8 * max_volume ** 3, "reproject": 8 * P + ws}
+        # a volume of a 4D mixed model is evaluated on a time slice at its t, built once per request
+        self.slice_bytes = (time_slice_bytes(model) + 255) // 256 * 256
+        per = {"slice": 8 * max_slice ** 2, "volume": 8 * max_volume ** 3 + self.slice_bytes, "reproject": 8 * P + ws}
         nslots = {k: max(1, min(max_slots, int(memory_budget * f // per[k])))
                   for k, f in zip(("slice", "reproject", "volume"), slot_mix)}
         self.pools = {"slice": _Pool(nslots["slice"], max_slice ** 2, self.dev),
-                      "volume": _Pool(nslots["volume"], max_volume ** 3, self.dev),
+                      "volume": _Pool(nslots["volume"], max_volume ** 3, self.dev, ws_bytes=self.slice_bytes),
                       "reproject": _Pool(nslots["reproject"], P, self.dev, ws_bytes=ws)}
         self.max_slice, self.max_volume = max_slice, max_volume
         self.queue: queue.Queue = queue.Queue()
@@ -521,18 +567,8 @@ class QueryServer:
                         reprojs.remove(st)
                         self._finish_on(st, ln)
                         flying.append(st)
-                elif not volumes:
+                elif not (volumes and self._volume_launch(volumes, ln, flying)):
                     break
-                else:
-                    batch, touched = self._pack(volumes, 4096)
-                    ev = ln.launch(batch)
-                    for st in touched:
-                        st["events"].append(ev)
-                        if st["items"].size == 0:
-                            st["req"].launched = time.perf_counter()
-                            self._finish_on(st, ln)
-                            volumes.remove(st)
-                            flying.append(st)
             # completions
             for st in list(flying):
                 if all(e.query() for e in st["events"]):
@@ -541,6 +577,34 @@ class QueryServer:
                     self._done_q.put(st)
             if self.queue.empty() and not slices and (flying or reprojs or volumes or waiting):
                 time.sleep(0.0001)
+
+    def _volume_launch(self, volumes: list[dict], ln: _Lane, flying: list[dict]) -> bool:
+        """One launch of at most 4096 chunks of volume items on lane ln: the
+        oldest requests' items packed together, or, for a 4D mixed model, the
+        oldest request's items on its time slice (built at its first launch,
+        on the lane that then runs all of its launches).  False when there was
+        nothing to launch on this lane."""
+        if self.slice_bytes:
+            st = next((x for x in volumes if x.get("lane") in (None, ln)), None)
+            if st is None:
+                return False
+            slc = self.pools["volume"].ws[st["slot"]]
+            if "lane" not in st:
+                time_slice(self.model, st["req"].t, out=slc, stream=ln.stream)
+                st["lane"] = ln
+            batch, touched = self._pack([st], 4096)
+            ev = ln.launch(batch, self.model, slc.data_ptr())
+        else:
+            batch, touched = self._pack(volumes, 4096)
+            ev = ln.launch(batch)
+        for st in touched:
+            st["events"].append(ev)
+            if st["items"].size == 0:
+                st["req"].launched = time.perf_counter()
+                self._finish_on(st, ln)
+                volumes.remove(st)
+                flying.append(st)
+        return True
 
     def _reproject_piece(self, st: dict, ln: _Lane) -> bool:
         """Launches the next piece of a re-projection on lane ln; True when it

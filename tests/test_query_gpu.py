@@ -83,6 +83,32 @@ def test_volume_and_slices_match_oracle(cuda_device, precision):
         assert rel(out.cpu(), oracle_sigma(m, levels, np.array(pts, np.float32), t)) < TOL[precision]
 
 
+def test_slice_queries_match_4d_queries_and_oracle(cuda_device):
+    """Volume and slice items of a 4D mixed model evaluated on its time slice
+    at t (nectb_time_slice + nectb_query_points_slice, 8 corners per level)
+    agree with the 16-corner 4D queries within 1e-2 and with the oracle within
+    the mixed tolerance; slices at two t differ where the model does."""
+    from nect_b200 import serving
+
+    m, geo, levels = model_and_geometry("mixed")
+    for t in (0.0, 0.3, 0.77, 1.0):
+        vol4, vols = torch.empty(12, 16, 20, device="cuda"), torch.empty(12, 16, 20, device="cuda")
+        sl4, sls = torch.empty(33, 47, device="cuda"), torch.empty(33, 47, device="cuda")
+        serving.query_points(m, np.concatenate([serving.volume_items(vol4, vol4.shape, t),
+                                                serving.slice_items(sl4, sl4.shape, t, centre=(0.4, 0.5, 0.6))]))
+        slc = serving.time_slice(m, t)
+        serving.query_points(m, np.concatenate([serving.volume_items(vols, vols.shape, 0.123),   # t ignored
+                                                serving.slice_items(sls, sls.shape, t, centre=(0.4, 0.5, 0.6))]),
+                             slice=slc)
+        torch.cuda.synchronize()
+        assert rel(vols.cpu(), vol4.cpu()) < 1e-2, t
+        assert rel(sls.cpu(), sl4.cpu()) < 1e-2, t
+        z, y, x = [serving.centres(n) for n in (12, 16, 20)]
+        Z, Y, X = np.meshgrid(z, y, x, indexing="ij")
+        ref = oracle_sigma(m, levels, np.stack([Z, Y, X], -1).reshape(-1, 3), t)
+        assert rel(vols.cpu(), ref) < TOL["mixed"], t
+
+
 @pytest.mark.parametrize("precision", ["plain_fp32", "mixed"])
 def test_reprojection_matches_oracle(cuda_device, precision):
     from nect_b200 import serving

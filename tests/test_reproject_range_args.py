@@ -73,3 +73,24 @@ def test_slice_room_only_for_4d_mixed_models():
     n3 = sum(1 << 12 if hsh[l] else ((res[l] + 1) ** 3 + 7) // 8 * 8 for l in range(L))
     want = (n3 * 2 * 2 + 255) // 256 * 256 + 256
     assert _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(g4), ctypes.byref(mlp()), 100) == want
+
+
+def test_time_slice_arguments():
+    """nectb_time_slice_bytes is the fp16 slice alone (0 without a slice);
+    nectb_time_slice rejects t outside [0, 1], a small buffer, 3D grids and
+    fp32 tables before any device work."""
+    g4 = grid(4)
+    n = _lib.lib.nectb_time_slice_bytes(ctypes.byref(g4))
+    assert n > 0
+    assert (n + 255) // 256 * 256 + 256 == _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(g4),
+                                                                                       ctypes.byref(mlp()), 1)
+    assert _lib.lib.nectb_time_slice_bytes(ctypes.byref(grid(3))) == 0
+    assert _lib.lib.nectb_time_slice_bytes(ctypes.byref(grid(4, _lib.F32))) == 0
+    ts = _lib.lib.nectb_time_slice
+    assert ts(ctypes.byref(g4), FAKE, 1.5, FAKE, n, None) == NECTB_ERR_INVALID
+    assert ts(ctypes.byref(g4), FAKE, float("nan"), FAKE, n, None) == NECTB_ERR_INVALID
+    assert ts(ctypes.byref(g4), FAKE, 0.5, FAKE, n - 2, None) == NECTB_ERR_WORKSPACE
+    assert ts(ctypes.byref(grid(3)), FAKE, 0.5, FAKE, n, None) == NECTB_ERR_INVALID
+    assert ts(ctypes.byref(g4), None, 0.5, FAKE, n, None) == NECTB_ERR_INVALID
+    q = _lib.lib.nectb_query_points_slice
+    assert q(ctypes.byref(grid(3)), ctypes.byref(mlp()), FAKE, FAKE, FAKE, 1, 1, FAKE, 0, None) == NECTB_ERR_INVALID
