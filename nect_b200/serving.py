@@ -362,8 +362,9 @@ class QueryServer:
     Slices run on ``n_fast`` high-priority lanes, packed several requests per
     launch.  Volumes and re-projections share ``n_slow`` low-priority lanes.
     Volume launches are persistent grids capped at ``slow_blocks`` (default
-    one block per SM): an SM keeps room for slice blocks while background
-    work runs, which is what keeps slice p99 near its unloaded latency.  A
+    three one-warpgroup blocks per SM, 384 of its 512 tensor-memory columns):
+    an SM keeps room for a slice block while background work runs, which is
+    what keeps slice p99 near its unloaded latency.  A
     re-projection runs as pieces of ``piece_pixels`` detector pixels, each a
     launch of about a millisecond with ``slow_warpgroups`` warpgroups per SM
     (4 take all of an SM's tensor memory, 2 leave half of it to slice blocks
@@ -383,7 +384,7 @@ class QueryServer:
         self.scale, self.offset = denormalisation(geometry.max_distance_traveled, minimum, maximum)
         self.points_per_ray = points_per_ray
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
-        self.slow_blocks = slow_blocks if slow_blocks is not None else sms
+        self.slow_blocks = slow_blocks if slow_blocks is not None else 3 * sms
         if not 1 <= slow_warpgroups <= 4 or piece_pixels < 1:
             raise ValueError("slow_warpgroups must be 1..4 and piece_pixels positive")
         self.slow_warpgroups = slow_warpgroups
