@@ -373,6 +373,9 @@ def main():
     ap.add_argument("--no-autotune", action="store_true",
                     help="skip the autotuner (launch shapes and scheduling tuned on this workload before the "
                          "warm-up, outside the timed region); the library defaults are used")
+    ap.add_argument("--tuning", default="",
+                    help="launch-shape settings KEY=VALUE[,KEY=VALUE] (NectbTuning fields) applied after the "
+                         "autotuner, e.g. forward_blocks_per_sm=4")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -438,6 +441,12 @@ def main():
             dist.broadcast_object_list(chosen, src=0)
             tuning = chosen[0]
             autotune.set_tuning(tuning)
+    if args.tuning:
+        cur = autotune.get_tuning()
+        for kv in args.tuning.split(","):
+            key, val = (x.strip() for x in kv.split("="))
+            cur[key] = int(float(val)) if isinstance(cur[key], int) else float(val)
+        autotune.set_tuning(cur)
     for k in range(args.warmup):
         trainer.step(make_step_batch(k))
     torch.cuda.synchronize()

@@ -216,7 +216,8 @@ typedef struct NectbQueryItem {
  * counter: two device uint32: [0] the work cursor (zeroed by every call) and
  * [1] an error word the launch sets to non-zero when a tensor-core wait timed
  * out (its items are then incomplete).  The library never clears [1]: the
- * caller zeroes it once and reads it (stream-ordered) when it wants to know. */
+ * caller zeroes it once and reads it (stream-ordered) when it wants to know.
+ * grid_params must be 16-byte aligned. */
 int nectb_query_points(const NectbHashGrid* grid, const NectbMLP* mlp, const void* grid_params,
                        const float* mlp_params, const NectbQueryItem* items, int32_t n_items,
                        int64_t total_chunks, unsigned int* counter, int32_t max_blocks, void* stream);
@@ -247,7 +248,8 @@ int nectb_query_points_slice(const NectbHashGrid* grid, const NectbMLP* mlp, con
  * with the training sampler (no jitter, no detector offset), i.e. the
  * reference's training forward (base_trainer.py:520-554) without the loss.
  * The reference has no standalone re-projection query.  workspace:
- * nectb_train_workspace_bytes(geometry, grid, mlp, P) bytes.
+ * nectb_train_workspace_bytes(geometry, grid, mlp, P) bytes; grid_params
+ * 16-byte aligned.
  * max_blocks > 0 caps the persistent grid of either query (a server keeps
  * SMs free for latency-critical launches on higher-priority streams). */
 int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* grid,
@@ -267,11 +269,11 @@ int nectb_query_reproject(const NectbGeometry* geometry, const NectbHashGrid* gr
  * bytes gathers 8 corners per level on a time slice at t, built in the
  * workspace by each call, instead of the 16 of the 4D interpolation (the
  * result agrees within fp16 rounding of the blended features).
- * warpgroups_per_sm 1..4: the mixed forward runs one block of that many
- * 128-thread warpgroups per SM (tensor memory is allocated in powers of two:
- * 1 and 2 take 128 and 256 of an SM's 512 columns and leave the rest to
- * query blocks on other streams, 3 and 4 take all of it); 0 = max_blocks'
- * rule.
+ * warpgroups_per_sm 1..6: the mixed forward runs one block of that many
+ * 128-thread warpgroups per SM, 64 tensor-memory columns each, allocated as
+ * a power of two (1, 2, 3-4, 5-6 warpgroups take 64, 128, 256, 512 of an
+ * SM's 512 columns; up to 4 leave room for query blocks on other streams);
+ * 0 = max_blocks' rule.
  * No reference counterpart. */
 int nectb_query_reproject_range(const NectbGeometry* geometry, const NectbHashGrid* grid,
                                 const NectbMLP* mlp, const void* grid_params, const float* mlp_params,
@@ -499,7 +501,7 @@ int nectb_profile_collect(int32_t* launches, double* total_ms);
 int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, void* stream);
 
 /* Launch shapes and scheduling of the mixed training path, process-wide:
- * warpgroups per SM of the forward (1..4), blocks per SM of the tensor-core
+ * warpgroups per SM of the forward (1..6), blocks per SM of the tensor-core
  * backward (1..3; the three-layer model's kernel takes at most 2),
  * of the gradient scatter (0 = as many as fit), the rounds the recommended
  * staging is sized for (nectb_train_staging_bytes, 1..64), the largest fp32
@@ -518,7 +520,7 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * only the ray order and the staged gradients (identical results: the
  * stored rows are the bits the gather produces).  nectb_train_staging_bytes
  * follows it.  nectb_set_tuning validates and applies to steps issued after
- * it returns; defaults: 4, 3, 0, 4, 48 MiB, 1.0, 3.0, 1, 1.  No reference
+ * it returns; defaults: 6, 3, 0, 4, 48 MiB, 1.0, 3.0, 1, 1.  No reference
  * counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;

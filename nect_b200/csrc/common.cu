@@ -113,7 +113,7 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
 namespace nectb {
 namespace {
 std::mutex g_tuning_mu;
-NectbTuning g_tuning = {4, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1, 1};
+NectbTuning g_tuning = {kFwdMaxWarpgroups, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1, 1};
 }  // namespace
 
 NectbTuning current_tuning() {
@@ -134,7 +134,8 @@ extern "C" int nectb_set_tuning(const NectbTuning* t) {
   using namespace nectb;
   clear_error();
   NECTB_REQUIRE(t, "null tuning");
-  NECTB_REQUIRE(t->forward_blocks_per_sm >= 1 && t->forward_blocks_per_sm <= 4, "forward_blocks_per_sm must be 1..4");
+  NECTB_REQUIRE(t->forward_blocks_per_sm >= 1 && t->forward_blocks_per_sm <= kFwdMaxWarpgroups,
+                "forward_blocks_per_sm must be 1..%d", kFwdMaxWarpgroups);
   NECTB_REQUIRE(t->backward_blocks_per_sm >= 1 && t->backward_blocks_per_sm <= 3, "backward_blocks_per_sm must be 1..3");
   NECTB_REQUIRE(t->scatter_blocks_per_sm >= 0 && t->scatter_blocks_per_sm <= 8, "scatter_blocks_per_sm must be 0..8");
   NECTB_REQUIRE(t->staged_rounds >= 1 && t->staged_rounds <= 64, "staged_rounds must be 1..64");

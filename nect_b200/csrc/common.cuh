@@ -25,6 +25,14 @@ inline int launch_status(const char* what) { return cuda_status(cudaGetLastError
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// Most warpgroups of the mixed forward on one SM (one block; 64 TMEM columns
+// and at most 85 registers per thread each): NectbTuning::forward_blocks_per_sm
+// and the re-projection's warpgroups_per_sm range over 1..kFwdMaxWarpgroups.
+#ifndef NECTB_FWD_BLOCKS_PER_SM
+#define NECTB_FWD_BLOCKS_PER_SM 6
+#endif
+constexpr int kFwdMaxWarpgroups = NECTB_FWD_BLOCKS_PER_SM;
+
 // The model shapes the fused kernels are instantiated for, as (inputs D,
 // features per level F, levels L, hidden layers H of width 64): 16 levels of
 // 2 or 4 features over 3 or 4 inputs with 2 or 3 hidden layers (the

@@ -282,6 +282,7 @@ int query_points_impl(const GridDev& g, bool f16_table, const NectbMLP* mlp, con
   NECTB_REQUIRE(grid_params && mlp_params && items && counter && n_items > 0 && total_chunks > 0,
                 "null pointer or empty query");
   NECTB_REQUIRE(total_chunks < (int64_t(1) << 31), "too many chunks in one launch");
+  NECTB_REQUIRE(((uintptr_t)grid_params & 15u) == 0, "grid_params must be 16-byte aligned");
   if (int rc = cuda_status(cudaMemsetAsync(counter, 0, sizeof(unsigned int), s), "memset query counter")) return rc;
   const int D = g.n_dims, F = g.n_features, L = g.n_levels, H = mlp->n_hidden_layers;
   const int act = mlp->activation, oact = mlp->output_activation;
@@ -350,6 +351,8 @@ extern "C" int nectb_time_slice(const NectbHashGrid* grid, const void* grid_para
   if (!slice_grid(grid, &g3) || !make_grid_dev(grid, &g))
     return set_error(NECTB_ERR_INVALID, "time slice: needs a valid 4D grid with an fp16 table");
   NECTB_REQUIRE(grid_params && slice, "null pointer");
+  NECTB_REQUIRE(((uintptr_t)grid_params & 15u) == 0 && ((uintptr_t)slice & 15u) == 0,
+                "grid_params and slice must be 16-byte aligned");
   NECTB_REQUIRE(t >= 0.f && t <= 1.f, "t must lie in [0, 1]");
   const size_t need = (size_t)g3.total_entries * g3.n_features * 2;
   if (slice_bytes < need) return set_error(NECTB_ERR_WORKSPACE, "slice of %zu bytes < required %zu", slice_bytes, need);
@@ -384,10 +387,12 @@ int reproject_range(const NectbGeometry* geometry, const NectbHashGrid* grid, co
   if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
   if (int rc = validate_mlp(mlp, g)) return rc;
   NECTB_REQUIRE(grid_params && mlp_params && out, "null pointer");
+  NECTB_REQUIRE(((uintptr_t)grid_params & 15u) == 0, "grid_params must be 16-byte aligned");
   NECTB_REQUIRE(num_points_per_ray >= 1 && max_distance_traveled > 0.f, "bad sampling parameters");
   const int P = geometry->nDetector[0] * geometry->nDetector[1];
   NECTB_REQUIRE(begin >= 0 && count >= 1 && (int64_t)begin + count <= P, "pixel range outside the detector");
-  NECTB_REQUIRE(warpgroups >= 0 && warpgroups <= 4, "warpgroups_per_sm must be 0..4");
+  NECTB_REQUIRE(warpgroups >= 0 && warpgroups <= kFwdMaxWarpgroups, "warpgroups_per_sm must be 0..%d",
+                kFwdMaxWarpgroups);
   if (!workspace || workspace_size < workspace_bytes(count, count))
     return set_error(NECTB_ERR_WORKSPACE, "workspace of %zu bytes < required %zu", workspace_size,
                      workspace_bytes(count, count));

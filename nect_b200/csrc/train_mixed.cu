@@ -75,18 +75,33 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
   return true;
 }
 
-// Warpgroups of the forward per SM.  A block is one to four independent
-// warpgroups (128 threads each, one 128-sample tile, its own TMEM quarter,
-// mbarrier and named barrier) that share one copy of the weight tiles: with
-// four, shared memory is 82 KB per SM instead of four blocks' 136 KB, and the
-// L1 that the gathers hit (neighbouring rays reuse table entries) grows from
-// 92 to 156 KB.  Re-projection queries, which share SMs with serving
-// kernels, run one warpgroup per block.
-#ifndef NECTB_FWD_BLOCKS_PER_SM
-#define NECTB_FWD_BLOCKS_PER_SM 4
-#endif
-constexpr int kFwdBlocksPerSM = NECTB_FWD_BLOCKS_PER_SM;
-static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 128 <= 512, "TMEM holds 512 columns per SM");
+// Warpgroups of the forward per SM.  A block is one to kFwdBlocksPerSM
+// independent warpgroups (128 threads each, one 128-sample tile, its own 64
+// TMEM columns, mbarrier and named barrier) that share one copy of the weight
+// tiles: with four, shared memory is 82 KB per SM instead of four blocks'
+// 136 KB, and the L1 that the gathers hit (neighbouring rays reuse table
+// entries) grows from 92 to 156 KB.  Every layer's product goes to the same
+// 64 columns: the next layer's MMA is issued only after the warpgroup has
+// read the previous result into registers, 32 columns at a time.  Six
+// warpgroups (24 warps, 80 registers each) keep more gathers in flight than
+// four (the forward is bound by gather latency and L1 throughput): C3
+// forward 16.0 -> 14.6 ms.  Re-projection queries, which share SMs with
+// serving kernels, run one warpgroup per block or the caller's number.
+constexpr int kFwdBlocksPerSM = kFwdMaxWarpgroups;
+static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 64 <= 512 && kFwdBlocksPerSM * 128 <= 1024,
+              "TMEM holds 512 columns per SM, a block 1024 threads");
+// The forward's warpgroups per SM for a model shape: all of them for two
+// hidden layers (80 registers a thread suffice); deeper MLPs keep four and 128
+// registers (at 80 they would spill).
+template <int L, int F, int H>
+struct FwdShape {
+  static constexpr int kMaxWarpgroups = H == 2 ? kFwdBlocksPerSM : (kFwdBlocksPerSM < 4 ? kFwdBlocksPerSM : 4);
+};
+
+// TMEM columns of a forward block of n_wg warpgroups: 64 each, allocated as a power of two.
+__host__ __device__ constexpr uint32_t fwd_tmem_cols(int n_wg) {
+  return n_wg <= 1 ? 64u : (n_wg == 2 ? 128u : (n_wg <= 4 ? 256u : 512u));
+}
 
 // Barrier over the 128 threads of warpgroup wg (named barrier wg + 1; 0 is
 // __syncthreads'), and its OR-reduction form.
@@ -105,7 +120,7 @@ __device__ __forceinline__ bool wg_or(int wg, bool p) {
 }
 
 template <int D, int F, int L, int H, int ACT>
-__global__ void __launch_bounds__(kFwdBlocksPerSM * kMixThreads, 1)
+__global__ void __launch_bounds__(FwdShape<L, F, H>::kMaxWarpgroups * kMixThreads, 1)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ y_pred, float* __restrict__ loss,
@@ -136,7 +151,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   uint64_t* bar = bars + wg;
   if (xstore && blockIdx.x == 0 && t == 0) ctrl[7] = xcap;  // rows this forward fills, for the backward
   stage_mixed_weights<L, F, H>(W, sW, sWout);
-  const uint32_t ncols = n_wg == 1 ? 128u : (n_wg == 2 ? 256u : 512u);
+  const uint32_t ncols = fwd_tmem_cols(n_wg);
   if (warp == 0) {
     tc::tmem_alloc(tslot, ncols);
     tc::tmem_relinquish();
@@ -146,7 +161,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
-  const uint32_t tm = *tslot + 128u * wg;  // this warpgroup's 128 columns
+  const uint32_t tm = *tslot + 64u * wg;  // this warpgroup's 64 columns
   const uint32_t my_lanes = tm + ((uint32_t)(32 * (warp & 3)) << 16);
   const uint32_t sX_a = tc::smem_u32(sX), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
   constexpr uint32_t idesc = tc::idesc_bf16(128, 64, false, false);
@@ -167,16 +182,12 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
     if (D == 4) p[3] = a.t;
     encode_row<D, F, L>(grid, table, p, valid, sX, r,
                         valid && cur.xrow >= 0 ? xstore + (size_t)(cur.xrow + i) * S::NCH : nullptr);
-    float h[64];
-    // layer k (0-based) writes TMEM columns 64 * (k & 1) of the warpgroup's
-    // quarter; its input is X for k = 0, else the previous layer's
-    // activations in sA
+    // layer k (0-based) writes the warpgroup's 64 TMEM columns; its input is
+    // X for k = 0, else the previous layer's activations in sA (which
+    // overwrite X once layer 0's MMA has completed)
+    float z = 0.f;
 #pragma unroll
     for (int k = 0; k < H; ++k) {
-      if (k > 0) {
-        uint32_t mlo, mhi;
-        act_row(h, sA, r, act, mlo, mhi);
-      }
       tc::fence_async_smem();
       tc::fence_before();
       wg_sync(wg);
@@ -190,8 +201,7 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         } else {
 #pragma unroll
           for (int q = 0; q < 4; ++q)
-            tc::mma(tm + 64 * (k & 1), tc::desc_k(sA_a, q), tc::desc_k(sW_a + (KT + k - 1) * kWTile, q), idesc,
-                    q > 0);
+            tc::mma(tm, tc::desc_k(sA_a, q), tc::desc_k(sW_a + (KT + k - 1) * kWTile, q), idesc, q > 0);
         }
         tc::commit(bar);
       }
@@ -202,12 +212,29 @@ fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
         break;
       }
       tc::fence_after();
-      ld64(my_lanes + 64 * (k & 1), h);
+      // the layer's 64 values, 32 columns at a time: the hidden activations
+      // into sA for the next layer, or the output layer's dot product
+#pragma unroll
+      for (int half = 0; half < 2; ++half) {
+        float v[32];
+        tc::tmem_ld16(my_lanes + 32 * half, v);
+        tc::tmem_ld16(my_lanes + 32 * half + 16, v + 16);
+        tc::tmem_wait_ld();
+        if (k + 1 < H) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            float a8[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) a8[q] = hidden_act(v[8 * c + q], act);
+            tc::st_chunk_bf16(sA, r, 4 * half + c, a8);
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) z = fmaf(sWout[32 * half + j], hidden_act(v[j], act), z);
+        }
+      }
     }
     if (timed_out) break;
-    float z = 0.f;
-#pragma unroll
-    for (int j = 0; j < 64; ++j) z = fmaf(sWout[j], hidden_act(h[j], act), z);
     if (valid) {  // Kahan-compensated accumulation along the ray
       const float y = act_fwd(z, out_act) - kcomp;
       const float s = ksum + y;
@@ -991,13 +1018,13 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // (which share SMs with serving kernels) one warpgroup per block, or the
   // caller's warpgroups per SM
   const bool shares_sms = a.max_blocks > 0 || a.fwd_warpgroups > 0;
+  constexpr int kMaxWg = FwdShape<L, F, H>::kMaxWarpgroups;
   const int wgs = a.max_blocks > 0       ? 1
-                  : a.fwd_warpgroups > 0 ? std::min(a.fwd_warpgroups, kFwdBlocksPerSM)
-                                         : std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM);
-  int fblocks = a.max_blocks > 0
-                    ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kFwdBlocksPerSM) * sms,
-                                                (int)ceil_div(a.num_rays, 4)))
-                    : std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * wgs)));
+                  : a.fwd_warpgroups > 0 ? std::min(a.fwd_warpgroups, kMaxWg)
+                                         : std::min(tune.forward_blocks_per_sm, kMaxWg);
+  int fblocks = a.max_blocks > 0 ? std::max(1, std::min<int>(std::min(tune.forward_blocks_per_sm, kMaxWg) * sms,
+                                                             (int)ceil_div(a.num_rays, 4)))
+                                 : std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * wgs)));
   // the general backward: two blocks per SM of 256 TMEM columns, one of 512
   const int bwd_per_sm = BwdPlan<L, F, H>::kCols == 512u ? 1 : std::min(tune.backward_blocks_per_sm, 2);
   int blocks = std::max(1, std::min<int>(bwd_per_sm * sms, (int)ceil_div(a.num_rays, 4)));

@@ -367,9 +367,9 @@ class QueryServer:
     what keeps slice p99 near its unloaded latency.  A
     re-projection runs as pieces of ``piece_pixels`` detector pixels, each a
     launch of about a millisecond with ``slow_warpgroups`` warpgroups per SM
-    (4 take all of an SM's tensor memory, 2 leave half of it to slice blocks
-    at half the throughput; a 4D mixed model runs on a time slice at the
-    request's t), so a slice waits at most one piece for SMs.  Volumes of a
+    (4 take half of an SM's tensor memory and two thirds of its registers,
+    leaving room for a slice block; a 4D mixed model runs on a time slice at
+    the request's t), so a slice waits at most one piece for SMs.  Volumes of a
     4D mixed model are evaluated on a time slice at their t too, built once
     per request."""
 
@@ -385,8 +385,8 @@ class QueryServer:
         self.points_per_ray = points_per_ray
         sms = torch.cuda.get_device_properties(self.dev).multi_processor_count
         self.slow_blocks = slow_blocks if slow_blocks is not None else 3 * sms
-        if not 1 <= slow_warpgroups <= 4 or piece_pixels < 1:
-            raise ValueError("slow_warpgroups must be 1..4 and piece_pixels positive")
+        if not 1 <= slow_warpgroups <= 6 or piece_pixels < 1:
+            raise ValueError("slow_warpgroups must be 1..6 and piece_pixels positive")
         self.slow_warpgroups = slow_warpgroups
         lo, hi = torch.cuda.Stream.priority_range()
         self.fast = [_Lane(self.dev, priority=hi) for _ in range(n_fast)]

@@ -45,7 +45,7 @@ def call(begin, count, ws_bytes, warpgroups=3):
     (-1, 10, 3, "pixel range"),
     (1900, 30, 3, "pixel range"),
     (0, 0, 3, "pixel range"),
-    (0, 100, 5, "warpgroups_per_sm"),
+    (0, 100, 7, "warpgroups_per_sm"),
 ])
 def test_bad_ranges_are_rejected(begin, count, warpgroups, message):
     assert call(begin, count, 1 << 30, warpgroups) == NECTB_ERR_INVALID
