@@ -90,12 +90,17 @@ __device__ __forceinline__ bool next_chunk(RayCursor& cur, const RayRec* recs, u
 constexpr int kFwdBlocksPerSM = kFwdMaxWarpgroups;
 static_assert(kFwdBlocksPerSM >= 1 && kFwdBlocksPerSM * 64 <= 512 && kFwdBlocksPerSM * 128 <= 1024,
               "TMEM holds 512 columns per SM, a block 1024 threads");
-// The forward's warpgroups per SM for a model shape: all of them for two
-// hidden layers (80 registers a thread suffice); deeper MLPs keep four and 128
-// registers (at 80 they would spill).
-template <int L, int F, int H>
+// The forward's warpgroups per SM for a model shape: all of them for 3D
+// grids and two hidden layers (80 registers a thread suffice); deeper MLPs
+// keep four and 128 registers (at 80 they would spill), and so do 4D grids:
+// compiled for 80 registers the 4D forward's stored encoding rows disagreed
+// with the recomputed ones (the staged backward's table gradient off by
+// 4e-4 of its largest entry, the y_pred identical), while at 128 they agree
+// bit for bit.  4D training runs the 3D kernels on the time slice.
+template <int D, int L, int F, int H>
 struct FwdShape {
-  static constexpr int kMaxWarpgroups = H == 2 ? kFwdBlocksPerSM : (kFwdBlocksPerSM < 4 ? kFwdBlocksPerSM : 4);
+  static constexpr int kMaxWarpgroups =
+      (D == 3 && H == 2) ? kFwdBlocksPerSM : (kFwdBlocksPerSM < 4 ? kFwdBlocksPerSM : 4);
 };
 
 // TMEM columns of a forward block of n_wg warpgroups: 64 each, allocated as a power of two.
@@ -120,7 +125,7 @@ __device__ __forceinline__ bool wg_or(int wg, bool p) {
 }
 
 template <int D, int F, int L, int H, int ACT>
-__global__ void __launch_bounds__(FwdShape<L, F, H>::kMaxWarpgroups * kMixThreads, 1)
+__global__ void __launch_bounds__(FwdShape<D, L, F, H>::kMaxWarpgroups * kMixThreads, 1)
 fwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                  RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                  int out_act, float* __restrict__ y_pred, float* __restrict__ loss,
@@ -1018,7 +1023,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // (which share SMs with serving kernels) one warpgroup per block, or the
   // caller's warpgroups per SM
   const bool shares_sms = a.max_blocks > 0 || a.fwd_warpgroups > 0;
-  constexpr int kMaxWg = FwdShape<L, F, H>::kMaxWarpgroups;
+  constexpr int kMaxWg = FwdShape<D, L, F, H>::kMaxWarpgroups;
   const int wgs = a.max_blocks > 0       ? 1
                   : a.fwd_warpgroups > 0 ? std::min(a.fwd_warpgroups, kMaxWg)
                                          : std::min(tune.forward_blocks_per_sm, kMaxWg);
