@@ -11,7 +11,9 @@ porous medium with a rising brine front and shrinking grains, 512 jittered
 samples per ray, 4D hash grid of 16 levels x 2 features, 2^21 entries per
 level, temporal base resolution 4, 2x64 MLP, mixed precision.  The plain fp32
 path is timed on the same workload in the same process (``plain_fp32`` and
-``mixed_over_plain`` in the line).  Inputs are seeded synthetic projections
+``mixed_over_plain`` in the line), and so is the mixed step with the other
+backward (encodings recomputed instead of read back from the store, or the
+reverse; ``other_backward``).  Inputs are seeded synthetic projections
 made before the timed region.  Timing: W warm-up steps, then K steps
 bracketed by a barrier and cuda synchronize, CUDA events on the launching
 stream, max over ranks.  Per-step state (tables, gradients, Adam moments)
@@ -366,6 +368,8 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=0,
                     help="timed steps of the plain fp32 arm (0: --steps, 2 on the large 4D workload)")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-other-backward", action="store_true",
+                    help="skip timing the other backward (recompute vs encoding store) on the same trainer")
     ap.add_argument("--rays", type=int, default=0, help="override rays per step (profiling of smaller cases)")
     ap.add_argument("--encoding-store", default="auto", choices=["auto", "on", "off"],
                     help="off: the mixed backward recomputes the encodings instead of reading the rows the forward "
@@ -571,6 +575,18 @@ def main():
         e2e = {"value": world * rays_per_step * args.steps / (ems / 1e3), "unit": "rays/s",
                "h2d_bytes_per_step": int(P * 4), "d2h_bytes_per_step": 4}
 
+    # ---- the other backward (encodings recomputed, or read from the store) on the same trainer
+    other = None
+    if args.precision == "mixed" and not args.no_other_backward and args.workload != "c5_large_cone":
+        autotune.set_tuning({"encoding_store": 1 if recompute else 0})
+        for k in range(2):
+            trainer.step(make_step_batch(k))
+        oms, _ = time_steps(trainer, make_step_batch, args.steps, 2, world)
+        other = {"backward": "encoding store" if recompute else "recompute (encodings gathered again)",
+                 "value": world * rays_per_step * args.steps / (oms / 1e3), "unit": "rays/s",
+                 "ms_per_step": oms / args.steps}
+        autotune.set_tuning({"encoding_store": 0 if recompute else 1})
+
     # ---- the plain fp32 path on the same workload, same process
     plain = None
     if args.precision == "mixed" and not args.no_plain:
@@ -612,6 +628,7 @@ def main():
         "roofline": roofline,
         "rooflines": rooflines,
         "probes": roofs,
+        "other_backward": other,
         "plain_fp32": plain,
         "mixed_over_plain": (value / plain["value"]) if plain else None,
         "cpu_baseline": cpu_baseline,
