@@ -519,14 +519,9 @@ int nectb_selftest_bounded_wait(unsigned int* error_word, uint32_t max_tries, vo
  * from the tables (positions are always regenerated), so the staging holds
  * only the ray order and the staged gradients (identical results: the
  * stored rows are the bits the gather produces).  nectb_train_staging_bytes
- * follows it.  overlap_rounds: 1 runs the staged backward's rounds as a
- * pipeline over two halves of the staging buffer, the tensor-core pass of
- * round r + 1 on the call's stream while the scatter passes of round r run
- * on a second stream the library owns (joined back before the call returns;
- * the events and the stream order keep the call stream-ordered and
- * capturable); 0 runs them one after the other.  nectb_set_tuning validates
- * and applies to steps issued after it returns; defaults: 6, 3, 0, 4,
- * 48 MiB, 1.0, 3.0, 1, 1, 0.  No reference counterpart. */
+ * follows it.  nectb_set_tuning validates and applies to steps issued after
+ * it returns; defaults: 6, 3, 0, 4, 48 MiB, 1.0, 3.0, 1, 1.  No reference
+ * counterpart. */
 typedef struct NectbTuning {
   int32_t forward_blocks_per_sm;
   int32_t backward_blocks_per_sm;
@@ -537,7 +532,6 @@ typedef struct NectbTuning {
   float run_threshold_4d;
   int32_t time_slice;
   int32_t encoding_store;
-  int32_t overlap_rounds;
 } NectbTuning;
 int nectb_get_tuning(NectbTuning* tuning);
 int nectb_set_tuning(const NectbTuning* tuning);

@@ -105,7 +105,6 @@ class NectbTuning(ctypes.Structure):
         ("run_threshold_4d", c_f32),
         ("time_slice", c_int),
         ("encoding_store", c_int),
-        ("overlap_rounds", c_int),
     ]
 
 

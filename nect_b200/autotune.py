@@ -21,8 +21,7 @@ import torch
 from . import _lib
 
 FIELDS = ("forward_blocks_per_sm", "backward_blocks_per_sm", "scatter_blocks_per_sm", "staged_rounds",
-          "scatter_group_bytes", "run_threshold_3d", "run_threshold_4d", "time_slice", "encoding_store",
-          "overlap_rounds")
+          "scatter_group_bytes", "run_threshold_3d", "run_threshold_4d", "time_slice", "encoding_store")
 
 # candidates per tunable, tried one tunable at a time
 SPACE = {

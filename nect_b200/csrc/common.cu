@@ -113,19 +113,8 @@ extern "C" int nectb_profile_collect(int32_t* launches, double* total_ms) {
 namespace nectb {
 namespace {
 std::mutex g_tuning_mu;
-NectbTuning g_tuning = {kFwdMaxWarpgroups, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1, 1, 0};
-std::mutex g_aux_mu;
-cudaStream_t g_aux[64] = {};
+NectbTuning g_tuning = {kFwdMaxWarpgroups, 3, 0, 4, int64_t(48) << 20, 1.0f, 3.0f, 1, 1};
 }  // namespace
-
-cudaStream_t aux_stream() {
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> lk(g_aux_mu);
-  if (!g_aux[dev] && cudaStreamCreateWithFlags(&g_aux[dev], cudaStreamNonBlocking) != cudaSuccess)
-    g_aux[dev] = nullptr;
-  return g_aux[dev];
-}
 
 NectbTuning current_tuning() {
   std::lock_guard<std::mutex> lk(g_tuning_mu);
@@ -156,7 +145,6 @@ extern "C" int nectb_set_tuning(const NectbTuning* t) {
                 "run thresholds must be in [0, 64]");
   NECTB_REQUIRE(t->time_slice == 0 || t->time_slice == 1, "time_slice must be 0 or 1");
   NECTB_REQUIRE(t->encoding_store == 0 || t->encoding_store == 1, "encoding_store must be 0 or 1");
-  NECTB_REQUIRE(t->overlap_rounds == 0 || t->overlap_rounds == 1, "overlap_rounds must be 0 or 1");
   std::lock_guard<std::mutex> lk(g_tuning_mu);
   g_tuning = *t;
   return NECTB_OK;

@@ -72,11 +72,6 @@ inline int input_padded(int n_input) { return (n_input + 15) / 16 * 16; }
 // The current launch shapes and scheduling (nectb_set_tuning), copied under a lock.
 NectbTuning current_tuning();
 
-// A second stream on the current device, created on first use and kept for
-// the process (work the library overlaps with its call's stream; always
-// joined back to that stream by an event).  nullptr if it cannot be created.
-cudaStream_t aux_stream();
-
 // Sets a kernel's dynamic shared memory and its L1/shared split.  An SM keeps
 // one split while any block is resident, so a kernel that shares SMs with
 // other launches (a capped background grid, serving queries) asks for a split

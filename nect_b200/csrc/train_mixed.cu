@@ -1122,83 +1122,35 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ks, kScatterThreads, 0);
   if (tune.scatter_blocks_per_sm > 0) per_sm = std::min(per_sm, tune.scatter_blocks_per_sm);
   const int sblocks = sms * std::max(per_sm, 1);
-  // one round of ranked rays [lo, hi): the tensor-core pass on stream sb
-  // stages dL/d(encoding) at st (slots per level), the scatter passes on sc
-  // apply it level group by level group
-  auto tensor_pass = [&](int64_t lo, int hi, float* st, int64_t slots, cudaStream_t sb) -> int {
-    if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), sb), "memset cursor"))
-      return rc;
+  const int64_t slots = per_round * a.S;
+  for (int64_t lo = 0; lo < R; lo += per_round) {
+    const int hi = (int)std::min<int64_t>(R, lo + per_round);
+    if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 1, 0, sizeof(unsigned int), s), "memset cursor")) return rc;
     {
-      ProfScope ps(kProfBackward, sb);
+      ProfScope ps(kProfBackward, s);
       if constexpr (kLean)
-        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, sb>>>(grid, table, W, a, ws.rays, ws.slot,
-                                                                        ws.counters, out_act, W_grad, (int)lo, hi, st,
-                                                                        slots, order, SL.offs, SL.xstore, SL.xcap);
+        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot,
+                                                                       ws.counters, out_act, W_grad, (int)lo, hi,
+                                                                       stage, slots, order, SL.offs, SL.xstore,
+                                                                       SL.xcap);
       else
-        bwd_mixed_kernel<D, F, L, H, true, ACT><<<blocks, kMixThreads, bsmem, sb>>>(
-            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, st, slots,
+        bwd_mixed_kernel<D, F, L, H, true, ACT><<<blocks, kMixThreads, bsmem, s>>>(
+            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
             order, SL.offs, SL.xstore, SL.xcap);
     }
-    return launch_status("bwd_mixed_kernel");
-  };
-  auto scatter_passes = [&](int64_t lo, int hi, float* st, int64_t slots, cudaStream_t sc) -> int {
+    if (int rc = launch_status("bwd_mixed_kernel")) return rc;
     for (int gi = 0; gi < n_groups; ++gi) {
-      if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 5, 0, sizeof(unsigned int), sc), "memset cursor"))
+      if (int rc = cuda_status(cudaMemsetAsync(ws.counters + 5, 0, sizeof(unsigned int), s), "memset cursor"))
         return rc;
       {
-        ProfScope ps(kProfScatter, sc);
-        ks<<<sblocks, kScatterThreads, 0, sc>>>(grid, a, ws.rays, ws.slot, ws.counters, st, slots, (int)lo, hi,
-                                                group_start[gi], group_start[gi + 1], table_grad, order);
+        ProfScope ps(kProfScatter, s);
+        ks<<<sblocks, kScatterThreads, 0, s>>>(grid, a, ws.rays, ws.slot, ws.counters, stage, slots, (int)lo, hi,
+                                               group_start[gi], group_start[gi + 1], table_grad, order);
       }
       if (int rc = launch_status("scatter_stage_kernel")) return rc;
     }
-    return NECTB_OK;
-  };
-  cudaStream_t aux = (tune.overlap_rounds && per_round >= 2) ? aux_stream() : nullptr;
-  if (!aux) {
-    const int64_t slots = per_round * a.S;
-    for (int64_t lo = 0; lo < R; lo += per_round) {
-      const int hi = (int)std::min<int64_t>(R, lo + per_round);
-      if (int rc = tensor_pass(lo, hi, stage, slots, s)) return rc;
-      if (int rc = scatter_passes(lo, hi, stage, slots, s)) return rc;
-    }
-    return NECTB_OK;
   }
-  // Pipelined rounds over two halves of the staging buffer: round r's
-  // tensor-core pass (stream s) writes half r & 1 once round r - 2's scatter
-  // passes (the aux stream) have read it; round r's scatter passes wait for
-  // its tensor-core pass.  The aux stream starts after the work already on s
-  // and s waits for the aux stream's last pass before anything after this.
-  const int64_t half = per_round / 2;
-  const int64_t slots = half * a.S;
-  float* buf[2] = {stage, stage + (size_t)slots * IN};
-  cudaEvent_t ev[5] = {};  // fork, tensor pass done (2), scatter done (2)
-  int rc = NECTB_OK;
-  for (auto& e : ev)
-    if (!rc) rc = cuda_status(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event create");
-  bool forked = false;
-  if (!rc) rc = cuda_status(cudaEventRecord(ev[0], s), "event record");
-  if (!rc) rc = cuda_status(cudaStreamWaitEvent(aux, ev[0], 0), "stream wait");
-  forked = rc == NECTB_OK;
-  int r = 0;
-  for (int64_t lo = 0; lo < R && !rc; lo += half, ++r) {
-    const int hi = (int)std::min<int64_t>(R, lo + half);
-    const int b = r & 1;
-    if (r >= 2) rc = cuda_status(cudaStreamWaitEvent(s, ev[3 + b], 0), "stream wait");
-    if (!rc) rc = tensor_pass(lo, hi, buf[b], slots, s);
-    if (!rc) rc = cuda_status(cudaEventRecord(ev[1 + b], s), "event record");
-    if (!rc) rc = cuda_status(cudaStreamWaitEvent(aux, ev[1 + b], 0), "stream wait");
-    if (!rc) rc = scatter_passes(lo, hi, buf[b], slots, aux);
-    if (!rc) rc = cuda_status(cudaEventRecord(ev[3 + b], aux), "event record");
-  }
-  if (forked) {  // join the aux stream back, also after an error, so no work is left unordered
-    const int jrc = cuda_status(cudaEventRecord(ev[0], aux), "event record");
-    const int wrc = jrc ? jrc : cuda_status(cudaStreamWaitEvent(s, ev[0], 0), "stream wait");
-    if (!rc) rc = wrc;
-  }
-  for (auto& e : ev)
-    if (e) cudaEventDestroy(e);
-  return rc;
+  return NECTB_OK;
 }
 
 }  // namespace

@@ -202,23 +202,6 @@ def test_staged_and_fused_backward_agree(cuda_device, n_dims, duplicates):
     assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
 
 
-@pytest.mark.parametrize("n_dims,store", [(3, 1), (4, 1), (3, 0)])
-def test_overlapped_rounds_agree(cuda_device, n_dims, store):
-    """Pipelined staged rounds (round r + 1's tensor-core pass beside round
-    r's scatter passes, on two halves of the staging buffer and a second
-    stream) give the sequential rounds' y_pred bit for bit and their
-    gradients up to fp32 reassociation of the reductions."""
-    from nect_b200.trainer import Workspace
-
-    with tuning(overlap_rounds=0, staged_rounds=8, encoding_store=store):
-        (y1, L1, gt1, gm1), _ = run_train_case(n_dims, "mixed", "l2", "cone", False, ws=Workspace(staging=True))
-    with tuning(overlap_rounds=1, staged_rounds=8, encoding_store=store):
-        (y2, L2, gt2, gm2), _ = run_train_case(n_dims, "mixed", "l2", "cone", False, ws=Workspace(staging=True))
-    assert torch.equal(y1, y2)
-    assert rel_max(gt1, gt2) < 1e-5, rel_max(gt1, gt2)
-    assert rel_max(gm1, gm2) < 1e-5, rel_max(gm1, gm2)
-
-
 @pytest.mark.parametrize("n_dims,duplicates,store_rows", [(3, False, 5600), (4, True, 5600), (3, False, 0),
                                                            (4, False, 0)])
 def test_encoding_store_partial_and_absent(cuda_device, n_dims, duplicates, store_rows):
