@@ -144,6 +144,15 @@ int64_t nectb_mlp_param_count(const NectbMLP* mlp);
 int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* params,
                           const float* x, int64_t n, float* out, void* stream);
 
+/* Backward of nectb_hashgrid_encode: for n points x[n*n_dims] and the
+ * gradient of their encodings dout[n * n_levels * n_features], ADDS
+ * sum over points of w_corner * dout into grad (fp32, the table's layout,
+ * 16-byte aligned) with fp32 atomics.  Replaces the tcnn Encoding backward
+ * behind the reference's composite encodings (nect/network/networks.py:
+ * 392-449, QuadCubes). */
+int nectb_hashgrid_encode_backward(const NectbHashGrid* grid, const float* x, int64_t n,
+                                   const float* dout, float* grad, void* stream);
+
 /* Diagnostic: per-level corner indices (entry index within the level, int32)
  * and d-linear weights of n points, idx/w[n][n_levels][2^n_dims].  No
  * counterpart in the reference (tiny-cuda-nn keeps them internal); it lets

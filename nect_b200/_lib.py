@@ -121,6 +121,7 @@ _SIGNATURES = {
         c_i64, [ctypes.POINTER(NectbHashGrid), c_ptr, c_ptr, c_ptr, c_ptr, c_ptr]),
     "nectb_mlp_param_count": (c_i64, [ctypes.POINTER(NectbMLP)]),
     "nectb_hashgrid_encode": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
+    "nectb_hashgrid_encode_backward": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "nectb_hashgrid_corners": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "nectb_model_forward": (
         c_int,

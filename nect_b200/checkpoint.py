@@ -40,7 +40,7 @@ def _adam_state(trainer: Trainer) -> dict:
                     "exp_avg_sq": v.detach().clone()}
     group = {"lr": trainer.lr, "betas": tuple(trainer.betas), "eps": trainer.eps,
              "weight_decay": trainer.weight_decay, "amsgrad": False, "maximize": False, "foreach": None,
-             "capturable": False, "differentiable": False, "fused": None, "params": [0, 1]}
+             "capturable": False, "differentiable": False, "fused": None, "params": sorted(state)}
     return {"state": state, "param_groups": [group]}
 
 
@@ -48,7 +48,9 @@ def _config_dict(model: _HashGridModel) -> dict:
     enc = asdict(model.encoding_config)
     enc.pop("nDetector", None)   # as Config.save drops them (config.py:504-505)
     enc.pop("nVoxel", None)
-    name = "hash_grid_4d" if model.n_dims == 4 else "hash_grid"
+    from .quadcubes import QuadCubes
+
+    name = "quadcubes" if isinstance(model, QuadCubes) else ("hash_grid_4d" if model.n_dims == 4 else "hash_grid")
     return {"model": name, "mode": "dynamic" if model.n_dims == 4 else "static", "precision": model.precision,
             "encoder": enc, "net": asdict(model.network_config), "geometry": "SAME_FOLDER"}
 
@@ -129,6 +131,6 @@ def resume(path: str | Path, model: _HashGridModel, trainer: Trainer | None = No
     model.load_state_dict(data["model"])
     if trainer is not None and "optim" in data:
         st = data["optim"]["state"]
-        trainer.load_optimizer_moments([(st[i]["exp_avg"], st[i]["exp_avg_sq"]) for i in (0, 1)])
+        trainer.load_optimizer_moments([(st[i]["exp_avg"], st[i]["exp_avg_sq"]) for i in sorted(st)])
         trainer.step_count = int(float(st[0]["step"]))
     return {"epoch": data.get("epoch", 0), "angle": data.get("angle", 0)}

@@ -109,7 +109,9 @@ def get_model(cfg: ModelConfig, device="cuda"):
 
     "hash_grid" is the static 3D model; "hash_grid_4d" is a single 4D (z,y,x,t)
     hash grid + MLP behind the dynamic ``model(x, t)`` interface (the 4D component
-    of HyperCubes, nect/network/networks.py:478-481)."""
+    of HyperCubes, nect/network/networks.py:478-481); "quadcubes" is the
+    reference's default dynamic model (networks.py:392-449), four 3D grids
+    and a wide MLP, trained by the module loop (quadcubes.ModuleTrainer)."""
     from .network import HashGrid, HashGrid4D
 
     if cfg.precision not in PRECISIONS:
@@ -118,4 +120,8 @@ def get_model(cfg: ModelConfig, device="cuda"):
         return HashGrid(cfg.encoder, cfg.net, precision=cfg.precision, device=device)
     if cfg.model in ("hash_grid_4d", "hypercubes_4d"):
         return HashGrid4D(cfg.encoder, cfg.net, precision=cfg.precision, device=device)
+    if cfg.model == "quadcubes":
+        from .quadcubes import QuadCubes
+
+        return QuadCubes(cfg.encoder, cfg.net, precision=cfg.precision, device=device)
     raise ValueError(f"Model type {cfg.model} is not supported by the B200 path")

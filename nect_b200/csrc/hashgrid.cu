@@ -106,6 +106,19 @@ __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g,
   }
 }
 
+// One thread per point: the point's encoding gradient dout[l * F + f] added
+// to its corners' entries, weighted (fp32 vector atomics).
+template <int D, int F>
+__global__ void encode_backward_kernel(GridDev g, const float* __restrict__ x, int64_t n,
+                                       const float* __restrict__ dout, float* __restrict__ grad) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float p[D];
+#pragma unroll
+  for (int k = 0; k < D; ++k) p[k] = x[i * D + k];
+  scatter_point<D, F>(g, grad, p, dout + i * (int64_t)g.n_levels * F);
+}
+
 template <int D, int F, typename T>
 int launch_encode(const GridDev& g, const void* params, const float* x, int64_t n, float* out, cudaStream_t s) {
   encode_kernel<D, F, T><<<(unsigned)ceil_div(n, 256), 256, 0, s>>>(g, (const T*)params, x, n, out);
@@ -205,6 +218,30 @@ extern "C" int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* para
   if (n == 0) return NECTB_OK;
   NECTB_REQUIRE(params && x && out && n > 0, "null pointer or negative size");
   return dispatch_encode(g, grid->feature_dtype, params, x, n, out, (cudaStream_t)stream);
+}
+
+extern "C" int nectb_hashgrid_encode_backward(const NectbHashGrid* grid, const float* x, int64_t n,
+                                              const float* dout, float* grad, void* stream) {
+  clear_error();
+  GridDev g;
+  if (!make_grid_dev(grid, &g)) return set_error(NECTB_ERR_INVALID, "invalid hash grid description");
+  if (n == 0) return NECTB_OK;
+  NECTB_REQUIRE(x && dout && grad && n > 0, "null pointer or negative size");
+  NECTB_REQUIRE(((uintptr_t)grad & 15u) == 0, "grad must be 16-byte aligned");
+  cudaStream_t s = (cudaStream_t)stream;
+  const unsigned blocks = (unsigned)ceil_div(n, 256);
+  ProfScope ps(kProfModel, s);
+  if (g.n_dims == 3 && g.n_features == 2)
+    encode_backward_kernel<3, 2><<<blocks, 256, 0, s>>>(g, x, n, dout, grad);
+  else if (g.n_dims == 3 && g.n_features == 4)
+    encode_backward_kernel<3, 4><<<blocks, 256, 0, s>>>(g, x, n, dout, grad);
+  else if (g.n_dims == 4 && g.n_features == 2)
+    encode_backward_kernel<4, 2><<<blocks, 256, 0, s>>>(g, x, n, dout, grad);
+  else if (g.n_dims == 4 && g.n_features == 4)
+    encode_backward_kernel<4, 4><<<blocks, 256, 0, s>>>(g, x, n, dout, grad);
+  else
+    return set_error(NECTB_ERR_INVALID, "unsupported grid (n_dims %d, n_features %d)", g.n_dims, g.n_features);
+  return launch_status("encode_backward_kernel");
 }
 
 namespace {

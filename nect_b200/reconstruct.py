@@ -29,6 +29,7 @@ from .network import _HashGridModel
 from .sampling import Geometry
 from .schedule import Schedule, bin_projection, s3im_patch_size
 from .serving import denormalisation, query_points, volume_items
+from .quadcubes import ModuleTrainer, QuadCubes
 from .trainer import Trainer
 
 
@@ -47,6 +48,8 @@ class Reconstruction:
         """Attenuation on the voxel-centre grid [z, y, x] (create_volume)."""
         shape = tuple(shape or self.geometry.nVoxel)
         scale, offset = denormalisation(self.geometry.max_distance_traveled, self.minimum, self.maximum)
+        if isinstance(self.model, QuadCubes):
+            return self.model.volume(shape, t, scale, offset)
         out = torch.empty(shape, device=self.model.table.device)
         query_points(self.model, volume_items(out, shape, t, scale, offset))
         return out
@@ -57,20 +60,34 @@ def default_model_config(geometry: Geometry, mode: str, precision: str, log2_has
     preset (nect/cfg/static/hash_grid.yaml:1-13): 19 levels x 4 features,
     2^21 entries (unless the quality preset sets another size), base
     resolution 8, finest 2 x the largest detector extent, 6 x 64 LeakyReLU
-    MLP with a ReLU output.  Dynamic: the reference's default (QuadCubes,
-    nect/cfg/dynamic/quadcubes.yaml) is four 3D grids that this path does not
-    build; its single-4D-grid model takes 16 levels x 2 features, temporal
-    base resolution 4 and a 2 x 64 ReLU MLP with a softplus output."""
+    MLP with a ReLU output.  Dynamic: its quadcubes preset
+    (nect/cfg/dynamic/quadcubes.yaml:1-16): four 3D grids of 23 levels x 4
+    features, 2^23 entries (or the preset's size), base resolution 16,
+    finest 2 x the largest detector extent, the raw inputs appended, 4 x 128
+    LeakyReLU MLP without an output activation.  The fused single-4D-grid
+    model ("hash_grid_4d") is the fast dynamic model (fused_dynamic_config)."""
     if mode == "dynamic":
-        enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_hashmap_size,
+        enc = HashEncoderConfig(n_levels=23, n_features_per_level=4, log2_hashmap_size=log2_hashmap_size,
                                 base_resolution=16, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
-                                nVoxel=list(geometry.nVoxel), base_resolution_t=4)
-        return ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision)
+                                nVoxel=list(geometry.nVoxel))
+        net = MLPNetConfig(n_hidden_layers=4, n_neurons=128, activation="LeakyReLU", output_activation="None",
+                           include_identity=True)
+        return ModelConfig("quadcubes", enc, net, precision)
     enc = HashEncoderConfig(n_levels=19, n_features_per_level=4, log2_hashmap_size=log2_hashmap_size,
                             base_resolution=8, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
                             nVoxel=list(geometry.nVoxel))
     net = MLPNetConfig(n_hidden_layers=6, n_neurons=64, activation="LeakyReLU", output_activation="ReLU")
     return ModelConfig("hash_grid", enc, net, precision)
+
+
+def fused_dynamic_config(geometry: Geometry, precision: str, log2_hashmap_size: int = 21) -> ModelConfig:
+    """The dynamic model of the fused kernels: one 4D grid of 16 levels x 2
+    features, temporal base resolution 4, 2 x 64 ReLU MLP with a softplus
+    output (the benchmark's 4D model)."""
+    enc = HashEncoderConfig(n_levels=16, n_features_per_level=2, log2_hashmap_size=log2_hashmap_size,
+                            base_resolution=16, max_resolution_factor=2.0, nDetector=list(geometry.nDetector),
+                            nVoxel=list(geometry.nVoxel), base_resolution_t=4)
+    return ModelConfig("hash_grid_4d", enc, MLPNetConfig(n_hidden_layers=2), precision)
 
 
 # ---------------------------------------------------------- quality presets ----
@@ -294,9 +311,16 @@ def fit(geometry: Geometry, projections: torch.Tensor, angles, timesteps=None, *
     torch.manual_seed(seed)
     model = get_model(cfg, device=dev)
     S = points_per_ray or int(math.ceil(1.5 * max(geometry.nDetector)))
-    trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
-                      loss=loss, lr=lr, betas=tuple(betas), weight_decay=weight_decay, device=dev,
-                      clip_grad_value=clip_grad_value)
+    if isinstance(model, QuadCubes):
+        # the module loop, at most the reference's 5 M points per batch (config.py:380-391)
+        trainer = ModuleTrainer(model, geometry, points_per_batch=min(points_per_batch or rays_per_batch * S,
+                                                                      5_000_000),
+                                points_per_ray=S, loss=loss, lr=lr, betas=tuple(betas), weight_decay=weight_decay,
+                                device=dev, clip_grad_value=clip_grad_value)
+    else:
+        trainer = Trainer(model, geometry, points_per_batch=points_per_batch or rays_per_batch * S, points_per_ray=S,
+                          loss=loss, lr=lr, betas=tuple(betas), weight_decay=weight_decay, device=dev,
+                          clip_grad_value=clip_grad_value)
     n_batches = 10 ** 9 if batch_per_proj == "all" else int(batch_per_proj)
     rec = Reconstruction(model, geometry, mn, mx, trainer)
     if isinstance(cancel_at, str):

@@ -24,8 +24,10 @@ def test_batch_windows(pixels, rays, expect):
 
 def test_default_models_of_reconstruct():
     """Static scans train the reference's default static model
-    (nect/cfg/static/hash_grid.yaml); dynamic scans the single-4D-grid model."""
-    from nect_b200.reconstruct import default_model_config, plan_reconstruction
+    (nect/cfg/static/hash_grid.yaml), dynamic scans its default dynamic model
+    (nect/cfg/dynamic/quadcubes.yaml); the fused single-4D-grid model stays
+    available."""
+    from nect_b200.reconstruct import default_model_config, fused_dynamic_config, plan_reconstruction
     from nect_b200.sampling import Geometry
 
     geo = Geometry(nDetector=[256, 256], dDetector=[1.0, 1.0], mode="cone", DSD=800.0, DSO=400.0,
@@ -36,8 +38,14 @@ def test_default_models_of_reconstruct():
     assert (st.net.n_hidden_layers, st.net.n_neurons, st.net.activation, st.net.output_activation) == (
         6, 64, "LeakyReLU", "ReLU")
     assert abs(st.encoder.per_level_scale - (2 * 256 / 8) ** (1 / 18)) < 1e-12
-    dy = default_model_config(geo, "dynamic", "mixed")
-    assert (dy.model, dy.encoder.n_levels, dy.encoder.n_features_per_level, dy.net.n_hidden_layers) == (
+    dy = default_model_config(geo, "dynamic", "mixed", log2_hashmap_size=23)
+    assert (dy.model, dy.encoder.n_levels, dy.encoder.n_features_per_level, dy.encoder.log2_hashmap_size,
+            dy.encoder.base_resolution) == ("quadcubes", 23, 4, 23, 16)
+    assert (dy.net.n_hidden_layers, dy.net.n_neurons, dy.net.activation, dy.net.output_activation,
+            dy.net.include_identity) == (4, 128, "LeakyReLU", "None", True)
+    assert abs(dy.encoder.per_level_scale - (2 * 256 / 16) ** (1 / 22)) < 1e-12
+    fu = fused_dynamic_config(geo, "mixed")
+    assert (fu.model, fu.encoder.n_levels, fu.encoder.n_features_per_level, fu.net.n_hidden_layers) == (
         "hash_grid_4d", 16, 2, 2)
     plan = plan_reconstruction(geo, "static", 100, quality="poor")
     assert plan.model_cfg.encoder.n_levels == 19 and plan.model_cfg.encoder.log2_hashmap_size == 19

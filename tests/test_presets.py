@@ -82,7 +82,7 @@ def test_plan_with_niter_and_points_per_batch():
     plan = plan_reconstruction(geometry(64), "dynamic", 30, "poor", niter=3, points_per_batch=1_000_000)
     assert plan.schedule.total_projections == 90 and plan.points_per_batch == 500_000
     assert plan.schedule.lr[0] == pytest.approx(2e-3)
-    assert plan.model_cfg.model == "hash_grid_4d" and plan.model_cfg.encoder.log2_hashmap_size == 19
+    assert plan.model_cfg.model == "quadcubes" and plan.model_cfg.encoder.log2_hashmap_size == 19
 
 
 def test_reconstruct_resolves_the_preset_and_turns_the_static_volume(monkeypatch):

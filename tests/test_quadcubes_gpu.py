@@ -1,0 +1,130 @@
+"""The reference's default dynamic model, QuadCubes (nect/network/networks.py:
+392-449): forward and backward against an fp64 restatement built from the
+oracle's hash-grid encoding (four 3D grids over (z,y,x), (y,x,t), (x,z,t),
+(z,y,t), the raw inputs appended, a bias-free MLP), the encoder backward
+kernel against autograd through the oracle, and fit() training it on a
+small dynamic scan through the module loop.
+
+Tolerances: plain fp32 forward within 1e-5 of the largest output, gradients
+within 1e-4 of the largest entry of each parameter."""
+import math
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import hashgrid as ohg
+
+pytestmark = pytest.mark.gpu
+
+
+def make(precision="plain_fp32", identity=True, F=4, hidden=2):
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig
+    from nect_b200.quadcubes import QuadCubes
+
+    enc = HashEncoderConfig(n_levels=6, n_features_per_level=F, log2_hashmap_size=11, base_resolution=4,
+                            finest_resolution=48)
+    net = MLPNetConfig(n_hidden_layers=hidden, n_neurons=128, activation="LeakyReLU", output_activation="None",
+                       include_identity=identity)
+    m = QuadCubes(enc, net, precision=precision, device="cuda", seed=3)
+    with torch.no_grad():
+        g = torch.Generator(device="cpu").manual_seed(5)
+        for tab in m.tables:
+            tab.copy_((torch.rand(tab.shape, generator=g) * 2 - 1) * 0.5)
+    levels, _ = ohg.layout(3, 6, 11, 4.0, float(enc.per_level_scale))
+    return m, levels
+
+
+def oracle_forward(m, levels, x, t, tables=None, weights=None):
+    """fp64 QuadCubes: the four grids' oracle encodings, the raw inputs, the MLP."""
+    x = x.double()
+    tcol = torch.full((x.shape[0], 1), float(t), dtype=torch.float64)
+    ins = [x, torch.cat([x[:, [1, 2]], tcol], 1), torch.cat([x[:, [2, 0]], tcol], 1),
+           torch.cat([x[:, [0, 1]], tcol], 1)]
+    tables = tables if tables is not None else [tab.detach().cpu().double() for tab in m.tables]
+    feats = [ohg.encode(inp.float(), tab, levels, 11) for inp, tab in zip(ins, tables)]
+    if m.include_identity:
+        feats.append(torch.cat([x, tcol], 1))
+    weights = weights if weights is not None else [lin.weight.detach().cpu().double() for lin in m.layers]
+    return ohg.mlp(torch.cat(feats, 1), weights, act="leakyrelu", out_act="none")
+
+
+def rel(a, b):
+    a, b = torch.as_tensor(a).double().flatten(), torch.as_tensor(b).double().flatten()
+    return float((a - b).abs().max() / b.abs().max())
+
+
+@pytest.mark.parametrize("identity", [True, False])
+def test_forward_matches_oracle(cuda_device, identity):
+    m, levels = make(identity=identity)
+    gen = torch.Generator(device="cpu").manual_seed(1)
+    x = torch.rand(3000, 3, generator=gen)
+    for t in (0.0, 0.37, 1.0):
+        y = m(x.cuda(), t)
+        assert y.shape == (3000, 1)
+        assert rel(y.detach().cpu(), oracle_forward(m, levels, x, t)) < 1e-5
+    # a CUDA timestep gives the same values
+    y_dev = m(x.cuda(), torch.tensor(0.37, device="cuda"))
+    assert torch.equal(y_dev, m(x.cuda(), 0.37))
+
+
+def test_backward_matches_fp64_autograd(cuda_device):
+    m, levels = make()
+    gen = torch.Generator(device="cpu").manual_seed(2)
+    x = torch.rand(2000, 3, generator=gen)
+    g = torch.randn(2000, 1, generator=gen)
+    t = 0.61
+    (m(x.cuda(), t) * g.cuda()).sum().backward()
+    tables = [tab.detach().cpu().double().requires_grad_() for tab in m.tables]
+    weights = [lin.weight.detach().cpu().double().requires_grad_() for lin in m.layers]
+    (oracle_forward(m, levels, x, t, tables, weights) * g.double()).sum().backward()
+    for tab, ref in zip(m.tables, tables):
+        assert rel(tab.grad.cpu(), ref.grad) < 1e-4, rel(tab.grad.cpu(), ref.grad)
+    for lin, ref in zip(m.layers, weights):
+        assert rel(lin.weight.grad.cpu(), ref.grad) < 1e-4, rel(lin.weight.grad.cpu(), ref.grad)
+
+
+def test_encoder_backward_kernel_against_autograd(cuda_device):
+    """nectb_hashgrid_encode_backward alone: the table gradient of
+    sum(encode(x) * dout) against autograd through the oracle's encoding."""
+    m, levels = make(F=2)
+    gen = torch.Generator(device="cpu").manual_seed(4)
+    x = torch.rand(5000, 3, generator=gen)
+    from nect_b200.quadcubes import GridEncode
+
+    tab = m.tables[0]
+    out = GridEncode.apply(tab, m.desc, m.n_enc, x.cuda())
+    dout = torch.randn(out.shape, generator=gen)
+    (out * dout.cuda()).sum().backward()
+    ref_tab = tab.detach().cpu().double().requires_grad_()
+    (ohg.encode(x, ref_tab, levels, 11) * dout.double()).sum().backward()
+    assert rel(tab.grad.cpu(), ref_tab.grad) < 1e-5
+
+
+def test_fit_trains_quadcubes_on_a_dynamic_scan(cuda_device):
+    """fit() on dynamic data builds the reference's default dynamic model
+    (here at a small size) and trains it by the module loop: the volume error
+    at t = 0.5 falls."""
+    from nect_b200 import phantoms
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig, ModelConfig
+    from nect_b200.quadcubes import ModuleTrainer, QuadCubes
+    from nect_b200.reconstruct import fit, psnr
+    from nect_b200.sampling import Geometry
+
+    n = 32
+    geo = Geometry(nDetector=[n, n], dDetector=[1 / n, 1 / n], mode="parallel", nVoxel=[n] * 3, dVoxel=[1 / n] * 3)
+    ph = phantoms.ellipsoid_phantom(8, 1)
+    angles = np.linspace(0, 4 * math.pi, 80, endpoint=False)
+    projs = torch.stack([phantoms.ellipsoid_projection(ph, geo, float(a), "cuda") for a in angles])
+    truth = phantoms.ellipsoid_volume(ph, n, "cuda")
+    ts = list(np.linspace(0, 1, len(angles)))
+    enc = HashEncoderConfig(n_levels=8, n_features_per_level=4, log2_hashmap_size=14, base_resolution=4,
+                            finest_resolution=64)
+    net = MLPNetConfig(n_hidden_layers=2, n_neurons=128, activation="LeakyReLU", output_activation="None",
+                       include_identity=True)
+    rec = fit(geo, projs, list(angles), timesteps=ts, model_cfg=ModelConfig("quadcubes", enc, net, "plain_fp32"),
+              niter=400, lr=2e-3, rays_per_batch=1024, points_per_ray=64, seed=0,
+              evaluate=lambda r: {"psnr": psnr(r.volume(0.5), truth)}, eval_every=400)
+    assert isinstance(rec.model, QuadCubes) and isinstance(rec.trainer, ModuleTrainer)
+    first, last = rec.history[0][2]["psnr"], rec.history[-1][2]["psnr"]
+    assert math.isfinite(last) and last > first + 5, (first, last)
