@@ -911,6 +911,49 @@ def run_psnr4d(args):
     print(json.dumps(out))
 
 
+def run_quadcubes(args):
+    """Training throughput of the reference's default dynamic model, QuadCubes
+    (nect/cfg/dynamic/quadcubes.yaml: four 3D grids of 23 levels x 4 features,
+    2^23 entries, the raw inputs appended, 4 x 128 LeakyReLU MLP) on the 4D cone
+    workload's geometry and projections, through the module loop
+    (quadcubes.ModuleTrainer: the library's sampler and encoder kernels, the MLP
+    on cuBLAS, the library's Adam), at the reference's 5 M points per batch; the
+    fused single-4D-grid model's line is the default bench."""
+    from nect_b200.config import get_model
+    from nect_b200.quadcubes import ModuleTrainer
+    from nect_b200.reconstruct import default_model_config
+    from nect_b200.sampling import Geometry
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    spec = workload_spec("c3_dynamic_cone", "mixed")
+    geometry = Geometry(**spec["geo"])
+    S = spec["S"]
+    cfg = default_model_config(geometry, "dynamic", args.precision, log2_hashmap_size=23)
+    model = get_model(cfg, device=dev)
+    projs, angles, ts = make_projections(spec, geometry, 8, dev)
+    tr = ModuleTrainer(model, geometry, points_per_batch=5_000_000, points_per_ray=S, loss="l2", lr=2e-4, device=dev)
+    P = projs.shape[1]
+
+    def batch(k):
+        perm = torch.randperm(P, dtype=torch.int64, device=dev)
+        return tr.make_batch(perm, 0, angles[k % len(angles)], projs[k % len(angles)], ts[k % len(angles)])
+
+    for k in range(args.warmup):
+        tr.step(batch(k))
+    ms, _ = time_steps(tr, batch, args.steps, args.warmup, 1)
+    rays = tr.batch_size
+    params = sum(p.numel() for p in model.parameters())
+    print(json.dumps({
+        "metric": "train rays/s fwd+bwd, the reference's default dynamic model (QuadCubes) through the module loop",
+        "value": rays * args.steps / (ms / 1e3), "unit": "rays/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "precision": args.precision,
+        "rays_per_step": rays, "samples_per_ray": S, "parameters": params,
+        "config": {"workload": "c3_dynamic_cone geometry and projections; QuadCubes 4 x (23 levels x 4 features, "
+                               "2^23), identity inputs, MLP 4 x 128 LeakyReLU, 5 M points per batch"},
+        "data": "synthetic (seeded dynamic porous phantom)"}))
+
+
 def run_scan(args):
     """Continuous-scan training steps (nect/trainers/continous_scanning_trainer.py:
     85-140) on the 4D cone workload: each step's prediction averages k
@@ -963,7 +1006,14 @@ def run_scan(args):
 
 
 if __name__ == "__main__":
-    if "--scan" in sys.argv:
+    if "--quadcubes" in sys.argv:
+        ap = argparse.ArgumentParser()
+        ap.add_argument("--quadcubes", action="store_true")
+        ap.add_argument("--steps", type=int, default=10)
+        ap.add_argument("--warmup", type=int, default=3)
+        ap.add_argument("--precision", default="mixed", choices=["mixed", "plain_fp32"])
+        run_quadcubes(ap.parse_args())
+    elif "--scan" in sys.argv:
         ap = argparse.ArgumentParser()
         ap.add_argument("--scan", action="store_true")
         ap.add_argument("--sub-angles", type=int, default=4)
