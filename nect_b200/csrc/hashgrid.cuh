@@ -35,6 +35,7 @@ struct GridDev {
   uint32_t stride[NECTB_MAX_LEVELS][4];
   int64_t offset[NECTB_MAX_LEVELS];  // first entry of level l
   int64_t total_entries;
+  unsigned long long tex = 0;        // texture object over an fp16 table (0: none)
 };
 
 // Host: fill GridDev from the C-ABI description (returns false when invalid).

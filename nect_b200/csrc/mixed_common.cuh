@@ -103,6 +103,18 @@ __device__ __forceinline__ void encode_row(const GridDev& g, const __half* __res
         LevelCorners<D> lc;
         level_corners<D>(g, l, p, lc);
         float vals[1 << D][F];
+        // the odd hashed levels' corners through the texture path (a second
+        // L1 data pipe beside the load/store unit's), the others as loads
+        if (F == 2 && g.tex && ((g.hashed_bits >> l) & 1u) && (l & 1)) {
+#pragma unroll
+          for (int c = 0; c < (1 << D); ++c) {
+            const unsigned int raw =
+                tex1Dfetch<unsigned int>((cudaTextureObject_t)g.tex, (int)(g.offset[l] + lc.idx[c]));
+            const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw));
+            vals[c][0] = v.x;
+            vals[c][F - 1] = v.y;
+          }
+        } else
 #pragma unroll
         for (int c = 0; c < (1 << D); ++c) Feat<F, __half>::load(table, g.offset[l] + lc.idx[c], vals[c]);
 #pragma unroll

@@ -371,7 +371,7 @@ size_t staging_bytes(const NectbHashGrid* grid, int R, int P, int S) {
                  align256(rows * row_bytes);
   GridDev g;
   if (tune.time_slice && grid->n_dims == 4 && make_grid_dev(grid, &g))
-    bytes += slice_bytes(g) + 256;  // the time slice and its gradient
+    bytes += slice_bytes(g) + 512;  // the time slice (512-byte aligned) and its gradient
   return bytes;
 }
 }  // namespace

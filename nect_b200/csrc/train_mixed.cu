@@ -24,6 +24,9 @@
 // One thread issues the MMAs and commits them to an mbarrier; every wait is
 // bounded and reports through an error word instead of hanging.
 #include <algorithm>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 #include "mixed_common.cuh"
 #include "train_common.cuh"
@@ -954,6 +957,36 @@ __global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, fl
   }
 }
 
+// A texture object over an fp16 table of 4-byte entries (created once per
+// buffer and kept), or 0 when the table exceeds the 1D linear texture width
+// or is not aligned for a texture.
+cudaTextureObject_t table_texture(const void* ptr, size_t bytes) {
+  static std::mutex mu;
+  static std::vector<std::tuple<const void*, size_t, cudaTextureObject_t>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& e : cache)
+    if (std::get<0>(e) == ptr && std::get<1>(e) == bytes) return std::get<2>(e);
+  int dev = 0, maxw = 0, align = 512;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture1DLinearWidth, dev);
+  cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev);
+  if (bytes / 4 > (size_t)maxw || align <= 0 || (reinterpret_cast<uintptr_t>(ptr) % (uintptr_t)align) != 0) return 0;
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = const_cast<void*>(ptr);
+  rd.res.linear.desc = cudaCreateChannelDesc<unsigned int>();
+  rd.res.linear.sizeInBytes = bytes;
+  cudaTextureDesc td = {};
+  td.readMode = cudaReadModeElementType;
+  cudaTextureObject_t tex = 0;
+  if (cudaCreateTextureObject(&tex, &rd, &td, nullptr) != cudaSuccess) {
+    cudaGetLastError();  // no texture: the loads take the LSU path
+    return 0;
+  }
+  cache.emplace_back(ptr, bytes, tex);
+  return tex;
+}
+
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
 // slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
 template <int D, int F, int L, int H, int ACT>
@@ -983,7 +1016,9 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
         ws3.stage = nullptr;
         ws3.stage_bytes = 0;
       } else {
-        ws3.stage_bytes = (ws.stage_bytes - sb) & ~size_t(255);
+        // the slice starts on a 512-byte boundary (a texture's alignment)
+        const uintptr_t st = reinterpret_cast<uintptr_t>(ws.stage);
+        ws3.stage_bytes = (size_t)(((st + ws.stage_bytes - sb) & ~uintptr_t(511)) - st);
         t3 = reinterpret_cast<__half*>(reinterpret_cast<char*>(ws.stage) + ws3.stage_bytes);
       }
       float* g3 =
@@ -1039,6 +1074,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   }
   using Shape = InShape<L, F>;
   constexpr int IN = Shape::IN, KT = Shape::KT;
+  GridDev gt = grid;  // the grid with a texture over the fp16 table for the encoders' gathers
+  if constexpr (F == 2) gt.tex = table_texture(table, (size_t)grid.total_entries * F * sizeof(__half));
   const int R = a.num_rays;
   // staging region: ray order and sample offsets, the encoding store (bf16
   // input rows with their zero padding), then dL/d(encoding) of one round of
@@ -1066,7 +1103,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     set_smem(k, smem, shares_sms);
     {
       ProfScope ps(kProfForward, s);
-      k<<<fblocks, kMixThreads * wgs, smem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
+      k<<<fblocks, kMixThreads * wgs, smem, s>>>(gt, table, W, a, ws.rays, ws.slot, ws.counters, out_act, y_pred, loss,
                                            SL.xstore ? SL.order : nullptr, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("fwd_mixed_kernel")) return rc;
@@ -1080,7 +1117,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     auto k = bwd_mixed_kernel<D, F, L, H, false, ACT>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bsmem);
     ProfScope ps(kProfBackward, s);
-    k<<<blocks, kMixThreads, bsmem, s>>>(grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
+    k<<<blocks, kMixThreads, bsmem, s>>>(gt, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad,
                                          W_grad, 0, 0x7fffffff, nullptr, 0, nullptr, nullptr, nullptr, 0u);
     return launch_status("bwd_mixed_kernel");
   }
@@ -1129,13 +1166,13 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     {
       ProfScope ps(kProfBackward, s);
       if constexpr (kLean)
-        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, s>>>(grid, table, W, a, ws.rays, ws.slot,
+        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, s>>>(gt, table, W, a, ws.rays, ws.slot,
                                                                        ws.counters, out_act, W_grad, (int)lo, hi,
                                                                        stage, slots, order, SL.offs, SL.xstore,
                                                                        SL.xcap);
       else
         bwd_mixed_kernel<D, F, L, H, true, ACT><<<blocks, kMixThreads, bsmem, s>>>(
-            grid, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
+            gt, table, W, a, ws.rays, ws.slot, ws.counters, out_act, table_grad, W_grad, (int)lo, hi, stage, slots,
             order, SL.offs, SL.xstore, SL.xcap);
     }
     if (int rc = launch_status("bwd_mixed_kernel")) return rc;
