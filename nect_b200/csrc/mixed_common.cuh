@@ -105,14 +105,24 @@ __device__ __forceinline__ void encode_row(const GridDev& g, const __half* __res
         float vals[1 << D][F];
         // the odd hashed levels' corners through the texture path (a second
         // L1 data pipe beside the load/store unit's), the others as loads
-        if (F == 2 && g.tex && ((g.hashed_bits >> l) & 1u) && (l & 1)) {
+        if (g.tex && ((g.hashed_bits >> l) & 1u) && (l & 1)) {
 #pragma unroll
           for (int c = 0; c < (1 << D); ++c) {
-            const unsigned int raw =
-                tex1Dfetch<unsigned int>((cudaTextureObject_t)g.tex, (int)(g.offset[l] + lc.idx[c]));
-            const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw));
-            vals[c][0] = v.x;
-            vals[c][F - 1] = v.y;
+            const int e = (int)(g.offset[l] + lc.idx[c]);
+            if constexpr (F == 2) {
+              const unsigned int raw = tex1Dfetch<unsigned int>((cudaTextureObject_t)g.tex, e);
+              const float2 v = __half22float2(*reinterpret_cast<const __half2*>(&raw));
+              vals[c][0] = v.x;
+              vals[c][1] = v.y;
+            } else {
+              const uint2 raw = tex1Dfetch<uint2>((cudaTextureObject_t)g.tex, e);
+              const float2 a = __half22float2(*reinterpret_cast<const __half2*>(&raw.x));
+              const float2 b = __half22float2(*reinterpret_cast<const __half2*>(&raw.y));
+              vals[c][0] = a.x;
+              vals[c][1] = a.y;
+              vals[c][2] = b.x;
+              vals[c][3] = b.y;
+            }
           }
         } else
 #pragma unroll

@@ -957,24 +957,25 @@ __global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, fl
   }
 }
 
-// A texture object over an fp16 table of 4-byte entries (created once per
-// buffer and kept), or 0 when the table exceeds the 1D linear texture width
-// or is not aligned for a texture.
-cudaTextureObject_t table_texture(const void* ptr, size_t bytes) {
+// A texture object over an fp16 table of entry_bytes-byte entries (4: two
+// features, 8: four; created once per buffer and kept), or 0 when the table
+// exceeds the 1D linear texture width or is not aligned for a texture.
+cudaTextureObject_t table_texture(const void* ptr, size_t bytes, int entry_bytes) {
   static std::mutex mu;
-  static std::vector<std::tuple<const void*, size_t, cudaTextureObject_t>> cache;
+  static std::vector<std::tuple<const void*, size_t, cudaTextureObject_t, int>> cache;
   std::lock_guard<std::mutex> lk(mu);
   for (auto& e : cache)
-    if (std::get<0>(e) == ptr && std::get<1>(e) == bytes) return std::get<2>(e);
+    if (std::get<0>(e) == ptr && std::get<1>(e) == bytes && std::get<3>(e) == entry_bytes) return std::get<2>(e);
   int dev = 0, maxw = 0, align = 512;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture1DLinearWidth, dev);
   cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev);
-  if (bytes / 4 > (size_t)maxw || align <= 0 || (reinterpret_cast<uintptr_t>(ptr) % (uintptr_t)align) != 0) return 0;
+  if (bytes / entry_bytes > (size_t)maxw || align <= 0 || (reinterpret_cast<uintptr_t>(ptr) % (uintptr_t)align) != 0)
+    return 0;
   cudaResourceDesc rd = {};
   rd.resType = cudaResourceTypeLinear;
   rd.res.linear.devPtr = const_cast<void*>(ptr);
-  rd.res.linear.desc = cudaCreateChannelDesc<unsigned int>();
+  rd.res.linear.desc = entry_bytes == 8 ? cudaCreateChannelDesc<uint2>() : cudaCreateChannelDesc<unsigned int>();
   rd.res.linear.sizeInBytes = bytes;
   cudaTextureDesc td = {};
   td.readMode = cudaReadModeElementType;
@@ -983,7 +984,7 @@ cudaTextureObject_t table_texture(const void* ptr, size_t bytes) {
     cudaGetLastError();  // no texture: the loads take the LSU path
     return 0;
   }
-  cache.emplace_back(ptr, bytes, tex);
+  cache.emplace_back(ptr, bytes, tex, entry_bytes);
   return tex;
 }
 
@@ -1075,7 +1076,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   using Shape = InShape<L, F>;
   constexpr int IN = Shape::IN, KT = Shape::KT;
   GridDev gt = grid;  // the grid with a texture over the fp16 table for the encoders' gathers
-  if constexpr (F == 2) gt.tex = table_texture(table, (size_t)grid.total_entries * F * sizeof(__half));
+  gt.tex = table_texture(table, (size_t)grid.total_entries * F * sizeof(__half), F * (int)sizeof(__half));
   const int R = a.num_rays;
   // staging region: ray order and sample offsets, the encoding store (bf16
   // input rows with their zero padding), then dL/d(encoding) of one round of
