@@ -243,8 +243,10 @@ int launch_query_mixed(const GridDev& g, const void* table, const float* W, cons
   set_smem(k, smem, true);
   int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, 3 * sm_count()));
   if (max_blocks > 0) blocks = std::min(blocks, max_blocks);
+  GridDev gt = g;  // with a texture over the table for the gathers
+  gt.tex = table_texture(table, (size_t)g.total_entries * F * sizeof(__half), F * (int)sizeof(__half));
   ProfScope ps(kProfModel, s);
-  k<<<blocks, kQThreads, smem, s>>>(g, (const __half*)table, W, items, n, chunks, counter, oact);
+  k<<<blocks, kQThreads, smem, s>>>(gt, (const __half*)table, W, items, n, chunks, counter, oact);
   return launch_status("query_mixed_kernel");
 }
 
@@ -459,5 +461,5 @@ extern "C" size_t nectb_query_reproject_slice_bytes(const NectbHashGrid* grid, c
   GridDev g;
   if (!grid || !mlp || pixel_count < 1 || !make_grid_dev(grid, &g)) return 0;
   if (g.n_dims != 4 || mlp->compute_dtype == NECTB_F32 || grid->feature_dtype != NECTB_F16) return 0;
-  return slice_half_bytes(g) + 256;
+  return slice_half_bytes(g) + 512;
 }

@@ -236,6 +236,11 @@ inline size_t slice_bytes(const GridDev& g) {
   return align256((size_t)n3 * g.n_features * 2) + align256((size_t)n3 * g.n_features * 4);
 }
 
+// A texture object over an fp16 table (entry_bytes 4 or 8), cached per
+// buffer, or 0 where none can be made; the encoders fetch the odd hashed
+// levels' corners through it.
+cudaTextureObject_t table_texture(const void* ptr, size_t bytes, int entry_bytes);
+
 // Bytes of the fp16 time slice alone (forward-only queries).
 inline size_t slice_half_bytes(const GridDev& g) {
   return align256((size_t)make_time_slice(g, 0.f).g3.total_entries * g.n_features * 2);

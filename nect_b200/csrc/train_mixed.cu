@@ -957,36 +957,6 @@ __global__ void time_spread_kernel(TimeSlice s, const float* __restrict__ g3, fl
   }
 }
 
-// A texture object over an fp16 table of entry_bytes-byte entries (4: two
-// features, 8: four; created once per buffer and kept), or 0 when the table
-// exceeds the 1D linear texture width or is not aligned for a texture.
-cudaTextureObject_t table_texture(const void* ptr, size_t bytes, int entry_bytes) {
-  static std::mutex mu;
-  static std::vector<std::tuple<const void*, size_t, cudaTextureObject_t, int>> cache;
-  std::lock_guard<std::mutex> lk(mu);
-  for (auto& e : cache)
-    if (std::get<0>(e) == ptr && std::get<1>(e) == bytes && std::get<3>(e) == entry_bytes) return std::get<2>(e);
-  int dev = 0, maxw = 0, align = 512;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture1DLinearWidth, dev);
-  cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev);
-  if (bytes / entry_bytes > (size_t)maxw || align <= 0 || (reinterpret_cast<uintptr_t>(ptr) % (uintptr_t)align) != 0)
-    return 0;
-  cudaResourceDesc rd = {};
-  rd.resType = cudaResourceTypeLinear;
-  rd.res.linear.devPtr = const_cast<void*>(ptr);
-  rd.res.linear.desc = entry_bytes == 8 ? cudaCreateChannelDesc<uint2>() : cudaCreateChannelDesc<unsigned int>();
-  rd.res.linear.sizeInBytes = bytes;
-  cudaTextureDesc td = {};
-  td.readMode = cudaReadModeElementType;
-  cudaTextureObject_t tex = 0;
-  if (cudaCreateTextureObject(&tex, &rd, &td, nullptr) != cudaSuccess) {
-    cudaGetLastError();  // no texture: the loads take the LSU path
-    return 0;
-  }
-  cache.emplace_back(ptr, bytes, tex, entry_bytes);
-  return tex;
-}
 
 // Level groups of the staged scatter: consecutive levels whose fp32 gradient
 // slices add up to at most the tuning's scatter_group_bytes (48 MiB by default).
@@ -1006,14 +976,14 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     // the start of its staging region, and runs without staging.
     const bool piece = args.fwd_warpgroups > 0 && !table_grad;
     const size_t sb = piece ? slice_half_bytes(grid) : slice_bytes(grid);
-    const size_t need = piece ? sb : sb + order_bytes(args.num_rays, args.n_pixels) + (size_t(1) << 20);
+    const size_t need = piece ? sb + 512 : sb + order_bytes(args.num_rays, args.n_pixels) + (size_t(1) << 20);
     if (tune.time_slice && args.max_blocks == 0 && ws.stage && ws.stage_bytes >= need) {
       const TimeSlice ts = make_time_slice(grid, args.t);
       const int64_t n3 = ts.g3.total_entries;
       Workspace ws3 = ws;
       __half* t3;
-      if (piece) {
-        t3 = reinterpret_cast<__half*>(ws.stage);
+      if (piece) {  // on a 512-byte boundary (a texture's alignment)
+        t3 = reinterpret_cast<__half*>((reinterpret_cast<uintptr_t>(ws.stage) + 511) & ~uintptr_t(511));
         ws3.stage = nullptr;
         ws3.stage_bytes = 0;
       } else {
@@ -1220,6 +1190,37 @@ int train_mixed(const NectbGeometry& geo, const GridDev& grid, const NectbMLP& m
   if (rc != kUnsupportedShape) return rc;
   return set_error(NECTB_ERR_INVALID, "mixed path: unsupported model shape (n_dims %d, n_features %d, n_levels %d, "
                    "hidden %d)", D, F, L, H);
+}
+
+// A texture object over an fp16 table of entry_bytes-byte entries (4: two
+// features, 8: four; created once per buffer and kept), or 0 when the table
+// exceeds the 1D linear texture width or is not aligned for a texture.
+cudaTextureObject_t table_texture(const void* ptr, size_t bytes, int entry_bytes) {
+  static std::mutex mu;
+  static std::vector<std::tuple<const void*, size_t, cudaTextureObject_t, int>> cache;
+  std::lock_guard<std::mutex> lk(mu);
+  for (auto& e : cache)
+    if (std::get<0>(e) == ptr && std::get<1>(e) == bytes && std::get<3>(e) == entry_bytes) return std::get<2>(e);
+  int dev = 0, maxw = 0, align = 512;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxw, cudaDevAttrMaxTexture1DLinearWidth, dev);
+  cudaDeviceGetAttribute(&align, cudaDevAttrTextureAlignment, dev);
+  if (bytes / entry_bytes > (size_t)maxw || align <= 0 || (reinterpret_cast<uintptr_t>(ptr) % (uintptr_t)align) != 0)
+    return 0;
+  cudaResourceDesc rd = {};
+  rd.resType = cudaResourceTypeLinear;
+  rd.res.linear.devPtr = const_cast<void*>(ptr);
+  rd.res.linear.desc = entry_bytes == 8 ? cudaCreateChannelDesc<uint2>() : cudaCreateChannelDesc<unsigned int>();
+  rd.res.linear.sizeInBytes = bytes;
+  cudaTextureDesc td = {};
+  td.readMode = cudaReadModeElementType;
+  cudaTextureObject_t tex = 0;
+  if (cudaCreateTextureObject(&tex, &rd, &td, nullptr) != cudaSuccess) {
+    cudaGetLastError();  // no texture: the loads take the LSU path
+    return 0;
+  }
+  cache.emplace_back(ptr, bytes, tex, entry_bytes);
+  return tex;
 }
 
 // The fp16 time slice of a 4D fp16 table at t (layout make_time_slice(grid, t).g3).

@@ -398,7 +398,7 @@ class QueryServer:
         self.piece_pixels = min(piece_pixels, P)
         ws = (reproject_workspace_bytes(model, geometry, self.piece_pixels) + 255) // 256 * 256
         # a volume of a 4D mixed model is evaluated on a time slice at its t, built once per request
-        self.slice_bytes = (time_slice_bytes(model) + 255) // 256 * 256
+        self.slice_bytes = (time_slice_bytes(model) + 511) // 512 * 512   # texture alignment
         per = {"slice": 8 * max_slice ** 2, "volume": 8 * max_volume ** 3 + self.slice_bytes, "reproject": 8 * P + ws}
         nslots = {k: max(1, min(max_slots, int(memory_budget * f // per[k])))
                   for k, f in zip(("slice", "reproject", "volume"), slot_mix)}

@@ -71,7 +71,7 @@ def test_slice_room_only_for_4d_mixed_models():
     assert _lib.lib.nectb_hashgrid_layout(ctypes.byref(g4), ctypes.addressof(res), ctypes.addressof(rt),
                                           ctypes.addressof(off), ctypes.addressof(ent), ctypes.addressof(hsh)) > 0
     n3 = sum(1 << 12 if hsh[l] else ((res[l] + 1) ** 3 + 7) // 8 * 8 for l in range(L))
-    want = (n3 * 2 * 2 + 255) // 256 * 256 + 256
+    want = (n3 * 2 * 2 + 255) // 256 * 256 + 512
     assert _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(g4), ctypes.byref(mlp()), 100) == want
 
 
@@ -82,7 +82,7 @@ def test_time_slice_arguments():
     g4 = grid(4)
     n = _lib.lib.nectb_time_slice_bytes(ctypes.byref(g4))
     assert n > 0
-    assert (n + 255) // 256 * 256 + 256 == _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(g4),
+    assert (n + 255) // 256 * 256 + 512 == _lib.lib.nectb_query_reproject_slice_bytes(ctypes.byref(g4),
                                                                                        ctypes.byref(mlp()), 1)
     assert _lib.lib.nectb_time_slice_bytes(ctypes.byref(grid(3))) == 0
     assert _lib.lib.nectb_time_slice_bytes(ctypes.byref(grid(4, _lib.F32))) == 0
