@@ -154,7 +154,7 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
                 const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
                 const float* dloss_dy, float* grid_grad, float* mlp_grad, float* y_pred, float* loss,
                 void* workspace, size_t workspace_size, void* stream, int phase, const float* sub_angles = nullptr,
-                int sub = 1) {
+                int sub = 1, bool texture = true) {
   clear_error();
   if (int rc = validate_geometry(geometry)) return rc;
   GridDev g;
@@ -204,6 +204,7 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
   a.loss_type = batch->loss_type;
   a.loss_scale = batch->loss_scale;
   a.max_blocks = 0;
+  a.texture = texture;
   a.phase = phase;
   a.sub = sub;
   for (int j = 0; j < sub; ++j) a.sub_angle[j] = sub_angles ? sub_angles[j] : batch->angle_rad;
@@ -264,6 +265,16 @@ int train_entry(const NectbGeometry* geometry, const NectbHashGrid* grid, const 
 }
 
 }  // namespace
+
+// The fused training step with loads only: no texture object is made over
+// the table (the allocation-free entry point creates no driver objects).
+int train_step_loads_only(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                          const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                          float* grid_grad, float* mlp_grad, float* y_pred, float* loss, void* workspace,
+                          size_t workspace_size, void* stream) {
+  return train_entry(geometry, grid, mlp, grid_params, mlp_params, batch, nullptr, grid_grad, mlp_grad, y_pred, loss,
+                     workspace, workspace_size, stream, kPhaseForward | kPhaseBackward, nullptr, 1, false);
+}
 }  // namespace nectb
 
 extern "C" size_t nectb_train_scan_workspace_bytes(const NectbGeometry* geometry, const NectbHashGrid* grid,

@@ -50,6 +50,9 @@ struct TrainArgs {
   // > 0: the forward runs one block of this many warpgroups per SM under the
   // shared-SM carveout (re-projection pieces beside serving kernels); 0: the tuning's
   int fwd_warpgroups = 0;
+  // the encoders may fetch corners through a texture object over the table
+  // (false: loads only, no texture object created)
+  bool texture = true;
   int phase = kPhaseForward | kPhaseBackward;  // which half of the step to run
   float run_threshold = 0.75f;                 // run merging of the scatter (set from the tuning)
   // Continuous scan (sub > 1): num_rays = sub * (pixels of the batch) virtual

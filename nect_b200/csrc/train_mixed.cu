@@ -1046,7 +1046,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   using Shape = InShape<L, F>;
   constexpr int IN = Shape::IN, KT = Shape::KT;
   GridDev gt = grid;  // the grid with a texture over the fp16 table for the encoders' gathers
-  gt.tex = table_texture(table, (size_t)grid.total_entries * F * sizeof(__half), F * (int)sizeof(__half));
+  if (a.texture)
+    gt.tex = table_texture(table, (size_t)grid.total_entries * F * sizeof(__half), F * (int)sizeof(__half));
   const int R = a.num_rays;
   // staging region: ray order and sample offsets, the encoding store (bf16
   // input rows with their zero padding), then dL/d(encoding) of one round of

@@ -26,6 +26,10 @@ extern "C" size_t nectb_train_workspace_bytes(const NectbGeometry* geometry, con
 
 namespace nectb {
 int validate_geometry(const NectbGeometry* g);
+int train_step_loads_only(const NectbGeometry* geometry, const NectbHashGrid* grid, const NectbMLP* mlp,
+                          const void* grid_params, const float* mlp_params, const NectbTrainBatch* batch,
+                          float* grid_grad, float* mlp_grad, float* y_pred, float* loss, void* workspace,
+                          size_t workspace_size, void* stream);
 namespace {
 
 constexpr size_t kStaticScratchBytes = (size_t(20) << 20) + 4096;
@@ -65,8 +69,10 @@ extern "C" int nectb_train_step_static(const NectbGeometry* geometry, const Nect
                      need, kStaticScratchBytes);
   void* scratch = nullptr;
   if (int rc = scratch_address(&scratch)) return rc;
-  return nectb_train_step(geometry, grid, mlp, grid_params, mlp_params, batch, grid_grad, mlp_grad, y_pred, loss,
-                          scratch, kStaticScratchBytes, stream);
+  // the step of nectb_train_step on the static scratch, with plain loads (no
+  // texture object: nothing is created on the caller's behalf)
+  return train_step_loads_only(geometry, grid, mlp, grid_params, mlp_params, batch, grid_grad, mlp_grad, y_pred,
+                               loss, scratch, kStaticScratchBytes, stream);
 }
 
 extern "C" const unsigned int* nectb_train_error_word(const NectbGeometry* geometry, int32_t num_rays,
