@@ -13,7 +13,7 @@ def test_tuning_round_trip_and_validation():
         autotune.set_tuning({"staged_rounds": 16, "run_threshold_3d": 0.5, "scatter_group_bytes": 8 << 20})
         now = autotune.get_tuning()
         assert now["staged_rounds"] == 16 and now["run_threshold_3d"] == 0.5 and now["scatter_group_bytes"] == 8 << 20
-        for bad in ({"forward_blocks_per_sm": 0}, {"forward_blocks_per_sm": 7}, {"backward_blocks_per_sm": 5},
+        for bad in ({"forward_blocks_per_sm": 0}, {"forward_blocks_per_sm": 7}, {"backward_blocks_per_sm": 4},
                     {"staged_rounds": 65}, {"scatter_group_bytes": 1000}, {"run_threshold_4d": -1.0}, {"encoding_store": 2}):
             with pytest.raises(RuntimeError):
                 autotune.set_tuning(bad)
