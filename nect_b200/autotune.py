@@ -26,7 +26,7 @@ FIELDS = ("forward_blocks_per_sm", "backward_blocks_per_sm", "scatter_blocks_per
 # candidates per tunable, tried one tunable at a time
 SPACE = {
     "forward_blocks_per_sm": (4, 5, 6),
-    "backward_blocks_per_sm": (3, 4),
+    "backward_blocks_per_sm": (2, 3),
     "scatter_blocks_per_sm": (0, 2, 3),
     "staged_rounds": (4, 8, 16),
     "scatter_group_bytes": (24 << 20, 48 << 20, 96 << 20),

@@ -136,7 +136,7 @@ extern "C" int nectb_set_tuning(const NectbTuning* t) {
   NECTB_REQUIRE(t, "null tuning");
   NECTB_REQUIRE(t->forward_blocks_per_sm >= 1 && t->forward_blocks_per_sm <= kFwdMaxWarpgroups,
                 "forward_blocks_per_sm must be 1..%d", kFwdMaxWarpgroups);
-  NECTB_REQUIRE(t->backward_blocks_per_sm >= 1 && t->backward_blocks_per_sm <= 4, "backward_blocks_per_sm must be 1..4");
+  NECTB_REQUIRE(t->backward_blocks_per_sm >= 1 && t->backward_blocks_per_sm <= 3, "backward_blocks_per_sm must be 1..3");
   NECTB_REQUIRE(t->scatter_blocks_per_sm >= 0 && t->scatter_blocks_per_sm <= 8, "scatter_blocks_per_sm must be 0..8");
   NECTB_REQUIRE(t->staged_rounds >= 1 && t->staged_rounds <= 64, "staged_rounds must be 1..64");
   NECTB_REQUIRE(t->scatter_group_bytes >= (int64_t(1) << 20), "scatter_group_bytes must be at least 1 MiB");

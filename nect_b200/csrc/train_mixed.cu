@@ -605,16 +605,8 @@ bwd_mixed_kernel(GridDev grid, const __half* __restrict__ table, const float* __
 //   Shared memory: W0, W1 | G2 | zero block | A1, then G1 | X.
 //   Accumulator rows are read 16 columns at a time; the w_out gradient is a
 //   16-column butterfly reduce-scatter per chunk.
-// Warpgroups of the lean backward per SM: one block of up to four, sharing
-// the weight tiles; each has its own G2 | zero block | A1/G1 | X region,
-// 128 TMEM columns, mbarrier and named barrier.
-constexpr int kLeanMaxWG = 4;
-constexpr uint32_t kLeanZero = 2048;                   // one K step of a 64-element MN block
-constexpr uint32_t kLeanRegion = 3 * kTile + kLeanZero;  // a warpgroup's tiles (1024-aligned size)
-static_assert(kLeanRegion % 1024 == 0, "warpgroup regions keep the tiles' 1024-byte alignment");
-
 template <int D, int F, int ACT>
-__global__ void __launch_bounds__(kLeanMaxWG * kMixThreads, 1)
+__global__ void __launch_bounds__(kMixThreads, 3)
 bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __restrict__ W, TrainArgs a,
                 const RayRec* __restrict__ recs, const int32_t* __restrict__ slot, unsigned int* __restrict__ ctrl,
                 int out_act, float* __restrict__ W_grad, int lo, int hi, float* __restrict__ stage,
@@ -630,38 +622,34 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   const uint32_t xrows = xstore ? min(xcap, ctrl[7]) : 0u;
   extern __shared__ uint8_t smem_raw[];
   uint8_t* base = align1024(smem_raw);
-  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const int n_wg = blockDim.x / kMixThreads;
-  const int wg = t / kMixThreads, r = t % kMixThreads, wq = warp & 3;  // warpgroup, tile row, lane quarter
-  uint8_t* sW = base;                                        // W0, W1 (shared by the warpgroups)
-  uint8_t* sG = sW + H * kWTile + wg * kLeanRegion;          // this warpgroup's G2
-  uint8_t* sZ = sG + kTile;                                  // zeros (1024-aligned)
-  uint8_t* sA = sZ + kLeanZero;                              // A1, then G1
-  uint8_t* sX = sA + kTile;                                  // X
-  float* sWout = reinterpret_cast<float*>(sW + H * kWTile + n_wg * kLeanRegion);
-  uint64_t* bars = reinterpret_cast<uint64_t*>(sWout + 64);  // [kLeanMaxWG]
-  uint64_t* bar = bars + wg;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + kLeanMaxWG);
-  float* red = reinterpret_cast<float*>(tslot + 4);          // [64] the block's w_out gradient
+  constexpr uint32_t kZero = 2048;    // one K step of a 64-element MN block
+  uint8_t* sW = base;                 // W0, W1
+  uint8_t* sG = sW + H * kWTile;      // G2
+  uint8_t* sZ = sG + kTile;           // zeros (1024-aligned)
+  uint8_t* sA = sZ + kZero;           // A1, then G1
+  uint8_t* sX = sA + kTile;           // X
+  float* sWout = reinterpret_cast<float*>(sX + kTile);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(sWout + 64);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bar + 1);
+  float* red = reinterpret_cast<float*>(tslot + 4);  // [4][64]
 
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   stage_mixed_weights<16, F, H>(W, sW, sWout);
-  for (int e = t; e < n_wg * (int)(kLeanZero / 16); e += blockDim.x) {
-    uint4* z = reinterpret_cast<uint4*>(sW + H * kWTile + (e / (kLeanZero / 16)) * kLeanRegion + kTile);
-    z[e % (kLeanZero / 16)] = make_uint4(0u, 0u, 0u, 0u);
+  {
+    uint4* z = reinterpret_cast<uint4*>(sZ);
+    for (int e = t; e < (int)(kZero / 16); e += kMixThreads) z[e] = make_uint4(0u, 0u, 0u, 0u);
   }
-  for (int e = t; e < 64; e += blockDim.x) red[e] = 0.f;
-  const uint32_t ncols = n_wg == 1 ? 128u : (n_wg == 2 ? 256u : 512u);
   if (warp == 0) {
-    tc::tmem_alloc(tslot, ncols);
+    tc::tmem_alloc(tslot, 128);
     tc::tmem_relinquish();
   }
-  if (r == 0) tc::mbar_init(bar, 1);
+  if (t == 0) tc::mbar_init(bar, 1);
   tc::fence_async_smem();
   tc::fence_before();
   __syncthreads();
   tc::fence_after();
-  const uint32_t tm = *tslot + 128u * wg;  // this warpgroup's 128 columns
-  const uint32_t my_lanes = tm + ((uint32_t)(32 * wq) << 16);
+  const uint32_t tm = *tslot;
+  const uint32_t my_lanes = tm + ((uint32_t)(32 * warp) << 16);
   const uint32_t sG_a = tc::smem_u32(sG), sZ_a = tc::smem_u32(sZ), sA_a = tc::smem_u32(sA), sW_a = tc::smem_u32(sW);
   const uint32_t sX_a = tc::smem_u32(sX);
   constexpr uint32_t id_fwd = tc::idesc_bf16(128, 64, false, false);
@@ -680,21 +668,21 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
   auto run_phase = [&](auto issue) -> bool {
     tc::fence_async_smem();
     tc::fence_before();
-    wg_sync(wg);
-    if (r == 0) {
+    __syncthreads();
+    if (t == 0) {
       tc::fence_after();
       issue();
       tc::commit(bar);
     }
     const bool to = !tc::mbar_wait(bar, phase);
     phase ^= 1;
-    if (wg_or(wg, to)) return false;
+    if (__syncthreads_or(to)) return false;
     tc::fence_after();
     return true;
   };
   while (true) {
     const bool active = next_chunk(cur, recs, ctrl + 1, slot, a, by_pixel, lane, lo, hi, order, n_valid, offs, xrows);
-    if (!wg_or(wg, active)) break;
+    if (!__syncthreads_or(active)) break;
     const int i = cur.base + lane;
     float p[4] = {0.f, 0.f, 0.f, 0.f};
     bool valid = false;
@@ -707,7 +695,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
         for (int j = 0; j < IN / 8; ++j) xn[j] = __ldcs(src + j);
       }
 #pragma unroll
-      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sX, r, j, valid ? xn[j] : make_uint4(0u, 0u, 0u, 0u));
+      for (int j = 0; j < IN / 8; ++j) tc::st_chunk_raw(sX, t, j, valid ? xn[j] : make_uint4(0u, 0u, 0u, 0u));
       pre_ok = cur.base + 32 < cur.rec.count;
       if (pre_ok && i + 32 < cur.rec.count) {
 #pragma unroll
@@ -715,7 +703,7 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       }
     } else {
       pre_ok = false;
-      encode_row<D, F, 16>(grid, table, p, valid, sX, r);
+      encode_row<D, F, 16>(grid, table, p, valid, sX, t);
     }
     // layer 0: h1 = X W0^T
     bool ok = run_phase([&] {
@@ -744,8 +732,8 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
         const int col = 16 * c + q;
         if (col < 32) m1lo |= bit << col; else m1hi |= bit << (col - 32);
       }
-      tc::st_chunk_bf16(sA, r, 2 * c, v);
-      tc::st_chunk_bf16(sA, r, 2 * c + 1, u);
+      tc::st_chunk_bf16(sA, t, 2 * c, v);
+      tc::st_chunk_bf16(sA, t, 2 * c + 1, u);
     }
     // layer 1: h2 = A1 W1^T
     ok = run_phase([&] {
@@ -778,8 +766,8 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
         v[q] = dz * hidden_act(h[q], act);
         g[q] = hidden_grad(dz * sWout[16 * c + q], h[q] > 0.f, act);
       }
-      tc::st_chunk_bf16(sG, r, 2 * c, g);
-      tc::st_chunk_bf16(sG, r, 2 * c + 1, g + 8);
+      tc::st_chunk_bf16(sG, t, 2 * c, g);
+      tc::st_chunk_bf16(sG, t, 2 * c + 1, g + 8);
       float r8[8], r4[4], r2[2], r1[1];
       detail::rs_step<8>(v, r8, lane, 16);
       detail::rs_step<4>(r8, r4, lane, 8);
@@ -813,8 +801,8 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
         const uint32_t bit = col < 32 ? (m1lo >> col) & 1u : (m1hi >> (col - 32)) & 1u;
         h[q] = hidden_grad(h[q], bit != 0, act);
       }
-      tc::st_chunk_bf16(sA, r, 2 * c, h);
-      tc::st_chunk_bf16(sA, r, 2 * c + 1, h + 8);
+      tc::st_chunk_bf16(sA, t, 2 * c, h);
+      tc::st_chunk_bf16(sA, t, 2 * c + 1, h + 8);
     }
     // dX = G1 W0 (transient); dW0 += [0; G1]^T X (lanes 64..127 of [64, 64 + IN))
     ok = run_phase([&] {
@@ -850,40 +838,40 @@ bwd_lean_kernel(GridDev grid, const __half* __restrict__ table, const float* __r
       }
     }
     tc::fence_before();
-    wg_sync(wg);
+    __syncthreads();
     if (active) cur.base += 32;
   }
   if (timed_out) {
-    if (r == 0) atomicOr(err, 2u);
+    if (t == 0) atomicOr(err, 2u);
     tc::mbar_wait(bar, phase);  // let the MMAs in flight retire (bounded) before freeing TMEM
   } else if (wacc) {
     tc::fence_after();
-    if (wq < 2) {  // dW1 rows o = r in lanes 0..63
+    if (warp < 2) {  // dW1 rows o = t in lanes 0..63
       float v[64];
       ld64(my_lanes + 64, v);
-      float* dst = W_grad + 64 * IN + r * 64;
+      float* dst = W_grad + 64 * IN + t * 64;
 #pragma unroll
       for (int j = 0; j < 64; ++j) atomicAdd(dst + j, v[j]);
-    } else {  // dW0 rows o = r - 64 in lanes 64..127
+    } else {  // dW0 rows o = t - 64 in lanes 64..127
       float v[IN];
 #pragma unroll
       for (int c = 0; c < IN / 16; ++c) tc::tmem_ld16(my_lanes + 64 + 16 * c, v + 16 * c);
       tc::tmem_wait_ld();
-      float* dst = W_grad + (r - 64) * IN;
+      float* dst = W_grad + (t - 64) * IN;
 #pragma unroll
       for (int j = 0; j < IN; ++j) atomicAdd(dst + j, v[j]);
     }
   }
   if (!(lane & 1)) {
 #pragma unroll
-    for (int c = 0; c < 4; ++c) atomicAdd(red + 16 * c + (lane >> 1), dwacc[c]);
+    for (int c = 0; c < 4; ++c) red[warp * 64 + 16 * c + (lane >> 1)] = dwacc[c];
   }
   tc::fence_before();
   __syncthreads();
-  if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t]);
+  if (t < 64) atomicAdd(W_grad + 64 * IN + 64 * 64 + t, red[t] + red[64 + t] + red[128 + t] + red[192 + t]);
   if (warp == 0) {
     tc::fence_after();
-    tc::tmem_dealloc(*tslot, ncols);
+    tc::tmem_dealloc(tm, 128);
   }
 }
 
@@ -1131,10 +1119,8 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
   // tensor-core pass of a round: the lean kernel for two hidden layers over at
   // most 64 inputs (up to three blocks per SM), else the general one (two)
   constexpr bool kLean = H == 2 && L == 16 && IN <= 64;
-  // the lean kernel: one block per SM of backward_blocks_per_sm warpgroups
-  const int lean_wg = std::max(1, std::min(tune.backward_blocks_per_sm, kLeanMaxWG));
-  const size_t lsmem = 1024 + 2 * kWTile + (size_t)lean_wg * kLeanRegion + 64 * 4 + kLeanMaxWG * 8 + 16 + 64 * 4;
-  const int lblocks = std::max(1, std::min<int>(sms, (int)ceil_div(a.num_rays, 4 * lean_wg)));
+  const size_t lsmem = 1024 + 2 * kWTile + 3 * kTile + 2048 + 64 * 4 + 64 + 4 * 64 * 4;
+  const int lblocks = std::max(1, std::min<int>(tune.backward_blocks_per_sm * sms, (int)ceil_div(a.num_rays, 4)));
   if constexpr (kLean)
     set_smem(bwd_lean_kernel<D, F, ACT>, lsmem, false);
   else
@@ -1152,7 +1138,7 @@ int run_mixed(const NectbGeometry& geo, const GridDev& grid, const __half* table
     {
       ProfScope ps(kProfBackward, s);
       if constexpr (kLean)
-        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads * lean_wg, lsmem, s>>>(gt, table, W, a, ws.rays, ws.slot,
+        bwd_lean_kernel<D, F, ACT><<<lblocks, kMixThreads, lsmem, s>>>(gt, table, W, a, ws.rays, ws.slot,
                                                                        ws.counters, out_act, W_grad, (int)lo, hi,
                                                                        stage, slots, order, SL.offs, SL.xstore,
                                                                        SL.xcap);
