@@ -107,16 +107,21 @@ __global__ void __launch_bounds__(kModelThreads) model_forward_kernel(GridDev g,
 }
 
 // One thread per point: the point's encoding gradient dout[l * F + f] added
-// to its corners' entries, weighted (fp32 vector atomics).
+// to its corners' entries, weighted (fp32 vector atomics).  A warp's 32
+// consecutive points merge their contributions on levels where they fall in
+// runs of equal cells (consecutive samples of a ray do on the coarse levels),
+// so such a run reduces each corner once.
 template <int D, int F>
 __global__ void encode_backward_kernel(GridDev g, const float* __restrict__ x, int64_t n,
                                        const float* __restrict__ dout, float* __restrict__ grad) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+  const bool valid = i < n;   // every lane takes part in the warp's shuffles
   float p[D];
 #pragma unroll
-  for (int k = 0; k < D; ++k) p[k] = x[i * D + k];
-  scatter_point<D, F>(g, grad, p, dout + i * (int64_t)g.n_levels * F);
+  for (int k = 0; k < D; ++k) p[k] = valid ? x[i * D + k] : 0.f;
+  const int64_t row = valid ? i : 0;
+  scatter_warp<D, F, false, true>(g, grad, p, valid, dout + row * (int64_t)g.n_levels * F, F, 1, 0u, 0,
+                                  g.n_levels);
 }
 
 template <int D, int F, typename T>

@@ -264,7 +264,11 @@ __device__ __forceinline__ float run_sum(float v, int lane, int end) {
 // (the staging buffer, fstride 1, rows aligned to F floats): one vector load
 // per level, evict-first, so the streamed rows do not push the gradient slice
 // out of L2.
-template <int D, int F, bool kStreamSrc = false>
+//
+// kAdaptive: agg_levels is ignored; every level merges runs when the warp's
+// 32 points form at most 24 runs of equal cells (points in no known order,
+// such as a module's batch).
+template <int D, int F, bool kStreamSrc = false, bool kAdaptive = false>
 __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict__ grad, const float* x, bool valid,
                                              const float* dsrc, int64_t lstride, int fstride, uint32_t agg_levels,
                                              int l0, int l1) {
@@ -290,13 +294,19 @@ __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict
       for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[l * lstride + f * fstride] : 0.f;
     }
     float* base = grad + g.offset[l] * F;
-    if ((agg_levels >> l) & 1u) {
+    bool merge = kAdaptive || ((agg_levels >> l) & 1u);
+    bool head = false;
+    uint32_t heads = 0;
+    if (merge) {
       // runs of lanes in the same spatial cell (t is the same for the whole
       // batch, so the spatial cell fixes every corner index)
       const uint64_t key = valid ? lc.cell : ~uint64_t(0);
       const uint64_t prev = __shfl_up_sync(0xffffffffu, key, 1);
-      const bool head = (lane == 0) || (prev != key);
-      const uint32_t heads = __ballot_sync(0xffffffffu, head);
+      head = (lane == 0) || (prev != key);
+      heads = __ballot_sync(0xffffffffu, head);
+      if constexpr (kAdaptive) merge = __popc(heads) <= 24;
+    }
+    if (merge) {
       const uint32_t later = heads & ~((2u << lane) - 1u);
       const int end = later ? (__ffs(later) - 2) : 31;
       constexpr int SC = D == 4 ? 8 : (1 << D);   // corners summed along the run
