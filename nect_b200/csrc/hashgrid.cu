@@ -62,9 +62,7 @@ __global__ void encode_kernel(GridDev g, const T* __restrict__ table, const floa
   float p[D];
 #pragma unroll
   for (int k = 0; k < D; ++k) p[k] = x[i * D + k];
-  float enc[NECTB_MAX_LEVELS * F];
-  encode_point<D, F, T>(g, table, p, enc);
-  for (int j = 0; j < g.n_levels * F; ++j) out[i * g.n_levels * F + j] = enc[j];
+  encode_point<D, F, T>(g, table, p, out + i * (int64_t)g.n_levels * F);
 }
 
 // One thread per point: encode into a shared-memory column, then the SIMT MLP.
