@@ -941,7 +941,7 @@ def run_quadcubes(args):
 
     for k in range(args.warmup):
         tr.step(batch(k))
-    ms, _ = time_steps(tr, batch, args.steps, args.warmup, 1)
+    ms, _ = time_steps(tr, batch, args.steps, args.warmup, 1, nvtx="timed")
     rays = tr.batch_size
     params = sum(p.numel() for p in model.parameters())
     print(json.dumps({

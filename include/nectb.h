@@ -153,6 +153,40 @@ int nectb_hashgrid_encode(const NectbHashGrid* grid, const void* params,
 int nectb_hashgrid_encode_backward(const NectbHashGrid* grid, const float* x, int64_t n,
                                    const float* dout, float* grad, void* stream);
 
+/* QuadCubes' Composite encoding (nect/network/networks.py:392-449, the
+ * reference's default dynamic model): four 3D grids of one configuration
+ * (n_dims 3, fp32 tables, 2 or 4 features, the same resolution on every
+ * axis) over (z, y, x), (y, x, t), (x, z, t) and (z, y, t) of each point, in
+ * the reference's input order (networks.py:438-446).  t is one fp32 value in
+ * device memory for every point of the call.
+ *
+ * nectb_quadcubes_encode writes row i of out (width out_ld, fp32 or bf16 per
+ * out_dtype): grid k's n_levels * n_features features at columns
+ * [k * L * F, (k + 1) * L * F), then, with identity != 0, the raw inputs
+ * (z, y, x, t) (include_identity), then zeros to the end of the row.  The
+ * three grids over (a, b, t) are evaluated on their plane at t (the blend of
+ * the two time vertices, built in the workspace once per grid and call:
+ * fp32, or fp16 when out_dtype is NECTB_BF16), equal to the 3D grid's
+ * trilinear interpolation up to fp32 reassociation or that fp16 rounding.
+ *
+ * nectb_quadcubes_encode_backward adds the table gradients of
+ * sum(out[:, :4 * L * F] * dout[:, :4 * L * F]) to grads[0..3] (fp32, the
+ * tables' shapes, 16-byte aligned); dout is fp32 or bf16 with rows of width
+ * dout_ld; the identity columns carry no gradient (the reference's points do
+ * not require one).
+ *
+ * tables[k] / grads[k] are 4 device pointers in a host array.  out, dout and
+ * their rows (ld * element size) are 16-byte aligned.  The workspace (16-byte
+ * aligned, nectb_quadcubes_workspace_bytes) holds one plane or one plane
+ * gradient at a time; calls on one stream may share it. */
+size_t nectb_quadcubes_workspace_bytes(const NectbHashGrid* grid);
+int nectb_quadcubes_encode(const NectbHashGrid* grid, const float* const* tables, const float* zyx, int64_t n,
+                           const float* t, int identity, void* out, int64_t out_ld, int out_dtype,
+                           void* workspace, size_t workspace_bytes, void* stream);
+int nectb_quadcubes_encode_backward(const NectbHashGrid* grid, const float* zyx, int64_t n, const float* t,
+                                    const void* dout, int64_t dout_ld, int dout_dtype, float* const* grads,
+                                    void* workspace, size_t workspace_bytes, void* stream);
+
 /* Diagnostic: per-level corner indices (entry index within the level, int32)
  * and d-linear weights of n points, idx/w[n][n_levels][2^n_dims].  No
  * counterpart in the reference (tiny-cuda-nn keeps them internal); it lets

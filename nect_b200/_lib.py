@@ -123,6 +123,13 @@ _SIGNATURES = {
     "nectb_hashgrid_encode": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_ptr, c_i64, c_ptr, c_ptr]),
     "nectb_hashgrid_encode_backward": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
     "nectb_hashgrid_corners": (c_int, [ctypes.POINTER(NectbHashGrid), c_ptr, c_i64, c_ptr, c_ptr, c_ptr]),
+    "nectb_quadcubes_workspace_bytes": (c_size, [ctypes.POINTER(NectbHashGrid)]),
+    "nectb_quadcubes_encode": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), c_ptr, c_ptr, c_i64, c_ptr, c_int, c_ptr, c_i64, c_int, c_ptr, c_size, c_ptr]),
+    "nectb_quadcubes_encode_backward": (
+        c_int,
+        [ctypes.POINTER(NectbHashGrid), c_ptr, c_i64, c_ptr, c_ptr, c_i64, c_int, c_ptr, c_ptr, c_size, c_ptr]),
     "nectb_model_forward": (
         c_int,
         [ctypes.POINTER(NectbHashGrid), ctypes.POINTER(NectbMLP), c_ptr, c_ptr, c_ptr, c_i64, c_f32, c_ptr, c_ptr],

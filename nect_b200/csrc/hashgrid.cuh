@@ -14,6 +14,7 @@
 // Corner c has bit k set when it takes the upper vertex along axis k; its
 // weight is the product over k of (bit ? frac_k : 1 - frac_k) in axis order.
 #pragma once
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cstdint>
 
@@ -238,6 +239,32 @@ __device__ __forceinline__ void red_entry(float* dst, const float* v) {
     for (int f = 0; f < F; ++f) atomicAdd(dst + f, v[f]);
 }
 
+// fp32 value of a gradient element held as fp32 or bf16.
+__device__ __forceinline__ float grad_value(float v) { return v; }
+__device__ __forceinline__ float grad_value(__nv_bfloat16 v) { return __bfloat162float(v); }
+
+// F consecutive gradient elements (fp32 or bf16) as one vector load; src is
+// aligned to F elements.
+template <int F, typename S>
+__device__ __forceinline__ void load_grad_row(const S* src, float* d) {
+  static_assert(F == 2 || F == 4, "F must be 2 or 4");
+  if constexpr (sizeof(S) == 4 && F == 4) {
+    const float4 v = *reinterpret_cast<const float4*>(src);
+    d[0] = v.x, d[1] = v.y, d[2] = v.z, d[3] = v.w;
+  } else if constexpr (sizeof(S) == 4) {
+    const float2 v = *reinterpret_cast<const float2*>(src);
+    d[0] = v.x, d[1] = v.y;
+  } else if constexpr (F == 4) {
+    const uint2 raw = *reinterpret_cast<const uint2*>(src);
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.x));
+    const float2 b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&raw.y));
+    d[0] = a.x, d[1] = a.y, d[2] = b.x, d[3] = b.y;
+  } else {
+    const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(src));
+    d[0] = a.x, d[1] = a.y;
+  }
+}
+
 // Sum of v over the lanes [lane, end] of the lane's run (lanes after it in the
 // same run); valid in the run's first lane.
 __device__ __forceinline__ float run_sum(float v, int lane, int end) {
@@ -259,8 +286,8 @@ __device__ __forceinline__ float run_sum(float v, int lane, int end) {
 // Other levels scatter per sample.  Sums equal the per-sample atomics up to
 // fp32 reassociation.
 //
-// dL/d(feature f of level l) is read at dsrc[l * lstride + f * fstride]; only
-// levels [l0, l1) are scattered.  kStreamSrc: dsrc is global memory read once
+// dL/d(feature f of level l) is read at dsrc[l * lstride + f * fstride] (fp32,
+// or bf16 with S = __nv_bfloat16); only levels [l0, l1) are scattered.  kStreamSrc: dsrc is global memory read once
 // (the staging buffer, fstride 1, rows aligned to F floats): one vector load
 // per level, evict-first, so the streamed rows do not push the gradient slice
 // out of L2.
@@ -268,10 +295,14 @@ __device__ __forceinline__ float run_sum(float v, int lane, int end) {
 // kAdaptive: agg_levels is ignored; every level merges runs when the warp's
 // 32 points form at most 24 runs of equal cells (points in no known order,
 // such as a module's batch).
-template <int D, int F, bool kStreamSrc = false, bool kAdaptive = false>
+//
+// kVecSrc: fstride is 1 and each level's F elements are one aligned vector
+// (load_grad_row).
+template <int D, int F, bool kStreamSrc = false, bool kAdaptive = false, typename S = float, bool kVecSrc = false>
 __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict__ grad, const float* x, bool valid,
-                                             const float* dsrc, int64_t lstride, int fstride, uint32_t agg_levels,
+                                             const S* dsrc, int64_t lstride, int fstride, uint32_t agg_levels,
                                              int l0, int l1) {
+  static_assert(!kStreamSrc || sizeof(S) == 4, "the streamed source is fp32");
   const int lane = threadIdx.x & 31;
 #pragma unroll 1
   for (int l = l0; l < l1; ++l) {
@@ -289,9 +320,16 @@ __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict
       d[1] = v.y;
       d[2] = v.z;
       d[3] = v.w;
+    } else if constexpr (kVecSrc) {
+      if (valid) {
+        load_grad_row<F, S>(dsrc + l * lstride, d);
+      } else {
+#pragma unroll
+        for (int f = 0; f < F; ++f) d[f] = 0.f;
+      }
     } else {
 #pragma unroll
-      for (int f = 0; f < F; ++f) d[f] = valid ? dsrc[l * lstride + f * fstride] : 0.f;
+      for (int f = 0; f < F; ++f) d[f] = valid ? grad_value(dsrc[l * lstride + f * fstride]) : 0.f;
     }
     float* base = grad + g.offset[l] * F;
     bool merge = kAdaptive || ((agg_levels >> l) & 1u);

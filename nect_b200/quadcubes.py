@@ -10,9 +10,12 @@ and runs a FullyFusedMLP without biases (default 4 hidden layers of 128,
 LeakyReLU, no output activation).  Here:
 
 - the grids are fp32 tables ``tables[k]`` [entries, features] in the
-  library's layout, encoded by ``nectb_hashgrid_encode`` and differentiated
-  by ``nectb_hashgrid_encode_backward`` (hand-written kernels, one autograd
-  node per grid);
+  library's layout, encoded together by ``nectb_quadcubes_encode`` straight
+  into the MLP's input rows (bf16 on the mixed path) and differentiated by
+  ``nectb_quadcubes_encode_backward`` (hand-written kernels, one autograd
+  node); the three grids over (a, b, t) are evaluated on their plane at the
+  call's t, 4 corners a level from an L2-sized blend of the two time
+  vertices;
 - the MLP is a chain of plain GEMMs (``torch.nn.Linear`` without bias, on
   cuBLAS; bf16 autocast when ``precision="mixed"``), weights Glorot-uniform,
   tables U(-1e-4, 1e-4) as for the hash-grid models.
@@ -81,6 +84,51 @@ class GridEncode(torch.autograd.Function):
         return grad, None, None, None
 
 
+class QuadEncode(torch.autograd.Function):
+    """The composite encoding of QuadCubes in one node: rows [N, ld] (fp32, or
+    bf16 on the mixed path) holding the four grids' features, the raw inputs
+    (z, y, x, t) with ``include_identity`` and zero columns up to ld
+    (nectb_quadcubes_encode); the backward adds the four table gradients
+    (nectb_quadcubes_encode_backward).  t is a 1-element fp32 CUDA tensor.  No
+    gradient flows to zyx or t."""
+
+    @staticmethod
+    def forward(ctx, t0, t1, t2, t3, model, zyx, t):
+        n = zyx.shape[0]
+        dtype = torch.bfloat16 if model.precision == "mixed" else torch.float32
+        out = torch.empty(n, model.row_width, device=zyx.device, dtype=dtype)
+        if n:
+            ws = torch.empty(model.workspace_bytes, device=zyx.device, dtype=torch.uint8)
+            ptrs = (ctypes.c_void_p * 4)(*[tab.data_ptr() for tab in (t0, t1, t2, t3)])
+            rc = _lib.lib.nectb_quadcubes_encode(
+                ctypes.byref(model.desc), ptrs, zyx.data_ptr(), n, t.data_ptr(), int(model.include_identity),
+                out.data_ptr(), model.row_width, _lib.BF16 if dtype == torch.bfloat16 else _lib.F32, ws.data_ptr(),
+                ws.numel(), _lib.stream_ptr(zyx.device))
+            _lib.check(rc, "nectb_quadcubes_encode")
+        ctx.model = model
+        ctx.save_for_backward(zyx, t)
+        return out
+
+    @staticmethod
+    def backward(ctx, dout):
+        zyx, t = ctx.saved_tensors
+        model = ctx.model
+        grads = [torch.zeros_like(tab) for tab in model.tables]
+        if zyx.shape[0]:
+            d = dout.detach()
+            if d.dtype not in (torch.float32, torch.bfloat16):
+                d = d.float()
+            d = d.contiguous()
+            ws = torch.empty(model.workspace_bytes, device=zyx.device, dtype=torch.uint8)
+            ptrs = (ctypes.c_void_p * 4)(*[g.data_ptr() for g in grads])
+            rc = _lib.lib.nectb_quadcubes_encode_backward(
+                ctypes.byref(model.desc), zyx.data_ptr(), zyx.shape[0], t.data_ptr(), d.data_ptr(), d.shape[1],
+                _lib.BF16 if d.dtype == torch.bfloat16 else _lib.F32, ptrs, ws.data_ptr(), ws.numel(),
+                _lib.stream_ptr(zyx.device))
+            _lib.check(rc, "nectb_quadcubes_encode_backward")
+        return (*grads, None, None, None)
+
+
 class QuadCubes(nn.Module):
     """forward(zyx [N, 3], t) -> sigma [N, 1] (networks.py:438-449)."""
     n_dims = 4
@@ -106,11 +154,19 @@ class QuadCubes(nn.Module):
         if total <= 0:
             raise ValueError("invalid hash-grid configuration")
         self.n_enc = L * enc.n_features_per_level
+        self.n_in = 4 * self.n_enc + (4 if self.include_identity else 0)
+        # rows of the encoding matrix: 16-byte aligned (fp32), or a multiple of
+        # 64 bf16 columns on the mixed path (aligned GEMM tiles); the padded
+        # columns are zero and meet zero weight columns
+        self.row_width = -(-self.n_in // 64) * 64 if precision == "mixed" else -(-self.n_in // 4) * 4
+        self.workspace_bytes = int(_lib.lib.nectb_quadcubes_workspace_bytes(ctypes.byref(self.desc)))
+        if self.workspace_bytes <= 0:
+            raise ValueError("invalid QuadCubes grid configuration")
         gen = torch.Generator(device="cpu").manual_seed(seed)
         self.tables = nn.ParameterList([
             nn.Parameter(((torch.rand(total, enc.n_features_per_level, generator=gen) * 2 - 1) * 1e-4).to(device))
             for _ in range(4)])
-        widths = [4 * self.n_enc + (4 if self.include_identity else 0)] + [net.n_neurons] * net.n_hidden_layers + [1]
+        widths = [self.n_in] + [net.n_neurons] * net.n_hidden_layers + [1]
         self.layers = nn.ModuleList()
         for a, b in zip(widths[:-1], widths[1:]):
             lin = nn.Linear(a, b, bias=False)
@@ -125,20 +181,18 @@ class QuadCubes(nn.Module):
         _lib.require_cuda(zyx, "zyx")
         if zyx.dtype != torch.float32 or zyx.dim() != 2 or zyx.shape[1] != 3:
             raise ValueError("zyx must be fp32 [N, 3] (z, y, x) in [0, 1]")
-        n = zyx.shape[0]
-        x = zyx.detach()
-        if isinstance(t, torch.Tensor):
-            tcol = t.detach().to(device=x.device, dtype=torch.float32).reshape(1, 1).expand(n, 1)
+        x = zyx.detach().contiguous()
+        if isinstance(t, torch.Tensor):   # stays on the device (no host sync)
+            tdev = t.detach().to(device=x.device, dtype=torch.float32).reshape(1).contiguous()
         else:
-            tcol = torch.full((n, 1), float(t), device=x.device)
-        inputs = (x, torch.cat([x[:, [1, 2]], tcol], 1), torch.cat([x[:, [2, 0]], tcol], 1),
-                  torch.cat([x[:, [0, 1]], tcol], 1))
-        feats = [GridEncode.apply(tab, self.desc, self.n_enc, inp.contiguous()) for tab, inp in zip(self.tables, inputs)]
-        if self.include_identity:
-            feats.append(torch.cat([x, tcol], 1))
-        h = torch.cat(feats, 1)
+            tdev = torch.full((1,), float(t), device=x.device, dtype=torch.float32)
+        h = QuadEncode.apply(*self.tables, self, x, tdev)
+        w0 = self.layers[0].weight
+        if self.row_width != self.n_in:
+            w0 = F_.pad(w0, (0, self.row_width - self.n_in))
         with torch.autocast("cuda", dtype=torch.bfloat16, enabled=self.precision == "mixed"):
-            for lin in self.layers[:-1]:
+            h = self.act(F_.linear(h, w0))
+            for lin in self.layers[1:-1]:
                 h = self.act(lin(h))
             out = self.layers[-1](h)
         return self.out_act(out.float())

@@ -101,3 +101,25 @@ def test_trainer_update_matches_torch_adam(cuda_device):
     torch.testing.assert_close(m.mlp.detach(), ref_m.detach(), rtol=1e-6, atol=1e-8)
     assert torch.equal(m.table_half.view(torch.int16), m.table.detach().half().view(torch.int16))
     assert not tr.table_grad.any() and not tr.mlp_grad.any()
+
+
+def test_adam_vector_and_scalar_paths_agree(cuda_device):
+    """Buffers 16-byte aligned take the four-element path; the same data one
+    element off that alignment take the one-element path: bit-identical."""
+    gen = torch.Generator(device="cpu").manual_seed(11)
+    n = 4099
+    bufs = [torch.randn(n + 1, generator=gen).to(cuda_device) for _ in range(4)]
+    bufs[3] = bufs[3].abs()
+    a = [b[:n].clone() for b in bufs]                       # aligned
+    u = [torch.zeros(n + 1, device=cuda_device) for _ in range(4)]
+    for dst, b in zip(u, bufs):
+        dst[1:] = b[:n]
+    u = [b[1:] for b in u]                                  # 4 bytes past alignment
+    ha = torch.empty(n, dtype=torch.float16, device=cuda_device)
+    hu = torch.empty(n + 1, dtype=torch.float16, device=cuda_device)[1:]
+    for step in (1, 2):
+        _adam(a[0], a[1], a[2], a[3], step, 1e-3, (0.9, 0.999), 1e-8, 1e-2, half=ha, zero_grad=0)
+        _adam(u[0], u[1], u[2], u[3], step, 1e-3, (0.9, 0.999), 1e-8, 1e-2, half=hu, zero_grad=0)
+    torch.cuda.synchronize()
+    for x, y in zip(a + [ha], u + [hu]):
+        assert torch.equal(x, y)

@@ -128,3 +128,96 @@ def test_fit_trains_quadcubes_on_a_dynamic_scan(cuda_device):
     assert isinstance(rec.model, QuadCubes) and isinstance(rec.trainer, ModuleTrainer)
     first, last = rec.history[0][2]["psnr"], rec.history[-1][2]["psnr"]
     assert math.isfinite(last) and last > first + 5, (first, last)
+
+
+def _rows(m, x, t, dtype):
+    from nect_b200.quadcubes import QuadEncode
+
+    m.precision = "mixed" if dtype == torch.bfloat16 else "plain_fp32"
+    m.row_width = -(-m.n_in // 64) * 64 if dtype == torch.bfloat16 else -(-m.n_in // 4) * 4
+    return QuadEncode.apply(*m.tables, m, x, torch.full((1,), t, device="cuda"))
+
+
+@pytest.mark.parametrize("F", [2, 4])
+def test_composite_rows_match_the_3d_grids(cuda_device, F):
+    """nectb_quadcubes_encode against the per-grid 3D encoder
+    (nectb_hashgrid_encode): the planes at t equal the trilinear grids up to
+    fp32 reassociation (fp32 rows, 1e-5 of the largest entry) and one fp16 +
+    one bf16 rounding (bf16
+    rows); identity columns exact, padding zero.  The small table puts levels
+    in all three plane forms (dense 3D, dense plane of a hashed level, hashed
+    plane)."""
+    from nect_b200.quadcubes import GridEncode
+
+    m, _ = make(F=F)
+    forms = set()
+    for r in ohg.layout(3, 6, 11, 4.0, float(m.encoding_config.per_level_scale))[0]:
+        v = r.res[0] + 1
+        forms.add("dense" if v ** 3 <= 2048 else ("plane" if v ** 2 <= 2048 else "hashed"))
+    assert forms == {"dense", "plane", "hashed"}, forms
+    gen = torch.Generator(device="cpu").manual_seed(7)
+    x = torch.rand(4000, 3, generator=gen).cuda()
+    x[:7] = torch.tensor([[0, 0, 0], [1, 1, 1], [1, 0, 1], [0.5, 0.5, 0.5], [0, 1, 0], [1e-7, 1, 0.999999], [0.25, 0.75, 1]],
+                         device="cuda")
+    for t in (0.0, 0.43, 1.0):
+        tcol = torch.full((x.shape[0], 1), t, device="cuda")
+        ins = (x, torch.cat([x[:, [1, 2]], tcol], 1), torch.cat([x[:, [2, 0]], tcol], 1),
+               torch.cat([x[:, [0, 1]], tcol], 1))
+        ref = torch.cat([GridEncode.apply(tab, m.desc, m.n_enc, i.contiguous()) for tab, i in zip(m.tables, ins)]
+                        + [x, tcol], 1).detach()
+        rows = _rows(m, x, t, torch.float32).detach()
+        assert rows.shape == (x.shape[0], m.row_width)
+        assert rel(rows[:, :m.n_in].cpu(), ref.cpu()) < 1e-5
+        assert torch.equal(rows[:, 4 * m.n_enc:m.n_in], ref[:, 4 * m.n_enc:])
+        rows16 = _rows(m, x, t, torch.bfloat16).detach()
+        assert rows16.dtype == torch.bfloat16 and rows16.shape[1] % 64 == 0
+        assert rel(rows16[:, :m.n_in].float().cpu(), ref.cpu()) < 8e-3
+        assert not rows16[:, m.n_in:].any()
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.bfloat16])
+def test_composite_backward_matches_the_3d_grids(cuda_device, dtype):
+    """nectb_quadcubes_encode_backward (planes' gradients spread to the two
+    time vertices) against nectb_hashgrid_encode_backward of each 3D grid on
+    the same dL/d(rows), fp32 or bf16 rows."""
+    from nect_b200.quadcubes import GridEncode
+
+    m, _ = make(F=4)
+    gen = torch.Generator(device="cpu").manual_seed(8)
+    x = torch.rand(6000, 3, generator=gen).cuda()
+    t = 0.71
+    rows = _rows(m, x, t, dtype)
+    dout = torch.randn(rows.shape, generator=gen).to(device="cuda", dtype=dtype)
+    got = torch.autograd.grad((rows.float() * dout.float()).sum(), list(m.tables))
+    tcol = torch.full((x.shape[0], 1), t, device="cuda")
+    ins = (x, torch.cat([x[:, [1, 2]], tcol], 1), torch.cat([x[:, [2, 0]], tcol], 1),
+           torch.cat([x[:, [0, 1]], tcol], 1))
+    for k, (tab, i) in enumerate(zip(m.tables, ins)):
+        out = GridEncode.apply(tab, m.desc, m.n_enc, i.contiguous())
+        d = dout[:, k * m.n_enc:(k + 1) * m.n_enc].float()
+        (ref,) = torch.autograd.grad((out * d).sum(), [tab])
+        assert rel(got[k].cpu(), ref.cpu()) < 1e-5, (k, rel(got[k].cpu(), ref.cpu()))
+
+
+def test_mixed_forward_and_backward_match_the_oracle(cuda_device):
+    """The mixed path (fp16 planes, bf16 rows and MLP, fp32 accumulation)
+    against the fp64 oracle: outputs within 2e-2 of the largest, gradients
+    with cosine > 0.99 and within 1e-1 of each parameter's largest entry (the
+    128-wide bf16 GEMMs' backward rounds dL/d(rows) to bf16; measured 6e-2)."""
+    m, levels = make(precision="mixed")
+    gen = torch.Generator(device="cpu").manual_seed(9)
+    x = torch.rand(3000, 3, generator=gen)
+    g = torch.randn(3000, 1, generator=gen)
+    t = 0.29
+    y = m(x.cuda(), t)
+    (y * g.cuda()).sum().backward()
+    tables = [tab.detach().cpu().double().requires_grad_() for tab in m.tables]
+    weights = [lin.weight.detach().cpu().double().requires_grad_() for lin in m.layers]
+    ref = oracle_forward(m, levels, x, t, tables, weights)
+    assert rel(y.detach().cpu(), ref.detach()) < 2e-2
+    (ref * g.double()).sum().backward()
+    for p, r in [(tab, rt) for tab, rt in zip(m.tables, tables)] + [(lin.weight, rw) for lin, rw in
+                                                                     zip(m.layers, weights)]:
+        a, b = p.grad.cpu().double().flatten(), r.grad.flatten()
+        assert float(torch.dot(a, b) / (a.norm() * b.norm())) > 0.99
+        assert rel(a, b) < 1e-1, rel(a, b)
