@@ -190,7 +190,7 @@ __global__ void plane_encode_kernel(Plane s, const P* __restrict__ plane, const 
   if (i >= n) return;
   const float a = zyx[i * 3 + ca], b = zyx[i * 3 + cb];
   O* row = out + i * ld + col0;
-#pragma unroll 1
+#pragma unroll 2   // two levels' gathers in flight
   for (int l = 0; l < s.n_levels; ++l) {
     PlaneCorners pc;
     plane_corners(s, l, a, b, pc);
@@ -219,7 +219,7 @@ __global__ void volume_encode_kernel(GridDev g, const float* __restrict__ table,
   if (i >= n) return;
   const float x[3] = {zyx[i * 3], zyx[i * 3 + 1], zyx[i * 3 + 2]};
   O* row = out + i * ld;
-#pragma unroll 1
+#pragma unroll 2   // two levels' gathers in flight
   for (int l = 0; l < g.n_levels; ++l) {
     LevelCorners<3> lc;
     level_corners<3>(g, l, x, lc);
@@ -245,18 +245,20 @@ __global__ void volume_encode_kernel(GridDev g, const float* __restrict__ table,
   for (int c = pad; c < ld; ++c) row[c] = from_float<O>(0.f);
 }
 
-// Gradient of the (z, y, x) grid: dL/d(features) in columns [0, L * F) of the
-// rows; warps merge runs of points in one cell (scatter_warp, adaptive).
+// Gradient of levels [l0, l1) of the (z, y, x) grid: dL/d(features) in
+// columns [0, L * F) of the rows; warps merge runs of points in one cell
+// (scatter_warp, adaptive).
 template <int F, typename S>
 __global__ void volume_scatter_kernel(GridDev g, const float* __restrict__ zyx, int64_t n,
-                                      const S* __restrict__ dout, int64_t ld, float* __restrict__ grad) {
+                                      const S* __restrict__ dout, int64_t ld, float* __restrict__ grad, int l0,
+                                      int l1) {
   const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
   const bool valid = i < n;   // every lane takes part in the warp's shuffles
   float p[3];
 #pragma unroll
   for (int k = 0; k < 3; ++k) p[k] = valid ? zyx[i * 3 + k] : 0.f;
   const int64_t row = valid ? i : 0;
-  scatter_warp<3, F, false, true, S, true>(g, grad, p, valid, dout + row * ld, F, 1, 0u, 0, g.n_levels);
+  scatter_warp<3, F, false, true, S, true>(g, grad, p, valid, dout + row * ld, F, 1, 0u, l0, l1);
 }
 
 // Gradient of a plane grid into the plane-shaped fp32 gradient: 4 corners a
@@ -407,13 +409,29 @@ int encode_all(const GridDev& g, const Plane& s, const float* const* tables, con
   return NECTB_OK;
 }
 
+constexpr int64_t kScatterGroupBytes = int64_t(64) << 20;
+
 template <int F, typename S>
 int backward_all(const GridDev& g, const Plane& s, const float* zyx, int64_t n, const float* t, const S* dout,
                  int64_t ld, float* const* grads, float* pgrad, cudaStream_t st) {
   const unsigned blocks = (unsigned)ceil_div(n, 256);
   const int LF = g.n_levels * F;
-  volume_scatter_kernel<F, S><<<blocks, 256, 0, st>>>(g, zyx, n, dout, ld, grads[0]);
-  if (int rc = launch_status("volume_scatter_kernel")) return rc;
+  // One pass per group of consecutive levels whose gradient slice is at most
+  // kScatterGroupBytes (a hashed level of 2^23 entries is a group of its own),
+  // so that a pass's reductions find their lines in L2 and each line is
+  // written back about once; the passes re-read the points and their rows.
+  for (int l0 = 0; l0 < g.n_levels;) {
+    int l1 = l0 + 1;
+    auto level_bytes = [&](int l) {
+      const int64_t end = l + 1 < g.n_levels ? g.offset[l + 1] : g.total_entries;
+      return (end - g.offset[l]) * F * 4;
+    };
+    int64_t bytes = level_bytes(l0);
+    while (l1 < g.n_levels && bytes + level_bytes(l1) <= kScatterGroupBytes) bytes += level_bytes(l1++);
+    volume_scatter_kernel<F, S><<<blocks, 256, 0, st>>>(g, zyx, n, dout, ld, grads[0], l0, l1);
+    if (int rc = launch_status("volume_scatter_kernel")) return rc;
+    l0 = l1;
+  }
   for (int k = 0; k < 3; ++k) {
     if (int rc = cuda_status(cudaMemsetAsync(pgrad, 0, (size_t)s.total2 * F * 4, st), "cudaMemsetAsync")) return rc;
     plane_scatter_kernel<F, S><<<blocks, 256, 0, st>>>(s, zyx, n, kPlaneCols[k][0], kPlaneCols[k][1], dout, ld,
