@@ -221,3 +221,38 @@ def test_mixed_forward_and_backward_match_the_oracle(cuda_device):
         a, b = p.grad.cpu().double().flatten(), r.grad.flatten()
         assert float(torch.dot(a, b) / (a.norm() * b.norm())) > 0.99
         assert rel(a, b) < 1e-1, rel(a, b)
+
+
+def test_composite_encoder_at_the_preset_size(cuda_device):
+    """The reference's preset (quadcubes.yaml: 23 levels x 4 features, 2^23
+    entries, base 16) on a 512^2 detector's finest resolution 1024: planes of
+    up to 1024^2 vertices on hashed levels.  Rows (fp32) and table gradients
+    of 200,000 points against the per-grid 3D kernels, within 2e-5 of the
+    largest entry (fp32 reassociation)."""
+    from nect_b200.config import HashEncoderConfig, MLPNetConfig
+    from nect_b200.quadcubes import GridEncode, QuadCubes
+
+    enc = HashEncoderConfig(n_levels=23, n_features_per_level=4, log2_hashmap_size=23, base_resolution=16,
+                            finest_resolution=1024)
+    net = MLPNetConfig(n_hidden_layers=4, n_neurons=128, activation="LeakyReLU", output_activation="None",
+                       include_identity=True)
+    m = QuadCubes(enc, net, device="cuda", seed=4)
+    with torch.no_grad():
+        for tab in m.tables:
+            tab.mul_(5000.0)   # U(-0.5, 0.5)
+    gen = torch.Generator(device="cpu").manual_seed(12)
+    x = torch.rand(200_000, 3, generator=gen).cuda()
+    t = 0.57
+    tcol = torch.full((x.shape[0], 1), t, device="cuda")
+    ins = (x, torch.cat([x[:, [1, 2]], tcol], 1), torch.cat([x[:, [2, 0]], tcol], 1),
+           torch.cat([x[:, [0, 1]], tcol], 1))
+    rows = _rows(m, x, t, torch.float32)
+    dout = torch.randn(rows.shape, generator=gen).cuda()
+    got = torch.autograd.grad((rows * dout).sum(), list(m.tables))
+    for k, (tab, i) in enumerate(zip(m.tables, ins)):
+        out = GridEncode.apply(tab, m.desc, m.n_enc, i.contiguous())
+        cols = slice(k * m.n_enc, (k + 1) * m.n_enc)
+        assert rel(rows[:, cols].detach().cpu(), out.detach().cpu()) < 2e-5, k
+        (ref,) = torch.autograd.grad((out * dout[:, cols]).sum(), [tab])
+        assert rel(got[k].cpu(), ref.cpu()) < 2e-5, (k, rel(got[k].cpu(), ref.cpu()))
+        del out, ref
