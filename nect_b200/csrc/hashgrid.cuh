@@ -56,7 +56,10 @@ __device__ __forceinline__ void level_corners(const GridDev& g, int l, const flo
 #pragma unroll
   for (int k = 0; k < D; ++k) {
     const int r = g.res[l][k];
-    const float p = x[k] * (float)r;
+    // p is the fp32-rounded product for the floor and the fraction alike:
+    // __fmul_rn keeps the compiler from contracting p - ci into an fma, which
+    // would give the unrounded product's fraction in some kernels only
+    const float p = __fmul_rn(x[k], (float)r);
     int ci = (int)floorf(p);
     ci = ci < 0 ? 0 : (ci > r - 1 ? r - 1 : ci);
     c[k] = ci;
@@ -356,7 +359,7 @@ __device__ __forceinline__ void scatter_warp(const GridDev& g, float* __restrict
 #pragma unroll
         for (int c = 0; c < 8; ++c) ws[c] = ls.w[c];
         const int r = g.res[l][3];
-        const float pt = x[3] * (float)r;
+        const float pt = __fmul_rn(x[3], (float)r);   // as level_corners
         int ct = (int)floorf(pt);
         ct = ct < 0 ? 0 : (ct > r - 1 ? r - 1 : ct);
         wt1 = pt - (float)ct;

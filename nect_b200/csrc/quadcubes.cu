@@ -75,7 +75,7 @@ struct TimeVertex {
   float w0, w1;
 };
 __device__ __forceinline__ TimeVertex time_vertex(float t, int r) {
-  const float p = t * (float)r;
+  const float p = __fmul_rn(t, (float)r);   // rounded product, as level_corners
   int ci = (int)floorf(p);
   ci = ci < 0 ? 0 : (ci > r - 1 ? r - 1 : ci);
   const float f = p - (float)ci;
@@ -163,7 +163,7 @@ struct PlaneCorners {
 };
 __device__ __forceinline__ void plane_corners(const Plane& s, int l, float a, float b, PlaneCorners& pc) {
   const int r = s.res[l];
-  const float pa = a * (float)r, pb = b * (float)r;
+  const float pa = __fmul_rn(a, (float)r), pb = __fmul_rn(b, (float)r);   // rounded products, as level_corners
   int ia = (int)floorf(pa), ib = (int)floorf(pb);
   ia = ia < 0 ? 0 : (ia > r - 1 ? r - 1 : ia);
   ib = ib < 0 ? 0 : (ib > r - 1 ? r - 1 : ib);
