@@ -261,6 +261,33 @@ __global__ void volume_scatter_kernel(GridDev g, const float* __restrict__ zyx, 
   scatter_warp<3, F, false, true, S, true>(g, grad, p, valid, dout + row * ld, F, 1, 0u, l0, l1);
 }
 
+// Gradient of one hashed level of the (z, y, x) grid, restricted to the
+// corners whose entry lies in half `half` of the level (entry >> shift ==
+// half): two such passes keep each pass's reductions within 67 MB of a 2^23 x 4
+// fp32 level, which L2 holds, where the whole level (134 MB) does not.  No run
+// merging (hashed levels' samples rarely share cells).
+template <int F, typename S>
+__global__ void volume_scatter_half_kernel(GridDev g, const float* __restrict__ zyx, int64_t n,
+                                           const S* __restrict__ dout, int64_t ld, float* __restrict__ grad, int l,
+                                           int shift, uint32_t half) {
+  const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float x[3] = {zyx[i * 3], zyx[i * 3 + 1], zyx[i * 3 + 2]};
+  LevelCorners<3> lc;
+  level_corners<3>(g, l, x, lc);
+  float d[F];
+  load_grad_row<F, S>(dout + i * ld + l * F, d);
+  float* base = grad + g.offset[l] * F;
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    if ((lc.idx[c] >> shift) != half) continue;
+    float v[F];
+#pragma unroll
+    for (int f = 0; f < F; ++f) v[f] = lc.w[c] * d[f];
+    red_entry<F>(base + (int64_t)lc.idx[c] * F, v);
+  }
+}
+
 // Gradient of a plane grid into the plane-shaped fp32 gradient: 4 corners a
 // level; on levels where a warp's 32 points form at most 24 runs of equal
 // cells, each run's sums are reduced once by its first lane.
@@ -428,8 +455,18 @@ int backward_all(const GridDev& g, const Plane& s, const float* zyx, int64_t n, 
     };
     int64_t bytes = level_bytes(l0);
     while (l1 < g.n_levels && bytes + level_bytes(l1) <= kScatterGroupBytes) bytes += level_bytes(l1++);
-    volume_scatter_kernel<F, S><<<blocks, 256, 0, st>>>(g, zyx, n, dout, ld, grads[0], l0, l1);
-    if (int rc = launch_status("volume_scatter_kernel")) return rc;
+    if (l1 == l0 + 1 && ((g.hashed_bits >> l0) & 1u) && bytes > kScatterGroupBytes) {
+      // a hashed level above the group size: one pass per half of its entries
+      int log2T = 0;
+      while ((1u << log2T) < g.hash_mask + 1u) ++log2T;
+      for (uint32_t h = 0; h < 2; ++h) {
+        volume_scatter_half_kernel<F, S><<<blocks, 256, 0, st>>>(g, zyx, n, dout, ld, grads[0], l0, log2T - 1, h);
+        if (int rc = launch_status("volume_scatter_half_kernel")) return rc;
+      }
+    } else {
+      volume_scatter_kernel<F, S><<<blocks, 256, 0, st>>>(g, zyx, n, dout, ld, grads[0], l0, l1);
+      if (int rc = launch_status("volume_scatter_kernel")) return rc;
+    }
     l0 = l1;
   }
   for (int k = 0; k < 3; ++k) {
