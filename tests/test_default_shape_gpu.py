@@ -77,7 +77,7 @@ def test_corner_indices_bit_exact(cuda_device):
     for l, lv in enumerate(levels):
         oi, ow = ohg.corner_indices(x, lv, enc.log2_hashmap_size)
         assert torch.equal(idx[:, l].to(torch.int64), oi), f"level {l}"
-        assert torch.allclose(w[:, l], ow, atol=2e-6, rtol=0)
+        assert torch.equal(w[:, l], ow)
 
 
 @pytest.mark.parametrize("precision,out_act", [("plain_fp32", "ReLU"), ("mixed", "ReLU"), ("mixed", "Softplus")])

@@ -2,7 +2,8 @@
 training step (called through the C ABI) against the fp64 oracle.
 
 Tolerances (plain fp32 path vs fp64 oracle): hash indices bit-exact;
-interpolation weights to 1 ulp-level (2e-6 abs); encodings and sigma rel
+interpolation weights bit-exact (the oracle's fp32 weights: the rounded
+position's fraction, products in axis order); encodings and sigma rel
 1e-5; y_pred and loss rel 1e-4; gradients within 1e-3 of the largest
 gradient entry.
 """
@@ -79,7 +80,7 @@ def test_corner_indices_bit_exact(cuda_device, n_dims):
     for l, lv in enumerate(levels):
         oi, ow = ohg.corner_indices(x, lv, enc.log2_hashmap_size)
         assert torch.equal(idx[:, l].to(torch.int64), oi), f"level {l} indices differ"
-        assert torch.allclose(w[:, l], ow, atol=2e-6, rtol=0), f"level {l} weights differ"
+        assert torch.equal(w[:, l], ow), f"level {l} weights differ"
 
 
 @pytest.mark.parametrize("n_dims,precision", [(3, "plain_fp32"), (4, "plain_fp32"), (3, "mixed"), (4, "mixed")])
